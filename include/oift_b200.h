@@ -1,0 +1,145 @@
+/*
+ * oift_b200.h -- C ABI of the B200 (sm_100a) OIFT + relaxation library.
+ *
+ * Drop-in boundary for the GPU path of jung0221/roift:
+ *   oift_fmax_gpu_run  replaces  gpu/oift_fmax_gpu.cu:139-149 (same signature and
+ *                      meaning; it additionally returns a negative status on error
+ *                      instead of running on unchecked allocations);
+ *   oift_gpu_run       replaces  gpu/oift_gpu.cu:149-158 (cost_mode 0 = f_max; the
+ *                      additive mode is not provided and returns OIFT_E_UNSUPPORTED).
+ * The extended entry points add what the CPU calls gft::ift::OIFT_Multi /
+ * OIFT_Multi_PerClass (gft/include/gft_ift.h:108-122) and ORelax_1_Multi /
+ * ORelax_1_Multi_PerClass (gft/include/gft_ift.h:451-465) compute, on one GPU:
+ * arc-weight building, oriented f_max OIFT with exported cost, relaxation sweeps,
+ * argmax labels and a mask.
+ *
+ * Conventions (the reference's, gft/include/gft_scene32.h:20-179):
+ *   voxel address p = x + y*xsize + z*xsize*ysize; 2D images are zsize == 1;
+ *   labels: NIL = -1 (unlabelled), 0 = background, >= 1 objects (< 32768);
+ *   polarity values are x100 (pol in [-1,1] -> per in [-100,100]).
+ * All pointers are plain host or device pointers; sizes are element counts; no
+ * function keeps a pointer after it returns.  Every function returns OIFT_OK (0) or
+ * a negative oift_status, except the two reference-compatible entry points which
+ * return the number of levels processed (>= 0) or -1.
+ */
+#ifndef OIFT_B200_H
+#define OIFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define OIFT_API __attribute__((visibility("default")))
+#else
+#define OIFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    OIFT_OK = 0,
+    OIFT_E_BAD_ARG = -1,        /* null pointer, bad size, bad adjacency, |per| > 100 ... */
+    OIFT_E_NO_SEEDS = -2,       /* empty seed list */
+    OIFT_E_OOM = -3,            /* device allocation failed */
+    OIFT_E_NOT_CONVERGED = -4,  /* a bounded wait inside a kernel ran out */
+    OIFT_E_QUEUE_OVERFLOW = -5, /* device work queue capacity exceeded */
+    OIFT_E_CUDA = -6,           /* other CUDA runtime error */
+    OIFT_E_RANGE = -7,          /* weight or intensity outside the supported range */
+    OIFT_E_UNSUPPORTED = -8,    /* option not provided (e.g. additive path cost) */
+    OIFT_E_SEED_RANGE = -9      /* a seed address is outside the volume */
+} oift_status;
+
+/* Arc-weight builders (row a1-a3): base weight of the undirected edge {p,q}. */
+typedef enum {
+    OIFT_W_GRAD = 0,    /* |I_p - I_q| exactly (<= 16383, else OIFT_E_RANGE) */
+    OIFT_W_GRAD_Q = 1,  /* min(|I_p - I_q|, wq); clamp events counted */
+    OIFT_W_RBF_Q = 2,   /* floor(wq*(1 - exp(-d^2/(2 sigma^2))) + 0.5), host LUT */
+    OIFT_W_BLEND_Q = 3  /* (int)(a|dI| + (1-a)(g_p+g_q)/2) with a Sobel map g, clamped */
+} oift_weight_mode;
+
+typedef struct oift_b200_ctx oift_b200_ctx;
+
+/* Parameters of one OIFT + relaxation job. */
+typedef struct {
+    int xsize, ysize, zsize;
+    int adjacency;        /* 4 or 8 (zsize == 1), 6 or 26 */
+    int weight_mode;      /* oift_weight_mode */
+    int wq;               /* quantisation ceiling for the _Q modes (e.g. 4095) */
+    float rbf_sigma;      /* OIFT_W_RBF_Q */
+    float blend_a;        /* OIFT_W_BLEND_Q */
+    float per;            /* global polarity x100 (label 0 uses -per), if per_class NULL */
+    const float *per_class; /* host array [max_label+1] of per-label polarity x100, or NULL */
+    int max_label;
+    int relax_sweeps;     /* K >= 0 */
+} oift_b200_params;
+
+/* Device-resident results of the extended entry points (device pointers, may be NULL). */
+typedef struct {
+    int32_t *cost;        /* [N] f_max cost (INT32_MAX if unreached) */
+    int32_t *oift_label;  /* [N] OIFT label before relaxation */
+    int32_t *label;       /* [N] final label (argmax of the relaxed membership) */
+    uint8_t *mask;        /* [N] 1 where the final label != 0 */
+    float *membership;    /* [nclasses][N] relaxed membership (planar) */
+} oift_b200_outputs;
+
+/* Per-run statistics. */
+typedef struct {
+    int levels;           /* (cost,label) levels processed by the OIFT */
+    long long tile_steps; /* tile activations */
+    long long clamped;    /* edges clamped by a _Q builder */
+    int nclasses;         /* relaxation classes */
+    float ms_weights, ms_oift, ms_relax, ms_total; /* CUDA-event stage times */
+} oift_b200_stats;
+
+/* Context: owns the device scratch for one device and one stream. */
+OIFT_API int oift_b200_create(oift_b200_ctx **out, int device);
+OIFT_API int oift_b200_destroy(oift_b200_ctx *ctx);
+/* Number of bytes of device scratch currently held. */
+OIFT_API size_t oift_b200_scratch_bytes(const oift_b200_ctx *ctx);
+/* Stream used by subsequent calls (cudaStream_t as void*; NULL = legacy default). */
+OIFT_API int oift_b200_set_stream(oift_b200_ctx *ctx, void *stream);
+OIFT_API const char *oift_b200_status_string(int status);
+
+/* Full pipeline on DEVICE pointers: image int16 [N]; seeds int32 [nseeds] addresses;
+ * seed_labels int32 [nseeds].  Outputs as requested in `out`.  Runs on the context's
+ * stream; synchronises before returning. */
+OIFT_API int oift_b200_run_device_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                             const int16_t *image, const int32_t *seeds,
+                             const int32_t *seed_labels, int nseeds,
+                             const oift_b200_outputs *out, oift_b200_stats *stats);
+
+/* Full pipeline on HOST pointers (int32 image as in the reference, already shifted
+ * and blurred by the caller).  label: in = NIL except seeds, out = final labels.
+ * cost (may be NULL) receives the f_max cost, membership (may be NULL) the relaxed
+ * membership [nclasses][N], mask (may be NULL) the uint8 mask. */
+OIFT_API int oift_b200_run_host(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                       const int32_t *image, int32_t *label, const int32_t *seeds, int nseeds,
+                       int32_t *cost, float *membership, int membership_cap_classes,
+                       uint8_t *mask, oift_b200_stats *stats);
+
+/* Stage entry points on device pointers (used by the batched driver and tests). */
+OIFT_API int oift_b200_build_weights_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                                const int16_t *image, uint16_t *weights /* [planes][N] */,
+                                long long *clamped);
+OIFT_API int oift_b200_weight_planes(int adjacency);
+
+/* Reference-compatible drop-in (gpu/oift_fmax_gpu.cu:139-149).  Host pointers.
+ * h_labels: in = labels (seed voxels carry their label, NIL elsewhere), out = OIFT
+ * labels.  h_per_class [max_label+1] polarity x100.  Returns the number of levels
+ * processed, or -1 on error (oift_b200_last_status() gives the reason). */
+OIFT_API int oift_fmax_gpu_run(const int *h_image, int *h_labels, int n, int xsize, int ysize,
+                      int zsize, const float *h_per_class, int max_label,
+                      const int *h_seeds, int n_seeds);
+/* gpu/oift_gpu.cu:149-158: cost_mode 0 (f_max) only. */
+OIFT_API int oift_gpu_run(int cost_mode, const int *h_image, int *h_labels, int n, int xsize,
+                 int ysize, int zsize, const float *h_per_class, int max_label,
+                 const int *h_seeds, int n_seeds);
+/* Status of the last reference-compatible call on this host thread. */
+OIFT_API int oift_b200_last_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,269 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the C restatement (liboracle.so) and to
+the reference gft library compiled from its own sources (_ref/libgft_ref.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / --impl reference
+legs may import this package, and only as the checker or the timed reference arm.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libgft_ref.so")
+REF_SRC = "/root/reference"
+
+NIL = -1
+W_MODES = {"grad": 0, "grad_q": 1, "rbf_q": 2, "blend_q": 3}
+
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+def build(with_ref: bool | None = None) -> None:
+    """Compile liboracle.so, and libgft_ref.so when the reference tree is present."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if with_ref is None:
+        with_ref = os.path.isdir(REF_SRC)
+    if with_ref:
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+
+
+class _Polarity(C.Structure):
+    _fields_ = [("table", C.POINTER(C.c_float)), ("ntable", C.c_int), ("dflt", C.c_float)]
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build(with_ref=False)
+        L = C.CDLL(ORACLE_SO)
+        L.or_build_weights.restype = C.c_longlong
+        L.or_build_weights.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_float,
+                                       _u16p]
+        L.or_rbf_lut.argtypes = [C.c_double, C.c_int, C.c_int, _u16p]
+        L.or_oift_fmax.restype = C.c_int
+        L.or_oift_fmax.argtypes = [_u16p, C.c_int, C.c_int, C.c_int, C.c_int, _Polarity,
+                                   _i32p, C.c_int, _i32p, _i32p, _i32p, C.c_void_p]
+        L.or_oift_prim.argtypes = [_u16p, C.c_int, C.c_int, C.c_int, C.c_int, _Polarity,
+                                   C.c_int, _i32p, C.c_int, _i32p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]
+        L.or_energy.restype = C.c_int
+        L.or_energy.argtypes = [_u16p, C.c_int, C.c_int, C.c_int, C.c_int, _Polarity, _i32p,
+                                C.c_int, _i32p]
+        L.or_relax_f32.restype = C.c_int
+        L.or_relax_f32.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                   C.c_void_p, C.c_int, _i32p, C.c_int, _i32p, C.c_int,
+                                   C.c_void_p]
+        L.or_relax_f64.restype = C.c_int
+        L.or_relax_f64.argtypes = L.or_relax_f32.argtypes
+        L.or_gaussian_blur.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        R = C.CDLL(REF_SO)
+        R.ref_oift_multi.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                     _i32p, C.c_int, _i32p]
+        R.ref_oift_multi_perclass.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                              _f32p, C.c_int, _i32p, C.c_int, _i32p]
+        R.ref_orelax_multi.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                       _i32p, C.c_int, _i32p, C.c_int]
+        R.ref_orelax_multi_perclass.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                _f32p, C.c_int, _i32p, C.c_int, _i32p, C.c_int]
+        R.ref_ift_fmax_graph.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, _i32p,
+                                         C.c_int, _i32p, _i32p]
+        R.ref_energy_min_graph.restype = C.c_int
+        R.ref_energy_min_graph.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, _i32p,
+                                           C.c_int]
+        R.ref_gaussian_blur.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        _ref = R
+    return _ref
+
+
+# ------------------------------------------------------------------ helpers ----
+def _dims(img):
+    if img.ndim == 2:
+        return img.shape[1], img.shape[0], 1
+    Z, Y, X = img.shape
+    return X, Y, Z
+
+
+def as_i32(img) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(img).reshape(-1), dtype=np.int32)
+
+
+def polarity(pol: float | None = None, per_class=None):
+    """Global mode: label 0 -> -per, others +per (gft_ift.cpp:968).  Per-class mode:
+    per_class[l] for l <= max_label, else 0 (gft_ift.cpp:1055-1060).  Values x100."""
+    if per_class is None:
+        per = np.float32(pol * 100.0) if not isinstance(pol, np.float32) else pol
+        table = np.array([-per], np.float32)
+        keep = table
+        return _Polarity(table.ctypes.data_as(C.POINTER(C.c_float)), 1, C.c_float(per)), keep
+    table = np.ascontiguousarray(per_class, np.float32)
+    return _Polarity(table.ctypes.data_as(C.POINTER(C.c_float)), len(table), 0.0), table
+
+
+def n_planes(adj: int) -> int:
+    return 13 if adj in (8, 26) else 3
+
+
+def build_weights(img, adj, mode="grad", wq=4095, rbf_sigma=150.0, grad=None, blend_a=0.5):
+    X, Y, Z = _dims(img)
+    flat = as_i32(img)
+    N = flat.size
+    W = np.zeros(n_planes(adj) * N, np.uint16)
+    lut = None
+    lut_len = 0
+    if mode == "rbf_q":
+        lut_len = int(np.abs(np.diff(np.sort(flat)[[0, -1]]))[0]) + 1 if N > 1 else 1
+        lut = np.zeros(lut_len, np.uint16)
+        lib().or_rbf_lut(float(rbf_sigma), int(wq), lut_len, lut)
+    g = as_i32(grad) if grad is not None else None
+    ncl = lib().or_build_weights(flat, X, Y, Z, adj, W_MODES[mode], int(wq),
+                                 lut.ctypes.data if lut is not None else None, lut_len,
+                                 g.ctypes.data if g is not None else None, float(blend_a), W)
+    return W, int(ncl)
+
+
+def oift_fmax(W, shape_xyz, adj, seeds, seed_labels, pol=None, per_class=None, want_pred=False):
+    """R2.  Returns (cost, label, levels[, pred])."""
+    X, Y, Z = shape_xyz
+    N = X * Y * Z
+    lab_in = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab_in[seeds] = seed_labels
+    cost = np.empty(N, np.int32)
+    label = np.empty(N, np.int32)
+    pred = np.empty(N, np.int32) if want_pred else None
+    P, keep = polarity(pol, per_class)
+    levels = lib().or_oift_fmax(W, X, Y, Z, adj, P, seeds, len(seeds), lab_in, cost, label,
+                                pred.ctypes.data if pred is not None else None)
+    return (cost, label, levels, pred) if want_pred else (cost, label, levels)
+
+
+def oift_prim(W, shape_xyz, adj, seeds, seed_labels, pol=None, per_class=None):
+    """R1 (restated OIFT_Multi).  Returns (label, value, pred, fmax)."""
+    X, Y, Z = shape_xyz
+    N = X * Y * Z
+    lab = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    val = np.empty(N, np.int32)
+    pred = np.empty(N, np.int32)
+    fmax = np.empty(N, np.int32)
+    P, keep = polarity(pol, per_class)
+    maxw = int((W & 0x3FFF).max()) if W.size else 0
+    maxp = 100.0 if per_class is None else float(np.abs(per_class).max())
+    buckets = int(maxw * (1.0 + max(abs(pol or 0) * 100, maxp) / 100.0)) + 2
+    lib().or_oift_prim(W, X, Y, Z, adj, P, buckets, seeds, len(seeds), lab,
+                       val.ctypes.data, pred.ctypes.data, fmax.ctypes.data)
+    return lab, val, pred, fmax
+
+
+def energy(W, shape_xyz, adj, label, nl, pol=None, per_class=None):
+    X, Y, Z = shape_xyz
+    e_lb = np.empty(max(nl, 1), np.int32)
+    P, keep = polarity(pol, per_class)
+    e = lib().or_energy(W, X, Y, Z, adj, P, np.ascontiguousarray(label, np.int32), nl, e_lb)
+    return e, e_lb[:nl]
+
+
+def relax(img, adj, seeds, label, ntimes, pol=None, per_class=None, fp64=False):
+    """R3.  Returns (label_out, membership [C, N], nclasses)."""
+    X, Y, Z = _dims(img)
+    flat = as_i32(img)
+    N = flat.size
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab = np.ascontiguousarray(label, np.int32).copy()
+    # class count first (membership size)
+    present = {0} | {int(l) for l in lab[seeds] if l >= 0}
+    nc = len(present)
+    mem = np.empty(nc * N, np.float64 if fp64 else np.float32)
+    pc = None
+    ml = 0
+    if per_class is not None:
+        pc = np.ascontiguousarray(per_class, np.float32)
+        ml = len(pc) - 1
+    fn = lib().or_relax_f64 if fp64 else lib().or_relax_f32
+    got = fn(flat, X, Y, Z, adj, float(np.float32((pol or 0.0) * 100.0)),
+             pc.ctypes.data if pc is not None else None, ml, seeds, len(seeds), lab, int(ntimes),
+             mem.ctypes.data)
+    assert got == nc, (got, nc)
+    return lab, mem.reshape(nc, N), nc
+
+
+def gaussian_blur(img):
+    X, Y, Z = _dims(img)
+    out = np.empty(X * Y * Z, np.int32)
+    lib().or_gaussian_blur(as_i32(img), X, Y, Z, out)
+    return out
+
+
+# ------------------------------------------------------- reference wrappers ----
+def ref_oift_multi(img, adj, seeds, seed_labels, pol=None, per_class=None):
+    X, Y, Z = _dims(img)
+    N = X * Y * Z
+    lab = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    if per_class is None:
+        ref().ref_oift_multi(as_i32(img), X, Y, Z, adj, np.float32(pol * 100.0), seeds,
+                             len(seeds), lab)
+    else:
+        pc = np.ascontiguousarray(per_class, np.float32)
+        ref().ref_oift_multi_perclass(as_i32(img), X, Y, Z, adj, pc, len(pc) - 1, seeds,
+                                      len(seeds), lab)
+    return lab
+
+
+def ref_orelax_multi(img, adj, seeds, label, ntimes, pol=None, per_class=None):
+    X, Y, Z = _dims(img)
+    lab = np.ascontiguousarray(label, np.int32).copy()
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    if per_class is None:
+        ref().ref_orelax_multi(as_i32(img), X, Y, Z, adj, np.float32(pol * 100.0), seeds,
+                               len(seeds), lab, int(ntimes))
+    else:
+        pc = np.ascontiguousarray(per_class, np.float32)
+        ref().ref_orelax_multi_perclass(as_i32(img), X, Y, Z, adj, pc, len(pc) - 1, seeds,
+                                        len(seeds), lab, int(ntimes))
+    return lab
+
+
+def ref_ift_fmax(img, adj, seeds, seed_labels):
+    X, Y, Z = _dims(img)
+    N = X * Y * Z
+    lab = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    cost = np.empty(N, np.int32)
+    ref().ref_ift_fmax_graph(as_i32(img), X, Y, Z, adj, seeds, len(seeds), lab, cost)
+    return cost, lab
+
+
+def ref_gaussian_blur(img):
+    X, Y, Z = _dims(img)
+    out = np.empty(X * Y * Z, np.int32)
+    ref().ref_gaussian_blur(as_i32(img), X, Y, Z, out)
+    return out

@@ -1,0 +1,618 @@
+/*
+ * oracle.c -- TEST INFRASTRUCTURE ONLY (see oracle.h).  CPU restatement of the
+ * reference OIFT + relaxation path, used as the checker of the CUDA library.
+ * Each routine cites the reference lines it restates.
+ */
+#include "oracle.h"
+
+#include <float.h>
+#include <limits.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MAX(a, b) ((a) > (b) ? (a) : (b))
+#define MIN(a, b) ((a) < (b) ? (a) : (b))
+
+/* gft/src/gft_adjrel3.cpp:47-85: Spheric(r) enumerates dz, dy, dx in [-r0, r0] with
+ * dx^2+dy^2+dz^2 <= (int)(r*r) and moves the centre to the front. */
+int or_adjacency(int adj, int *dx, int *dy, int *dz) {
+    int r2 = (adj == 26 || adj == 8) ? 3 : 1;
+    int n = 0;
+    for (int z = -1; z <= 1; z++)
+        for (int y = -1; y <= 1; y++)
+            for (int x = -1; x <= 1; x++) {
+                if (x == 0 && y == 0 && z == 0) continue;
+                if (x * x + y * y + z * z <= r2) {
+                    dx[n] = x;
+                    dy[n] = y;
+                    dz[n] = z;
+                    n++;
+                }
+            }
+    return n;
+}
+
+static inline int in_bounds(int x, int y, int z, int X, int Y, int Z) {
+    return x >= 0 && x < X && y >= 0 && y < Y && z >= 0 && z < Z;
+}
+
+void or_rbf_lut(double sigma, int wq, int len, uint16_t *lut) {
+    for (int d = 0; d < len; d++) {
+        double a = exp(-((double)d * (double)d) / (2.0 * sigma * sigma));
+        double v = floor((double)wq * (1.0 - a) + 0.5);
+        if (v < 0) v = 0;
+        if (v > wq) v = wq;
+        lut[d] = (uint16_t)v;
+    }
+}
+
+long long or_build_weights(const int *img, int X, int Y, int Z, int adj, int mode, int wq,
+                           const uint16_t *lut, int lut_len, const int *grad, float blend_a,
+                           uint16_t *W) {
+    int dx[26], dy[26], dz[26];
+    int n = or_adjacency(adj, dx, dy, dz);
+    int half = n / 2;
+    size_t N = (size_t)X * Y * Z;
+    long long nclamp = 0;
+    int cap = (mode == OR_W_GRAD) ? OR_WMAX_BASE : MIN(wq, OR_WMAX_BASE);
+    for (int k = 0; k < half; k++) {
+        int d = half + k;
+        uint16_t *plane = W + (size_t)k * N;
+        for (int z = 0; z < Z; z++)
+            for (int y = 0; y < Y; y++)
+                for (int x = 0; x < X; x++) {
+                    size_t p = (size_t)x + (size_t)y * X + (size_t)z * X * Y;
+                    int qx = x + dx[d], qy = y + dy[d], qz = z + dz[d];
+                    if (!in_bounds(qx, qy, qz, X, Y, Z)) {
+                        plane[p] = 0;
+                        continue;
+                    }
+                    size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
+                    int ip = img[p], iq = img[q];
+                    int ad = abs(ip - iq);
+                    long long b;
+                    switch (mode) {
+                        case OR_W_GRAD:
+                        case OR_W_GRAD_Q:
+                            b = ad;
+                            break;
+                        case OR_W_RBF_Q:
+                            b = (ad < lut_len) ? lut[ad] : lut[lut_len - 1];
+                            break;
+                        default: { /* BLEND_Q, exp_gradient_weight.cpp:244-247 */
+                            float gavg = (float)(grad[p] + grad[q]) * 0.5f;
+                            float wf = blend_a * (float)ad + (1.0f - blend_a) * gavg;
+                            b = (long long)wf;
+                            if (b < 0) b = 0;
+                        }
+                    }
+                    if (b > cap) {
+                        b = cap;
+                        nclamp++;
+                    }
+                    uint16_t code = (uint16_t)b;
+                    if (ip > iq) code |= 0x8000u;
+                    if (ip < iq) code |= 0x4000u;
+                    plane[p] = code;
+                }
+    }
+    return nclamp;
+}
+
+/* gft/src/gft_ift.cpp:965-973: int w = |dI|; w *= (1.0 + per_pq/100.0) if I_p > I_q,
+ * w *= (1.0 - per_pq/100.0) if I_p < I_q.  The int *= double truncates toward zero. */
+int or_oriented(uint16_t base, int tail_gt, int tail_lt, float pol) {
+    int w = base;
+    if (tail_gt)
+        w = (int)((double)w * (1.0 + (double)pol / 100.0));
+    else if (tail_lt)
+        w = (int)((double)w * (1.0 - (double)pol / 100.0));
+    return w;
+}
+
+static inline float polarity_of(or_polarity pol, int lb) {
+    if (lb >= 0 && lb < pol.ntable) return pol.table[lb];
+    return pol.dflt;
+}
+
+/* Arc weight p -> q where q = p + d_i.  For i in the positive half the edge lives in
+ * plane (i - half) at p; otherwise in plane (n-1-i - half) at q with the bits read
+ * from q's side, i.e. swapped. */
+static inline int arc_weight(const uint16_t *W, size_t N, int n, int i, size_t p, size_t q,
+                             float pol) {
+    int half = n / 2;
+    uint16_t code;
+    int gt, lt;
+    if (i >= half) {
+        code = W[(size_t)(i - half) * N + p];
+        gt = (code >> 15) & 1;
+        lt = (code >> 14) & 1;
+    } else {
+        code = W[(size_t)(n - 1 - i - half) * N + q];
+        gt = (code >> 14) & 1; /* I_q < I_p seen from q means I_p > I_q */
+        lt = (code >> 15) & 1;
+    }
+    return or_oriented((uint16_t)(code & 0x3fffu), gt, lt, pol);
+}
+
+/* ---------------------------------------------------------------- binary heap --- */
+typedef struct {
+    uint64_t *k;
+    size_t n, cap;
+} heap64;
+
+static void hpush(heap64 *h, uint64_t v) {
+    if (h->n == h->cap) {
+        h->cap = h->cap ? h->cap * 2 : 1024;
+        h->k = (uint64_t *)realloc(h->k, h->cap * sizeof(uint64_t));
+    }
+    size_t i = h->n++;
+    while (i > 0) {
+        size_t par = (i - 1) / 2;
+        if (h->k[par] <= v) break;
+        h->k[i] = h->k[par];
+        i = par;
+    }
+    h->k[i] = v;
+}
+
+static uint64_t hpop(heap64 *h) {
+    uint64_t top = h->k[0];
+    uint64_t v = h->k[--h->n];
+    size_t i = 0;
+    for (;;) {
+        size_t l = 2 * i + 1, r = l + 1, m = i;
+        uint64_t mv = v;
+        if (l < h->n && h->k[l] < mv) { m = l; mv = h->k[l]; }
+        if (r < h->n && h->k[r] < mv) { m = r; mv = h->k[r]; }
+        if (m == i) break;
+        h->k[i] = h->k[m];
+        i = m;
+    }
+    if (h->n) h->k[i] = v;
+    return top;
+}
+
+/* R2.  Key = (cost << 32 | label) << 24 | voxel would not fit; the heap holds
+ * (cost << 48 | label << 32 | voxel) with voxel < 2^32, cost < 2^16, label < 2^16.
+ * Ties inside one (cost,label) level pop in any order: the set conquered at a level
+ * is a reachability closure, so the result does not depend on that order. */
+int or_oift_fmax(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
+                 const int *seeds, int nseeds, const int *label_in,
+                 int *cost, int *label, int *pred) {
+    int dx[26], dy[26], dz[26];
+    int n = or_adjacency(adj, dx, dy, dz);
+    size_t N = (size_t)X * Y * Z;
+    unsigned char *done = (unsigned char *)calloc(N, 1);
+    heap64 h = {0};
+    for (size_t p = 0; p < N; p++) {
+        cost[p] = INT32_MAX;
+        label[p] = OR_NIL;
+        if (pred) pred[p] = -1;
+    }
+    for (int i = 0; i < nseeds; i++) {
+        int p = seeds[i];
+        if (p < 0 || (size_t)p >= N) continue;
+        int lb = label_in[p] < 0 ? 0 : label_in[p];
+        if (cost[p] == 0 && label[p] <= lb) continue;
+        cost[p] = 0;
+        label[p] = lb;
+        hpush(&h, ((uint64_t)0 << 48) | ((uint64_t)lb << 32) | (uint64_t)p);
+    }
+    int levels = 0;
+    uint64_t lastkey = UINT64_MAX;
+    while (h.n) {
+        uint64_t e = hpop(&h);
+        size_t p = (size_t)(e & 0xffffffffu);
+        int c = (int)(e >> 48), lb = (int)((e >> 32) & 0xffff);
+        if (done[p] || c != cost[p] || lb != label[p]) continue; /* stale */
+        done[p] = 1;
+        if ((e >> 32) != lastkey) {
+            levels++;
+            lastkey = e >> 32;
+        }
+        float pl = polarity_of(pol, lb);
+        int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / ((size_t)X * Y));
+        for (int i = 0; i < n; i++) {
+            int qx = x + dx[i], qy = y + dy[i], qz = z + dz[i];
+            if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
+            size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
+            if (done[q]) continue;
+            int w = arc_weight(W, N, n, i, p, q, pl);
+            int nc = MAX(c, w);
+            if (nc < cost[q] || (nc == cost[q] && lb < label[q])) {
+                cost[q] = nc;
+                label[q] = lb;
+                if (pred) pred[q] = (int)p;
+                hpush(&h, ((uint64_t)nc << 48) | ((uint64_t)lb << 32) | (uint64_t)q);
+            }
+        }
+    }
+    free(h.k);
+    free(done);
+    return levels;
+}
+
+/* ------------------------------------------------------- R1: Prim / Dial queue --- */
+/* Restates PQueue32 (gft/src/gft_pqueue32.cpp:231-245 _BucketFIFO, 300-324
+ * FastInsertElem with the backwards-moving minvalue at 312-313, 353-377
+ * FastRemoveElem, 433-451 FastRemoveMinFIFO) and OIFT_Multi's loop
+ * (gft/src/gft_ift.cpp:934-985). */
+enum { WHITE = 0, GRAY = 1, BLACK = 2 };
+
+typedef struct {
+    int *first, *last, nb, minv;
+    int *next, *prev;
+    unsigned char *color;
+    int *value;
+} dialq;
+
+static void dq_insert(dialq *Q, int e) {
+    int b = Q->value[e];
+    if (b < Q->minv) Q->minv = b;
+    if (Q->first[b] == -1) {
+        Q->first[b] = e;
+        Q->prev[e] = -1;
+    } else {
+        Q->next[Q->last[b]] = e;
+        Q->prev[e] = Q->last[b];
+    }
+    Q->last[b] = e;
+    Q->next[e] = -1;
+    Q->color[e] = GRAY;
+}
+
+static void dq_remove(dialq *Q, int e) {
+    int b = Q->value[e], pv = Q->prev[e], nx = Q->next[e];
+    if (Q->first[b] == e) {
+        Q->first[b] = nx;
+        if (nx == -1)
+            Q->last[b] = -1;
+        else
+            Q->prev[nx] = -1;
+    } else {
+        Q->next[pv] = nx;
+        if (nx == -1)
+            Q->last[b] = pv;
+        else
+            Q->prev[nx] = pv;
+    }
+    Q->color[e] = BLACK;
+}
+
+static int dq_popmin(dialq *Q) {
+    while (Q->first[Q->minv] == -1) Q->minv++;
+    int b = Q->minv;
+    int e = Q->first[b], nx = Q->next[e];
+    if (nx == -1)
+        Q->first[b] = Q->last[b] = -1;
+    else {
+        Q->first[b] = nx;
+        Q->prev[nx] = -1;
+    }
+    Q->color[e] = BLACK;
+    return e;
+}
+
+void or_oift_prim(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
+                  int wmax_buckets, const int *seeds, int nseeds, int *label,
+                  int *value_out, int *pred_out, int *fmax_out) {
+    int dx[26], dy[26], dz[26];
+    int n = or_adjacency(adj, dx, dy, dz);
+    size_t N = (size_t)X * Y * Z;
+    dialq Q;
+    Q.nb = wmax_buckets + 2;
+    Q.first = (int *)malloc(sizeof(int) * (Q.nb + 1));
+    Q.last = (int *)malloc(sizeof(int) * (Q.nb + 1));
+    for (int b = 0; b <= Q.nb; b++) Q.first[b] = Q.last[b] = -1;
+    Q.minv = Q.nb;
+    Q.next = (int *)malloc(sizeof(int) * N);
+    Q.prev = (int *)malloc(sizeof(int) * N);
+    Q.color = (unsigned char *)calloc(N, 1);
+    Q.value = (int *)malloc(sizeof(int) * N);
+    int *pred = (int *)malloc(sizeof(int) * N);
+    int *order = fmax_out ? (int *)malloc(sizeof(int) * N) : NULL;
+    size_t norder = 0;
+    for (size_t p = 0; p < N; p++) {
+        Q.value[p] = (label[p] == OR_NIL) ? INT_MAX : 0;
+        pred[p] = -1;
+    }
+    for (int i = 0; i < nseeds; i++) dq_insert(&Q, seeds[i]);
+    /* Queue emptiness: count of GRAY elements. */
+    size_t ingray = 0;
+    for (size_t p = 0; p < N; p++) ingray += (Q.color[p] == GRAY);
+    /* Duplicate seeds were inserted twice in the reference as well; mirror the list
+     * semantics by counting list occupancy instead of colours. */
+    long long occ = nseeds;
+    (void)ingray;
+    while (occ > 0) {
+        int p = dq_popmin(&Q);
+        occ--;
+        if (order) order[norder++] = p;
+        int x = p % X, y = (p / X) % Y, z = p / (X * Y);
+        float pl = polarity_of(pol, label[p]);
+        for (int i = 0; i < n; i++) {
+            int qx = x + dx[i], qy = y + dy[i], qz = z + dz[i];
+            if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
+            int q = qx + qy * X + qz * X * Y;
+            if (Q.color[q] == BLACK) continue;
+            int w = arc_weight(W, N, n, i, (size_t)p, (size_t)q, pl);
+            if (w < Q.value[q]) {
+                if (Q.color[q] == GRAY) {
+                    dq_remove(&Q, q);
+                    occ--;
+                }
+                Q.value[q] = w;
+                label[q] = label[p];
+                pred[q] = p;
+                dq_insert(&Q, q);
+                occ++;
+            }
+        }
+    }
+    if (value_out) memcpy(value_out, Q.value, sizeof(int) * N);
+    if (pred_out) memcpy(pred_out, pred, sizeof(int) * N);
+    if (fmax_out) {
+        for (size_t p = 0; p < N; p++) fmax_out[p] = (label[p] == OR_NIL) ? INT32_MAX : 0;
+        for (size_t k = 0; k < norder; k++) {
+            int p = order[k];
+            if (pred[p] >= 0) fmax_out[p] = MAX(fmax_out[pred[p]], Q.value[p]);
+        }
+        free(order);
+    }
+    free(pred);
+    free(Q.first);
+    free(Q.last);
+    free(Q.next);
+    free(Q.prev);
+    free(Q.color);
+    free(Q.value);
+}
+
+/* R4: gft/src/gft_ift.cpp:287-319 (GetEnergy_Min) in 3D with OIFT_Multi's oriented
+ * arc weights (gft_ift.cpp:965-973), tail label selecting the polarity. */
+int or_energy(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
+              const int *label, int nl, int *energy_lb) {
+    int dx[26], dy[26], dz[26];
+    int n = or_adjacency(adj, dx, dy, dz);
+    size_t N = (size_t)X * Y * Z;
+    int e = INT32_MAX;
+    for (int l = 0; l < nl; l++) energy_lb[l] = INT32_MAX;
+    for (int z = 0; z < Z; z++)
+        for (int y = 0; y < Y; y++)
+            for (int x = 0; x < X; x++) {
+                size_t p = (size_t)x + (size_t)y * X + (size_t)z * X * Y;
+                int lp = label[p];
+                float pl = polarity_of(pol, lp);
+                for (int i = 0; i < n; i++) {
+                    int qx = x + dx[i], qy = y + dy[i], qz = z + dz[i];
+                    if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
+                    size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
+                    if (label[q] == lp) continue;
+                    int w = arc_weight(W, N, n, i, p, q, pl);
+                    e = MIN(e, w);
+                    if (lp >= 0 && lp < nl) energy_lb[lp] = MIN(energy_lb[lp], w);
+                }
+            }
+    return e;
+}
+
+/* gft/src/gft_ift.cpp:8684-8720 */
+int or_relax_classes(const int *seeds, int nseeds, const int *label, int n,
+                     int *class_labels, int cap) {
+    int maxl = 0;
+    for (int i = 0; i < nseeds; i++) {
+        int p = seeds[i];
+        if (p >= 0 && p < n) maxl = MAX(maxl, label[p]);
+    }
+    maxl = MAX(0, maxl);
+    char *present = (char *)calloc((size_t)maxl + 1, 1);
+    present[0] = 1;
+    for (int i = 0; i < nseeds; i++) {
+        int p = seeds[i];
+        if (p >= 0 && p < n) {
+            int lb = label[p];
+            if (lb >= 0 && lb <= maxl) present[lb] = 1;
+        }
+    }
+    int nc = 0;
+    for (int l = 0; l <= maxl; l++)
+        if (present[l]) {
+            if (nc < cap) class_labels[nc] = l;
+            nc++;
+        }
+    free(present);
+    return nc;
+}
+
+/* ------------------------------------------------------------------ R3 relax --- */
+/* One template body for FP32 and FP64: T is the membership / weight type.  The FP32
+ * instance performs exactly the float operations of gft_ift.cpp:8778-8833 (global)
+ * and 9058-9110 (per class) in the same order. */
+#define RELAX_BODY(T, FABS, SQRT)                                                          \
+    int dxa[26], dya[26], dza[26];                                                          \
+    int na = or_adjacency(adj, dxa, dya, dza);                                              \
+    int n = X * Y * Z;                                                                      \
+    int cl[512];                                                                            \
+    int nc = or_relax_classes(seeds, nseeds, label, n, cl, 512);                            \
+    if (nc > 512) return -1;                                                                \
+    int maxl = cl[nc - 1];                                                                  \
+    int *l2c = (int *)malloc(sizeof(int) * (maxl + 1));                                     \
+    for (int l = 0; l <= maxl; l++) l2c[l] = -1;                                            \
+    for (int c = 0; c < nc; c++) l2c[cl[c]] = c;                                            \
+    int bgc = l2c[0] < 0 ? 0 : l2c[0];                                                      \
+    T pcm[512];                                                                             \
+    float max_abs_per = 0.0f;                                                               \
+    if (per_class) {                                                                        \
+        for (int c = 0; c < nc; c++) {                                                      \
+            float v = (cl[c] <= max_label) ? per_class[cl[c]] : 0.0f;                       \
+            pcm[c] = (T)v;                                                                  \
+            if (fabsf(v) > max_abs_per) max_abs_per = fabsf(v);                             \
+        }                                                                                   \
+    } else {                                                                                \
+        max_abs_per = fabsf(per);                                                           \
+    }                                                                                       \
+    T Dpq[26];                                                                              \
+    for (int i = 0; i < na; i++)                                                            \
+        Dpq[i] = SQRT((T)(dxa[i] * dxa[i]) * (T)1 * (T)1 + (T)(dya[i] * dya[i]) * (T)1 * (T)1 + \
+                      (T)(dza[i] * dza[i]) * (T)1 * (T)1) / (T)1;                           \
+    int imax = img[0];                                                                      \
+    for (int p = 1; p < n; p++) imax = MAX(imax, img[p]);                                   \
+    T Wmax = (T)imax;                                                                       \
+    Wmax = (T)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));                         \
+    size_t tot = (size_t)n * nc;                                                            \
+    T *f1 = (T *)calloc(tot, sizeof(T)), *f2 = (T *)calloc(tot, sizeof(T));                 \
+    int *mask_nodes = (int *)malloc(sizeof(int) * (n + 1));                                 \
+    unsigned char *mask = (unsigned char *)calloc(n, 1);                                    \
+    mask_nodes[0] = 0;                                                                      \
+    for (int p = 0; p < n; p++) {                                                           \
+        int lb = label[p], c = bgc;                                                         \
+        if (lb >= 0 && lb <= maxl && l2c[lb] >= 0) c = l2c[lb];                             \
+        f1[(size_t)p * nc + c] = (T)1;                                                      \
+        int x = p % X, y = (p / X) % Y, z = p / (X * Y);                                    \
+        for (int i = 0; i < na; i++) {                                                      \
+            int qx = x + dxa[i], qy = y + dya[i], qz = z + dza[i];                          \
+            if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;                                  \
+            int q = qx + qy * X + qz * X * Y;                                               \
+            if (label[p] != label[q]) {                                                     \
+                mask[p] = 1;                                                                \
+                mask_nodes[++mask_nodes[0]] = p;                                            \
+                break;                                                                      \
+            }                                                                               \
+        }                                                                                   \
+    }                                                                                       \
+    int ninic = 1;                                                                          \
+    while (ntimes > 0) {                                                                    \
+        memcpy(f2, f1, tot * sizeof(T));                                                    \
+        for (int j = 1; j <= mask_nodes[0]; j++) {                                          \
+            int p = mask_nodes[j];                                                          \
+            int x = p % X, y = (p / X) % Y, z = p / (X * Y);                                \
+            size_t po = (size_t)p * nc;                                                     \
+            for (int k = 0; k < nc; k++) f2[po + k] = (T)0;                                 \
+            T sw = (T)0;                                                                    \
+            for (int i = 0; i < na; i++) {                                                  \
+                int qx = x + dxa[i], qy = y + dya[i], qz = z + dza[i];                      \
+                if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;                              \
+                int q = qx + qy * X + qz * X * Y;                                           \
+                size_t qo = (size_t)q * nc;                                                 \
+                T w = FABS((T)(img[p] - img[q]));                                           \
+                T per_pq;                                                                   \
+                if (per_class) {                                                            \
+                    per_pq = (T)0;                                                          \
+                    for (int k = 0; k < nc; k++) per_pq += pcm[k] * f1[qo + k];             \
+                } else {                                                                    \
+                    T p_bg = f1[qo + bgc];                                                  \
+                    per_pq = (T)per * ((T)2 * p_bg - (T)1);                                 \
+                }                                                                           \
+                if (img[p] > img[q])                                                        \
+                    w *= ((T)1 + per_pq / (T)100);                                          \
+                else if (img[p] < img[q])                                                   \
+                    w *= ((T)1 - per_pq / (T)100);                                          \
+                w = Wmax - w;                                                               \
+                if (w < (T)0) w = (T)0;                                                     \
+                w = w * w;                                                                  \
+                w = w * w;                                                                  \
+                w = w * w;                                                                  \
+                w /= Dpq[i];                                                                \
+                sw += w;                                                                    \
+                for (int k = 0; k < nc; k++) f2[po + k] += w * f1[qo + k];                  \
+            }                                                                               \
+            if (sw > (T)0) {                                                                \
+                for (int k = 0; k < nc; k++) f2[po + k] /= sw;                              \
+            } else {                                                                        \
+                for (int k = 0; k < nc; k++) f2[po + k] = f1[po + k];                       \
+            }                                                                               \
+        }                                                                                   \
+        T *tmp = f1;                                                                        \
+        f1 = f2;                                                                            \
+        f2 = tmp;                                                                           \
+        for (int i = 0; i < nseeds; i++) {                                                  \
+            int p = seeds[i];                                                               \
+            if (p < 0 || p >= n) continue;                                                  \
+            int lb = label[p], c = bgc;                                                     \
+            if (lb >= 0 && lb <= maxl && l2c[lb] >= 0) c = l2c[lb];                         \
+            size_t po = (size_t)p * nc;                                                     \
+            for (int k = 0; k < nc; k++) f1[po + k] = (T)0;                                 \
+            f1[po + c] = (T)1;                                                              \
+        }                                                                                   \
+        ntimes--;                                                                           \
+        if (ntimes > 0) {                                                                   \
+            int nlast = mask_nodes[0];                                                      \
+            for (int j = ninic; j <= mask_nodes[0]; j++) {                                  \
+                int p = mask_nodes[j];                                                      \
+                int x = p % X, y = (p / X) % Y, z = p / (X * Y);                            \
+                for (int i = 0; i < na; i++) {                                              \
+                    int qx = x + dxa[i], qy = y + dya[i], qz = z + dza[i];                  \
+                    if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;                          \
+                    int q = qx + qy * X + qz * X * Y;                                       \
+                    if (!mask[q]) {                                                         \
+                        mask[q] = 1;                                                        \
+                        mask_nodes[++nlast] = q;                                            \
+                    }                                                                       \
+                }                                                                           \
+            }                                                                               \
+            ninic = mask_nodes[0] + 1;                                                      \
+            mask_nodes[0] = nlast;                                                          \
+        }                                                                                   \
+    }                                                                                       \
+    for (int p = 0; p < n; p++) {                                                           \
+        size_t po = (size_t)p * nc;                                                         \
+        int best = 0;                                                                       \
+        T bv = f1[po];                                                                      \
+        for (int k = 1; k < nc; k++)                                                        \
+            if (f1[po + k] > bv) {                                                          \
+                bv = f1[po + k];                                                            \
+                best = k;                                                                   \
+            }                                                                               \
+        label[p] = cl[best];                                                                \
+    }                                                                                       \
+    if (membership)                                                                         \
+        for (int k = 0; k < nc; k++)                                                        \
+            for (int p = 0; p < n; p++) membership[(size_t)k * n + p] = f1[(size_t)p * nc + k]; \
+    free(l2c);                                                                              \
+    free(f1);                                                                               \
+    free(f2);                                                                               \
+    free(mask_nodes);                                                                       \
+    free(mask);                                                                             \
+    return nc;
+
+int or_relax_f32(const int *img, int X, int Y, int Z, int adj, float per,
+                 const float *per_class, int max_label,
+                 const int *seeds, int nseeds, int *label, int ntimes, float *membership) {
+    RELAX_BODY(float, fabsf, sqrtf)
+}
+
+int or_relax_f64(const int *img, int X, int Y, int Z, int adj, float per,
+                 const float *per_class, int max_label,
+                 const int *seeds, int nseeds, int *label, int ntimes, double *membership) {
+    RELAX_BODY(double, fabs, sqrt)
+}
+
+/* ------------------------------------------------------------------- blur --- */
+/* Kernel3::SphericalGaussian(scn, 1.0, 10.0, 1.0) + Normalize + Convolution
+ * (gft_filtering3.cpp:106-126, 72-83, 321-346, 385-397) with unit voxel spacing. */
+void or_gaussian_blur(const int *img, int X, int Y, int Z, int *out) {
+    int dx[27], dy[27], dz[27];
+    dx[0] = dy[0] = dz[0] = 0;
+    int n = 1 + or_adjacency(6, dx + 1, dy + 1, dz + 1);
+    float val[27], R = 1.0f, s = 10.0f, f = 1.0f, R2 = R * R;
+    for (int i = 0; i < n; i++) {
+        float r2 = (float)(dx[i] * dx[i]) + (float)(dy[i] * dy[i]) + (float)(dz[i] * dz[i]);
+        val[i] = (float)(s * exp(-f * (r2 / R2)));
+    }
+    float wt = 0.0f;
+    for (int i = 0; i < n; i++) wt += val[i];
+    for (int i = 0; i < n; i++) val[i] /= wt;
+    for (int z = 0; z < Z; z++)
+        for (int y = 0; y < Y; y++)
+            for (int x = 0; x < X; x++) {
+                float conv = 0.0f;
+                for (int i = 0; i < n; i++) {
+                    int qx = x + dx[i], qy = y + dy[i], qz = z + dz[i];
+                    if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
+                    conv += ((float)img[qx + qy * X + qz * X * Y]) * val[i];
+                }
+                out[x + y * X + z * X * Y] = (conv < 0) ? (int)(conv - 0.5) : (int)(conv + 0.5);
+            }
+}

@@ -1,0 +1,141 @@
+// Test infrastructure only: a flat C entry layer over the reference gft library
+// (jung0221/roift, gft/src), compiled together with the reference's own sources
+// into oracle/_ref/libgft_ref.so by oracle/Makefile.  Nothing in the product links
+// this file; tests, the golden-fixture generator and the CPU baseline of bench.py
+// call it through ctypes as the checker and as the timed reference arm.
+//
+// Each function wraps one reference routine on plain arrays:
+//   ref_oift_multi            -> gft::ift::OIFT_Multi            (gft/src/gft_ift.cpp:911-989)
+//   ref_oift_multi_perclass   -> gft::ift::OIFT_Multi_PerClass   (gft/src/gft_ift.cpp:991-1083)
+//   ref_orelax_multi          -> gft::ift::ORelax_1_Multi        (gft/src/gft_ift.cpp:8655-8911)
+//   ref_orelax_multi_perclass -> gft::ift::ORelax_1_Multi_PerClass (gft/src/gft_ift.cpp:8913-9187)
+//   ref_ift_fmax_graph        -> gft::ift::IFT_fmax(sGraph*) on Graph::ByEuclideanDistance
+//                                (gft/src/gft_ift.cpp:4753-4809, gft/src/gft_graph.cpp:126-155)
+//   ref_gaussian_blur         -> gft::Scene32::GaussianBlur      (gft/src/gft_filtering3.cpp:385-397)
+//   ref_energy_min_graph      -> gft::ift::GetEnergy_Min(sGraph*) (gft/src/gft_ift.cpp:4xx)
+//
+// Seeds are passed 0-based without a count; the 1-based S[0]=count list the
+// reference expects is built here.  Adjacency radius: 6-adj = Spheric(1.0),
+// 26-adj = Spheric(1.75) (gft/src/gft_adjrel3.cpp:47-85); with zsize == 1 they
+// reduce to 4-adj and 8-adj.
+#include "gft.h"
+#include <cstring>
+#include <cstdlib>
+#include <vector>
+
+using namespace gft;
+
+static sScene32 *make_scene(const int *data, int X, int Y, int Z) {
+    sScene32 *s = Scene32::Create(X, Y, Z);
+    if (data) std::memcpy(s->data, data, sizeof(int) * (size_t)X * Y * Z);
+    return s;
+}
+
+static int *make_S(const int *seeds, int nseeds) {
+    int *S = (int *)calloc((size_t)nseeds + 1, sizeof(int));
+    S[0] = nseeds;
+    for (int i = 0; i < nseeds; i++) S[i + 1] = seeds[i];
+    return S;
+}
+
+static sAdjRel3 *make_adj(int adj) {
+    return (adj == 26 || adj == 8) ? AdjRel3::Spheric(1.75f) : AdjRel3::Spheric(1.0f);
+}
+
+#define REF_API __attribute__((visibility("default")))
+
+extern "C" {
+
+REF_API void ref_oift_multi(const int *img, int X, int Y, int Z, int adj, float per,
+                    const int *seeds, int nseeds, int *label) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    sScene32 *lab = make_scene(label, X, Y, Z);
+    sAdjRel3 *A = make_adj(adj);
+    int *S = make_S(seeds, nseeds);
+    ift::OIFT_Multi(A, scn, per, S, lab);
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y * Z);
+    free(S);
+    AdjRel3::Destroy(&A);
+    Scene32::Destroy(&lab);
+    Scene32::Destroy(&scn);
+}
+
+REF_API void ref_oift_multi_perclass(const int *img, int X, int Y, int Z, int adj,
+                             const float *per_class, int max_label,
+                             const int *seeds, int nseeds, int *label) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    sScene32 *lab = make_scene(label, X, Y, Z);
+    sAdjRel3 *A = make_adj(adj);
+    int *S = make_S(seeds, nseeds);
+    ift::OIFT_Multi_PerClass(A, scn, per_class, max_label, S, lab);
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y * Z);
+    free(S);
+    AdjRel3::Destroy(&A);
+    Scene32::Destroy(&lab);
+    Scene32::Destroy(&scn);
+}
+
+REF_API void ref_orelax_multi(const int *img, int X, int Y, int Z, int adj, float per,
+                      const int *seeds, int nseeds, int *label, int ntimes) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    sScene32 *lab = make_scene(label, X, Y, Z);
+    sAdjRel3 *A = make_adj(adj);
+    int *S = make_S(seeds, nseeds);
+    ift::ORelax_1_Multi(A, scn, per, S, lab, ntimes);
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y * Z);
+    free(S);
+    AdjRel3::Destroy(&A);
+    Scene32::Destroy(&lab);
+    Scene32::Destroy(&scn);
+}
+
+REF_API void ref_orelax_multi_perclass(const int *img, int X, int Y, int Z, int adj,
+                               const float *per_class, int max_label,
+                               const int *seeds, int nseeds, int *label, int ntimes) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    sScene32 *lab = make_scene(label, X, Y, Z);
+    sAdjRel3 *A = make_adj(adj);
+    int *S = make_S(seeds, nseeds);
+    ift::ORelax_1_Multi_PerClass(A, scn, per_class, max_label, S, lab, ntimes);
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y * Z);
+    free(S);
+    AdjRel3::Destroy(&A);
+    Scene32::Destroy(&lab);
+    Scene32::Destroy(&scn);
+}
+
+// Un-oriented f_max IFT with exported cost.  Arc weights are |I_p - I_q| + 1
+// (ByEuclideanDistance), so cost(q) = our f_max cost + 1 on non-seed voxels.
+REF_API void ref_ift_fmax_graph(const int *img, int X, int Y, int Z, int adj,
+                        const int *seeds, int nseeds, int *label, int *cost) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    float r = (adj == 26 || adj == 8) ? 1.75f : 1.0f;
+    sGraph *g = Graph::ByEuclideanDistance(scn, r);
+    int *S = make_S(seeds, nseeds);
+    ift::IFT_fmax(g, S, label, cost);
+    free(S);
+    Graph::Destroy(&g);
+    Scene32::Destroy(&scn);
+}
+
+// Un-oriented minimum cut energy on the ByEuclideanDistance graph (weights |dI|+1).
+REF_API int ref_energy_min_graph(const int *img, int X, int Y, int Z, int adj,
+                         const int *label, int lb) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    float r = (adj == 26 || adj == 8) ? 1.75f : 1.0f;
+    sGraph *g = Graph::ByEuclideanDistance(scn, r);
+    int e = ift::GetEnergy_Min(g, const_cast<int *>(label), lb);
+    Graph::Destroy(&g);
+    Scene32::Destroy(&scn);
+    return e;
+}
+
+REF_API void ref_gaussian_blur(const int *img, int X, int Y, int Z, int *out) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    sScene32 *b = Scene32::GaussianBlur(scn);
+    std::memcpy(out, b->data, sizeof(int) * (size_t)X * Y * Z);
+    Scene32::Destroy(&b);
+    Scene32::Destroy(&scn);
+}
+
+}  // extern "C"

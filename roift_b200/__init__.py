@@ -1,0 +1,259 @@
+"""roift_b200 -- B200-native (sm_100a) OIFT + relaxation, Python host mirror.
+
+The compute path is liboift_b200.so (CUDA kernels behind the C ABI declared in
+include/oift_b200.h).  This module binds that ABI with ctypes and mirrors the
+reference call surface of the path:
+
+  * oift_fmax_gpu_run / oift_gpu_run   -- gpu/oift_fmax_gpu.cu:139-149, gpu/oift_gpu.cu:149-158
+  * OIFT_Multi / OIFT_Multi_PerClass   -- gft/include/gft_ift.h:108-122 (labels in place)
+  * ORelax_1_Multi / ORelax_1_Multi_PerClass -- gft/include/gft_ift.h:451-465
+
+There is no CPU fallback: importing works without a GPU (so the ABI can be inspected),
+but every compute call raises if the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboift_b200.so")
+HEADER = os.path.join(HERE, "..", "include", "oift_b200.h")
+
+NIL = -1
+OK = 0
+STATUS = {0: "OK", -1: "BAD_ARG", -2: "NO_SEEDS", -3: "OOM", -4: "NOT_CONVERGED",
+          -5: "QUEUE_OVERFLOW", -6: "CUDA", -7: "RANGE", -8: "UNSUPPORTED", -9: "SEED_RANGE"}
+W_MODES = {"grad": 0, "grad_q": 1, "rbf_q": 2, "blend_q": 3}
+
+
+class OiftError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+
+
+class Params(C.Structure):
+    _fields_ = [("xsize", C.c_int), ("ysize", C.c_int), ("zsize", C.c_int),
+                ("adjacency", C.c_int), ("weight_mode", C.c_int), ("wq", C.c_int),
+                ("rbf_sigma", C.c_float), ("blend_a", C.c_float), ("per", C.c_float),
+                ("per_class", C.POINTER(C.c_float)), ("max_label", C.c_int),
+                ("relax_sweeps", C.c_int)]
+
+
+class Outputs(C.Structure):
+    _fields_ = [("cost", C.c_void_p), ("oift_label", C.c_void_p), ("label", C.c_void_p),
+                ("mask", C.c_void_p), ("membership", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("levels", C.c_int), ("tile_steps", C.c_longlong), ("clamped", C.c_longlong),
+                ("nclasses", C.c_int), ("ms_weights", C.c_float), ("ms_oift", C.c_float),
+                ("ms_relax", C.c_float), ("ms_total", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
+           "oift_b200_set_stream", "oift_b200_status_string", "oift_b200_run_device_i16",
+           "oift_b200_run_host", "oift_b200_build_weights_i16", "oift_b200_weight_planes",
+           "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status"]
+
+_lib = None
+
+
+def lib():
+    """Load liboift_b200.so (build it first with roift_b200.build.build())."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: the CUDA extension is not built "
+                          "(python -m roift_b200.build); there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        vp, i32p = C.c_void_p, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        L.oift_b200_create.argtypes = [C.POINTER(vp), C.c_int]
+        L.oift_b200_destroy.argtypes = [vp]
+        L.oift_b200_scratch_bytes.restype = C.c_size_t
+        L.oift_b200_scratch_bytes.argtypes = [vp]
+        L.oift_b200_set_stream.argtypes = [vp, vp]
+        L.oift_b200_status_string.restype = C.c_char_p
+        L.oift_b200_run_device_i16.argtypes = [vp, C.POINTER(Params), vp, vp, vp, C.c_int,
+                                               C.POINTER(Outputs), C.POINTER(Stats)]
+        L.oift_b200_run_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
+                                         vp, vp, C.c_int, vp, C.POINTER(Stats)]
+        L.oift_b200_build_weights_i16.argtypes = [vp, C.POINTER(Params), vp, vp,
+                                                  C.POINTER(C.c_longlong)]
+        L.oift_fmax_gpu_run.argtypes = [i32p, i32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"),
+                                        C.c_int, i32p, C.c_int]
+        L.oift_gpu_run.argtypes = [C.c_int] + L.oift_fmax_gpu_run.argtypes
+        _lib = L
+    return _lib
+
+
+def make_params(shape_zyx, adjacency=6, weight_mode="grad", wq=4095, rbf_sigma=150.0,
+                blend_a=0.5, pol=None, per_class=None, sweeps=0):
+    """Parameters; pol in [-1,1] becomes per = (float)(pol*100.0) as the CLI passes it
+    (oiftrelax.cpp:387), per_class values are already x100."""
+    if len(shape_zyx) == 2:
+        Z, (Y, X) = 1, shape_zyx
+    else:
+        Z, Y, X = shape_zyx
+    p = Params()
+    p.xsize, p.ysize, p.zsize = X, Y, Z
+    p.adjacency = adjacency
+    p.weight_mode = W_MODES[weight_mode]
+    p.wq = wq
+    p.rbf_sigma = rbf_sigma
+    p.blend_a = blend_a
+    keep = None
+    if per_class is not None:
+        keep = np.ascontiguousarray(per_class, np.float32)
+        p.per_class = keep.ctypes.data_as(C.POINTER(C.c_float))
+        p.max_label = len(keep) - 1
+        p.per = 0.0
+    else:
+        p.per = float(np.float32((pol or 0.0) * 100.0))
+        p.per_class = None
+        p.max_label = 0
+    p.relax_sweeps = sweeps
+    p._keep = keep
+    return p
+
+
+class Context:
+    """Device scratch + stream owner (oift_b200_create / oift_b200_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        rc = lib().oift_b200_create(C.byref(self._h), device)
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_create")
+        self.device = device
+
+    def close(self):
+        if self._h:
+            lib().oift_b200_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        rc = lib().oift_b200_set_stream(self._h, C.c_void_p(stream_ptr or 0))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_set_stream")
+
+    def scratch_bytes(self) -> int:
+        return int(lib().oift_b200_scratch_bytes(self._h))
+
+    def run_device(self, params, image_ptr, seeds_ptr, labels_ptr, nseeds, cost=None,
+                   oift_label=None, label=None, mask=None, membership=None) -> Stats:
+        """Full pipeline on device pointers (ints).  Output pointers may be None."""
+        out = Outputs(cost or 0, oift_label or 0, label or 0, mask or 0, membership or 0)
+        st = Stats()
+        rc = lib().oift_b200_run_device_i16(self._h, C.byref(params), C.c_void_p(image_ptr),
+                                            C.c_void_p(seeds_ptr), C.c_void_p(labels_ptr),
+                                            int(nseeds), C.byref(out), C.byref(st))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_run_device_i16")
+        return st
+
+    def run_host(self, params, image, label, seeds, want_cost=False, want_membership=0,
+                 want_mask=False):
+        """Full pipeline on host arrays (reference-style int32 image, labels in/out)."""
+        img = np.ascontiguousarray(np.asarray(image).reshape(-1), np.int32)
+        lab = np.ascontiguousarray(label, np.int32)
+        sd = np.ascontiguousarray(seeds, np.int32)
+        N = img.size
+        cost = np.empty(N, np.int32) if want_cost else None
+        memb = np.empty(want_membership * N, np.float32) if want_membership else None
+        mask = np.empty(N, np.uint8) if want_mask else None
+        st = Stats()
+        rc = lib().oift_b200_run_host(self._h, C.byref(params), img, lab, sd, len(sd),
+                                      cost.ctypes.data if cost is not None else None,
+                                      memb.ctypes.data if memb is not None else None,
+                                      int(want_membership),
+                                      mask.ctypes.data if mask is not None else None,
+                                      C.byref(st))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_run_host")
+        if memb is not None:
+            memb = memb[: st.nclasses * N].reshape(st.nclasses, N)
+        return lab, cost, memb, mask, st
+
+    def build_weights(self, params, image_ptr, weights_ptr) -> int:
+        cl = C.c_longlong(0)
+        rc = lib().oift_b200_build_weights_i16(self._h, C.byref(params), C.c_void_p(image_ptr),
+                                               C.c_void_p(weights_ptr), C.byref(cl))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_build_weights_i16")
+        return cl.value
+
+
+def weight_planes(adjacency: int) -> int:
+    return int(lib().oift_b200_weight_planes(adjacency))
+
+
+# ------------------------------------------------ reference call surface ----
+def oift_fmax_gpu_run(image, labels, xsize, ysize, zsize, per_class, seeds) -> int:
+    """gpu/oift_fmax_gpu.cu:139-149: labels (int32, NIL except seeds) updated in place;
+    returns the number of levels, raises on error."""
+    img = np.ascontiguousarray(np.asarray(image).reshape(-1), np.int32)
+    pc = np.ascontiguousarray(per_class, np.float32)
+    sd = np.ascontiguousarray(seeds, np.int32)
+    assert labels.dtype == np.int32 and labels.flags.c_contiguous
+    r = lib().oift_fmax_gpu_run(img, labels, img.size, xsize, ysize, zsize, pc, len(pc) - 1,
+                                sd, len(sd))
+    if r < 0:
+        raise OiftError(lib().oift_b200_last_status(), "oift_fmax_gpu_run")
+    return r
+
+
+_default_ctx = None
+
+
+def _ctx():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _shape_of(scn):
+    a = np.asarray(scn)
+    return a.shape if a.ndim == 3 else (1,) + a.shape
+
+
+def OIFT_Multi(adjacency, scn, per, S, label, per_class=None):
+    """gft::ift::OIFT_Multi(A, scn, per, S, label) on the GPU: label (flat int32, NIL
+    except seeds) is overwritten with the OIFT labels.  per is x100 as in the reference.
+    Returns the f_max cost map."""
+    shp = _shape_of(scn)
+    if per_class is None:
+        p = make_params(shp, adjacency=adjacency, weight_mode="grad", pol=None)
+        p.per = float(np.float32(per))
+    else:
+        p = make_params(shp, adjacency=adjacency, weight_mode="grad", per_class=per_class)
+    lab, cost, _, _, _ = _ctx().run_host(p, scn, label, S, want_cost=True)
+    return cost
+
+
+def ORelax_1_Multi(adjacency, scn, per, S, label, ntimes, per_class=None):
+    """OIFT + gft::ift::ORelax_1_Multi on the GPU (label in = seeds, out = relaxed labels).
+    Returns the relaxed membership [classes, N]."""
+    shp = _shape_of(scn)
+    if per_class is None:
+        p = make_params(shp, adjacency=adjacency, weight_mode="grad", sweeps=ntimes)
+        p.per = float(np.float32(per))
+    else:
+        p = make_params(shp, adjacency=adjacency, weight_mode="grad", per_class=per_class,
+                        sweeps=ntimes)
+    _, _, memb, _, _ = _ctx().run_host(p, scn, label, S, want_membership=8)
+    return memb

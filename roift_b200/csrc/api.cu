@@ -1,0 +1,580 @@
+// api.cu -- C ABI of liboift_b200 (include/oift_b200.h): context, device scratch,
+// pipeline orchestration and the reference-compatible entry points.
+//
+// Pipeline of one job (all on the context's stream):
+//   minmax(image) -> build_weights -> OIFT (persistent kernel) -> finalize labels/cost
+//   -> relax init -> K sweeps (ping-pong membership) -> argmax labels + mask.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace oiftb;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct oift_b200_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev[8];
+    // scratch (grow-only)
+    DevBuf img32, img16, W, key, tpend, inq, queue, glob, flag, minmax, seeds, slabels, cost,
+        olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8;
+    size_t total = 0;
+};
+
+static thread_local int g_last_status = OIFT_OK;
+
+static int grow(oift_b200_ctx *c, DevBuf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return OIFT_OK;
+    if (b.p) {
+        cudaFree(b.p);
+        c->total -= b.bytes;
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return OIFT_E_OOM;
+    }
+    b.bytes = bytes;
+    c->total += bytes;
+    return OIFT_OK;
+}
+
+#define TRY(x)                        \
+    do {                              \
+        int _s = (x);                 \
+        if (_s != OIFT_OK) return _s; \
+    } while (0)
+#define CU(x)                                  \
+    do {                                       \
+        if ((x) != cudaSuccess) {              \
+            cudaGetLastError();                \
+            return OIFT_E_CUDA;                \
+        }                                      \
+    } while (0)
+
+extern "C" {
+
+const char *oift_b200_status_string(int s) {
+    switch (s) {
+        case OIFT_OK: return "ok";
+        case OIFT_E_BAD_ARG: return "bad argument";
+        case OIFT_E_NO_SEEDS: return "no seeds";
+        case OIFT_E_OOM: return "device allocation failed";
+        case OIFT_E_NOT_CONVERGED: return "bounded wait expired (not converged)";
+        case OIFT_E_QUEUE_OVERFLOW: return "device work queue overflow";
+        case OIFT_E_CUDA: return "CUDA runtime error";
+        case OIFT_E_RANGE: return "weight or intensity out of supported range";
+        case OIFT_E_UNSUPPORTED: return "unsupported option";
+        case OIFT_E_SEED_RANGE: return "seed address outside the volume";
+        default: return "unknown status";
+    }
+}
+
+int oift_b200_create(oift_b200_ctx **out, int device) {
+    if (!out) return OIFT_E_BAD_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return OIFT_E_CUDA;
+    }
+    CU(cudaSetDevice(device));
+    oift_b200_ctx *c = new oift_b200_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (!coop) {
+        delete c;
+        return OIFT_E_UNSUPPORTED;
+    }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return OIFT_E_CUDA;
+    }
+    c->own_stream = true;
+    for (auto &e : c->ev) cudaEventCreate(&e);
+    *out = c;
+    return OIFT_OK;
+}
+
+int oift_b200_destroy(oift_b200_ctx *c) {
+    if (!c) return OIFT_E_BAD_ARG;
+    cudaSetDevice(c->device);
+    DevBuf *bufs[] = {&c->img32, &c->img16,  &c->W,      &c->key,     &c->tpend,   &c->inq,
+                      &c->queue, &c->glob,   &c->flag,   &c->minmax,  &c->seeds,   &c->slabels,
+                      &c->cost,  &c->olabel, &c->flabel, &c->memb,    &c->seedc,   &c->l2c,
+                      &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8};
+    for (DevBuf *b : bufs)
+        if (b->p) cudaFree(b->p);
+    for (auto &e : c->ev) cudaEventDestroy(e);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return OIFT_OK;
+}
+
+size_t oift_b200_scratch_bytes(const oift_b200_ctx *c) { return c ? c->total : 0; }
+
+int oift_b200_set_stream(oift_b200_ctx *c, void *stream) {
+    if (!c) return OIFT_E_BAD_ARG;
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+    return OIFT_OK;
+}
+
+int oift_b200_weight_planes(int adjacency) {
+    if (adjacency == 6 || adjacency == 4) return 3;
+    if (adjacency == 26 || adjacency == 8) return 13;
+    return 0;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ helpers ----
+static int check_params(const oift_b200_params *p) {
+    if (!p) return OIFT_E_BAD_ARG;
+    if (p->xsize <= 0 || p->ysize <= 0 || p->zsize <= 0) return OIFT_E_BAD_ARG;
+    if ((size_t)p->xsize * p->ysize * p->zsize > 0x7fffffffULL) return OIFT_E_BAD_ARG;
+    if (p->adjacency == 4 || p->adjacency == 8) {
+        if (p->zsize != 1) return OIFT_E_BAD_ARG;
+    } else if (p->adjacency != 6 && p->adjacency != 26) {
+        return OIFT_E_BAD_ARG;
+    }
+    if (p->weight_mode < 0 || p->weight_mode > 3) return OIFT_E_BAD_ARG;
+    if (p->weight_mode != OIFT_W_GRAD && (p->wq <= 0 || p->wq > OIFT_MAX_BASE)) return OIFT_E_BAD_ARG;
+    if (p->relax_sweeps < 0) return OIFT_E_BAD_ARG;
+    if (p->per_class) {
+        if (p->max_label < 0 || p->max_label > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
+        for (int i = 0; i <= p->max_label; i++)
+            if (!(std::fabs(p->per_class[i]) <= 100.0f)) return OIFT_E_BAD_ARG;
+    } else if (!(std::fabs(p->per) <= 100.0f)) {
+        return OIFT_E_BAD_ARG;
+    }
+    if (p->weight_mode == OIFT_W_BLEND_Q) return OIFT_E_UNSUPPORTED;
+    if (p->weight_mode == OIFT_W_RBF_Q && !(p->rbf_sigma > 0.0f)) return OIFT_E_BAD_ARG;
+    // the tile OIFT handles the 6 / 4 neighbourhoods
+    if (p->adjacency == 26 || p->adjacency == 8) return OIFT_E_UNSUPPORTED;
+    return OIFT_OK;
+}
+
+// Polarity table of the OIFT: global mode -> [ -per ] with default +per
+// (gft_ift.cpp:968); per-class mode -> per_class[0..max_label], default 0.
+static int upload_polarity(oift_b200_ctx *c, const oift_b200_params *p, int *npol,
+                           float *dflt) {
+    std::vector<float> t;
+    if (p->per_class) {
+        t.assign(p->per_class, p->per_class + p->max_label + 1);
+        *dflt = 0.0f;
+    } else {
+        t.push_back(-p->per);
+        *dflt = p->per;
+    }
+    TRY(grow(c, c->pol, t.size() * sizeof(float)));
+    CU(cudaMemcpyAsync(c->pol.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice,
+                       c->stream));
+    *npol = (int)t.size();
+    return OIFT_OK;
+}
+
+template <typename T>
+static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_img,
+                        const int32_t *d_seeds, const int32_t *d_slabels, int nseeds,
+                        const oift_b200_outputs *out, oift_b200_stats *st) {
+    cudaStream_t s = c->stream;
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    const size_t N = (size_t)X * Y * Z;
+    const int planes = oift_b200_weight_planes(p->adjacency);
+    Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
+    OiftPlan plan = oift_plan(X, Y, Z);
+
+    TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
+    TRY(grow(c, c->key, N * sizeof(uint32_t)));
+    TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
+    TRY(grow(c, c->inq, (size_t)plan.ntiles * sizeof(uint32_t)));
+    TRY(grow(c, c->queue, (size_t)plan.qcap * sizeof(uint32_t)));
+    TRY(grow(c, c->glob, oift_globals_bytes()));
+    TRY(grow(c, c->flag, 4 * sizeof(int)));
+    TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
+    TRY(grow(c, c->olabel, N * sizeof(int32_t)));
+    TRY(grow(c, c->presence, 1024 * sizeof(uint32_t)));
+
+    cudaEventRecord(c->ev[0], s);
+    // ---- intensity range (Wmax of the relaxation, RBF table length) ----
+    int mm_init[2] = {0x7fffffff, (int)0x80000000};
+    int *d_mm = (int *)c->minmax.p;
+    unsigned long long *d_clamp = (unsigned long long *)((char *)c->minmax.p + 2 * sizeof(int) + 8);
+    CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(d_clamp, 0, sizeof(unsigned long long), s));
+    CU(launch_minmax<T>(d_img, N, d_mm, c->sms, s));
+    int hmm[2];
+    CU(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+
+    // ---- arc weights ----
+    BuildArgs ba;
+    ba.X = X;
+    ba.Y = Y;
+    ba.Z = Z;
+    ba.planes = planes;
+    ba.mode = p->weight_mode;
+    ba.cap = (p->weight_mode == OIFT_W_GRAD) ? OIFT_MAX_BASE : p->wq;
+    for (int k = 0; k < planes; k++) {
+        int i = adj.n / 2 + k;
+        ba.dx[k] = adj.dx[i];
+        ba.dy[k] = adj.dy[i];
+        ba.dz[k] = adj.dz[i];
+    }
+    ba.lut = nullptr;
+    ba.lut_len = 0;
+    ba.grad = nullptr;
+    ba.blend_a = p->blend_a;
+    ba.clamped = d_clamp;
+    if (p->weight_mode == OIFT_W_RBF_Q) {
+        long long range = (long long)hmm[1] - (long long)hmm[0];
+        int len = (int)(range + 1);
+        std::vector<uint16_t> lut(len);
+        double sg = p->rbf_sigma;
+        for (int d = 0; d < len; d++) {
+            double a = std::exp(-((double)d * (double)d) / (2.0 * sg * sg));
+            double v = std::floor((double)p->wq * (1.0 - a) + 0.5);
+            if (v < 0) v = 0;
+            if (v > p->wq) v = p->wq;
+            lut[d] = (uint16_t)v;
+        }
+        TRY(grow(c, c->lut, len * sizeof(uint16_t)));
+        CU(cudaMemcpyAsync(c->lut.p, lut.data(), len * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        CU(cudaStreamSynchronize(s));
+        ba.lut = (const uint16_t *)c->lut.p;
+        ba.lut_len = len;
+    }
+    CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
+    cudaEventRecord(c->ev[1], s);
+
+    // ---- OIFT ----
+    int npol = 0;
+    float dflt = 0.0f;
+    TRY(upload_polarity(c, p, &npol, &dflt));
+    OiftScratch S;
+    S.key = (uint32_t *)c->key.p;
+    S.tpend = (uint32_t *)c->tpend.p;
+    S.inq = (uint32_t *)c->inq.p;
+    S.queue = (uint32_t *)c->queue.p;
+    S.g = (OiftGlobals *)c->glob.p;
+    int32_t *d_cost = out ? out->cost : nullptr;
+    int32_t *d_olab = (out && out->oift_label) ? out->oift_label : (int32_t *)c->olabel.p;
+    int levels = 0;
+    long long steps = 0;
+    int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
+                      (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
+                      c->sms, s, &levels, &steps);
+    if (rc != OIFT_OK) return rc;
+    unsigned long long hclamp = 0;
+    CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));
+    cudaEventRecord(c->ev[2], s);
+
+    // ---- relaxation ----
+    const int K = p->relax_sweeps;
+    int nclasses = 0;
+    std::vector<int> classes;
+    bool want_relax = out && (out->label || out->mask || out->membership);
+    if (want_relax) {
+        // classes = labels present among seeds, plus 0 (gft_ift.cpp:8684-8712)
+        CU(cudaMemsetAsync(c->presence.p, 0, 1024 * sizeof(uint32_t), s));
+        if (nseeds > 0)
+            seed_presence_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(d_slabels, nseeds,
+                                                                      (uint32_t *)c->presence.p);
+        std::vector<uint32_t> bits(1024);
+        CU(cudaMemcpyAsync(bits.data(), c->presence.p, 1024 * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        bits[0] |= 1u;
+        for (int l = 0; l <= OIFT_MAX_LABEL; l++)
+            if ((bits[l >> 5] >> (l & 31)) & 1u) classes.push_back(l);
+        nclasses = (int)classes.size();
+        if (nclasses > 8) return OIFT_E_UNSUPPORTED;
+        int maxl = classes.back();
+        std::vector<int> l2c(maxl + 1, -1);
+        for (int k = 0; k < nclasses; k++) l2c[classes[k]] = k;
+        int bg = l2c[0] < 0 ? 0 : l2c[0];
+        // Wmax (gft_ift.cpp:8733-8734) on the image shifted to >= 0 as the CLI does
+        float max_abs_per = 0.0f;
+        std::vector<float> pcm(nclasses, 0.0f);
+        if (p->per_class) {
+            for (int k = 0; k < nclasses; k++) {
+                float v = (classes[k] <= p->max_label) ? p->per_class[classes[k]] : 0.0f;
+                pcm[k] = v;
+                if (std::fabs(v) > max_abs_per) max_abs_per = std::fabs(v);
+            }
+        } else {
+            max_abs_per = std::fabs(p->per);
+        }
+        long long imax = hmm[1], imin = hmm[0];
+        long long shifted_max = imin < 0 ? imax - imin : imax;
+        float Wmax = (float)shifted_max;
+        Wmax = (float)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));
+        double deg = (p->adjacency == 26) ? 26 : (p->adjacency == 8 ? 8 : (p->adjacency == 6 ? 6 : 4));
+        if ((double)Wmax > std::pow(3.0e38 / deg, 0.125)) return OIFT_E_RANGE;
+
+        RelaxArgs ra;
+        ra.X = X;
+        ra.Y = Y;
+        ra.Z = Z;
+        ra.N = N;
+        ra.nadj = adj.n;
+        for (int i = 0; i < adj.n; i++) {
+            ra.dx[i] = adj.dx[i];
+            ra.dy[i] = adj.dy[i];
+            ra.dz[i] = adj.dz[i];
+            // Dpq = sqrtf(dx^2 + dy^2 + dz^2) / dmin with unit spacing (gft_ift.cpp:8723-8731)
+            ra.dpq[i] = sqrtf((float)(adj.dx[i] * adj.dx[i]) + (float)(adj.dy[i] * adj.dy[i]) +
+                              (float)(adj.dz[i] * adj.dz[i])) /
+                        1.0f;
+        }
+        ra.Wmax = Wmax;
+        ra.per = p->per;
+        ra.bg = bg;
+        for (int k = 0; k < 8; k++) ra.pcm[k] = k < nclasses ? pcm[k] : 0.0f;
+
+        TRY(grow(c, c->memb, 2 * (size_t)nclasses * N * sizeof(float)));
+        TRY(grow(c, c->seedc, N));
+        TRY(grow(c, c->l2c, (maxl + 1) * sizeof(int)));
+        TRY(grow(c, c->classes, nclasses * sizeof(int)));
+        CU(cudaMemcpyAsync(c->l2c.p, l2c.data(), (maxl + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(c->classes.p, classes.data(), nclasses * sizeof(int), cudaMemcpyHostToDevice, s));
+        float *m0 = (float *)c->memb.p, *m1 = m0 + (size_t)nclasses * N;
+        int blocks = (int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16);
+        relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m0);
+        CU(cudaMemsetAsync(c->seedc.p, 0xFF, N, s));
+        if (nseeds > 0)
+            relax_seed_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(d_seeds, nseeds, d_olab, N,
+                                                                   (const int *)c->l2c.p, maxl, bg,
+                                                                   (uint8_t *)c->seedc.p);
+        float *cur = m0, *nxt = m1;
+        for (int it = 0; it < K; it++) {
+            CU(launch_relax_sweep<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, ra,
+                                     p->per_class != nullptr, c->sms, s));
+            std::swap(cur, nxt);
+        }
+        relax_argmax_kernel<<<blocks, 256, 0, s>>>(cur, N, nclasses, (const int *)c->classes.p,
+                                                   out->label, out->mask);
+        if (out->membership)
+            CU(cudaMemcpyAsync(out->membership, cur, (size_t)nclasses * N * sizeof(float),
+                               cudaMemcpyDeviceToDevice, s));
+    }
+    cudaEventRecord(c->ev[3], s);
+    CU(cudaStreamSynchronize(s));
+    CU(cudaGetLastError());
+    if (p->weight_mode == OIFT_W_GRAD && hclamp) return OIFT_E_RANGE;
+    if (st) {
+        st->levels = levels;
+        st->tile_steps = steps;
+        st->clamped = (long long)hclamp;
+        st->nclasses = nclasses;
+        cudaEventElapsedTime(&st->ms_weights, c->ev[0], c->ev[1]);
+        cudaEventElapsedTime(&st->ms_oift, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&st->ms_relax, c->ev[2], c->ev[3]);
+        cudaEventElapsedTime(&st->ms_total, c->ev[0], c->ev[3]);
+    }
+    return OIFT_OK;
+}
+
+extern "C" {
+
+int oift_b200_run_device_i16(oift_b200_ctx *c, const oift_b200_params *p, const int16_t *image,
+                             const int32_t *seeds, const int32_t *seed_labels, int nseeds,
+                             const oift_b200_outputs *out, oift_b200_stats *stats) {
+    if (!c || !image || (nseeds > 0 && (!seeds || !seed_labels))) return OIFT_E_BAD_ARG;
+    TRY(check_params(p));
+    if (nseeds <= 0) return OIFT_E_NO_SEEDS;
+    cudaSetDevice(c->device);
+    return run_pipeline<int16_t>(c, p, image, seeds, seed_labels, nseeds, out, stats);
+}
+
+int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *image,
+                       int32_t *label, const int32_t *seeds, int nseeds, int32_t *cost,
+                       float *membership, int membership_cap_classes, uint8_t *mask,
+                       oift_b200_stats *stats) {
+    if (!c || !image || !label || (nseeds > 0 && !seeds)) return OIFT_E_BAD_ARG;
+    TRY(check_params(p));
+    if (nseeds <= 0) return OIFT_E_NO_SEEDS;
+    cudaSetDevice(c->device);
+    const size_t N = (size_t)p->xsize * p->ysize * p->zsize;
+    cudaStream_t s = c->stream;
+    std::vector<int32_t> slab(nseeds);
+    for (int i = 0; i < nseeds; i++) {
+        if (seeds[i] < 0 || (size_t)seeds[i] >= N) return OIFT_E_SEED_RANGE;
+        int lb = label[seeds[i]];
+        slab[i] = lb < 0 ? 0 : lb;
+        if (slab[i] > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
+    }
+    TRY(grow(c, c->img32, N * sizeof(int32_t)));
+    TRY(grow(c, c->seeds, (size_t)nseeds * sizeof(int32_t)));
+    TRY(grow(c, c->slabels, (size_t)nseeds * sizeof(int32_t)));
+    TRY(grow(c, c->flabel, N * sizeof(int32_t)));
+    if (cost) TRY(grow(c, c->cost, N * sizeof(int32_t)));
+    if (mask) TRY(grow(c, c->mask8, N));
+    CU(cudaMemcpyAsync(c->img32.p, image, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->seeds.p, seeds, (size_t)nseeds * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->slabels.p, slab.data(), (size_t)nseeds * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, s));
+    oift_b200_outputs o{};
+    o.cost = cost ? (int32_t *)c->cost.p : nullptr;
+    const bool relax = p->relax_sweeps > 0 || membership || mask;
+    // without sweeps the labels are the OIFT labels (argmax of the one-hot start)
+    if (relax)
+        o.label = (int32_t *)c->flabel.p;
+    else
+        o.oift_label = (int32_t *)c->flabel.p;
+    o.mask = mask ? (uint8_t *)c->mask8.p : nullptr;
+    DevBuf tmpm;
+    oift_b200_stats lst{};
+    oift_b200_stats *sp = stats ? stats : &lst;
+    int rc;
+    if (membership) {
+        if (cudaMalloc(&tmpm.p, (size_t)membership_cap_classes * N * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            return OIFT_E_OOM;
+        }
+        o.membership = (float *)tmpm.p;
+    }
+    rc = run_pipeline<int32_t>(c, p, (const int32_t *)c->img32.p, (const int32_t *)c->seeds.p,
+                               (const int32_t *)c->slabels.p, nseeds, &o, sp);
+    if (rc == OIFT_OK && membership && sp->nclasses > membership_cap_classes) rc = OIFT_E_BAD_ARG;
+    if (rc == OIFT_OK) {
+        cudaMemcpyAsync(label, c->flabel.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (cost) cudaMemcpyAsync(cost, o.cost, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        if (mask) cudaMemcpyAsync(mask, o.mask, N, cudaMemcpyDeviceToHost, s);
+        if (membership)
+            cudaMemcpyAsync(membership, o.membership, (size_t)sp->nclasses * N * sizeof(float),
+                            cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) rc = OIFT_E_CUDA;
+    }
+    if (tmpm.p) cudaFree(tmpm.p);
+    return rc;
+}
+
+int oift_b200_build_weights_i16(oift_b200_ctx *c, const oift_b200_params *p,
+                                const int16_t *image, uint16_t *weights, long long *clamped) {
+    if (!c || !image || !weights) return OIFT_E_BAD_ARG;
+    int chk = check_params(p);
+    if (chk != OIFT_OK && chk != OIFT_E_UNSUPPORTED) return chk;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    const size_t N = (size_t)X * Y * Z;
+    Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
+    TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
+    unsigned long long *d_clamp = (unsigned long long *)((char *)c->minmax.p + 2 * sizeof(int) + 8);
+    int *d_mm = (int *)c->minmax.p;
+    BuildArgs ba;
+    ba.X = X;
+    ba.Y = Y;
+    ba.Z = Z;
+    ba.planes = oift_b200_weight_planes(p->adjacency);
+    ba.mode = p->weight_mode;
+    ba.cap = (p->weight_mode == OIFT_W_GRAD) ? OIFT_MAX_BASE : p->wq;
+    for (int k = 0; k < ba.planes; k++) {
+        int i = adj.n / 2 + k;
+        ba.dx[k] = adj.dx[i];
+        ba.dy[k] = adj.dy[i];
+        ba.dz[k] = adj.dz[i];
+    }
+    ba.lut = nullptr;
+    ba.lut_len = 0;
+    ba.grad = nullptr;
+    ba.blend_a = p->blend_a;
+    ba.clamped = d_clamp;
+    if (p->weight_mode == OIFT_W_BLEND_Q) return OIFT_E_UNSUPPORTED;
+    if (p->weight_mode == OIFT_W_RBF_Q) {
+        int mm_init[2] = {0x7fffffff, (int)0x80000000};
+        CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+        CU(launch_minmax<int16_t>(image, N, d_mm, c->sms, s));
+        int hmm[2];
+        CU(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        int len = hmm[1] - hmm[0] + 1;
+        std::vector<uint16_t> lut(len);
+        double sg = p->rbf_sigma;
+        for (int d = 0; d < len; d++) {
+            double a = std::exp(-((double)d * (double)d) / (2.0 * sg * sg));
+            double v = std::floor((double)p->wq * (1.0 - a) + 0.5);
+            lut[d] = (uint16_t)(v < 0 ? 0 : (v > p->wq ? p->wq : v));
+        }
+        TRY(grow(c, c->lut, len * sizeof(uint16_t)));
+        CU(cudaMemcpyAsync(c->lut.p, lut.data(), len * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        ba.lut = (const uint16_t *)c->lut.p;
+        ba.lut_len = len;
+    }
+    CU(cudaMemsetAsync(d_clamp, 0, sizeof(unsigned long long), s));
+    CU(launch_build_weights<int16_t>(image, weights, ba, c->sms, s));
+    unsigned long long h = 0;
+    CU(cudaMemcpyAsync(&h, d_clamp, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (clamped) *clamped = (long long)h;
+    return OIFT_OK;
+}
+
+// ----------------------------------------------------- reference drop-in ----
+static std::mutex g_dropin_mu;
+static oift_b200_ctx *g_dropin_ctx = nullptr;
+
+int oift_b200_last_status(void) { return g_last_status; }
+
+int oift_gpu_run(int cost_mode, const int *h_image, int *h_labels, int n, int xsize, int ysize,
+                 int zsize, const float *h_per_class, int max_label, const int *h_seeds,
+                 int n_seeds) {
+    if (cost_mode != 0) {
+        g_last_status = OIFT_E_UNSUPPORTED;
+        return -1;
+    }
+    return oift_fmax_gpu_run(h_image, h_labels, n, xsize, ysize, zsize, h_per_class, max_label,
+                             h_seeds, n_seeds);
+}
+
+int oift_fmax_gpu_run(const int *h_image, int *h_labels, int n, int xsize, int ysize, int zsize,
+                      const float *h_per_class, int max_label, const int *h_seeds, int n_seeds) {
+    std::lock_guard<std::mutex> lk(g_dropin_mu);
+    g_last_status = OIFT_E_BAD_ARG;
+    if (!h_image || !h_labels || !h_per_class || n <= 0 || max_label < 0) return -1;
+    if ((long long)xsize * ysize * zsize != n) return -1;
+    if (!g_dropin_ctx) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int rc = oift_b200_create(&g_dropin_ctx, dev);
+        if (rc != OIFT_OK) {
+            g_last_status = rc;
+            return -1;
+        }
+    }
+    oift_b200_params p{};
+    p.xsize = xsize;
+    p.ysize = ysize;
+    p.zsize = zsize;
+    p.adjacency = zsize == 1 ? 4 : 6;
+    p.weight_mode = OIFT_W_GRAD;
+    p.wq = OIFT_MAX_BASE;
+    p.per_class = h_per_class;
+    p.max_label = max_label;
+    p.relax_sweeps = 0;
+    oift_b200_stats st{};
+    int rc = oift_b200_run_host(g_dropin_ctx, &p, h_image, h_labels, h_seeds, n_seeds, nullptr,
+                                nullptr, 0, nullptr, &st);
+    g_last_status = rc;
+    return rc == OIFT_OK ? st.levels : -1;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// common.cuh -- shared definitions of the sm_100a OIFT + relaxation kernels.
+//
+// Layout in HBM (one volume, N = X*Y*Z voxels, p = x + y*X + z*X*Y as in
+// gft/include/gft_scene32.h:164-179):
+//   image     int16 or int32 [N]
+//   weights   uint16 [P][N]; plane k holds the edge {p, p + d_k} for the k-th "positive"
+//             neighbour offset of the gft Spheric order (gft/src/gft_adjrel3.cpp:47-85):
+//             6-adj: +x, +y, +z; 26-adj: the 13 offsets after the centre.  bits 0..13
+//             base weight, bit 14 = (I_p < I_q), bit 15 = (I_p > I_q).
+//   key       uint32 [N] OIFT state: cost << 17 | label << 1 | U  (U = 1 not yet
+//             expanded), 0xFFFFFFFF = unreached.  Integer order = (cost, label) order.
+//   membership float [C][N] planar relaxation state (two buffers).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/oift_b200.h"
+
+#define OIFT_KEY_INF 0xFFFFFFFFu
+#define OIFT_BASE_MASK 0x3FFFu
+#define OIFT_MAX_BASE 16383
+#define OIFT_MAX_COST 32766
+#define OIFT_MAX_LABEL 32767
+
+namespace oiftb {
+
+// Neighbour offsets in gft Spheric order without the centre.  Entry i and entry
+// n-1-i are opposite; the positive half is i >= n/2.
+struct Adjacency {
+    int n;
+    int dx[26], dy[26], dz[26];
+};
+
+inline Adjacency make_adjacency(int adj) {
+    Adjacency A;
+    int r2 = (adj == 26 || adj == 8) ? 3 : 1;
+    A.n = 0;
+    for (int z = -1; z <= 1; z++)
+        for (int y = -1; y <= 1; y++)
+            for (int x = -1; x <= 1; x++) {
+                if (x == 0 && y == 0 && z == 0) continue;
+                if (x * x + y * y + z * z <= r2) {
+                    A.dx[A.n] = x;
+                    A.dy[A.n] = y;
+                    A.dz[A.n] = z;
+                    A.n++;
+                }
+            }
+    return A;
+}
+
+__host__ __device__ inline uint32_t make_key(int cost, int label, int unexpanded) {
+    return ((uint32_t)cost << 17) | ((uint32_t)label << 1) | (uint32_t)unexpanded;
+}
+__host__ __device__ inline int key_cost(uint32_t k) { return (int)(k >> 17); }
+__host__ __device__ inline int key_label(uint32_t k) { return (int)((k >> 1) & 0xFFFFu); }
+
+// Oriented arc weight, gft/src/gft_ift.cpp:965-973: int w = |dI|; w *= (1 +/- per/100)
+// evaluated in double and truncated.  fgt = 1.0 + per/100.0, flt = 1.0 - per/100.0 are
+// computed once per label with the same double expression as the reference.
+__host__ __device__ inline int oriented_weight(uint32_t base, bool tail_gt, bool tail_lt,
+                                               double fgt, double flt) {
+    if (tail_gt) return (int)((double)base * fgt);
+    if (tail_lt) return (int)((double)base * flt);
+    return (int)base;
+}
+
+// Largest base b in [0, OIFT_MAX_BASE] with (int)(b * f) <= c; trunc(b*f) is monotone
+// in b for f >= 0, so "oriented weight <= c" is "base <= threshold".
+__host__ __device__ inline int max_base_for_cost(int c, double f) {
+    if (f <= 0.0) return OIFT_MAX_BASE;
+    double b = floor((double)(c + 1) / f);
+    int bi = b > (double)OIFT_MAX_BASE ? OIFT_MAX_BASE : (b < 0.0 ? 0 : (int)b);
+    while (bi > 0 && (int)((double)bi * f) > c) bi--;
+    while (bi < OIFT_MAX_BASE && (int)((double)(bi + 1) * f) <= c) bi++;
+    return bi;
+}
+
+}  // namespace oiftb
+
+// Kernel-side error codes written to a device flag (read by the host after a launch).
+#define OIFT_DEV_OK 0
+#define OIFT_DEV_TIMEOUT 1
+#define OIFT_DEV_QUEUE 2

@@ -1,0 +1,82 @@
+// kernels.cuh -- host-visible launch interfaces of the kernel translation units.
+#pragma once
+#include "common.cuh"
+
+namespace oiftb {
+
+struct BuildArgs {
+    int X, Y, Z;
+    int planes;
+    int mode, cap;
+    int dx[13], dy[13], dz[13];
+    const uint16_t *lut;
+    int lut_len;
+    const int32_t *grad;
+    float blend_a;
+    unsigned long long *clamped;
+};
+
+struct RelaxArgs {
+    int X, Y, Z;
+    size_t N;
+    int nadj;
+    int dx[26], dy[26], dz[26];
+    float dpq[26];
+    float Wmax;
+    float per;
+    int bg;
+    float pcm[8];
+};
+
+struct OiftGlobals {
+    unsigned int nextmin[2];
+    int outstanding[2];
+    unsigned long long qhead, qtail;
+    unsigned int bar_count, bar_gen;
+    int error;
+    int levels;
+    unsigned long long tile_steps;
+    unsigned long long pushes;
+};
+
+struct OiftPlan {
+    int TY, TZ, ntx, nty, ntz, ntiles;
+    unsigned int qcap;
+};
+
+// Scratch layout for one OIFT run (device pointers supplied by the caller).
+struct OiftScratch {
+    uint32_t *key;       // [N]
+    uint32_t *tpend;     // [ntiles]
+    uint32_t *inq;       // [ntiles]
+    uint32_t *queue;     // [qcap]
+    OiftGlobals *g;
+};
+
+template <typename T>
+cudaError_t launch_build_weights(const T *img, uint16_t *W, const BuildArgs &a, int sms,
+                                 cudaStream_t s);
+template <typename T>
+cudaError_t launch_minmax(const T *img, size_t n, int *mm, int sms, cudaStream_t s);
+template <typename T>
+cudaError_t launch_relax_sweep(int C, const float *in, float *out, const T *img,
+                               const uint8_t *seedc, const RelaxArgs &a, bool perclass,
+                               int sms, cudaStream_t s);
+
+__global__ void relax_init_kernel(const int32_t *label, size_t N, int C, const int *l2c,
+                                  int maxl, int bg, float *m);
+__global__ void relax_seed_kernel(const int32_t *seeds, int nseeds, const int32_t *label,
+                                  size_t N, const int *l2c, int maxl, int bg, uint8_t *seedc);
+__global__ void seed_presence_kernel(const int32_t *seed_labels, int nseeds, uint32_t *bits);
+__global__ void relax_argmax_kernel(const float *m, size_t N, int C, const int *classes,
+                                    int32_t *label, uint8_t *mask);
+
+OiftPlan oift_plan(int X, int Y, int Z);
+size_t oift_globals_bytes();
+int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
+             const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
+             const float *d_pol_table, int npol, float pol_default, int32_t *cost,
+             int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
+             long long *steps_out);
+
+}  // namespace oiftb

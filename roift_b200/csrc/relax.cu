@@ -1,0 +1,186 @@
+// relax.cu -- ROIFT fuzzy-membership relaxation sweeps (row a7) and argmax (row a10).
+//
+// Restates gft::ift::ORelax_1_Multi (gft/src/gft_ift.cpp:8655-8911) and
+// ORelax_1_Multi_PerClass (gft_ift.cpp:8913-9187) in FP32 with the reference's exact
+// operation order, so that memberships and labels are bit-identical to the CPU code:
+//   w      = |I_p - I_q|                                   (8798)
+//   per_pq = per * (2 p_bg(q) - 1)  or  sum_k per_k m_k(q)  (8800-8801, 9076-9079)
+//   w     *= 1 +/- per_pq / 100                            (8803-8806)
+//   w      = max(Wmax - w, 0)^8 / Dpq                      (8808-8815)
+//   m'(p)  = sum_q w m(q) / sum_q w   (m(p) kept if sum w == 0)   (8817-8832)
+//   seeds re-clamped one-hot after every sweep              (8839-8855)
+// Every multiply/add/divide is an explicit round-to-nearest intrinsic: no FMA
+// contraction, IEEE division, neighbours summed in the gft Spheric order.
+//
+// Dense update == masked update.  The reference updates only a "mask" that starts at
+// voxels with a differently-labelled neighbour and dilates by one ring per sweep.  A
+// voxel outside that mask at sweep t has only never-updated neighbours carrying its own
+// one-hot class, so the dense formula gives sum(w*1)/sum(w) = 1 and 0 elsewhere --
+// identical bits, provided sum(w) is finite (Wmax^8 * degree < FLT_MAX; the host
+// rejects larger Wmax with OIFT_E_RANGE, where the reference itself would produce
+// inf/inf = NaN).  So the sweep is a plain dense stencil with no mask state.
+#include "kernels.cuh"
+
+namespace oiftb {
+
+
+template <int C, typename T, bool PERCLASS>
+__global__ void __launch_bounds__(256) relax_sweep_kernel(const float *__restrict__ min_,
+                                                          float *__restrict__ mout,
+                                                          const T *__restrict__ img,
+                                                          const uint8_t *__restrict__ seedc,
+                                                          RelaxArgs a) {
+    const int X = a.X, Y = a.Y, Z = a.Z;
+    const size_t N = a.N, XY = (size_t)X * Y;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / XY);
+        const int ip = (int)img[p];
+        float acc[C];
+#pragma unroll
+        for (int k = 0; k < C; k++) acc[k] = 0.0f;
+        float sw = 0.0f;
+        for (int i = 0; i < a.nadj; i++) {
+            const int qx = x + a.dx[i], qy = y + a.dy[i], qz = z + a.dz[i];
+            if (qx < 0 || qx >= X || qy < 0 || qy >= Y || qz < 0 || qz >= Z) continue;
+            const size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * XY;
+            const int iq = (int)img[q];
+            float mq[C];
+#pragma unroll
+            for (int k = 0; k < C; k++) mq[k] = __ldg(&min_[(size_t)k * N + q]);
+            float w = fabsf((float)(ip - iq));
+            float per_pq;
+            if (PERCLASS) {
+                per_pq = 0.0f;
+#pragma unroll
+                for (int k = 0; k < C; k++) per_pq = __fadd_rn(per_pq, __fmul_rn(a.pcm[k], mq[k]));
+            } else {
+                float pbg = mq[0];
+#pragma unroll
+                for (int k = 1; k < C; k++)
+                    if (k == a.bg) pbg = mq[k];
+                per_pq = __fmul_rn(a.per, __fsub_rn(__fmul_rn(2.0f, pbg), 1.0f));
+            }
+            if (ip > iq)
+                w = __fmul_rn(w, __fadd_rn(1.0f, __fdiv_rn(per_pq, 100.0f)));
+            else if (ip < iq)
+                w = __fmul_rn(w, __fsub_rn(1.0f, __fdiv_rn(per_pq, 100.0f)));
+            w = __fsub_rn(a.Wmax, w);
+            if (w < 0.0f) w = 0.0f;
+            w = __fmul_rn(w, w);
+            w = __fmul_rn(w, w);
+            w = __fmul_rn(w, w);
+            if (a.dpq[i] != 1.0f) w = __fdiv_rn(w, a.dpq[i]);
+            sw = __fadd_rn(sw, w);
+#pragma unroll
+            for (int k = 0; k < C; k++) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, mq[k]));
+        }
+        float out[C];
+        if (sw > 0.0f) {
+#pragma unroll
+            for (int k = 0; k < C; k++) out[k] = __fdiv_rn(acc[k], sw);
+        } else {
+#pragma unroll
+            for (int k = 0; k < C; k++) out[k] = min_[(size_t)k * N + p];
+        }
+        const uint8_t sc = seedc[p];
+        if (sc != 0xFF) {
+#pragma unroll
+            for (int k = 0; k < C; k++) out[k] = (k == sc) ? 1.0f : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < C; k++) mout[(size_t)k * N + p] = out[k];
+    }
+}
+
+// One-hot initial membership from the OIFT labels (gft_ift.cpp:8745-8752).
+__global__ void relax_init_kernel(const int32_t *label, size_t N, int C, const int *l2c,
+                                  int maxl, int bg, float *m) {
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        int lb = label[p], c = bg;
+        if (lb >= 0 && lb <= maxl && l2c[lb] >= 0) c = l2c[lb];
+        for (int k = 0; k < C; k++) m[(size_t)k * N + p] = (k == c) ? 1.0f : 0.0f;
+    }
+}
+
+// Seed class map: 0xFF = not a seed, else the class of the seed's label.
+__global__ void relax_seed_kernel(const int32_t *seeds, int nseeds, const int32_t *label,
+                                  size_t N, const int *l2c, int maxl, int bg, uint8_t *seedc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nseeds) return;
+    int p = seeds[i];
+    if (p < 0 || (size_t)p >= N) return;
+    int lb = label[p], c = bg;
+    if (lb >= 0 && lb <= maxl && l2c[lb] >= 0) c = l2c[lb];
+    seedc[p] = (uint8_t)c;
+}
+
+// Labels present among the seeds (gft_ift.cpp:8684-8712): bitmap over label values.
+__global__ void seed_presence_kernel(const int32_t *seed_labels, int nseeds, uint32_t *bits) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nseeds) return;
+    int lb = seed_labels[i];
+    if (lb < 0) lb = 0;
+    if (lb > OIFT_MAX_LABEL) return;
+    atomicOr(&bits[lb >> 5], 1u << (lb & 31));
+}
+
+// Argmax with strict '>' so the lowest class wins ties (gft_ift.cpp:8889-8904).
+__global__ void relax_argmax_kernel(const float *m, size_t N, int C, const int *classes,
+                                    int32_t *label, uint8_t *mask) {
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        int best = 0;
+        float bv = m[p];
+        for (int k = 1; k < C; k++) {
+            float v = m[(size_t)k * N + p];
+            if (v > bv) {
+                bv = v;
+                best = k;
+            }
+        }
+        int lb = classes[best];
+        if (label) label[p] = lb;
+        if (mask) mask[p] = (uint8_t)(lb != 0);
+    }
+}
+
+template <int C, typename T>
+static cudaError_t launch_sweep_c(const float *in, float *out, const T *img,
+                                  const uint8_t *seedc, const RelaxArgs &a, bool perclass,
+                                  int sms, cudaStream_t s) {
+    int blocks = (int)((a.N + 255) / 256);
+    if (blocks > sms * 16) blocks = sms * 16;
+    if (perclass)
+        relax_sweep_kernel<C, T, true><<<blocks, 256, 0, s>>>(in, out, img, seedc, a);
+    else
+        relax_sweep_kernel<C, T, false><<<blocks, 256, 0, s>>>(in, out, img, seedc, a);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_relax_sweep(int C, const float *in, float *out, const T *img,
+                               const uint8_t *seedc, const RelaxArgs &a, bool perclass,
+                               int sms, cudaStream_t s) {
+    switch (C) {
+        case 1: return launch_sweep_c<1, T>(in, out, img, seedc, a, perclass, sms, s);
+        case 2: return launch_sweep_c<2, T>(in, out, img, seedc, a, perclass, sms, s);
+        case 3: return launch_sweep_c<3, T>(in, out, img, seedc, a, perclass, sms, s);
+        case 4: return launch_sweep_c<4, T>(in, out, img, seedc, a, perclass, sms, s);
+        case 5: return launch_sweep_c<5, T>(in, out, img, seedc, a, perclass, sms, s);
+        case 6: return launch_sweep_c<6, T>(in, out, img, seedc, a, perclass, sms, s);
+        case 7: return launch_sweep_c<7, T>(in, out, img, seedc, a, perclass, sms, s);
+        case 8: return launch_sweep_c<8, T>(in, out, img, seedc, a, perclass, sms, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template cudaError_t launch_relax_sweep<int16_t>(int, const float *, float *, const int16_t *,
+                                                 const uint8_t *, const RelaxArgs &, bool, int,
+                                                 cudaStream_t);
+template cudaError_t launch_relax_sweep<int32_t>(int, const float *, float *, const int32_t *,
+                                                 const uint8_t *, const RelaxArgs &, bool, int,
+                                                 cudaStream_t);
+
+}  // namespace oiftb

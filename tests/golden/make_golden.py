@@ -1,0 +1,65 @@
+"""Generate the golden fixtures of tests/golden/ from the reference gft library itself.
+
+The reference sources are compiled into oracle/_ref/libgft_ref.so (oracle/Makefile,
+target `ref`); this script runs the reference routines on small seeded inputs and stores
+inputs and outputs as .npz files.  The CPU test-suite checks the C restatement (the
+oracle) against these files, so parity stays pinned even where the reference tree is
+absent.  Run:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import oracle as O  # noqa: E402
+from roift_b200 import synth  # noqa: E402
+
+CASES = [
+    # name, shape (Z,Y,X), pol, adjacency, nlabels, per_class
+    ("g3d_a", (12, 14, 16), -0.3, 6, 1, None),
+    ("g3d_b", (10, 16, 20), 0.5, 6, 2, None),
+    ("g3d_alpha0", (12, 12, 18), 0.0, 6, 1, None),
+    ("g3d_26", (8, 10, 12), -0.5, 26, 2, None),
+    ("g2d_4", (1, 24, 32), 0.5, 4, 1, None),
+    ("g2d_8", (1, 20, 28), -0.2, 8, 2, None),
+    ("g3d_perclass", (10, 14, 18), 0.0, 6, 3, [-30.0, 20.0, 45.0, -10.0]),
+]
+SWEEPS = 6
+
+
+def make(name, shape, pol, adj, nl, per_class, seed):
+    c = synth.small_case(seed=seed, shape=shape, pol=pol, adjacency=adj, nlabels=nl,
+                         noise=120, contrast=400)
+    img = c.image.astype(np.int32)
+    img -= min(0, int(img.min()))
+    pc = None if per_class is None else np.array(per_class, np.float32)
+    lab_oift = O.ref_oift_multi(img, adj, c.seeds, c.seed_labels,
+                                pol=None if pc is not None else pol, per_class=pc)
+    lab_relax = O.ref_orelax_multi(img, adj, c.seeds, lab_oift, SWEEPS,
+                                   pol=None if pc is not None else pol, per_class=pc)
+    out = dict(image=img.reshape(shape), seeds=c.seeds, seed_labels=c.seed_labels,
+               adjacency=np.int32(adj), pol=np.float32(pol), sweeps=np.int32(SWEEPS),
+               per_class=pc if pc is not None else np.zeros(0, np.float32),
+               ref_oift_label=lab_oift, ref_relax_label=lab_relax,
+               ref_blur=O.ref_gaussian_blur(img))
+    if pol == 0.0 and pc is None:
+        cost, lab = O.ref_ift_fmax(img, adj, c.seeds, c.seed_labels)
+        out["ref_ift_fmax_cost"] = cost
+        out["ref_ift_fmax_label"] = lab
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
+def main():
+    O.build(with_ref=True)
+    for i, (name, shape, pol, adj, nl, pc) in enumerate(CASES):
+        make(name, shape, pol, adj, nl, pc, seed=100 + i)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()

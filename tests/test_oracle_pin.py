@@ -1,0 +1,102 @@
+"""CPU: the oracle (C restatement) pinned against the reference itself.
+
+Two anchors: the golden fixtures in tests/golden/ (produced by the reference library,
+tests/golden/make_golden.py), and -- where oracle/_ref/libgft_ref.so is present -- the
+live reference on fresh seeded inputs.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from roift_b200 import synth
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def _pol_args(d):
+    pc = d["per_class"]
+    if pc.size:
+        return dict(pol=None, per_class=pc)
+    return dict(pol=float(d["pol"]), per_class=None)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_oracle_matches_golden(oracle_lib, path):
+    d = np.load(path)
+    img = d["image"]
+    Z, Y, X = img.shape
+    adj = int(d["adjacency"])
+    seeds, sl = d["seeds"], d["seed_labels"]
+    pa = _pol_args(d)
+    W, ncl = O.build_weights(img, adj, "grad")
+    assert ncl == 0
+    # R1 (restated OIFT_Multi) reproduces the reference labels bit for bit
+    lab_r1, val, pred, fmax = O.oift_prim(W, (X, Y, Z), adj, seeds, sl, **pa)
+    assert np.array_equal(lab_r1, d["ref_oift_label"])
+    # R2 (lexicographic f_max): same cut energy as the reference segmentation, and the
+    # f_max derived along the reference forest equals the R2 cost map
+    cost, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), adj, seeds, sl, **pa)
+    nl = int(max(sl.max(), 0)) + 1
+    e_ref, elb_ref = O.energy(W, (X, Y, Z), adj, d["ref_oift_label"], nl, **pa)
+    e_r2, elb_r2 = O.energy(W, (X, Y, Z), adj, lab_r2, nl, **pa)
+    assert e_ref == e_r2
+    assert np.array_equal(fmax, cost)
+    if "ref_ift_fmax_cost" in d.files:
+        ns = np.ones(img.size, bool)
+        ns[seeds] = False
+        assert np.array_equal(d["ref_ift_fmax_cost"][ns] - 1, cost[ns])
+    # R3 FP32 relaxation reproduces ORelax_1_Multi labels
+    lab_rel, m32, nc = O.relax(img, adj, seeds, d["ref_oift_label"], int(d["sweeps"]), **pa)
+    assert np.array_equal(lab_rel, d["ref_relax_label"])
+    lab64, m64, _ = O.relax(img, adj, seeds, d["ref_oift_label"], int(d["sweeps"]), fp64=True, **pa)
+    assert np.abs(m32.astype(np.float64) - m64).max() < 1e-5
+    # blur restatement
+    assert np.array_equal(O.gaussian_blur(img), d["ref_blur"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("seed,shape,pol,adj,nl", [
+    (1, (14, 18, 22), -0.3, 6, 1), (2, (14, 18, 22), 0.4, 6, 2), (3, (8, 10, 14), 0.2, 26, 2),
+    (4, (1, 50, 60), 0.5, 4, 1), (5, (1, 40, 44), -0.4, 8, 3)])
+def test_oracle_matches_live_reference(oracle_lib, seed, shape, pol, adj, nl):
+    c = synth.small_case(seed=seed, shape=shape, pol=pol, adjacency=adj, nlabels=nl,
+                         noise=150, contrast=300)
+    img = c.image.astype(np.int32)
+    Z, Y, X = c.shape
+    W, _ = O.build_weights(img, adj, "grad")
+    lab_ref = O.ref_oift_multi(img, adj, c.seeds, c.seed_labels, pol=pol)
+    lab_r1, _, _, fmax = O.oift_prim(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=pol)
+    assert np.array_equal(lab_r1, lab_ref)
+    cost, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=pol)
+    e1, _ = O.energy(W, (X, Y, Z), adj, lab_ref, nl + 1, pol=pol)
+    e2, _ = O.energy(W, (X, Y, Z), adj, lab_r2, nl + 1, pol=pol)
+    assert e1 == e2
+    rel_ref = O.ref_orelax_multi(img, adj, c.seeds, lab_ref, 4, pol=pol)
+    rel, _, _ = O.relax(img, adj, c.seeds, lab_ref, 4, pol=pol)
+    assert np.array_equal(rel, rel_ref)
+
+
+def test_oracle_planted_mistake_is_caught(oracle_lib):
+    """A wrong polarity sign in the oracle input must change the labels or energy: the
+    checker is sensitive to the orientation it is meant to pin."""
+    c = synth.small_case(seed=9, shape=(12, 16, 20), pol=-0.5, nlabels=1, noise=150,
+                         contrast=300)
+    img = c.image.astype(np.int32)
+    Z, Y, X = c.shape
+    W, _ = O.build_weights(img, 6, "grad")
+    c1, l1, _ = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels, pol=-0.5)
+    c2, l2, _ = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels, pol=+0.5)
+    assert not np.array_equal(c1, c2)
+
+
+def test_weight_builder_modes(oracle_lib):
+    img = np.array([[[0, 10, 5000, 4990]]], np.int32)
+    W, ncl = O.build_weights(img, 6, "grad_q", wq=4095)
+    # plane +x: |0-10| with I_p < I_q, |10-5000| clamped, |5000-4990| with I_p > I_q
+    assert W[0] == (10 | 0x4000) and W[1] == (4095 | 0x4000) and W[2] == (10 | 0x8000)
+    assert ncl == 1
+    W, _ = O.build_weights(img, 6, "rbf_q", wq=4095, rbf_sigma=150.0)
+    assert (W[1] & 0x3FFF) == 4095 and (W[0] & 0x3FFF) == round(4095 * (1 - np.exp(-100 / 45000)))
