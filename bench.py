@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""bench.py -- OIFT + relaxation throughput of liboift_b200 on B200.
+
+Workload (one step): the 256^3 int16 ellipsoid volume (ellipsoid (90,70,60) at 1200 on
+200, bias 1+0.1 sin(2 pi x/256), noise sigma 80), 6-adjacency, uint16 [0,4095]
+gradient arc weights, polarity alpha = -0.3, seeds = sphere r=6 (object) + distance<=2
+boundary shell (background); arc-weight build + oriented f_max OIFT + 50 FP32
+relaxation sweeps + argmax labels/mask, inputs resident in HBM.
+
+Metric: Gvox/s = voxels / step time (whole job over all ranks: every rank processes
+its own volume, weak scaling, no data-path collective -- one volume does not shard).
+`e2e` is the same metric through the public host entry point oift_b200_run_host with
+pinned host buffers: H2D of the int32 image and seeds, D2H of the labels, every step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference's own CPU implementation (gft OIFT_Multi +
+ORelax_1_Multi compiled from the reference sources into oracle/_ref) on all host
+cores: P independent processes, each on a 160^3 sample of the same generator.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "OIFT+relax Gvox/s at 256^3 (exact cut energy) vs plain GPU & CPU; batched vol/s; HBM GB/s"
+UNIT = "Gvox/s"
+CPU_SAMPLE = 160  # edge of the bounded CPU sample (same generator, semi-axes scaled)
+
+
+def workload_case(size=256, seed=2, sweeps=50):
+    from roift_b200 import synth
+    return synth.ellipsoid3d(seed=seed, size=size, sweeps=sweeps)
+
+
+def workload_name(c):
+    Z, Y, X = c.shape
+    return (f"ellipsoid {X}x{Y}x{Z} int16, 6-adj, uint16 gradient weights [0,4095], "
+            f"alpha={c.pol}, OIFT f_max + {c.sweeps} FP32 relaxation sweeps + argmax")
+
+
+# ------------------------------------------------------------------ clocks ----
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"roift_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in open(self.path):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU baseline ----
+def _ref_worker_init(size):
+    global _REF_CASE
+    import oracle as O
+    c = workload_case(size=size, seed=2)
+    img = c.image.astype(np.int32)
+    img -= min(0, int(img.min()))  # the CLI's shift to >= 0 (oiftrelax.cpp:263-268)
+    _REF_CASE = (O, c, img)
+
+
+def _ref_worker_step(_):
+    O, c, img = _REF_CASE
+    t = time.perf_counter()
+    lab = O.ref_oift_multi(img, 6, c.seeds, c.seed_labels, pol=c.pol)
+    O.ref_orelax_multi(img, 6, c.seeds, lab, c.sweeps, pol=c.pol)
+    return time.perf_counter() - t, c.n
+
+
+def cpu_reference_throughput(procs: int, steps: int, warmup: int, size=CPU_SAMPLE):
+    """Reference CPU path on `procs` processes (one sample each); returns per-step Gvox/s."""
+    import multiprocessing as mp
+    import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    if kind != "reference":
+        raise RuntimeError("oracle/_ref/libgft_ref.so is missing (build with make -C oracle ref)")
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs, initializer=_ref_worker_init, initargs=(size,)) as pool:
+        vals = []
+        for i in range(warmup + steps):
+            t = time.perf_counter()
+            res = pool.map(_ref_worker_step, range(procs), chunksize=1)
+            dt = time.perf_counter() - t
+            vox = sum(r[1] for r in res)
+            if i >= warmup:
+                vals.append(vox / dt / 1e9)
+    return vals, kind
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    procs = max(1, min(cores, 32))
+    c = workload_case(size=CPU_SAMPLE)
+    try:
+        vals, kind = cpu_reference_throughput(procs, args.steps, args.warmup)
+    except Exception as e:  # pragma: no cover - only when the reference did not build
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return
+    v = statistics.mean(vals)
+    sample = (f"{procs} concurrent processes, each gft::ift::OIFT_Multi + ORelax_1_Multi "
+              f"({c.sweeps} sweeps) on a {CPU_SAMPLE}^3 sample of the workload generator")
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": procs * c.n / v / 1e6,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/fp32",
+           "data": "synthetic", "impl": "reference",
+           "config": {"workload": workload_name(workload_case(size=256)), "sample": sample},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": kind,
+                            "sample": sample},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------- our arm ----
+def read_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for ln in open(path):
+        parts = ln.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            return float(parts[2])
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    import roift_b200 as rb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+
+    c = workload_case(size=args.size, seed=2 + rank)
+    N = c.n
+    img_t = torch.from_numpy(c.image.copy()).to(dev)
+    s_t = torch.from_numpy(c.seeds).to(dev)
+    l_t = torch.from_numpy(c.seed_labels).to(dev)
+    lab_t = torch.empty(N, dtype=torch.int32, device=dev)
+    mask_t = torch.empty(N, dtype=torch.uint8, device=dev)
+    cost_t = torch.empty(N, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    ctx = rb.Context(local_rank)
+    prm = rb.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095, pol=c.pol,
+                         sweeps=c.sweeps)
+
+    def step():
+        return ctx.run_device(prm, img_t.data_ptr(), s_t.data_ptr(), l_t.data_ptr(),
+                              len(c.seeds), cost=cost_t.data_ptr(), label=lab_t.data_ptr(),
+                              mask=mask_t.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    torch.cuda.synchronize()
+    stats = []
+    for _ in range(args.steps):
+        flush.fill_(1)  # L2 flush between timed steps (outside the CUDA-event window)
+        torch.cuda.synchronize()
+        stats.append(step())
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    tot_ms = sum(s.ms_total for s in stats)
+    t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item()) / args.steps
+    value = world * N / (ms_step * 1e-3) / 1e9
+
+    # ---- end to end through the host entry point (pinned buffers) ----
+    e2e = None
+    if not args.no_e2e:
+        img32 = torch.from_numpy(c.image.astype(np.int32)).pin_memory()
+        lab_pin = torch.empty(N, dtype=torch.int32).pin_memory()
+        lab_init = torch.from_numpy(c.label_map())
+        img_np, lab_np = img32.numpy(), lab_pin.numpy()
+        prm_h = rb.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095, pol=c.pol,
+                               sweeps=c.sweeps)
+        lab_pin.copy_(lab_init)
+        ctx.run_host(prm_h, img_np, lab_np, c.seeds)  # warm the host path
+        times = []
+        for _ in range(max(3, args.steps // 2)):
+            lab_pin.copy_(lab_init)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.run_host(prm_h, img_np, lab_np, c.seeds)
+            times.append(time.perf_counter() - t0)
+        et = torch.tensor([statistics.mean(times)], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * N / float(et.item()) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * N + 8 * len(c.seeds), "d2h_bytes_per_step": 4 * N}
+
+    # ---- roofline of the dominant kernel (CUDA events on the launching stream) ----
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    C = stats[0].nclasses
+    ms_sweep = statistics.mean(s.ms_sweeps for s in stats) / c.sweeps
+    ms_oiftk = statistics.mean(s.ms_oift_kernel for s in stats)
+    relax_bytes = N * (8 * C + 2)        # per sweep launch: C planes in + out, int16 image
+    oift_bytes = N * 12                  # 6 B weights + 1 B seed/label + 4 B cost + 1 B label
+    if ms_sweep * c.sweeps >= ms_oiftk:
+        dom, bytes_, ms_k = "relax_sweep_kernel", relax_bytes, ms_sweep
+    else:
+        dom, bytes_, ms_k = "oift_persistent_kernel", oift_bytes, ms_oiftk
+    achieved = bytes_ / (ms_k * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "kernel": dom,
+                "algorithmic_bytes_per_launch": bytes_, "ms_per_launch": ms_k,
+                "traffic": read_traffic(dom, f"{args.size}^3")}
+    stages = {"ms_weights": statistics.mean(s.ms_weights for s in stats),
+              "ms_oift": statistics.mean(s.ms_oift for s in stats),
+              "ms_oift_kernel": ms_oiftk,
+              "ms_relax": statistics.mean(s.ms_relax for s in stats),
+              "ms_sweep": ms_sweep,
+              "oift_levels": stats[0].levels, "oift_tile_steps": stats[0].tile_steps,
+              "oift_gbs": oift_bytes / (ms_oiftk * 1e-3) / 1e9,
+              "relax_sweep_gbs": relax_bytes / (ms_sweep * 1e-3) / 1e9}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            vals, kind = cpu_reference_throughput(1, 1, 0)
+            cpu = {"value": vals[0], "unit": UNIT, "cores": 1, "kind": kind,
+                   "sample": f"gft OIFT_Multi + ORelax_1_Multi ({c.sweeps} sweeps), one "
+                             f"thread, {CPU_SAMPLE}^3 sample of the workload generator"}
+        except Exception as e:
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "int32/fp32", "data": "synthetic",
+               "config": {"workload": workload_name(c), "voxels_per_rank": N,
+                          "ranks": world, "parallelism": f"replicas{world}",
+                          "l2": "flushed between timed steps (256 MiB write)"},
+               "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+               "clocks": clocks, "gpu_launches": sum(s.kernels for s in stats),
+               "stages": stages}
+        print(json.dumps(out))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

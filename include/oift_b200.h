@@ -91,6 +91,9 @@ typedef struct {
     long long clamped;    /* edges clamped by a _Q builder */
     int nclasses;         /* relaxation classes */
     float ms_weights, ms_oift, ms_relax, ms_total; /* CUDA-event stage times */
+    int kernels;          /* kernel launches issued by the call */
+    float ms_oift_kernel; /* persistent OIFT kernel alone (CUDA events around the launch) */
+    float ms_sweeps;      /* the K relaxation sweep launches alone */
 } oift_b200_stats;
 
 /* Context: owns the device scratch for one device and one stream. */

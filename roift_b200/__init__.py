@@ -51,7 +51,8 @@ class Outputs(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("levels", C.c_int), ("tile_steps", C.c_longlong), ("clamped", C.c_longlong),
                 ("nclasses", C.c_int), ("ms_weights", C.c_float), ("ms_oift", C.c_float),
-                ("ms_relax", C.c_float), ("ms_total", C.c_float)]
+                ("ms_relax", C.c_float), ("ms_total", C.c_float), ("kernels", C.c_int),
+                ("ms_oift_kernel", C.c_float), ("ms_sweeps", C.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

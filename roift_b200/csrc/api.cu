@@ -280,7 +280,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     long long steps = 0;
     int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
                       (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
-                      c->sms, s, &levels, &steps);
+                      c->sms, s, &levels, &steps, c->ev[4], c->ev[5]);
     if (rc != OIFT_OK) return rc;
     unsigned long long hclamp = 0;
     CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));
@@ -364,11 +364,13 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
                                                                    (const int *)c->l2c.p, maxl, bg,
                                                                    (uint8_t *)c->seedc.p);
         float *cur = m0, *nxt = m1;
+        cudaEventRecord(c->ev[6], s);
         for (int it = 0; it < K; it++) {
             CU(launch_relax_sweep<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, ra,
                                      p->per_class != nullptr, c->sms, s));
             std::swap(cur, nxt);
         }
+        cudaEventRecord(c->ev[7], s);
         relax_argmax_kernel<<<blocks, 256, 0, s>>>(cur, N, nclasses, (const int *)c->classes.p,
                                                    out->label, out->mask);
         if (out->membership)
@@ -388,6 +390,12 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         cudaEventElapsedTime(&st->ms_oift, c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&st->ms_relax, c->ev[2], c->ev[3]);
         cudaEventElapsedTime(&st->ms_total, c->ev[0], c->ev[3]);
+        // minmax, build, seeds, persistent OIFT, finalize (+ presence, init, seed map,
+        // K sweeps, argmax when relaxing)
+        st->kernels = 5 + (want_relax ? 4 + K : 0);
+        cudaEventElapsedTime(&st->ms_oift_kernel, c->ev[4], c->ev[5]);
+        st->ms_sweeps = 0.0f;
+        if (want_relax) cudaEventElapsedTime(&st->ms_sweeps, c->ev[6], c->ev[7]);
     }
     return OIFT_OK;
 }

@@ -77,6 +77,6 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
-             long long *steps_out);
+             long long *steps_out, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr);
 
 }  // namespace oiftb

@@ -480,7 +480,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
-             long long *steps_out) {
+             long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
     size_t N = (size_t)X * Y * Z;
     cudaMemsetAsync(S.key, 0xFF, N * sizeof(uint32_t), st);
     cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
@@ -526,6 +526,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     size_t smem = oift_smem_bytes();
     void *args[] = {&A};
     cudaError_t err;
+    if (ev_begin) cudaEventRecord(ev_begin, st);
     if (P.TZ == 1) {
         auto kfn = oift_persistent_kernel<32, 1>;
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -538,6 +539,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
                                           smem, st);
     }
     if (err != cudaSuccess) return OIFT_E_CUDA;
+    if (ev_end) cudaEventRecord(ev_end, st);
     if (cost || label) {
         int blocks = (int)((N + 255) / 256);
         if (blocks > sms * 16) blocks = sms * 16;

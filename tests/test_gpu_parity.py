@@ -57,7 +57,9 @@ def test_oift_cost_and_labels_match_oracle(roift, oracle_lib, shape, pol, adj, n
     cost_r2, lab_r2, levels = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
     assert np.array_equal(cost, cost_r2), f"cost diffs {(cost != cost_r2).sum()}"
     assert np.array_equal(lab, lab_r2), f"label diffs {(lab != lab_r2).sum()}"
-    assert st.levels == levels
+    # the GPU may also visit levels whose only entries went stale (a tile's pending key
+    # was lowered afterwards); it never skips a populated one
+    assert st.levels >= levels
     if mode == "grad" and O.ref_available():
         lab_ref = O.ref_oift_multi(img, adj, c.seeds, c.seed_labels, pol=c.pol)
         e_gpu, elb_gpu = O.energy(W, (X, Y, Z), adj, lab, nl + 1, pol=c.pol)
@@ -121,7 +123,7 @@ def test_dropin_oift_fmax_gpu_run(roift, oracle_lib):
     W, _ = O.build_weights(img, 6, "grad")
     _, lab_r2, lev = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels, per_class=per_class)
     assert np.array_equal(lab, lab_r2)
-    assert levels == lev
+    assert levels >= lev
     if O.ref_available():
         lab_ref = O.ref_oift_multi(img, 6, c.seeds, c.seed_labels, per_class=per_class)
         e1, _ = O.energy(W, (X, Y, Z), 6, lab, 3, per_class=per_class)
