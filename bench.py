@@ -301,6 +301,9 @@ def main():
               "ms_relax": statistics.mean(s.ms_relax for s in stats),
               "ms_sweep": ms_sweep,
               "oift_levels": stats[0].levels, "oift_tile_steps": stats[0].tile_steps,
+              "oift_warp_cycles": list(stats[-1].oift_cycles),
+              "oift_tiles_stale_sparse_dense": list(stats[-1].oift_cycles)[7:10],
+              "oift_cycles_stage_sparse_dense": list(stats[-1].oift_cycles)[4:7],
               "oift_gbs": oift_bytes / (ms_oiftk * 1e-3) / 1e9,
               "relax_sweep_gbs": relax_bytes / (ms_sweep * 1e-3) / 1e9}
 

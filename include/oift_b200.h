@@ -94,6 +94,9 @@ typedef struct {
     int kernels;          /* kernel launches issued by the call */
     float ms_oift_kernel; /* persistent OIFT kernel alone (CUDA events around the launch) */
     float ms_sweeps;      /* the K relaxation sweep launches alone */
+    long long oift_cycles[10]; /* OIFT SM cycles summed over warps: level switch, owner
+                                  tiles, queued tiles, drain (incl. idle); per tile step:
+                                  staging, masks, flood, expansion, faces, pending */
 } oift_b200_stats;
 
 /* Context: owns the device scratch for one device and one stream. */
@@ -127,6 +130,9 @@ OIFT_API int oift_b200_build_weights_i16(oift_b200_ctx *ctx, const oift_b200_par
                                 const int16_t *image, uint16_t *weights /* [planes][N] */,
                                 long long *clamped);
 OIFT_API int oift_b200_weight_planes(int adjacency);
+/* Per-level profile of the last OIFT run: pairs (SM cycles, tile activations) for the
+ * first `cap` levels.  Returns the number of pairs written or a negative status. */
+OIFT_API int oift_b200_level_profile(oift_b200_ctx *ctx, unsigned int *cycles_steps, int cap);
 
 /* Reference-compatible drop-in (gpu/oift_fmax_gpu.cu:139-149).  Host pointers.
  * h_labels: in = labels (seed voxels carry their label, NIL elsewhere), out = OIFT

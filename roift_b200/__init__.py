@@ -52,16 +52,20 @@ class Stats(C.Structure):
     _fields_ = [("levels", C.c_int), ("tile_steps", C.c_longlong), ("clamped", C.c_longlong),
                 ("nclasses", C.c_int), ("ms_weights", C.c_float), ("ms_oift", C.c_float),
                 ("ms_relax", C.c_float), ("ms_total", C.c_float), ("kernels", C.c_int),
-                ("ms_oift_kernel", C.c_float), ("ms_sweeps", C.c_float)]
+                ("ms_oift_kernel", C.c_float), ("ms_sweeps", C.c_float),
+                ("oift_cycles", C.c_longlong * 10)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["oift_cycles"] = list(self.oift_cycles)
+        return d
 
 
 EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_set_stream", "oift_b200_status_string", "oift_b200_run_device_i16",
            "oift_b200_run_host", "oift_b200_build_weights_i16", "oift_b200_weight_planes",
-           "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status"]
+           "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status",
+           "oift_b200_level_profile"]
 
 _lib = None
 
@@ -85,6 +89,7 @@ def lib():
                                                C.POINTER(Outputs), C.POINTER(Stats)]
         L.oift_b200_run_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
                                          vp, vp, C.c_int, vp, C.POINTER(Stats)]
+        L.oift_b200_level_profile.argtypes = [vp, vp, C.c_int]
         L.oift_b200_build_weights_i16.argtypes = [vp, C.POINTER(Params), vp, vp,
                                                   C.POINTER(C.c_longlong)]
         L.oift_fmax_gpu_run.argtypes = [i32p, i32p, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -188,6 +193,14 @@ class Context:
         if memb is not None:
             memb = memb[: st.nclasses * N].reshape(st.nclasses, N)
         return lab, cost, memb, mask, st
+
+    def level_profile(self, cap=8192):
+        """(cycles, tile activations) per OIFT level of the last run."""
+        buf = np.zeros(2 * cap, np.uint32)
+        n = lib().oift_b200_level_profile(self._h, buf.ctypes.data_as(C.c_void_p), cap)
+        if n < 0:
+            raise OiftError(n, "oift_b200_level_profile")
+        return buf[: 2 * n].reshape(n, 2)
 
     def build_weights(self, params, image_ptr, weights_ptr) -> int:
         cl = C.c_longlong(0)

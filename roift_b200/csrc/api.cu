@@ -28,8 +28,9 @@ struct oift_b200_ctx {
     cudaEvent_t ev[8];
     // scratch (grow-only)
     DevBuf img32, img16, W, key, tpend, inq, queue, glob, flag, minmax, seeds, slabels, cost,
-        olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8;
+        olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8, ctaq, lprof;
     size_t total = 0;
+    unsigned long long oift_cycles[10] = {0};
 };
 
 static thread_local int g_last_status = OIFT_OK;
@@ -117,7 +118,7 @@ int oift_b200_destroy(oift_b200_ctx *c) {
     DevBuf *bufs[] = {&c->img32, &c->img16,  &c->W,      &c->key,     &c->tpend,   &c->inq,
                       &c->queue, &c->glob,   &c->flag,   &c->minmax,  &c->seeds,   &c->slabels,
                       &c->cost,  &c->olabel, &c->flabel, &c->memb,    &c->seedc,   &c->l2c,
-                      &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8};
+                      &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8, &c->ctaq};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -134,6 +135,16 @@ int oift_b200_set_stream(oift_b200_ctx *c, void *stream) {
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
     return OIFT_OK;
+}
+
+int oift_b200_level_profile(oift_b200_ctx *c, unsigned int *cycles_steps, int cap) {
+    if (!c || !cycles_steps || cap < 0) return OIFT_E_BAD_ARG;
+    if (!c->lprof.p) return 0;
+    int n = cap < 8192 ? cap : 8192;
+    if (cudaMemcpy(cycles_steps, c->lprof.p, (size_t)n * 2 * sizeof(unsigned int),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+        return OIFT_E_CUDA;
+    return n;
 }
 
 int oift_b200_weight_planes(int adjacency) {
@@ -204,8 +215,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
     TRY(grow(c, c->key, N * sizeof(uint32_t)));
     TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
-    TRY(grow(c, c->inq, (size_t)plan.ntiles * sizeof(uint32_t)));
-    TRY(grow(c, c->queue, (size_t)plan.qcap * sizeof(uint32_t)));
+    TRY(grow(c, c->queue, oift_mbox_bytes(plan, c->sms)));
     TRY(grow(c, c->glob, oift_globals_bytes()));
     TRY(grow(c, c->flag, 4 * sizeof(int)));
     TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
@@ -271,16 +281,18 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     OiftScratch S;
     S.key = (uint32_t *)c->key.p;
     S.tpend = (uint32_t *)c->tpend.p;
-    S.inq = (uint32_t *)c->inq.p;
-    S.queue = (uint32_t *)c->queue.p;
+    S.mbox = (unsigned long long *)c->queue.p;
     S.g = (OiftGlobals *)c->glob.p;
+    TRY(grow(c, c->lprof, 8192 * 2 * sizeof(unsigned int)));
+    S.lprof = (unsigned int *)c->lprof.p;
+    S.lprof_cap = 8192;
     int32_t *d_cost = out ? out->cost : nullptr;
     int32_t *d_olab = (out && out->oift_label) ? out->oift_label : (int32_t *)c->olabel.p;
     int levels = 0;
     long long steps = 0;
     int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
                       (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
-                      c->sms, s, &levels, &steps, c->ev[4], c->ev[5]);
+                      c->sms, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles);
     if (rc != OIFT_OK) return rc;
     unsigned long long hclamp = 0;
     CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));
@@ -295,8 +307,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         // classes = labels present among seeds, plus 0 (gft_ift.cpp:8684-8712)
         CU(cudaMemsetAsync(c->presence.p, 0, 1024 * sizeof(uint32_t), s));
         if (nseeds > 0)
-            seed_presence_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(d_slabels, nseeds,
-                                                                      (uint32_t *)c->presence.p);
+            seed_presence_kernel<<<std::min((nseeds + 255) / 256, c->sms * 4), 256, 0, s>>>(
+                d_slabels, nseeds, (uint32_t *)c->presence.p);
         std::vector<uint32_t> bits(1024);
         CU(cudaMemcpyAsync(bits.data(), c->presence.p, 1024 * sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, s));
@@ -395,6 +407,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         st->kernels = 5 + (want_relax ? 4 + K : 0);
         cudaEventElapsedTime(&st->ms_oift_kernel, c->ev[4], c->ev[5]);
         st->ms_sweeps = 0.0f;
+        for (int i = 0; i < 10; i++) st->oift_cycles[i] = (long long)c->oift_cycles[i];
         if (want_relax) cudaEventElapsedTime(&st->ms_sweeps, c->ev[6], c->ev[7]);
     }
     return OIFT_OK;

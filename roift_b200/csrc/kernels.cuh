@@ -28,16 +28,27 @@ struct RelaxArgs {
     float pcm[8];
 };
 
+// Hot scheduling counters of the persistent OIFT kernel, one 128-byte line each so
+// that polling one does not serialise atomics on another.
 struct OiftGlobals {
     unsigned int nextmin[2];
+    unsigned int pad0[30];
     int outstanding[2];
-    unsigned long long qhead, qtail;
-    unsigned int bar_count, bar_gen;
+    unsigned int pad1[30];
+    unsigned int bar_count;
+    unsigned int pad2[31];
+    unsigned int bar_gen;
+    unsigned int pad3[31];
     int error;
     int levels;
     unsigned long long tile_steps;
     unsigned long long pushes;
+    unsigned long long cycles[10];  // summed warp cycles: level sync, owner phase, queued
+                                    // tiles, drain; then per tile step: staging, masks, flood,
+                                    // expansion, faces, pending
+    unsigned int pad4[6];
 };
+
 
 struct OiftPlan {
     int TY, TZ, ntx, nty, ntz, ntiles;
@@ -46,11 +57,12 @@ struct OiftPlan {
 
 // Scratch layout for one OIFT run (device pointers supplied by the caller).
 struct OiftScratch {
-    uint32_t *key;       // [N]
-    uint32_t *tpend;     // [ntiles]
-    uint32_t *inq;       // [ntiles]
-    uint32_t *queue;     // [qcap]
+    uint32_t *key;                // [N]
+    uint32_t *tpend;              // [ntiles]
+    unsigned long long *mbox;     // [warps][words] re-activation bitmasks
     OiftGlobals *g;
+    unsigned int *lprof = nullptr;  // optional per-level profile [cap][2]
+    int lprof_cap = 0;
 };
 
 template <typename T>
@@ -73,10 +85,14 @@ __global__ void relax_argmax_kernel(const float *m, size_t N, int C, const int *
 
 OiftPlan oift_plan(int X, int Y, int Z);
 size_t oift_globals_bytes();
+int oift_mbox_words(const OiftPlan &P, int ctas);
+size_t oift_mbox_bytes(const OiftPlan &P, int ctas);
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
-             long long *steps_out, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr);
+             long long *steps_out, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr,
+             unsigned long long *cycles_out = nullptr);
+constexpr int OIFT_WARPS_PER_CTA = 16;
 
 }  // namespace oiftb

@@ -37,9 +37,11 @@ struct OiftArgs {
     uint32_t *key;
     const uint16_t *W;
     uint32_t *tpend;
-    uint32_t *inq;
-    uint32_t *queue;
-    unsigned int qmask;
+    unsigned long long *mbox;  // [nwarps][mbox_words] re-activation bitmasks
+    unsigned int *lprof;       // [lprof_cap][2]: per-level SM cycles and tile steps
+    int lprof_cap;
+    int mbox_words;
+    int nwarps;
     int X, Y, Z;
     size_t N;
     int ntx, nty, ntz, ntiles;
@@ -52,7 +54,8 @@ struct OiftArgs {
 };
 
 constexpr int OIFT_WARPS = 16;
-constexpr uint32_t QEMPTY = 0xFFFFFFFFu;
+constexpr int OIFT_SPARSE_MAX = 64;   // level voxels in a tile up to which it runs sparse
+constexpr int OIFT_WORKLIST = 256;    // per-warp voxel worklist of the sparse mode
 
 __device__ __forceinline__ unsigned int vload(const volatile unsigned int *p) { return *p; }
 __device__ __forceinline__ int vload(const volatile int *p) { return *p; }
@@ -103,14 +106,10 @@ __device__ __forceinline__ bool arc_ok(uint32_t code, bool tail_low, int c, int 
     return (int)base <= thr;
 }
 
-__device__ __forceinline__ void enqueue_tile(const OiftArgs &A, int par, int t) {
-    if (atomicExch(&A.inq[t], 1u) == 0u) {
-        atomicAdd(&A.g->outstanding[par], 1);
-        __threadfence();  // key updates that caused the queueing are visible first
-        unsigned long long slot = atomicAdd(&A.g->qtail, 1ULL);
-        atomicExch(&A.queue[slot & A.qmask], (uint32_t)t);
-    }
-}
+// Re-activating a tile at the current level: tile t is owned by warp t % nwarps; each warp
+// has a bitmask mailbox (bit t / nwarps).  The producer raises the level's outstanding
+// count, then sets the bit; if the bit was already set the tile is already pending and
+// the count is given back.  The owner warp takes all its bits with one exchange.
 
 template <int TY, int TZ>
 __device__ __forceinline__ int tile_of(const OiftArgs &A, int x, int y, int z) {
@@ -121,7 +120,9 @@ __device__ __forceinline__ int tile_of(const OiftArgs &A, int x, int y, int z) {
 template <int TY, int TZ>
 __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
                              double fgt, double flt, int bgt, int blt, uint32_t *skey,
-                             uint16_t *sw, uint32_t &next_min) {
+                             uint16_t *sw, uint16_t *shx, uint16_t *shy, uint16_t *shz,
+                             uint32_t *wl, int *wcount, uint32_t *rmask, long long *cyc) {
+    long long tc0 = clock64();
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int X = A.X, Y = A.Y, Z = A.Z;
@@ -132,24 +133,269 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
     const bool has_z = (Z > 1);
 
     uint32_t myF = 0, myOpen = 0, cpx = 0, cmx = 0, cpy = 0, cmy = 0, cpz = 0, cmz = 0;
-    // ---- pass 1: rows -> shared memory, level masks (ballots) ----
+    const uint32_t kexp = kk - 1u;
+    const uint32_t lab_bits = ((uint32_t)l << 1) | 1u;
+    auto arc_key = [&](uint32_t code, bool tail_low) -> uint32_t {
+        const bool hi = (code >> 15) & 1, lo = (code >> 14) & 1;
+        const int w = oriented_weight(code & OIFT_BASE_MASK, tail_low ? hi : lo,
+                                      tail_low ? lo : hi, fgt, flt);
+        const int nc = w > c ? w : c;
+        return ((uint32_t)nc << 17) | lab_bits;
+    };
+    // A successful out-of-tile push either continues this level next door (the
+    // face-neighbour tile is marked for re-activation; all marks of the tile step are
+    // published together by flush_reactivations) or lowers the neighbour's pending key.
+    auto settle = [&](uint32_t nk, uint32_t old, int qx, int qy, int qz) {
+        if (nk < old) {
+            if (nk == kk) {
+                const int face = qx < x0 ? 0 : qx >= x0 + 32 ? 1 : qy < y0 ? 2 : qy >= y0 + TY ? 3
+                                 : qz < z0 ? 4 : 5;
+                atomicOr(rmask, 1u << face);
+            } else {
+                atomicMin(&A.tpend[tile_of<TY, TZ>(A, qx, qy, qz)], nk);
+            }
+        }
+    };
+    auto flush_reactivations = [&]() {
+        __syncwarp();
+        const uint32_t m = *(volatile uint32_t *)rmask;
+        if (m == 0u) return;
+        __threadfence();  // every lane's key updates precede the mailbox bits
+        __syncwarp();
+        if (lane == 0) {
+            atomicAdd(&A.g->outstanding[par], __popc(m));
+            __threadfence();
+            *rmask = 0u;
+        }
+        __syncwarp();
+        bool dup = false;
+        if (lane < 6 && ((m >> lane) & 1u)) {
+            const int nt = tx + (lane == 0 ? -1 : lane == 1 ? 1 : 0);
+            const int ny = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
+            const int nz = tz + (lane == 4 ? -1 : lane == 5 ? 1 : 0);
+            const int tq = nt + ny * A.ntx + nz * A.ntx * A.nty;
+            const int w = tq % A.nwarps, j = tq / A.nwarps;
+            const unsigned long long bit = 1ull << (j & 63);
+            const unsigned long long old =
+                atomicOr(&A.mbox[(size_t)w * A.mbox_words + (j >> 6)], bit);
+            dup = (old & bit) != 0ull;
+        }
+        const uint32_t dups = __ballot_sync(FULL, dup);
+        if (lane == 0 && dups) atomicSub(&A.g->outstanding[par], __popc(dups));
+    };
+    auto pending = [&]() {
+        uint32_t m = OIFT_KEY_INF;
+#pragma unroll 8
+        for (int r = 0; r < 32; r++) {
+            uint32_t v = skey[r * 32 + lane];
+            if (v > kk && v < m) m = v;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            uint32_t v = __shfl_xor_sync(FULL, m, o);
+            m = v < m ? v : m;
+        }
+        if (lane == 0 && m != OIFT_KEY_INF) atomicMin(&A.tpend[t], m);
+    };
+    // ---- stage the keys of the tile in shared memory ----
+    const bool full = (x0 + 32 <= X) && (y0 + TY <= Y) && (z0 + TZ <= Z) && ((X & 7) == 0);
+    if (full) {
+        uint4 kv[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const int j = lane + 32 * m, r = j >> 3, col = j & 7;
+            const size_t p0 = (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
+            kv[m] = __ldcg(reinterpret_cast<const uint4 *>(A.key + p0) + col);
+        }
+#pragma unroll
+        for (int m = 0; m < 8; m++) reinterpret_cast<uint4 *>(skey)[lane + 32 * m] = kv[m];
+    } else {
+#pragma unroll 4
+        for (int r = 0; r < 32; r++) {
+            const int y = y0 + (r % TY), z = z0 + (r / TY);
+            const bool valid = (x < X) && (y < Y) && (z < Z);
+            skey[r * 32 + lane] =
+                valid ? __ldcg(&A.key[(size_t)x + (size_t)y * X + (size_t)z * XY]) : 0u;
+        }
+    }
+    // ---- stage the edge codes of the tile and of its -x/-y/-z halo faces ----
+    {
+        const int yr = y0 + (lane % TY), zr = z0 + (lane / TY);
+        uint16_t hx = 0, hy[TZ], hz[TY];
+        if (x0 > 0 && yr < Y && zr < Z)
+            hx = __ldg(&A.W[(size_t)(x0 - 1) + (size_t)yr * X + (size_t)zr * XY]);
+#pragma unroll
+        for (int zl = 0; zl < TZ; zl++)
+            hy[zl] = (y0 > 0 && x < X && z0 + zl < Z)
+                ? __ldg(&A.W[N + (size_t)x + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY]) : 0;
+#pragma unroll
+        for (int yl = 0; yl < TY; yl++)
+            hz[yl] = (TZ > 1 && has_z && z0 > 0 && x < X && y0 + yl < Y)
+                ? __ldg(&A.W[2 * N + (size_t)x + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY]) : 0;
+        if (full) {
+            uint4 cv[12];
+#pragma unroll
+            for (int m = 0; m < 12; m++) {
+                const int j = lane + 32 * m, pl = j >> 7, r = (j >> 2) & 31, col = j & 3;
+                const size_t p0 =
+                    (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
+                if (pl < 2 || has_z)
+                    cv[m] = __ldg(reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
+                else
+                    cv[m] = make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int m = 0; m < 12; m++) reinterpret_cast<uint4 *>(sw)[lane + 32 * m] = cv[m];
+        } else {
+            for (int r = 0; r < 32; r++) {
+                const int y = y0 + (r % TY), z = z0 + (r / TY);
+                const bool valid = (x < X) && (y < Y) && (z < Z);
+                const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+                sw[r * 32 + lane] = valid ? __ldg(&A.W[p]) : 0;
+                sw[1024 + r * 32 + lane] = valid ? __ldg(&A.W[N + p]) : 0;
+                sw[2048 + r * 32 + lane] = (valid && has_z) ? __ldg(&A.W[2 * N + p]) : 0;
+            }
+        }
+        shx[lane] = hx;
+#pragma unroll
+        for (int zl = 0; zl < TZ; zl++) shy[zl * 32 + lane] = hy[zl];
+        if (TZ > 1) {
+#pragma unroll
+            for (int yl = 0; yl < TY; yl++) shz[yl * 32 + lane] = hz[yl];
+        }
+    }
+    __syncwarp();
+    // ---- how many voxels of the tile sit at this level? ----
+    int nf0 = 0;
+#pragma unroll 8
+    for (int r = 0; r < 32; r++) nf0 += (skey[r * 32 + lane] == kk);
+    for (int o = 16; o > 0; o >>= 1) nf0 += __shfl_xor_sync(FULL, nf0, o);
+    const long long tcount = clock64();
+    cyc[0] += tcount - tc0;
+    if (nf0 == 0) {  // stale activation: only the pending key is refreshed
+        pending();
+        cyc[3] += 1;
+        return;
+    }
+    bool dense = nf0 > OIFT_SPARSE_MAX;
+    if (!dense) {
+        // ---- sparse mode: flood and expand from a voxel worklist ----
+        if (lane == 0) *wcount = 0;
+        __syncwarp();
+        for (int r = 0; r < 32; r++) {
+            const bool isf = skey[r * 32 + lane] == kk;
+            const uint32_t b = __ballot_sync(FULL, isf);
+            if (!b) continue;
+            int base = 0;
+            if (lane == 0) base = atomicAdd(wcount, __popc(b));
+            base = __shfl_sync(FULL, base, 0);
+            if (isf) wl[base + __popc(b & ((1u << lane) - 1u))] = (uint32_t)(r << 5 | lane);
+        }
+        int done = 0;
+        for (;;) {
+            __syncwarp();
+            const int cnt = *(volatile int *)wcount;
+            if (cnt > OIFT_WORKLIST) {  // overflow: the dense path finishes the level
+                dense = true;
+                break;
+            }
+            if (done >= cnt) break;
+            const int idx = done + lane;
+            if (idx < cnt) {
+                const uint32_t li = wl[idx];
+                const int r = (int)(li >> 5), xl = (int)(li & 31);
+                const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
+                const size_t p = (size_t)xg + (size_t)y * X + (size_t)z * XY;
+                const uint32_t cxp = sw[r * 32 + xl];
+                const uint32_t cxm = xl > 0 ? sw[r * 32 + xl - 1] : shx[r];
+                const uint32_t cyp = sw[1024 + r * 32 + xl];
+                const uint32_t cym = (r % TY) > 0 ? sw[1024 + (r - 1) * 32 + xl]
+                                                  : shy[(r / TY) * 32 + xl];
+                const uint32_t czp = sw[2048 + r * 32 + xl];
+                const uint32_t czm = r >= TY ? sw[2048 + (r - TY) * 32 + xl]
+                                             : (TZ > 1 ? shz[(r % TY) * 32 + xl] : 0u);
+                A.key[p] = kexp;
+                skey[li] = kexp;
+                uint32_t onk[6], oold[6];
+                int oq[6];
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    onk[d] = OIFT_KEY_INF;
+                    oold[d] = 0;
+                    oq[d] = -1;
+                    int qx = xg, qy = y, qz = z, rq = r, xq = xl;
+                    uint32_t code;
+                    bool tail_low, ok, in_tile;
+                    if (d == 0) {  // -z
+                        ok = has_z && z > 0; qz = z - 1; rq = r - TY; in_tile = r >= TY;
+                        code = czm; tail_low = false;
+                    } else if (d == 1) {  // -y
+                        ok = y > 0; qy = y - 1; rq = r - 1; in_tile = (r % TY) > 0;
+                        code = cym; tail_low = false;
+                    } else if (d == 2) {  // -x
+                        ok = xg > 0; qx = xg - 1; xq = xl - 1; in_tile = xl > 0;
+                        code = cxm; tail_low = false;
+                    } else if (d == 3) {  // +x
+                        ok = xg + 1 < X; qx = xg + 1; xq = xl + 1; in_tile = xl < 31;
+                        code = cxp; tail_low = true;
+                    } else if (d == 4) {  // +y
+                        ok = y + 1 < Y; qy = y + 1; rq = r + 1; in_tile = (r % TY) < TY - 1;
+                        code = cyp; tail_low = true;
+                    } else {  // +z
+                        ok = has_z && z + 1 < Z; qz = z + 1; rq = r + TY; in_tile = r + TY < 32;
+                        code = czp; tail_low = true;
+                    }
+                    if (!ok) continue;
+                    const size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * XY;
+                    if (in_tile) {
+                        const int lq = rq * 32 + xq;
+                        const uint32_t sk = *(volatile uint32_t *)&skey[lq];
+                        if (sk <= kk) continue;  // already at this level or expanded
+                        if (arc_ok(code, tail_low, c, bgt, blt)) {
+                            const uint32_t old = atomicMin(&skey[lq], kk);
+                            if (old > kk) {
+                                const int pos = atomicAdd(wcount, 1);
+                                if (pos < OIFT_WORKLIST) wl[pos] = (uint32_t)lq;
+                            }
+                        } else {
+                            const uint32_t nk = arc_key(code, tail_low);
+                            const uint32_t old = atomicMin(&skey[lq], nk);
+                            if (nk < old) atomicMin(&A.key[q], nk);
+                        }
+                    } else {
+                        onk[d] = arc_key(code, tail_low);
+                        oold[d] = atomicMin(&A.key[q], onk[d]);
+                        oq[d] = d;
+                    }
+                }
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    if (oq[d] < 0) continue;
+                    const int qx = xg + (d == 2 ? -1 : d == 3 ? 1 : 0);
+                    const int qy = y + (d == 1 ? -1 : d == 4 ? 1 : 0);
+                    const int qz = z + (d == 0 ? -1 : d == 5 ? 1 : 0);
+                    settle(onk[d], oold[d], qx, qy, qz);
+                }
+            }
+            done = (done + 32 < cnt) ? done + 32 : cnt;
+        }
+        __syncwarp();
+        if (!dense) {
+            flush_reactivations();
+            pending();
+            cyc[1] += clock64() - tcount;
+            cyc[4] += 1;
+            return;
+        }
+    }
+    // ---- level masks (one ballot per row and arc family) ----
 #pragma unroll 4
     for (int r = 0; r < 32; r++) {
         const int y = y0 + (r % TY), z = z0 + (r / TY);
         const bool valid = (x < X) && (y < Y) && (z < Z);
-        const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
-        uint32_t k = 0;
-        uint32_t cx = 0, cy = 0, cz = 0;
-        if (valid) {
-            k = __ldcg(&A.key[p]);
-            cx = __ldg(&A.W[p]);
-            cy = __ldg(&A.W[N + p]);
-            if (has_z) cz = __ldg(&A.W[2 * N + p]);
-        }
-        skey[r * 32 + lane] = k;
-        sw[r * 32 + lane] = (uint16_t)cx;
-        sw[1024 + r * 32 + lane] = (uint16_t)cy;
-        sw[2048 + r * 32 + lane] = (uint16_t)cz;
+        const uint32_t k = skey[r * 32 + lane];
+        const uint32_t cx = sw[r * 32 + lane];
+        const uint32_t cy = sw[1024 + r * 32 + lane];
+        const uint32_t cz = sw[2048 + r * 32 + lane];
         const uint32_t bF = __ballot_sync(FULL, valid && k == kk);
         const uint32_t bO = __ballot_sync(FULL, valid && k > kk);
         const uint32_t cxm1 = __shfl_up_sync(FULL, cx, 1);
@@ -187,112 +433,125 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         F = nF;
     }
     __syncwarp();
-    // ---- pass 2: expand every voxel conquered at this level ----
-    const uint32_t kexp = kk - 1u;
-    const int lo_shift = 17;
+    // ---- pass 2a: expand the voxels conquered at this level; in-tile targets ----
+    // In-tile tentative keys go to shared memory and to global memory as fire-and-forget
+    // reductions (no return value is awaited).
     for (int r = 0; r < 32; r++) {
         const uint32_t ne = __shfl_sync(FULL, F, r);
         if (ne == 0u) continue;
-        const int y = y0 + (r % TY), z = z0 + (r / TY);
         if ((ne >> lane) & 1u) {
+            const int y = y0 + (r % TY), z = z0 + (r / TY);
             const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
             A.key[p] = kexp;
             skey[r * 32 + lane] = kexp;
-            // six neighbours: -z,-y,-x,+x,+y,+z
 #pragma unroll
             for (int d = 0; d < 6; d++) {
-                int qx = x, qy = y, qz = z;
+                int rq = r, xq = lane;
                 uint32_t code;
                 bool tail_low;
-                bool in_tile;
-                int rq = r, xq = lane;
+                long long off;
                 if (d == 0) {  // -z
-                    if (!has_z || z == 0) continue;
-                    qz = z - 1;
-                    tail_low = false;
-                    in_tile = (r >= TY);
-                    rq = r - TY;
-                    code = in_tile ? sw[2048 + rq * 32 + lane] : __ldg(&A.W[2 * N + p - XY]);
+                    if (!(r >= TY)) continue;
+                    rq = r - TY; code = sw[2048 + rq * 32 + lane]; tail_low = false; off = -(long long)XY;
                 } else if (d == 1) {  // -y
-                    if (y == 0) continue;
-                    qy = y - 1;
-                    tail_low = false;
-                    in_tile = (r % TY) > 0;
-                    rq = r - 1;
-                    code = in_tile ? sw[1024 + rq * 32 + lane] : __ldg(&A.W[N + p - X]);
+                    if (!((r % TY) > 0)) continue;
+                    rq = r - 1; code = sw[1024 + rq * 32 + lane]; tail_low = false; off = -(long long)X;
                 } else if (d == 2) {  // -x
-                    if (x == 0) continue;
-                    qx = x - 1;
-                    tail_low = false;
-                    in_tile = lane > 0;
-                    xq = lane - 1;
-                    code = in_tile ? sw[r * 32 + lane - 1] : __ldg(&A.W[p - 1]);
+                    if (lane == 0) continue;
+                    xq = lane - 1; code = sw[r * 32 + lane - 1]; tail_low = false; off = -1;
                 } else if (d == 3) {  // +x
-                    if (x + 1 >= X) continue;
-                    qx = x + 1;
-                    tail_low = true;
-                    in_tile = lane < 31;
-                    xq = lane + 1;
-                    code = sw[r * 32 + lane];
+                    if (lane == 31 || x + 1 >= X) continue;
+                    xq = lane + 1; code = sw[r * 32 + lane]; tail_low = true; off = 1;
                 } else if (d == 4) {  // +y
-                    if (y + 1 >= Y) continue;
-                    qy = y + 1;
-                    tail_low = true;
-                    in_tile = (r % TY) < TY - 1;
-                    rq = r + 1;
-                    code = sw[1024 + r * 32 + lane];
+                    if (!((r % TY) < TY - 1) || y + 1 >= Y) continue;
+                    rq = r + 1; code = sw[1024 + r * 32 + lane]; tail_low = true; off = X;
                 } else {  // +z
-                    if (!has_z || z + 1 >= Z) continue;
-                    qz = z + 1;
-                    tail_low = true;
-                    in_tile = (r + TY) < 32;
-                    rq = r + TY;
-                    code = sw[2048 + r * 32 + lane];
+                    if (!((r + TY) < 32) || z + 1 >= Z) continue;
+                    rq = r + TY; code = sw[2048 + r * 32 + lane]; tail_low = true; off = (long long)XY;
                 }
-                const bool hi = (code >> 15) & 1, lo = (code >> 14) & 1;
-                const int w = oriented_weight(code & OIFT_BASE_MASK, tail_low ? hi : lo,
-                                              tail_low ? lo : hi, fgt, flt);
-                const int nc = w > c ? w : c;
-                const uint32_t nk = ((uint32_t)nc << lo_shift) | ((uint32_t)l << 1) | 1u;
-                const size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * XY;
-                if (in_tile) {
-                    uint32_t sk = skey[rq * 32 + xq];
-                    if (nk < sk) {
-                        atomicMin(&skey[rq * 32 + xq], nk);
-                        atomicMin(&A.key[q], nk);
-                    }
-                } else {
-                    uint32_t gk = __ldcg(&A.key[q]);
-                    if (nk < gk) {
-                        uint32_t old = atomicMin(&A.key[q], nk);
-                        if (nk < old) {
-                            int tq = tile_of<TY, TZ>(A, qx, qy, qz);
-                            if (nk == kk) {
-                                enqueue_tile(A, par, tq);
-                            } else {
-                                atomicMin(&A.tpend[tq], nk);
-                                next_min = nk < next_min ? nk : next_min;
-                            }
-                        }
-                    }
+                const uint32_t nk = arc_key(code, tail_low);
+                if (nk < skey[rq * 32 + xq]) {
+                    atomicMin(&skey[rq * 32 + xq], nk);
+                    atomicMin(&A.key[(size_t)((long long)p + off)], nk);
                 }
             }
         }
     }
+    // ---- pass 2b: out-of-tile targets, face by face; the atomics of a face are all
+    // issued before their results are examined ----
+    {   // -x / +x faces: lane = row
+        const int y = y0 + (lane % TY), z = z0 + (lane / TY);
+        const size_t prow = (size_t)y * X + (size_t)z * XY;
+        const bool mx = (F & 1u) && x0 > 0;
+        const bool px = ((F >> 31) & 1u) && x0 + 32 < X;
+        uint32_t nkm = OIFT_KEY_INF, nkp = OIFT_KEY_INF, om = 0, op = 0;
+        if (mx) {
+            nkm = arc_key(shx[lane], false);
+            om = atomicMin(&A.key[prow + x0 - 1], nkm);
+        }
+        if (px) {
+            nkp = arc_key(sw[lane * 32 + 31], true);
+            op = atomicMin(&A.key[prow + x0 + 32], nkp);
+        }
+        if (mx) settle(nkm, om, x0 - 1, y, z);
+        if (px) settle(nkp, op, x0 + 32, y, z);
+    }
+    {   // -y / +y faces: rows r % TY == 0 and TY - 1, lane = x
+        uint32_t nk[2 * TZ], old[2 * TZ];
+#pragma unroll
+        for (int i = 0; i < 2 * TZ; i++) {
+            const int zl = i >> 1, up = i & 1;
+            const int r = zl * TY + (up ? TY - 1 : 0);
+            const int y = y0 + (up ? TY - 1 : 0), z = z0 + zl;
+            const bool on = ((__shfl_sync(FULL, F, r) >> lane) & 1u) &&
+                            (up ? (y + 1 < Y) : (y0 > 0));
+            nk[i] = OIFT_KEY_INF;
+            old[i] = 0;
+            if (on) {
+                const size_t q = (size_t)x + (size_t)(up ? y + 1 : y - 1) * X + (size_t)z * XY;
+                nk[i] = up ? arc_key(sw[1024 + r * 32 + lane], true)
+                           : arc_key(shy[zl * 32 + lane], false);
+                old[i] = atomicMin(&A.key[q], nk[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 2 * TZ; i++) {
+            const int zl = i >> 1, up = i & 1;
+            if (nk[i] != OIFT_KEY_INF)
+                settle(nk[i], old[i], x, up ? y0 + TY : y0 - 1, z0 + zl);
+        }
+    }
+    if (TZ > 1 && has_z) {   // -z / +z faces: rows r < TY and r >= 32 - TY, lane = x
+        uint32_t nk[2 * TY], old[2 * TY];
+#pragma unroll
+        for (int i = 0; i < 2 * TY; i++) {
+            const int yl = i >> 1, up = i & 1;
+            const int r = up ? (32 - TY + yl) : yl;
+            const int y = y0 + yl, z = up ? z0 + TZ - 1 : z0;
+            const bool on = ((__shfl_sync(FULL, F, r) >> lane) & 1u) &&
+                            (up ? (z + 1 < Z) : (z0 > 0));
+            nk[i] = OIFT_KEY_INF;
+            old[i] = 0;
+            if (on) {
+                const size_t q = (size_t)x + (size_t)y * X + (size_t)(up ? z + 1 : z - 1) * XY;
+                nk[i] = up ? arc_key(sw[2048 + r * 32 + lane], true)
+                           : arc_key(shz[yl * 32 + lane], false);
+                old[i] = atomicMin(&A.key[q], nk[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 2 * TY; i++) {
+            const int yl = i >> 1, up = i & 1;
+            if (nk[i] != OIFT_KEY_INF)
+                settle(nk[i], old[i], x, y0 + yl, up ? z0 + TZ : z0 - 1);
+        }
+    }
     __syncwarp();
-    // ---- pass 3: pending key of this tile ----
-    uint32_t m = OIFT_KEY_INF;
-#pragma unroll 8
-    for (int r = 0; r < 32; r++) {
-        uint32_t v = skey[r * 32 + lane];
-        if (v > kk && v < m) m = v;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        uint32_t v = __shfl_xor_sync(FULL, m, o);
-        m = v < m ? v : m;
-    }
-    if (lane == 0 && m != OIFT_KEY_INF) atomicMin(&A.tpend[t], m);
-    if (m < next_min) next_min = m;
+    // ---- pass 3: publish re-activations, pending key of this tile ----
+    flush_reactivations();
+    pending();
+    cyc[2] += clock64() - tcount;
+    cyc[5] += 1;
 }
 
 template <int TY, int TZ>
@@ -302,15 +561,30 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *skey = reinterpret_cast<uint32_t *>(smem_raw) + warp * 1024;
     uint16_t *sw = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * 4096) + warp * 3072;
+    uint16_t *shx = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * (4096 + 6144)) + warp * 416;
+    uint16_t *shy = shx + 32;
+    uint16_t *shz = shx + 32 + 4 * 32;
     __shared__ uint32_t blk_min[OIFT_WARPS];
     __shared__ uint32_t s_level;
+    long long cyc_tile[6] = {0, 0, 0, 0, 0, 0};
+    __shared__ uint32_t s_wl[OIFT_WARPS][OIFT_WORKLIST];
+    __shared__ int s_wcount[OIFT_WARPS];
+    __shared__ uint32_t s_rmask[OIFT_WARPS];
+    uint32_t *rmask = &s_rmask[warp];
+    if (lane == 0) *rmask = 0u;
+    __syncwarp();
+    uint32_t *wl = s_wl[warp];
+    int *wcount = &s_wcount[warp];
     OiftGlobals *g = A.g;
     const int gwarp = blockIdx.x * OIFT_WARPS + warp;
     const int nwarps = gridDim.x * OIFT_WARPS;
 
     uint32_t prev_level = 0;
+    long long lvl_t0 = 0;
+    long long cyc_levelsync = 0, cyc_owner = 0, cyc_busy = 0, cyc_drain = 0;
     for (int e = 0;; e++) {
         const int par = e & 1;
+        const long long t_r0 = clock64();
         // ---- R: global minimum of the pending keys ----
         uint32_t m = OIFT_KEY_INF;
         for (int t = gwarp * 32 + lane; t < A.ntiles; t += nwarps * 32) {
@@ -333,6 +607,13 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
             }
         }
         grid_barrier(g, A.spin_limit);
+        if (blockIdx.x == 0 && threadIdx.x == 0 && A.lprof && e > 0 && e - 1 < A.lprof_cap) {
+            const long long now = clock64();
+            A.lprof[2 * (e - 1)] = (unsigned int)min(now - lvl_t0, 0xffffffffll);
+            lvl_t0 = now;
+        } else if (blockIdx.x == 0 && threadIdx.x == 0 && e == 0) {
+            lvl_t0 = clock64();
+        }
         if (threadIdx.x == 0) s_level = vload(&g->nextmin[par]);
         __syncthreads();
         const uint32_t kk = s_level;
@@ -348,71 +629,94 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
         const double per = (double)polarity_of(A, l);
         const double fgt = 1.0 + per / 100.0, flt = 1.0 - per / 100.0;
         const int bgt = max_base_for_cost(c, fgt), blt = max_base_for_cost(c, flt);
-        // ---- S: queue the tiles of this level ----
-        for (int t0 = gwarp * 32; t0 < A.ntiles; t0 += nwarps * 32) {
-            int t = t0 + lane;
-            bool hit = t < A.ntiles && __ldcg(&A.tpend[t]) == kk;
-            if (hit) {
-                A.tpend[t] = OIFT_KEY_INF;
-                enqueue_tile(A, par, t);
+        // ---- S: the owner warp of each tile of this level processes it directly ----
+        unsigned long long steps = 0;
+        const long long t_s0 = clock64();
+        cyc_levelsync += t_s0 - t_r0;
+        for (int j0 = 0; gwarp + j0 * nwarps < A.ntiles; j0 += 32) {
+            const int t = gwarp + (j0 + lane) * nwarps;
+            const bool hit = t < A.ntiles && __ldcg(&A.tpend[t]) == kk;
+            uint32_t hits = __ballot_sync(FULL, hit);
+            while (hits) {
+                const int b = __ffs(hits) - 1;
+                hits &= hits - 1;
+                const int th = gwarp + (j0 + b) * nwarps;
+                if (lane == 0) A.tpend[th] = OIFT_KEY_INF;
+                __syncwarp();
+                process_tile<TY, TZ>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey, sw,
+                                     shx, shy, shz, wl, wcount, rmask, cyc_tile);
+                steps++;
             }
         }
         __threadfence();
         __syncwarp();
         if (lane == 0) atomicSub(&g->outstanding[par], 1);
-        // ---- P: drain the level ----
-        uint32_t next_min = OIFT_KEY_INF;
+        const long long t_p0 = clock64();
+        cyc_owner += t_p0 - t_s0;
+        // ---- P: take this warp's re-activated tiles until the level is complete ----
+        unsigned long long *mybox = A.mbox + (size_t)gwarp * A.mbox_words;
         long long spins = 0;
-        unsigned long long steps = 0;
+        int idle = 0;
         for (;;) {
-            int t = -1;
-            if (lane == 0) {
-                unsigned long long h = vload(&g->qhead), tl = vload(&g->qtail);
-                if (h < tl) {
-                    if (atomicCAS(&g->qhead, h, h + 1) == h) {
-                        uint32_t v = QEMPTY;
-                        long long ws = 0;
-                        while ((v = atomicExch(&A.queue[h & A.qmask], QEMPTY)) == QEMPTY) {
-                            if (++ws > A.spin_limit || vload(&g->error)) {
-                                atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
-                                break;
-                            }
-                        }
-                        if (v != QEMPTY) {
-                            atomicExch(&A.inq[v], 0u);
-                            t = (int)v;
-                        }
-                    } else {
-                        t = -2;
-                    }
+            unsigned long long bits = 0;
+            int word = -1;
+            if (lane < A.mbox_words) {
+                if (*(volatile unsigned long long *)&mybox[lane]) {
+                    bits = atomicExch(&mybox[lane], 0ull);
+                    word = lane;
                 }
             }
-            t = __shfl_sync(FULL, t, 0);
-            if (t >= 0) {
-                process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey, sw,
-                                     next_min);
-                steps++;
+            const uint32_t have = __ballot_sync(FULL, bits != 0ull);
+            if (have) {
                 __threadfence();
-                __syncwarp();
-                if (lane == 0) atomicSub(&g->outstanding[par], 1);
+                const long long tb = clock64();
+                for (uint32_t hv = have; hv; hv &= hv - 1) {
+                    const int src = __ffs(hv) - 1;
+                    unsigned long long b = __shfl_sync(FULL, bits, src);
+                    const int wd = __shfl_sync(FULL, word, src);
+                    while (b) {
+                        const int j = wd * 64 + __ffsll((long long)b) - 1;
+                        b &= b - 1;
+                        const int t = gwarp + j * nwarps;
+                        process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey,
+                                             sw, shx, shy, shz, wl, wcount, rmask, cyc_tile);
+                        steps++;
+                        __threadfence();
+                        __syncwarp();
+                        if (lane == 0) atomicSub(&g->outstanding[par], 1);
+                    }
+                }
+                cyc_busy += clock64() - tb;
                 spins = 0;
+                idle = 0;
                 continue;
             }
-            if (t == -2) continue;
             int done = 0;
             if (lane == 0) {
-                done = vload(&g->outstanding[par]) == 0 || vload(&g->error) != 0;
+                // the global counter is polled sparsely; the CTA queue every time
+                if ((idle & 3) == 0)
+                    done = vload(&g->outstanding[par]) == 0 || vload(&g->error) != 0;
                 if (!done && ++spins > A.spin_limit) {
                     atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
                     done = 1;
                 }
             }
+            idle++;
             done = __shfl_sync(FULL, done, 0);
             if (done) break;
-            __nanosleep(32);
+            __nanosleep(64);
         }
         if (lane == 0 && steps) atomicAdd(&g->tile_steps, steps);
-        (void)next_min;
+        if (lane == 0 && steps && A.lprof && e < A.lprof_cap)
+            atomicAdd(&A.lprof[2 * e + 1], (unsigned int)steps);
+        cyc_drain += clock64() - t_p0;
+    }
+    if (lane == 0) {
+        atomicAdd(&g->cycles[0], (unsigned long long)cyc_levelsync);
+        atomicAdd(&g->cycles[1], (unsigned long long)cyc_owner);
+        atomicAdd(&g->cycles[2], (unsigned long long)cyc_busy);
+        atomicAdd(&g->cycles[3], (unsigned long long)cyc_drain);
+        for (int i = 0; i < 6; i++) atomicAdd(&g->cycles[4 + i], (unsigned long long)cyc_tile[i]);
     }
 }
 
@@ -464,28 +768,34 @@ OiftPlan oift_plan(int X, int Y, int Z) {
     P.nty = (Y + P.TY - 1) / P.TY;
     P.ntz = (Z + P.TZ - 1) / P.TZ;
     P.ntiles = P.ntx * P.nty * P.ntz;
-    unsigned int q = 1024;
-    while (q < (unsigned int)P.ntiles + 64) q <<= 1;
-    P.qcap = q;
+    P.qcap = 0;
     return P;
 }
 
-size_t oift_smem_bytes() { return (size_t)OIFT_WARPS * (4096 + 6144); }
+size_t oift_smem_bytes() { return (size_t)OIFT_WARPS * (4096 + 6144 + 832); }
 
 
 size_t oift_globals_bytes() { return sizeof(OiftGlobals); }
+int oift_mbox_words(const OiftPlan &P, int ctas) {
+    const int nw = ctas * OIFT_WARPS;
+    const int per_warp = (P.ntiles + nw - 1) / nw;
+    return (per_warp + 63) / 64;
+}
+size_t oift_mbox_bytes(const OiftPlan &P, int ctas) {
+    return (size_t)ctas * OIFT_WARPS * oift_mbox_words(P, ctas) * sizeof(unsigned long long);
+}
 
 // Runs the seeds kernel, the persistent kernel and (optionally) the finalize kernel.
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
-             long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
+             long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end,
+             unsigned long long *cycles_out) {
     size_t N = (size_t)X * Y * Z;
     cudaMemsetAsync(S.key, 0xFF, N * sizeof(uint32_t), st);
     cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
-    cudaMemsetAsync(S.inq, 0, (size_t)P.ntiles * sizeof(uint32_t), st);
-    cudaMemsetAsync(S.queue, 0xFF, (size_t)P.qcap * sizeof(uint32_t), st);
+    cudaMemsetAsync(S.mbox, 0, oift_mbox_bytes(P, sms), st);
     cudaMemsetAsync(S.g, 0, sizeof(OiftGlobals), st);
     OiftGlobals init{};
     init.nextmin[0] = init.nextmin[1] = OIFT_KEY_INF;
@@ -506,9 +816,12 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.key = S.key;
     A.W = W;
     A.tpend = S.tpend;
-    A.inq = S.inq;
-    A.queue = S.queue;
-    A.qmask = P.qcap - 1;
+    A.mbox = S.mbox;
+    A.lprof = S.lprof;
+    A.lprof_cap = S.lprof_cap;
+    if (S.lprof) cudaMemsetAsync(S.lprof, 0, (size_t)S.lprof_cap * 2 * sizeof(unsigned int), st);
+    A.nwarps = sms * OIFT_WARPS;
+    A.mbox_words = oift_mbox_words(P, sms);
     A.X = X;
     A.Y = Y;
     A.Z = Z;
@@ -550,6 +863,8 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     if (cudaStreamSynchronize(st) != cudaSuccess) return OIFT_E_CUDA;
     if (levels_out) *levels_out = hg.levels;
     if (steps_out) *steps_out = (long long)hg.tile_steps;
+    if (cycles_out)
+        for (int i = 0; i < 10; i++) cycles_out[i] = hg.cycles[i];
     if (hg.error == OIFT_DEV_TIMEOUT) return OIFT_E_NOT_CONVERGED;
     if (hg.error == OIFT_DEV_QUEUE) return OIFT_E_QUEUE_OVERFLOW;
     return OIFT_OK;

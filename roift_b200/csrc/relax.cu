@@ -24,6 +24,104 @@
 namespace oiftb {
 
 
+// Contribution of one neighbour q to the sums of voxel p, in the reference order.
+template <int C, bool PERCLASS>
+__device__ __forceinline__ void relax_accumulate(const RelaxArgs &a, int ip, int iq,
+                                                 const float (&mq)[C], float dpq, float &sw,
+                                                 float (&acc)[C]) {
+    float w = fabsf((float)(ip - iq));
+    float per_pq;
+    if (PERCLASS) {
+        per_pq = 0.0f;
+#pragma unroll
+        for (int k = 0; k < C; k++) per_pq = __fadd_rn(per_pq, __fmul_rn(a.pcm[k], mq[k]));
+    } else {
+        float pbg = mq[0];
+#pragma unroll
+        for (int k = 1; k < C; k++)
+            if (k == a.bg) pbg = mq[k];
+        per_pq = __fmul_rn(a.per, __fsub_rn(__fmul_rn(2.0f, pbg), 1.0f));
+    }
+    if (ip > iq)
+        w = __fmul_rn(w, __fadd_rn(1.0f, __fdiv_rn(per_pq, 100.0f)));
+    else if (ip < iq)
+        w = __fmul_rn(w, __fsub_rn(1.0f, __fdiv_rn(per_pq, 100.0f)));
+    w = __fsub_rn(a.Wmax, w);
+    if (w < 0.0f) w = 0.0f;
+    w = __fmul_rn(w, w);
+    w = __fmul_rn(w, w);
+    w = __fmul_rn(w, w);
+    if (dpq != 1.0f) w = __fdiv_rn(w, dpq);
+    sw = __fadd_rn(sw, w);
+#pragma unroll
+    for (int k = 0; k < C; k++) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, mq[k]));
+}
+
+template <int C, typename T, bool PERCLASS>
+__device__ __forceinline__ void relax_finish(const RelaxArgs &a, const float *__restrict__ min_,
+                                             float *__restrict__ mout,
+                                             const uint8_t *__restrict__ seedc, size_t p,
+                                             float sw, const float (&acc)[C]) {
+    const size_t N = a.N;
+    float out[C];
+    if (sw > 0.0f) {
+#pragma unroll
+        for (int k = 0; k < C; k++) out[k] = __fdiv_rn(acc[k], sw);
+    } else {
+#pragma unroll
+        for (int k = 0; k < C; k++) out[k] = __ldg(&min_[(size_t)k * N + p]);
+    }
+    const uint8_t sc = __ldg(&seedc[p]);
+    if (sc != 0xFF) {
+#pragma unroll
+        for (int k = 0; k < C; k++) out[k] = (k == sc) ? 1.0f : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < C; k++) mout[(size_t)k * N + p] = out[k];
+}
+
+// 6-neighbourhood sweep: block (32, 8) threads over an x-y tile of one z plane.
+// Neighbours in the Spheric order -z, -y, -x, +x, +y, +z (Dpq = 1).
+template <int C, typename T, bool PERCLASS>
+__global__ void __launch_bounds__(256) relax_sweep6_kernel(const float *__restrict__ min_,
+                                                           float *__restrict__ mout,
+                                                           const T *__restrict__ img,
+                                                           const uint8_t *__restrict__ seedc,
+                                                           RelaxArgs a) {
+    const int X = a.X, Y = a.Y, Z = a.Z;
+    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= X || y >= Y) return;
+    const size_t N = a.N, XY = (size_t)X * Y;
+    const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+    const int ip = (int)__ldg(&img[p]);
+    float acc[C];
+#pragma unroll
+    for (int k = 0; k < C; k++) acc[k] = 0.0f;
+    float sw = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        long long off;
+        bool ok;
+        switch (i) {
+            case 0: ok = z > 0; off = -(long long)XY; break;
+            case 1: ok = y > 0; off = -(long long)X; break;
+            case 2: ok = x > 0; off = -1; break;
+            case 3: ok = x + 1 < X; off = 1; break;
+            case 4: ok = y + 1 < Y; off = X; break;
+            default: ok = z + 1 < Z; off = (long long)XY; break;
+        }
+        if (!ok) continue;
+        const size_t q = (size_t)((long long)p + off);
+        float mq[C];
+#pragma unroll
+        for (int k = 0; k < C; k++) mq[k] = __ldg(&min_[(size_t)k * N + q]);
+        relax_accumulate<C, PERCLASS>(a, ip, (int)__ldg(&img[q]), mq, 1.0f, sw, acc);
+    }
+    relax_finish<C, T, PERCLASS>(a, min_, mout, seedc, p, sw, acc);
+}
+
+// General neighbourhood (26 / 8 / 4): same arithmetic over the Spheric list.
 template <int C, typename T, bool PERCLASS>
 __global__ void __launch_bounds__(256) relax_sweep_kernel(const float *__restrict__ min_,
                                                           float *__restrict__ mout,
@@ -31,66 +129,26 @@ __global__ void __launch_bounds__(256) relax_sweep_kernel(const float *__restric
                                                           const uint8_t *__restrict__ seedc,
                                                           RelaxArgs a) {
     const int X = a.X, Y = a.Y, Z = a.Z;
+    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= X || y >= Y) return;
     const size_t N = a.N, XY = (size_t)X * Y;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
-         p += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / XY);
-        const int ip = (int)img[p];
-        float acc[C];
+    const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+    const int ip = (int)__ldg(&img[p]);
+    float acc[C];
 #pragma unroll
-        for (int k = 0; k < C; k++) acc[k] = 0.0f;
-        float sw = 0.0f;
-        for (int i = 0; i < a.nadj; i++) {
-            const int qx = x + a.dx[i], qy = y + a.dy[i], qz = z + a.dz[i];
-            if (qx < 0 || qx >= X || qy < 0 || qy >= Y || qz < 0 || qz >= Z) continue;
-            const size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * XY;
-            const int iq = (int)img[q];
-            float mq[C];
+    for (int k = 0; k < C; k++) acc[k] = 0.0f;
+    float sw = 0.0f;
+    for (int i = 0; i < a.nadj; i++) {
+        const int qx = x + a.dx[i], qy = y + a.dy[i], qz = z + a.dz[i];
+        if (qx < 0 || qx >= X || qy < 0 || qy >= Y || qz < 0 || qz >= Z) continue;
+        const size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * XY;
+        float mq[C];
 #pragma unroll
-            for (int k = 0; k < C; k++) mq[k] = __ldg(&min_[(size_t)k * N + q]);
-            float w = fabsf((float)(ip - iq));
-            float per_pq;
-            if (PERCLASS) {
-                per_pq = 0.0f;
-#pragma unroll
-                for (int k = 0; k < C; k++) per_pq = __fadd_rn(per_pq, __fmul_rn(a.pcm[k], mq[k]));
-            } else {
-                float pbg = mq[0];
-#pragma unroll
-                for (int k = 1; k < C; k++)
-                    if (k == a.bg) pbg = mq[k];
-                per_pq = __fmul_rn(a.per, __fsub_rn(__fmul_rn(2.0f, pbg), 1.0f));
-            }
-            if (ip > iq)
-                w = __fmul_rn(w, __fadd_rn(1.0f, __fdiv_rn(per_pq, 100.0f)));
-            else if (ip < iq)
-                w = __fmul_rn(w, __fsub_rn(1.0f, __fdiv_rn(per_pq, 100.0f)));
-            w = __fsub_rn(a.Wmax, w);
-            if (w < 0.0f) w = 0.0f;
-            w = __fmul_rn(w, w);
-            w = __fmul_rn(w, w);
-            w = __fmul_rn(w, w);
-            if (a.dpq[i] != 1.0f) w = __fdiv_rn(w, a.dpq[i]);
-            sw = __fadd_rn(sw, w);
-#pragma unroll
-            for (int k = 0; k < C; k++) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, mq[k]));
-        }
-        float out[C];
-        if (sw > 0.0f) {
-#pragma unroll
-            for (int k = 0; k < C; k++) out[k] = __fdiv_rn(acc[k], sw);
-        } else {
-#pragma unroll
-            for (int k = 0; k < C; k++) out[k] = min_[(size_t)k * N + p];
-        }
-        const uint8_t sc = seedc[p];
-        if (sc != 0xFF) {
-#pragma unroll
-            for (int k = 0; k < C; k++) out[k] = (k == sc) ? 1.0f : 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < C; k++) mout[(size_t)k * N + p] = out[k];
+        for (int k = 0; k < C; k++) mq[k] = __ldg(&min_[(size_t)k * N + q]);
+        relax_accumulate<C, PERCLASS>(a, ip, (int)__ldg(&img[q]), mq, a.dpq[i], sw, acc);
     }
+    relax_finish<C, T, PERCLASS>(a, min_, mout, seedc, p, sw, acc);
 }
 
 // One-hot initial membership from the OIFT labels (gft_ift.cpp:8745-8752).
@@ -116,14 +174,23 @@ __global__ void relax_seed_kernel(const int32_t *seeds, int nseeds, const int32_
     seedc[p] = (uint8_t)c;
 }
 
-// Labels present among the seeds (gft_ift.cpp:8684-8712): bitmap over label values.
+// Labels present among the seeds (gft_ift.cpp:8684-8712): bitmap over label values,
+// aggregated in shared memory so that a million seeds of two labels cost two global
+// atomics per block.
 __global__ void seed_presence_kernel(const int32_t *seed_labels, int nseeds, uint32_t *bits) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nseeds) return;
-    int lb = seed_labels[i];
-    if (lb < 0) lb = 0;
-    if (lb > OIFT_MAX_LABEL) return;
-    atomicOr(&bits[lb >> 5], 1u << (lb & 31));
+    __shared__ uint32_t sb[1024];
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) sb[i] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nseeds; i += gridDim.x * blockDim.x) {
+        int lb = seed_labels[i];
+        if (lb < 0) lb = 0;
+        if (lb > OIFT_MAX_LABEL) continue;
+        const uint32_t bit = 1u << (lb & 31);
+        if (!(sb[lb >> 5] & bit)) atomicOr(&sb[lb >> 5], bit);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x)
+        if (sb[i]) atomicOr(&bits[i], sb[i]);
 }
 
 // Argmax with strict '>' so the lowest class wins ties (gft_ift.cpp:8889-8904).
@@ -150,12 +217,20 @@ template <int C, typename T>
 static cudaError_t launch_sweep_c(const float *in, float *out, const T *img,
                                   const uint8_t *seedc, const RelaxArgs &a, bool perclass,
                                   int sms, cudaStream_t s) {
-    int blocks = (int)((a.N + 255) / 256);
-    if (blocks > sms * 16) blocks = sms * 16;
-    if (perclass)
-        relax_sweep_kernel<C, T, true><<<blocks, 256, 0, s>>>(in, out, img, seedc, a);
-    else
-        relax_sweep_kernel<C, T, false><<<blocks, 256, 0, s>>>(in, out, img, seedc, a);
+    (void)sms;
+    dim3 block(32, 8), grid((a.X + 31) / 32, (a.Y + 7) / 8, a.Z);
+    const bool six = (a.nadj == 6);
+    if (perclass) {
+        if (six)
+            relax_sweep6_kernel<C, T, true><<<grid, block, 0, s>>>(in, out, img, seedc, a);
+        else
+            relax_sweep_kernel<C, T, true><<<grid, block, 0, s>>>(in, out, img, seedc, a);
+    } else {
+        if (six)
+            relax_sweep6_kernel<C, T, false><<<grid, block, 0, s>>>(in, out, img, seedc, a);
+        else
+            relax_sweep_kernel<C, T, false><<<grid, block, 0, s>>>(in, out, img, seedc, a);
+    }
     return cudaGetLastError();
 }
 
