@@ -284,7 +284,10 @@ def main():
     C = stats[0].nclasses
     ms_sweep = statistics.mean(s.ms_sweeps for s in stats) / c.sweeps
     ms_oiftk = statistics.mean(s.ms_oift_kernel for s in stats)
-    relax_bytes = N * (8 * C + 2)        # per sweep launch: C planes in + out, int16 image
+    # per sweep launch: C membership planes read + written and the int16 image, over the
+    # voxels the sweep computes (the reference's growing mask; skipped tiles move nothing)
+    active_per_sweep = stats[-1].relax_active_voxel_sweeps / c.sweeps
+    relax_bytes = active_per_sweep * (8 * C + 2)
     oift_bytes = N * 12                  # 6 B weights + 1 B seed/label + 4 B cost + 1 B label
     if ms_sweep * c.sweeps >= ms_oiftk:
         dom, bytes_, ms_k = "relax_sweep_kernel", relax_bytes, ms_sweep
@@ -300,6 +303,7 @@ def main():
               "ms_oift_kernel": ms_oiftk,
               "ms_relax": statistics.mean(s.ms_relax for s in stats),
               "ms_sweep": ms_sweep,
+              "relax_active_fraction": active_per_sweep / N,
               "oift_levels": stats[0].levels, "oift_tile_steps": stats[0].tile_steps,
               "oift_warp_cycles": list(stats[-1].oift_cycles),
               "oift_tiles_stale_sparse_dense": list(stats[-1].oift_cycles)[7:10],

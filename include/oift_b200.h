@@ -97,6 +97,8 @@ typedef struct {
     long long oift_cycles[10]; /* OIFT SM cycles summed over warps: level switch, owner
                                   tiles, queued tiles, drain (incl. idle); per tile step:
                                   staging, masks, flood, expansion, faces, pending */
+    long long relax_active_voxel_sweeps; /* voxels computed over all sweeps (tiles outside
+                                            the reference's growing mask are skipped) */
 } oift_b200_stats;
 
 /* Context: owns the device scratch for one device and one stream. */
@@ -133,6 +135,12 @@ OIFT_API int oift_b200_weight_planes(int adjacency);
 /* Per-level profile of the last OIFT run: pairs (SM cycles, tile activations) for the
  * first `cap` levels.  Returns the number of pairs written or a negative status. */
 OIFT_API int oift_b200_level_profile(oift_b200_ctx *ctx, unsigned int *cycles_steps, int cap);
+
+/* Device self-test of the FP32 division by 100 used inside the relaxation sweeps:
+ * counts, over all 2^32 FP32 bit patterns (NaN/Inf skipped, signed zeros equal), the
+ * inputs whose quotient differs from the IEEE division; first_bad = smallest such
+ * pattern (0xFFFFFFFF if none).  Uses device 0 of the calling thread's context. */
+OIFT_API int oift_b200_selftest_div100(unsigned long long *mismatches, unsigned int *first_bad);
 
 /* Reference-compatible drop-in (gpu/oift_fmax_gpu.cu:139-149).  Host pointers.
  * h_labels: in = labels (seed voxels carry their label, NIL elsewhere), out = OIFT

@@ -53,7 +53,8 @@ class Stats(C.Structure):
                 ("nclasses", C.c_int), ("ms_weights", C.c_float), ("ms_oift", C.c_float),
                 ("ms_relax", C.c_float), ("ms_total", C.c_float), ("kernels", C.c_int),
                 ("ms_oift_kernel", C.c_float), ("ms_sweeps", C.c_float),
-                ("oift_cycles", C.c_longlong * 10)]
+                ("oift_cycles", C.c_longlong * 10),
+                ("relax_active_voxel_sweeps", C.c_longlong)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -65,7 +66,7 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_set_stream", "oift_b200_status_string", "oift_b200_run_device_i16",
            "oift_b200_run_host", "oift_b200_build_weights_i16", "oift_b200_weight_planes",
            "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status",
-           "oift_b200_level_profile"]
+           "oift_b200_level_profile", "oift_b200_selftest_div100"]
 
 _lib = None
 
@@ -90,6 +91,7 @@ def lib():
         L.oift_b200_run_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
                                          vp, vp, C.c_int, vp, C.POINTER(Stats)]
         L.oift_b200_level_profile.argtypes = [vp, vp, C.c_int]
+        L.oift_b200_selftest_div100.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]
         L.oift_b200_build_weights_i16.argtypes = [vp, C.POINTER(Params), vp, vp,
                                                   C.POINTER(C.c_longlong)]
         L.oift_fmax_gpu_run.argtypes = [i32p, i32p, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -209,6 +211,15 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_build_weights_i16")
         return cl.value
+
+
+def selftest_div100():
+    """(mismatches, first bad bit pattern) of the sweep's x/100 against IEEE division."""
+    bad, first = C.c_ulonglong(0), C.c_uint(0)
+    rc = lib().oift_b200_selftest_div100(C.byref(bad), C.byref(first))
+    if rc != OK:
+        raise OiftError(rc, "oift_b200_selftest_div100")
+    return bad.value, first.value
 
 
 def weight_planes(adjacency: int) -> int:

@@ -28,7 +28,7 @@ struct oift_b200_ctx {
     cudaEvent_t ev[8];
     // scratch (grow-only)
     DevBuf img32, img16, W, key, tpend, inq, queue, glob, flag, minmax, seeds, slabels, cost,
-        olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8, ctaq, lprof;
+        olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8, ctaq, lprof, rtdist;
     size_t total = 0;
     unsigned long long oift_cycles[10] = {0};
 };
@@ -118,7 +118,8 @@ int oift_b200_destroy(oift_b200_ctx *c) {
     DevBuf *bufs[] = {&c->img32, &c->img16,  &c->W,      &c->key,     &c->tpend,   &c->inq,
                       &c->queue, &c->glob,   &c->flag,   &c->minmax,  &c->seeds,   &c->slabels,
                       &c->cost,  &c->olabel, &c->flabel, &c->memb,    &c->seedc,   &c->l2c,
-                      &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8, &c->ctaq};
+                      &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8, &c->ctaq,
+                      &c->lprof, &c->rtdist};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -301,6 +302,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     // ---- relaxation ----
     const int K = p->relax_sweeps;
     int nclasses = 0;
+    long long relax_active = 0;
+    int relax_dilations = 0;
     std::vector<int> classes;
     bool want_relax = out && (out->label || out->mask || out->membership);
     if (want_relax) {
@@ -369,21 +372,55 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         CU(cudaMemcpyAsync(c->classes.p, classes.data(), nclasses * sizeof(int), cudaMemcpyHostToDevice, s));
         float *m0 = (float *)c->memb.p, *m1 = m0 + (size_t)nclasses * N;
         int blocks = (int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16);
+        // both ping-pong buffers start one-hot: tiles skipped at a sweep keep that value
         relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m0);
+        relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m1);
         CU(cudaMemsetAsync(c->seedc.p, 0xFF, N, s));
         if (nseeds > 0)
             relax_seed_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(d_seeds, nseeds, d_olab, N,
                                                                    (const int *)c->l2c.p, maxl, bg,
                                                                    (uint8_t *)c->seedc.p);
+        // block distance of every relaxation tile to the label boundary (exact skipping)
+        const int rtx = (X + 31) / 32, rty = (Y + 7) / 8, rtz = (Z + 3) / 4;
+        const int rnt = rtx * rty * rtz;
+        TRY(grow(c, c->rtdist, 2 * (size_t)rnt * sizeof(uint16_t) + (size_t)(K + 1) * sizeof(unsigned)));
+        uint16_t *td0 = (uint16_t *)c->rtdist.p, *td1 = td0 + rnt;
+        unsigned *hist = (unsigned *)(td1 + rnt);  // byte offset 4 * rnt
+        CU(cudaMemsetAsync(td0, 0xFF, 2 * (size_t)rnt * sizeof(uint16_t), s));
+        relax_boundary_tiles_kernel<<<dim3((X + 31) / 32, (Y + 7) / 8, Z), dim3(32, 8), 0, s>>>(
+            d_olab, X, Y, Z, adj.n, ra, td0, rtx, rty);
+        const int cheb = (adj.n == 26);
+        // exact lower bound of the voxel distance to the mask: three separable passes
+        relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 0, 32, cheb);
+        relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td1, td0, rtx, rty, rtz, 1, 8, cheb);
+        relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 2, 4, cheb);
+        std::swap(td0, td1);
+        long long active_vs = 0;
+        if (K > 0) {
+            CU(cudaMemsetAsync(hist, 0, (size_t)(K + 1) * sizeof(unsigned), s));
+            relax_tile_hist_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, rnt, K, hist);
+        }
         float *cur = m0, *nxt = m1;
         cudaEventRecord(c->ev[6], s);
         for (int it = 0; it < K; it++) {
-            CU(launch_relax_sweep<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, ra,
-                                     p->per_class != nullptr, c->sms, s));
+            CU(launch_relax_tiles<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, td0,
+                                     it + 1, ra, p->per_class != nullptr, rnt, rtx, rty, s));
             std::swap(cur, nxt);
         }
+        if (K > 0) {
+            std::vector<unsigned> h(K);
+            CU(cudaMemcpyAsync(h.data(), hist, K * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s));
+            long long run = 0;
+            for (int t = 1; t <= K; t++) {  // tiles with distance <= t-1 run at sweep t
+                run += h[t - 1];
+                active_vs += run * 1024;
+            }
+        }
+        relax_active = active_vs;
+        relax_dilations = 3;
         cudaEventRecord(c->ev[7], s);
-        relax_argmax_kernel<<<blocks, 256, 0, s>>>(cur, N, nclasses, (const int *)c->classes.p,
+        relax_argmax_kernel<<<(int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16), 256, 0, s>>>(cur, N, nclasses, (const int *)c->classes.p,
                                                    out->label, out->mask);
         if (out->membership)
             CU(cudaMemcpyAsync(out->membership, cur, (size_t)nclasses * N * sizeof(float),
@@ -404,7 +441,10 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         cudaEventElapsedTime(&st->ms_total, c->ev[0], c->ev[3]);
         // minmax, build, seeds, persistent OIFT, finalize (+ presence, init, seed map,
         // K sweeps, argmax when relaxing)
-        st->kernels = 5 + (want_relax ? 4 + K : 0);
+        // minmax, build, seeds, persistent OIFT, finalize; relaxing adds presence, 2 inits,
+        // seed map, boundary tiles, dilations, histogram, K sweeps, argmax
+        st->kernels = 5 + (want_relax ? 7 + relax_dilations + K : 0);
+        st->relax_active_voxel_sweeps = relax_active;
         cudaEventElapsedTime(&st->ms_oift_kernel, c->ev[4], c->ev[5]);
         st->ms_sweeps = 0.0f;
         for (int i = 0; i < 10; i++) st->oift_cycles[i] = (long long)c->oift_cycles[i];

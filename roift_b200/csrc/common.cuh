@@ -76,6 +76,20 @@ __host__ __device__ inline int max_base_for_cost(int c, double f) {
     return bi;
 }
 
+// x / 100 rounded to nearest-even in FP32, for all finite x (exhaustively checked against
+// the IEEE quotient by oift_b200_selftest_div100): the product with r = RN(1/100) is
+// corrected once by the exact FMA residual e = x - q*100 (Markstein's correction step).
+// The residual is exact only while the quotient is a normal number, so |x| < 2^-100
+// (never reached by the sweeps, whose |per_pq| is 0 or >= 2^-24 * |per|) takes the IEEE
+// division.
+__device__ __forceinline__ float div100_rn(float x) {
+    if (fabsf(x) < 7.88860905e-31f) return __fdiv_rn(x, 100.0f);  // 2^-100
+    const float r = 0.00999999977648258209228515625f;  // RN(1/100) = 0x3C23D70A
+    const float q = __fmul_rn(x, r);
+    const float e = __fmaf_rn(-q, 100.0f, x);
+    return __fmaf_rn(e, r, q);
+}
+
 }  // namespace oiftb
 
 // Kernel-side error codes written to a device flag (read by the host after a launch).

@@ -163,3 +163,27 @@ def test_device_pipeline_ellipsoid(roift, oracle_lib):
     lab32, m32, nc = O.relax(shifted, 6, c.seeds, lab_r2, c.sweeps, pol=c.pol)
     assert np.array_equal(memb_t.cpu().numpy().reshape(nc, N).view(np.uint32), m32.view(np.uint32))
     assert np.array_equal(lab_t.cpu().numpy(), lab32)
+
+
+def test_div100_exhaustive(roift):
+    """The sweeps' x/100 equals the IEEE FP32 quotient for every finite input."""
+    bad, first = roift.selftest_div100()
+    assert bad == 0, f"{bad} mismatches, first bit pattern {first:#010x}"
+
+
+@pytest.mark.parametrize("size", [96])
+def test_relax_tile_skipping_exact(roift, oracle_lib, size):
+    """Clean ellipsoid boundary: early sweeps skip most tiles, membership stays bit-exact."""
+    c = synth.ellipsoid3d(seed=4, size=size, sweeps=12)
+    img = c.image.astype(np.int32)
+    img -= min(0, int(img.min()))
+    Z, Y, X = c.shape
+    K = c.sweeps
+    lab, cost, memb, mask, st = _run(roift, c, img, "grad_q", sweeps=K)
+    W, _ = O.build_weights(img, 6, "grad_q")
+    _, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels, pol=c.pol)
+    lab32, m32, nc = O.relax(img, 6, c.seeds, lab_r2, K, pol=c.pol)
+    assert np.array_equal(memb.view(np.uint32), m32.view(np.uint32))
+    assert np.array_equal(lab, lab32)
+    tiles = ((X + 31) // 32) * ((Y + 7) // 8) * ((Z + 3) // 4)
+    assert st.relax_active_voxel_sweeps < 0.8 * K * tiles * 1024
