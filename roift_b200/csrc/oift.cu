@@ -23,7 +23,7 @@
 //      expand the newly conquered voxels: in-tile neighbours get tentative keys, out-of-
 //      tile neighbours are lowered with a 32-bit atomicMin; a same-level crossing
 //      re-queues the neighbour tile, a higher one lowers its pending key.
-// The level ends when the queue is empty and no tile is in flight (outstanding counter).
+// The level ends when no tile is pending or in flight (the level's outstanding counter).
 // Every wait (grid barrier, queue slot, level end) is bounded; on expiry the kernel sets
 // an error flag, every warp leaves, and the host reports OIFT_E_NOT_CONVERGED.
 #include <cooperative_groups.h>
