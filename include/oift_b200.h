@@ -142,6 +142,29 @@ OIFT_API int oift_b200_level_profile(oift_b200_ctx *ctx, unsigned int *cycles_st
  * pattern (0xFFFFFFFF if none).  Uses device 0 of the calling thread's context. */
 OIFT_API int oift_b200_selftest_div100(unsigned long long *mismatches, unsigned int *first_bad);
 
+/* OIFT without device allocation (no counterpart in the reference): for callers that
+ * cannot let a library call cudaMalloc while they run -- an application whose own memory
+ * pool already holds the GPU's memory, a pipeline that must not allocate (and so
+ * synchronise the device) after start-up, a host that forbids plug-ins to allocate.
+ * Builds the 6-/4-adjacency arc weights (OIFT_W_GRAD or OIFT_W_GRAD_Q) from the int16
+ * DEVICE image and runs the f_max OIFT, with every intermediate buffer inside one static
+ * device array of oift_b200_noalloc_scratch_bytes() bytes (about 10.3 MB, held by each GPU
+ * that loads the library until the process exits).  Inputs and outputs are device
+ * pointers owned by the caller: seeds / seed_labels [nseeds], cost and/or label [N]
+ * (either may be NULL).  per / per_class / max_label as in oift_b200_params.
+ * Limits: at most OIFT_NOALLOC_MAX_VOXELS voxels and 65536 warp tiles; larger volumes
+ * return OIFT_E_RANGE before any device work.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) -- make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race and corrupt each other.
+ * Runs on `stream` (cudaStream_t as void*) and synchronises it before returning. */
+#define OIFT_NOALLOC_MAX_VOXELS (1u << 20)
+OIFT_API int oift_b200_oift_noalloc(const int16_t *image, int xsize, int ysize, int zsize,
+                                    int adjacency, int weight_mode, int wq, float per,
+                                    const float *per_class, int max_label,
+                                    const int32_t *seeds, const int32_t *seed_labels,
+                                    int nseeds, int32_t *cost, int32_t *label, void *stream);
+OIFT_API size_t oift_b200_noalloc_scratch_bytes(void);
+
 /* Reference-compatible drop-in (gpu/oift_fmax_gpu.cu:139-149).  Host pointers.
  * h_labels: in = labels (seed voxels carry their label, NIL elsewhere), out = OIFT
  * labels.  h_per_class [max_label+1] polarity x100.  Returns the number of levels

@@ -66,7 +66,8 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_set_stream", "oift_b200_status_string", "oift_b200_run_device_i16",
            "oift_b200_run_host", "oift_b200_build_weights_i16", "oift_b200_weight_planes",
            "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status",
-           "oift_b200_level_profile", "oift_b200_selftest_div100"]
+           "oift_b200_level_profile", "oift_b200_selftest_div100",
+           "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes"]
 
 _lib = None
 
@@ -92,6 +93,10 @@ def lib():
                                          vp, vp, C.c_int, vp, C.POINTER(Stats)]
         L.oift_b200_level_profile.argtypes = [vp, vp, C.c_int]
         L.oift_b200_selftest_div100.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]
+        L.oift_b200_oift_noalloc.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.c_int, C.c_float, vp, C.c_int, vp, vp, C.c_int,
+                                             vp, vp, vp]
+        L.oift_b200_noalloc_scratch_bytes.restype = C.c_size_t
         L.oift_b200_build_weights_i16.argtypes = [vp, C.POINTER(Params), vp, vp,
                                                   C.POINTER(C.c_longlong)]
         L.oift_fmax_gpu_run.argtypes = [i32p, i32p, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -211,6 +216,31 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_build_weights_i16")
         return cl.value
+
+
+def oift_noalloc(image_ptr, shape_zyx, seeds_ptr, labels_ptr, nseeds, cost_ptr=None,
+                 label_ptr=None, adjacency=6, weight_mode="grad_q", wq=4095, pol=None,
+                 per_class=None, stream_ptr=None) -> None:
+    """OIFT on device buffers with no device allocation (oift_b200_oift_noalloc).
+
+    For callers that cannot allow a library to call cudaMalloc while they run: the
+    weights and the OIFT state live in a static device array of the library (limit
+    OIFT_NOALLOC_MAX_VOXELS = 2^20 voxels).  Calls that overlap on the GPU race."""
+    Z, Y, X = shape_zyx if len(shape_zyx) == 3 else (1,) + tuple(shape_zyx)
+    keep = None
+    if per_class is not None:
+        keep = np.ascontiguousarray(per_class, np.float32)
+        pc, ml, per = keep.ctypes.data, len(keep) - 1, 0.0
+    else:
+        pc, ml, per = None, 0, float(np.float32((pol or 0.0) * 100.0))
+    rc = lib().oift_b200_oift_noalloc(C.c_void_p(image_ptr), X, Y, Z, adjacency,
+                                      W_MODES[weight_mode], wq, per, pc, ml,
+                                      C.c_void_p(seeds_ptr), C.c_void_p(labels_ptr), int(nseeds),
+                                      C.c_void_p(cost_ptr or 0), C.c_void_p(label_ptr or 0),
+                                      C.c_void_p(stream_ptr or 0))
+    del keep
+    if rc != OK:
+        raise OiftError(rc, "oift_b200_oift_noalloc")
 
 
 def selftest_div100():
