@@ -23,17 +23,28 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+# (source, object, extra flags): the tile sweep is compiled once per class count
+UNITS = [(s, s.replace(".cu", ".o"), []) for s in SOURCES] + [
+    ("relax_tiles_inst.cu", f"relax_tiles_c{c}.o", [f"-DRELAX_TILE_C={c}"]) for c in range(1, 9)]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, "-dc", os.path.join(CSRC, src), "-o", obj]
+    from concurrent.futures import ThreadPoolExecutor
+
+    def compile_unit(unit):
+        src, obj, extra = unit
+        obj = os.path.join(CSRC, obj)
+        cmd = [NVCC, *FLAGS, *extra, "-dc", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+        return obj
+
+    workers = max(1, min(len(UNITS), os.cpu_count() or 1))
+    with ThreadPoolExecutor(workers) as ex:
+        objs = list(ex.map(compile_unit, UNITS))
     subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs,
                     "-o", LIB, "-lcudart"], check=True)
     for o in objs:

@@ -70,10 +70,6 @@ cudaError_t launch_build_weights(const T *img, uint16_t *W, const BuildArgs &a, 
                                  cudaStream_t s);
 template <typename T>
 cudaError_t launch_minmax(const T *img, size_t n, int *mm, int sms, cudaStream_t s);
-template <typename T>
-cudaError_t launch_relax_sweep(int C, const float *in, float *out, const T *img,
-                               const uint8_t *seedc, const RelaxArgs &a, bool perclass,
-                               int sms, cudaStream_t s);
 
 template <typename T>
 cudaError_t launch_relax_tiles(int C, const float *in, float *out, const T *img,
@@ -84,8 +80,6 @@ __global__ void relax_boundary_tiles_kernel(const int32_t *label, int X, int Y, 
                                             RelaxArgs a, uint16_t *tdist, int ntx, int nty);
 __global__ void relax_tile_gap_pass_kernel(const uint16_t *din, uint16_t *dout, int ntx, int nty,
                                            int ntz, int ax, int dim, int cheb);
-__global__ void relax_tile_dilate_kernel(const uint16_t *din, uint16_t *dout, int ntx, int nty,
-                                         int ntz, int cheb);
 __global__ void relax_tile_hist_kernel(const uint16_t *tdist, int nt, int K, unsigned int *hist);
 __global__ void relax_init_kernel(const int32_t *label, size_t N, int C, const int *l2c,
                                   int maxl, int bg, float *m);
