@@ -308,6 +308,8 @@ def main():
               "oift_warp_cycles": list(stats[-1].oift_cycles),
               "oift_tiles_stale_sparse_dense": list(stats[-1].oift_cycles)[7:10],
               "oift_cycles_stage_sparse_dense": list(stats[-1].oift_cycles)[4:7],
+              "oift_dense_cycles_masks_flood_iters_expand_faces_pending":
+                  list(stats[-1].oift_cycles)[10:16],
               "oift_gbs": oift_bytes / (ms_oiftk * 1e-3) / 1e9,
               "relax_sweep_gbs": relax_bytes / (ms_sweep * 1e-3) / 1e9}
 

@@ -94,9 +94,11 @@ typedef struct {
     int kernels;          /* kernel launches issued by the call */
     float ms_oift_kernel; /* persistent OIFT kernel alone (CUDA events around the launch) */
     float ms_sweeps;      /* the K relaxation sweep launches alone */
-    long long oift_cycles[10]; /* OIFT SM cycles summed over warps: level switch, owner
-                                  tiles, queued tiles, drain (incl. idle); per tile step:
-                                  staging, masks, flood, expansion, faces, pending */
+    long long oift_cycles[16]; /* OIFT SM cycles summed over warps: level switch, owner
+                                  phase, queued tiles, drain; key staging, sparse tiles,
+                                  dense tiles; counts of stale, sparse, dense tiles; dense
+                                  tiles: masks, flood, flood iterations, expansion, faces,
+                                  pending */
     long long relax_active_voxel_sweeps; /* voxels computed over all sweeps (tiles outside
                                             the reference's growing mask are skipped) */
 } oift_b200_stats;

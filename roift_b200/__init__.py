@@ -53,7 +53,7 @@ class Stats(C.Structure):
                 ("nclasses", C.c_int), ("ms_weights", C.c_float), ("ms_oift", C.c_float),
                 ("ms_relax", C.c_float), ("ms_total", C.c_float), ("kernels", C.c_int),
                 ("ms_oift_kernel", C.c_float), ("ms_sweeps", C.c_float),
-                ("oift_cycles", C.c_longlong * 10),
+                ("oift_cycles", C.c_longlong * 16),
                 ("relax_active_voxel_sweeps", C.c_longlong)]
 
     def as_dict(self):

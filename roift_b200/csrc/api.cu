@@ -30,7 +30,7 @@ struct oift_b200_ctx {
     DevBuf img32, img16, W, key, tpend, inq, queue, glob, flag, minmax, seeds, slabels, cost,
         olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8, ctaq, lprof, rtdist;
     size_t total = 0;
-    unsigned long long oift_cycles[10] = {0};
+    unsigned long long oift_cycles[16] = {0};
 };
 
 static thread_local int g_last_status = OIFT_OK;
@@ -447,7 +447,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         st->relax_active_voxel_sweeps = relax_active;
         cudaEventElapsedTime(&st->ms_oift_kernel, c->ev[4], c->ev[5]);
         st->ms_sweeps = 0.0f;
-        for (int i = 0; i < 10; i++) st->oift_cycles[i] = (long long)c->oift_cycles[i];
+        for (int i = 0; i < 16; i++) st->oift_cycles[i] = (long long)c->oift_cycles[i];
         if (want_relax) cudaEventElapsedTime(&st->ms_sweeps, c->ev[6], c->ev[7]);
     }
     return OIFT_OK;

@@ -43,10 +43,11 @@ struct OiftGlobals {
     int levels;
     unsigned long long tile_steps;
     unsigned long long pushes;
-    unsigned long long cycles[10];  // summed warp cycles: level sync, owner phase, queued
-                                    // tiles, drain; then per tile step: staging, masks, flood,
-                                    // expansion, faces, pending
-    unsigned int pad4[6];
+    unsigned long long cycles[16];  // summed warp cycles: level sync, owner phase, queued
+                                    // tiles, drain; key staging, sparse tiles, dense tiles,
+                                    // #stale, #sparse, #dense; dense: masks, flood, flood
+                                    // iterations, expansion, faces, pending
+    unsigned int pad4[26];
 };
 
 

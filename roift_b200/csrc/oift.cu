@@ -299,6 +299,7 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
                 break;
             }
             if (done >= cnt) break;
+
             const int idx = done + lane;
             if (idx < cnt) {
                 const uint32_t li = wl[idx];
@@ -387,6 +388,7 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
             return;
         }
     }
+    long long td0 = clock64();
     // ---- level masks (one ballot per row and arc family) ----
 #pragma unroll 4
     for (int r = 0; r < 32; r++) {
@@ -416,11 +418,15 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         if (lane == r + 1 && ((r % TY) < TY - 1)) cpy = bFY;
         if (TZ > 1 && lane == r + TY) cpz = bFZ;
     }
+    long long td1 = clock64();
+    cyc[6] += td1 - td0;
     // ---- flood of the level inside the tile ----
     const bool ylo = (lane % TY) != 0, yhi = (lane % TY) != TY - 1;
     const bool zlo = lane >= TY, zhi = lane + TY < 32;
     uint32_t F = myF;
+    int flood_it = 0;
     for (int it = 0; it < 2048; it++) {
+        flood_it++;
         uint32_t fym = __shfl_up_sync(FULL, F, 1);
         uint32_t fyp = __shfl_down_sync(FULL, F, 1);
         uint32_t fzm = __shfl_up_sync(FULL, F, TY);
@@ -433,50 +439,52 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         F = nF;
     }
     __syncwarp();
-    // ---- pass 2a: expand the voxels conquered at this level; in-tile targets ----
-    // In-tile tentative keys go to shared memory and to global memory as fire-and-forget
-    // reductions (no return value is awaited).
+    long long td2 = clock64();
+    cyc[7] += td2 - td1;
+    cyc[8] += flood_it;
+    // ---- pass 2a: mark the voxels conquered at this level as expanded and give every open
+    // in-tile voxel outside the flood the best key offered by its flooded neighbours
+    // ("pull": one lane per target, one global update per improved target) ----
+    const uint32_t targets = myOpen & ~F;
     for (int r = 0; r < 32; r++) {
-        const uint32_t ne = __shfl_sync(FULL, F, r);
-        if (ne == 0u) continue;
-        if ((ne >> lane) & 1u) {
-            const int y = y0 + (r % TY), z = z0 + (r / TY);
-            const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+        const uint32_t fr = __shfl_sync(FULL, F, r);
+        const uint32_t tr = __shfl_sync(FULL, targets, r);
+        if ((fr | tr) == 0u) continue;
+        const int y = y0 + (r % TY), z = z0 + (r / TY);
+        const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+        if ((fr >> lane) & 1u) {
             A.key[p] = kexp;
             skey[r * 32 + lane] = kexp;
-#pragma unroll
-            for (int d = 0; d < 6; d++) {
-                int rq = r, xq = lane;
-                uint32_t code;
-                bool tail_low;
-                long long off;
-                if (d == 0) {  // -z
-                    if (!(r >= TY)) continue;
-                    rq = r - TY; code = sw[2048 + rq * 32 + lane]; tail_low = false; off = -(long long)XY;
-                } else if (d == 1) {  // -y
-                    if (!((r % TY) > 0)) continue;
-                    rq = r - 1; code = sw[1024 + rq * 32 + lane]; tail_low = false; off = -(long long)X;
-                } else if (d == 2) {  // -x
-                    if (lane == 0) continue;
-                    xq = lane - 1; code = sw[r * 32 + lane - 1]; tail_low = false; off = -1;
-                } else if (d == 3) {  // +x
-                    if (lane == 31 || x + 1 >= X) continue;
-                    xq = lane + 1; code = sw[r * 32 + lane]; tail_low = true; off = 1;
-                } else if (d == 4) {  // +y
-                    if (!((r % TY) < TY - 1) || y + 1 >= Y) continue;
-                    rq = r + 1; code = sw[1024 + r * 32 + lane]; tail_low = true; off = X;
-                } else {  // +z
-                    if (!((r + TY) < 32) || z + 1 >= Z) continue;
-                    rq = r + TY; code = sw[2048 + r * 32 + lane]; tail_low = true; off = (long long)XY;
-                }
-                const uint32_t nk = arc_key(code, tail_low);
-                if (nk < skey[rq * 32 + xq]) {
-                    atomicMin(&skey[rq * 32 + xq], nk);
-                    atomicMin(&A.key[(size_t)((long long)p + off)], nk);
-                }
+        }
+        if (tr == 0u) continue;
+        const bool hasm_z = r >= TY, hasp_z = r + TY < 32;
+        const bool hasm_y = (r % TY) > 0, hasp_y = (r % TY) < TY - 1;
+        const uint32_t f_mz = __shfl_sync(FULL, F, hasm_z ? r - TY : r);
+        const uint32_t f_pz = __shfl_sync(FULL, F, hasp_z ? r + TY : r);
+        const uint32_t f_my = __shfl_sync(FULL, F, hasm_y ? r - 1 : r);
+        const uint32_t f_py = __shfl_sync(FULL, F, hasp_y ? r + 1 : r);
+        if ((tr >> lane) & 1u) {
+            uint32_t best = OIFT_KEY_INF;
+            if (hasm_z && ((f_mz >> lane) & 1u))
+                best = min(best, arc_key(sw[2048 + (r - TY) * 32 + lane], true));
+            if (hasm_y && ((f_my >> lane) & 1u))
+                best = min(best, arc_key(sw[1024 + (r - 1) * 32 + lane], true));
+            if (lane > 0 && ((fr >> (lane - 1)) & 1u))
+                best = min(best, arc_key(sw[r * 32 + lane - 1], true));
+            if (lane < 31 && ((fr >> (lane + 1)) & 1u))
+                best = min(best, arc_key(sw[r * 32 + lane], false));
+            if (hasp_y && ((f_py >> lane) & 1u))
+                best = min(best, arc_key(sw[1024 + r * 32 + lane], false));
+            if (hasp_z && ((f_pz >> lane) & 1u))
+                best = min(best, arc_key(sw[2048 + r * 32 + lane], false));
+            if (best < skey[r * 32 + lane]) {
+                skey[r * 32 + lane] = best;
+                atomicMin(&A.key[p], best);
             }
         }
     }
+    long long td3 = clock64();
+    cyc[9] += td3 - td2;
     // ---- pass 2b: out-of-tile targets, face by face; the atomics of a face are all
     // issued before their results are examined ----
     {   // -x / +x faces: lane = row
@@ -547,9 +555,12 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         }
     }
     __syncwarp();
+    long long td4 = clock64();
+    cyc[10] += td4 - td3;
     // ---- pass 3: publish re-activations, pending key of this tile ----
     flush_reactivations();
     pending();
+    cyc[11] += clock64() - td4;
     cyc[2] += clock64() - tcount;
     cyc[5] += 1;
 }
@@ -566,7 +577,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
     uint16_t *shz = shx + 32 + 4 * 32;
     __shared__ uint32_t blk_min[OIFT_WARPS];
     __shared__ uint32_t s_level;
-    long long cyc_tile[6] = {0, 0, 0, 0, 0, 0};
+    long long cyc_tile[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     __shared__ uint32_t s_wl[OIFT_WARPS][OIFT_WORKLIST];
     __shared__ int s_wcount[OIFT_WARPS];
     __shared__ uint32_t s_rmask[OIFT_WARPS];
@@ -716,7 +727,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
         atomicAdd(&g->cycles[1], (unsigned long long)cyc_owner);
         atomicAdd(&g->cycles[2], (unsigned long long)cyc_busy);
         atomicAdd(&g->cycles[3], (unsigned long long)cyc_drain);
-        for (int i = 0; i < 6; i++) atomicAdd(&g->cycles[4 + i], (unsigned long long)cyc_tile[i]);
+        for (int i = 0; i < 12; i++) atomicAdd(&g->cycles[4 + i], (unsigned long long)cyc_tile[i]);
     }
 }
 
@@ -864,7 +875,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     if (levels_out) *levels_out = hg.levels;
     if (steps_out) *steps_out = (long long)hg.tile_steps;
     if (cycles_out)
-        for (int i = 0; i < 10; i++) cycles_out[i] = hg.cycles[i];
+        for (int i = 0; i < 16; i++) cycles_out[i] = hg.cycles[i];
     if (hg.error == OIFT_DEV_TIMEOUT) return OIFT_E_NOT_CONVERGED;
     if (hg.error == OIFT_DEV_QUEUE) return OIFT_E_QUEUE_OVERFLOW;
     return OIFT_OK;
