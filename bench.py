@@ -176,6 +176,62 @@ def read_traffic(kernel: str, workload: str):
     return None
 
 
+def run_batch_workload(args):
+    """Configuration 4: 64 int16 volumes (axes from {96..256}), 2-8 seed sets each, 6-adj
+    uint16 gradient weights, alpha ~ U(-0.5, 0.5), 20 sweeps.  Times the per-volume path
+    (one job at a time on the whole GPU) and the batched driver (autotuned lanes)."""
+    import torch
+    import roift_b200 as rb
+    from roift_b200 import synth
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    mix = synth.batch_mix(seed=4, nvol=args.nvol, sweeps=20)
+    keep, jobs_py = [], []
+    for case, sets in mix:
+        img = torch.from_numpy(case.image.copy()).to(dev)
+        keep.append(img)
+        for sd, sl in sets:
+            st = torch.from_numpy(sd).to(dev)
+            lt = torch.from_numpy(sl).to(dev)
+            mask = torch.empty(case.n, dtype=torch.uint8, device=dev)
+            keep += [st, lt, mask]
+            jobs_py.append((case, img, st, lt, mask, len(sd)))
+    jobs = (rb.Job * len(jobs_py))()
+    for i, (case, img, st, lt, mask, ns) in enumerate(jobs_py):
+        Z, Y, X = case.shape
+        jobs[i] = rb.Job(img.data_ptr(), X, Y, Z, st.data_ptr(), lt.data_ptr(), ns,
+                         float(np.float32(case.pol * 100.0)), None, None, mask.data_ptr(), 0)
+    vox = sum(j[0].n for j in jobs_py)
+    common = rb.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=20)
+    ctx = rb.Context(0)
+    ctx.run_batch(common, jobs, lanes=0)            # warm-up; the autotuner picks its lanes
+    tuned = ctx.run_batch(common, jobs, lanes=0).lanes
+    scan = {}
+    for lanes in (1, 2, 4, 8):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.run_batch(common, jobs, lanes=lanes)
+        torch.cuda.synchronize()
+        scan[lanes] = time.perf_counter() - t0
+    per_volume_s = scan[1]
+    batched_s = scan[tuned]
+    out = {"metric": "batched vol/s (config 4: 64-volume mix, OIFT + 20 sweeps per seed set)",
+           "value": args.nvol / batched_s, "unit": "vol/s", "n_gpus": 1,
+           "higher_is_better": True, "data": "synthetic", "dtype": "int32/fp32",
+           "config": {"workload": f"{args.nvol} int16 volumes, axes from {{96..256}}, "
+                                  f"{len(jobs_py)} seed sets, 6-adj uint16 gradient weights, "
+                                  "20 FP32 sweeps", "voxels_per_pass": vox},
+           "jobs": len(jobs_py), "lanes": tuned,
+           "lane_scan_s": {str(k): v for k, v in scan.items()},
+           "per_volume_path": {"s": per_volume_s, "vol_s": args.nvol / per_volume_s,
+                               "gvox_s": vox / per_volume_s / 1e9},
+           "batched": {"s": batched_s, "vol_s": args.nvol / batched_s,
+                       "gvox_s": vox / batched_s / 1e9},
+           "speedup_vs_per_volume": per_volume_s / batched_s}
+    print(json.dumps(out))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -185,6 +241,9 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain-gpu", action="store_true")
+    ap.add_argument("--workload", default="ellipsoid256", choices=["ellipsoid256", "batch64"])
+    ap.add_argument("--nvol", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -194,6 +253,10 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.workload == "batch64":
+        if rank == 0:
+            run_batch_workload(args)
         return
 
     import torch
@@ -313,6 +376,33 @@ def main():
               "oift_gbs": oift_bytes / (ms_oiftk * 1e-3) / 1e9,
               "relax_sweep_gbs": relax_bytes / (ms_sweep * 1e-3) / 1e9}
 
+    # ---- the reference's own plain-GPU OIFT beside our drop-in of the same entry point ----
+    plain = None
+    if rank == 0 and world == 1 and not args.no_plain_gpu:
+        import oracle as O
+        if O.ref_gpu_available():
+            img32 = c.image.astype(np.int32)
+            img32 -= min(0, int(img32.min()))
+            per = float(np.float32(c.pol * 100.0))
+            pc = np.array([-per, per], np.float32)  # bg = -pol (gpu/oiftrelax_fmax_gpu.cpp:146-151)
+            ref_t, ours_t = [], []
+            for i in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                lab_ref, waves = O.ref_oift_fmax_gpu_run(img32, c.seeds, c.seed_labels, pc)
+                ref_t.append(time.perf_counter() - t0)
+                lab = c.label_map()
+                t0 = time.perf_counter()
+                levels = rb.oift_fmax_gpu_run(img32, lab, c.shape[2], c.shape[1], c.shape[0], pc,
+                                              c.seeds)
+                ours_t.append(time.perf_counter() - t0)
+            plain = {"scope": "OIFT only through oift_fmax_gpu_run (host int32 buffers, "
+                              "allocation and copies inside the call)",
+                     "reference_ms": 1e3 * min(ref_t[1:]), "reference_waves": int(waves),
+                     "ours_ms": 1e3 * min(ours_t[1:]), "ours_levels": int(levels),
+                     "speedup": min(ref_t[1:]) / min(ours_t[1:]),
+                     "label_mismatch_voxels": int((lab_ref != lab).sum())}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -334,6 +424,7 @@ def main():
                           "l2": "flushed between timed steps (256 MiB write)"},
                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
                "clocks": clocks, "gpu_launches": sum(s.kernels for s in stats),
+               "plain_gpu_reference": plain,
                "stages": stages}
         print(json.dumps(out))
     ctx.close()

@@ -129,6 +129,38 @@ OIFT_API int oift_b200_run_host(oift_b200_ctx *ctx, const oift_b200_params *prm,
                        int32_t *cost, float *membership, int membership_cap_classes,
                        uint8_t *mask, oift_b200_stats *stats);
 
+/* One job of the batched driver: a volume and one seed set (device pointers). */
+typedef struct {
+    const int16_t *image;
+    int xsize, ysize, zsize;
+    const int32_t *seeds, *seed_labels;
+    int nseeds;
+    float per;          /* polarity x100 of this job (global mode) */
+    int32_t *cost;      /* device outputs, each may be NULL */
+    int32_t *label;
+    uint8_t *mask;
+    int status;         /* out: oift_status of this job */
+} oift_b200_job;
+
+typedef struct {
+    int lanes;          /* concurrent lanes used for the timed part */
+    int jobs;
+    int tuned_jobs;     /* jobs run while the autotuner measured lane counts */
+    float ms_wall;      /* host wall time of the jobs after tuning */
+} oift_b200_batch_stats;
+
+/* Batched driver (configuration-4 style work: many volumes of uneven sizes, several seed
+ * sets per volume).  Runs the full pipeline of `common` (adjacency, weights, sweeps) for
+ * every job; jobs run concurrently on `lanes` GPU partitions, each with its own stream,
+ * scratch and a persistent OIFT grid of sms/lanes CTAs.  lanes = 0 lets an autotuner
+ * measure 1, 2, 4 and 8 lanes on the first jobs (once per context) and keep the fastest.
+ * Returns the first failing job status, OIFT_OK otherwise. */
+OIFT_API int oift_b200_run_batch(oift_b200_ctx *ctx, const oift_b200_params *common,
+                                 oift_b200_job *jobs, int njobs, int lanes,
+                                 oift_b200_batch_stats *stats);
+/* CTAs of the persistent OIFT grid of this context (0 = one per SM, the default). */
+OIFT_API int oift_b200_set_oift_grid(oift_b200_ctx *ctx, int ctas);
+
 /* Stage entry points on device pointers (used by the batched driver and tests). */
 OIFT_API int oift_b200_build_weights_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
                                 const int16_t *image, uint16_t *weights /* [planes][N] */,

@@ -15,6 +15,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgft_ref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "liboift_fmax_ref.so")
 REF_SRC = "/root/reference"
 
 NIL = -1
@@ -33,6 +34,8 @@ def build(with_ref: bool | None = None) -> None:
         with_ref = os.path.isdir(REF_SRC)
     if with_ref:
         subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+        if os.path.exists("/usr/local/cuda/bin/nvcc"):
+            subprocess.run(["make", "-s", "-C", HERE, "refgpu"], check=True)
 
 
 class _Polarity(C.Structure):
@@ -260,6 +263,38 @@ def ref_ift_fmax(img, adj, seeds, seed_labels):
     cost = np.empty(N, np.int32)
     ref().ref_ift_fmax_graph(as_i32(img), X, Y, Z, adj, seeds, len(seeds), lab, cost)
     return cost, lab
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+def ref_oift_fmax_gpu_run(img, seeds, seed_labels, per_class):
+    """The reference's own plain-GPU f_max OIFT (gpu/oift_fmax_gpu.cu:139-259) compiled for
+    sm_100a.  Returns (labels, waves).  Its labels depend on arrival order."""
+    L = C.CDLL(REF_GPU_SO)
+    L.oift_fmax_gpu_run.argtypes = [_i32p, _i32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
+                                    C.c_int, _i32p, C.c_int]
+    X, Y, Z = _dims(img)
+    N = X * Y * Z
+    lab = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    pc = np.ascontiguousarray(per_class, np.float32)
+    im = as_i32(img)
+    # the reference prints its wave progress on stdout; keep it off the caller's stdout
+    import sys
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    try:
+        os.dup2(devnull, 1)
+        waves = L.oift_fmax_gpu_run(im, lab, N, X, Y, Z, pc, len(pc) - 1, seeds, len(seeds))
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    return lab, waves
 
 
 def ref_gaussian_blur(img):

@@ -62,12 +62,26 @@ class Stats(C.Structure):
         return d
 
 
+class Job(C.Structure):
+    """oift_b200_job: one (volume, seed set) of the batched driver (device pointers)."""
+    _fields_ = [("image", C.c_void_p), ("xsize", C.c_int), ("ysize", C.c_int),
+                ("zsize", C.c_int), ("seeds", C.c_void_p), ("seed_labels", C.c_void_p),
+                ("nseeds", C.c_int), ("per", C.c_float), ("cost", C.c_void_p),
+                ("label", C.c_void_p), ("mask", C.c_void_p), ("status", C.c_int)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("lanes", C.c_int), ("jobs", C.c_int), ("tuned_jobs", C.c_int),
+                ("ms_wall", C.c_float)]
+
+
 EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_set_stream", "oift_b200_status_string", "oift_b200_run_device_i16",
            "oift_b200_run_host", "oift_b200_build_weights_i16", "oift_b200_weight_planes",
            "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status",
            "oift_b200_level_profile", "oift_b200_selftest_div100",
-           "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes"]
+           "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes",
+           "oift_b200_run_batch", "oift_b200_set_oift_grid"]
 
 _lib = None
 
@@ -92,6 +106,9 @@ def lib():
         L.oift_b200_run_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
                                          vp, vp, C.c_int, vp, C.POINTER(Stats)]
         L.oift_b200_level_profile.argtypes = [vp, vp, C.c_int]
+        L.oift_b200_run_batch.argtypes = [vp, C.POINTER(Params), C.POINTER(Job), C.c_int, C.c_int,
+                                          C.POINTER(BatchStats)]
+        L.oift_b200_set_oift_grid.argtypes = [vp, C.c_int]
         L.oift_b200_selftest_div100.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]
         L.oift_b200_oift_noalloc.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_int, C.c_float, vp, C.c_int, vp, vp, C.c_int,
@@ -200,6 +217,21 @@ class Context:
         if memb is not None:
             memb = memb[: st.nclasses * N].reshape(st.nclasses, N)
         return lab, cost, memb, mask, st
+
+    def run_batch(self, params, jobs, lanes=0) -> BatchStats:
+        """Batched driver: `jobs` is a ctypes array of Job (device pointers); lanes = 0
+        autotunes the number of concurrent GPU partitions."""
+        st = BatchStats()
+        rc = lib().oift_b200_run_batch(self._h, C.byref(params), jobs, len(jobs), int(lanes),
+                                       C.byref(st))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_run_batch")
+        return st
+
+    def set_oift_grid(self, ctas: int):
+        rc = lib().oift_b200_set_oift_grid(self._h, int(ctas))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_set_oift_grid")
 
     def level_profile(self, cap=8192):
         """(cycles, tile activations) per OIFT level of the last run."""

@@ -8,7 +8,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -23,6 +26,9 @@ struct DevBuf {
 struct oift_b200_ctx {
     int device = 0;
     int sms = 148;
+    int oift_ctas = 0;  // CTAs of the persistent OIFT grid (0 = one per SM)
+    std::vector<oift_b200_ctx *> lanes;  // sub-contexts of the batched driver
+    int tuned_lanes = 0;                 // lane count chosen by the batch autotuner
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev[8];
@@ -114,6 +120,8 @@ int oift_b200_create(oift_b200_ctx **out, int device) {
 
 int oift_b200_destroy(oift_b200_ctx *c) {
     if (!c) return OIFT_E_BAD_ARG;
+    for (oift_b200_ctx *l : c->lanes) oift_b200_destroy(l);
+    c->lanes.clear();
     cudaSetDevice(c->device);
     DevBuf *bufs[] = {&c->img32, &c->img16,  &c->W,      &c->key,     &c->tpend,   &c->inq,
                       &c->queue, &c->glob,   &c->flag,   &c->minmax,  &c->seeds,   &c->slabels,
@@ -129,6 +137,12 @@ int oift_b200_destroy(oift_b200_ctx *c) {
 }
 
 size_t oift_b200_scratch_bytes(const oift_b200_ctx *c) { return c ? c->total : 0; }
+
+int oift_b200_set_oift_grid(oift_b200_ctx *c, int ctas) {
+    if (!c || ctas < 0) return OIFT_E_BAD_ARG;
+    c->oift_ctas = ctas;
+    return OIFT_OK;
+}
 
 int oift_b200_set_stream(oift_b200_ctx *c, void *stream) {
     if (!c) return OIFT_E_BAD_ARG;
@@ -216,7 +230,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
     TRY(grow(c, c->key, N * sizeof(uint32_t)));
     TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
-    TRY(grow(c, c->queue, oift_mbox_bytes(plan, c->sms)));
+    const int octas = (c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms;
+    TRY(grow(c, c->queue, oift_mbox_bytes(plan, octas)));
     TRY(grow(c, c->glob, oift_globals_bytes()));
     TRY(grow(c, c->flag, 4 * sizeof(int)));
     TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
@@ -293,7 +308,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     long long steps = 0;
     int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
                       (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
-                      c->sms, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles);
+                      octas, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles);
     if (rc != OIFT_OK) return rc;
     unsigned long long hclamp = 0;
     CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));
@@ -636,6 +651,113 @@ int oift_fmax_gpu_run(const int *h_image, int *h_labels, int n, int xsize, int y
                                 nullptr, 0, nullptr, &st);
     g_last_status = rc;
     return rc == OIFT_OK ? st.levels : -1;
+}
+
+
+// ----------------------------------------------------------------- batched driver ----
+// Jobs (volume, seed set) run concurrently on `lanes` partitions of the GPU: each lane is a
+// sub-context with its own stream and scratch whose persistent OIFT grid has sms/lanes
+// CTAs, so that several latency-bound OIFT launches are resident at once; relaxation
+// sweeps of all lanes share the whole device.  One host thread per lane pulls the next
+// job index from a shared counter.
+static int ensure_lanes(oift_b200_ctx *c, int lanes) {
+    while ((int)c->lanes.size() < lanes) {
+        oift_b200_ctx *l = nullptr;
+        int rc = oift_b200_create(&l, c->device);
+        if (rc != OIFT_OK) return rc;
+        c->lanes.push_back(l);
+    }
+    for (int i = 0; i < lanes; i++) c->lanes[i]->oift_ctas = c->sms / lanes;
+    return OIFT_OK;
+}
+
+static int run_jobs(oift_b200_ctx *c, const oift_b200_params *common, oift_b200_job *jobs,
+                    int first, int count, int lanes, double *wall_ms) {
+    int rc = ensure_lanes(c, lanes);
+    if (rc != OIFT_OK) return rc;
+    std::atomic<int> next(first);
+    const int end = first + count;
+    auto worker = [&](int lane) {
+        cudaSetDevice(c->device);
+        oift_b200_ctx *l = c->lanes[lane];
+        for (;;) {
+            const int j = next.fetch_add(1);
+            if (j >= end) break;
+            oift_b200_job &job = jobs[j];
+            oift_b200_params p = *common;
+            p.xsize = job.xsize;
+            p.ysize = job.ysize;
+            p.zsize = job.zsize;
+            p.per = job.per;
+            p.per_class = nullptr;
+            p.max_label = 0;
+            int st = check_params(&p);
+            if (st == OIFT_OK && job.nseeds <= 0) st = OIFT_E_NO_SEEDS;
+            if (st == OIFT_OK) {
+                oift_b200_outputs o{};
+                o.cost = job.cost;
+                o.label = job.label;
+                o.mask = job.mask;
+                if (!o.label && !o.mask) o.oift_label = nullptr;
+                st = run_pipeline<int16_t>(l, &p, job.image, job.seeds, job.seed_labels,
+                                           job.nseeds, &o, nullptr);
+            }
+            job.status = st;
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> ths;
+    for (int i = 0; i < lanes; i++) ths.emplace_back(worker, i);
+    for (auto &t : ths) t.join();
+    const auto t1 = std::chrono::steady_clock::now();
+    if (wall_ms) *wall_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    for (int j = first; j < end; j++)
+        if (jobs[j].status != OIFT_OK) return jobs[j].status;
+    return OIFT_OK;
+}
+
+int oift_b200_run_batch(oift_b200_ctx *c, const oift_b200_params *common, oift_b200_job *jobs,
+                        int njobs, int lanes, oift_b200_batch_stats *stats) {
+    if (!c || !common || !jobs || njobs < 0 || lanes < 0 || lanes > 16) return OIFT_E_BAD_ARG;
+    if (njobs == 0) return OIFT_OK;
+    cudaSetDevice(c->device);
+    int first = 0;
+    if (lanes == 0) {
+        // autotune once per context: time each candidate lane count on a few jobs (those
+        // jobs are then done) and keep the fastest in voxels per second
+        if (c->tuned_lanes == 0) {
+            const int cands[] = {1, 2, 4, 8};
+            double best = -1.0;
+            int best_l = 1;
+            for (int ci = 0; ci < 4 && first < njobs; ci++) {
+                const int l = cands[ci];
+                const int cnt = std::min(njobs - first, 2 * l);
+                double ms = 0;
+                int rc = run_jobs(c, common, jobs, first, cnt, l, &ms);
+                if (rc != OIFT_OK) return rc;
+                double vox = 0;
+                for (int j = first; j < first + cnt; j++)
+                    vox += (double)jobs[j].xsize * jobs[j].ysize * jobs[j].zsize;
+                const double rate = vox / std::max(ms, 1e-3);
+                if (rate > best) {
+                    best = rate;
+                    best_l = l;
+                }
+                first += cnt;
+            }
+            c->tuned_lanes = best_l;
+        }
+        lanes = c->tuned_lanes;
+    }
+    double ms = 0;
+    int rc = run_jobs(c, common, jobs, first, njobs - first, lanes, &ms);
+    if (stats) {
+        stats->lanes = lanes;
+        stats->jobs = njobs;
+        stats->tuned_jobs = first;
+        stats->ms_wall = (float)ms;
+    }
+    return rc;
 }
 
 }  // extern "C"

@@ -63,14 +63,15 @@ __device__ __forceinline__ unsigned long long vload(const volatile unsigned long
     return *p;
 }
 
-// Grid barrier for the cooperative launch, with a bounded wait.
-__device__ bool grid_barrier(OiftGlobals *g, long long limit) {
+// Barrier over the `nctas` CTAs that share `g` (the whole cooperative grid, or one team of
+// the batched kernel), with a bounded wait.
+__device__ bool team_barrier(OiftGlobals *g, long long limit, unsigned int nctas) {
     __syncthreads();
     bool ok = true;
     if (threadIdx.x == 0) {
         unsigned int gen = vload(&g->bar_gen);
         __threadfence();
-        if (atomicAdd(&g->bar_count, 1u) == gridDim.x - 1) {
+        if (atomicAdd(&g->bar_count, 1u) == nctas - 1) {
             g->bar_count = 0;
             __threadfence();
             atomicAdd(&g->bar_gen, 1u);
@@ -222,15 +223,15 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         const int yr = y0 + (lane % TY), zr = z0 + (lane / TY);
         uint16_t hx = 0, hy[TZ], hz[TY];
         if (x0 > 0 && yr < Y && zr < Z)
-            hx = __ldg(&A.W[(size_t)(x0 - 1) + (size_t)yr * X + (size_t)zr * XY]);
+            hx = __ldcg(&A.W[(size_t)(x0 - 1) + (size_t)yr * X + (size_t)zr * XY]);
 #pragma unroll
         for (int zl = 0; zl < TZ; zl++)
             hy[zl] = (y0 > 0 && x < X && z0 + zl < Z)
-                ? __ldg(&A.W[N + (size_t)x + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY]) : 0;
+                ? __ldcg(&A.W[N + (size_t)x + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY]) : 0;
 #pragma unroll
         for (int yl = 0; yl < TY; yl++)
             hz[yl] = (TZ > 1 && has_z && z0 > 0 && x < X && y0 + yl < Y)
-                ? __ldg(&A.W[2 * N + (size_t)x + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY]) : 0;
+                ? __ldcg(&A.W[2 * N + (size_t)x + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY]) : 0;
         if (full) {
             uint4 cv[12];
 #pragma unroll
@@ -239,7 +240,7 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
                 const size_t p0 =
                     (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
                 if (pl < 2 || has_z)
-                    cv[m] = __ldg(reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
+                    cv[m] = __ldcg(reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
                 else
                     cv[m] = make_uint4(0, 0, 0, 0);
             }
@@ -250,9 +251,9 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
                 const int y = y0 + (r % TY), z = z0 + (r / TY);
                 const bool valid = (x < X) && (y < Y) && (z < Z);
                 const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
-                sw[r * 32 + lane] = valid ? __ldg(&A.W[p]) : 0;
-                sw[1024 + r * 32 + lane] = valid ? __ldg(&A.W[N + p]) : 0;
-                sw[2048 + r * 32 + lane] = (valid && has_z) ? __ldg(&A.W[2 * N + p]) : 0;
+                sw[r * 32 + lane] = valid ? __ldcg(&A.W[p]) : 0;
+                sw[1024 + r * 32 + lane] = valid ? __ldcg(&A.W[N + p]) : 0;
+                sw[2048 + r * 32 + lane] = (valid && has_z) ? __ldcg(&A.W[2 * N + p]) : 0;
             }
         }
         shx[lane] = hx;
@@ -565,9 +566,20 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
     cyc[5] += 1;
 }
 
+// Shared-memory working set of one CTA of the persistent kernels.
+struct OiftCtaSmem {
+    uint32_t blk_min[OIFT_WARPS];
+    uint32_t level;
+    uint32_t wl[OIFT_WARPS][OIFT_WORKLIST];
+    int wcount[OIFT_WARPS];
+    uint32_t rmask[OIFT_WARPS];
+};
+
+// The level loop of one OIFT job, run by the `team_ctas` CTAs starting at team CTA index
+// `team_cta` (0 .. team_ctas-1).  A.nwarps must equal team_ctas * OIFT_WARPS.
 template <int TY, int TZ>
-__global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(OiftArgs A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftCtaSmem &cs,
+                           unsigned char *smem_raw) {
     const unsigned FULL = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *skey = reinterpret_cast<uint32_t *>(smem_raw) + warp * 1024;
@@ -575,21 +587,17 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
     uint16_t *shx = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * (4096 + 6144)) + warp * 416;
     uint16_t *shy = shx + 32;
     uint16_t *shz = shx + 32 + 4 * 32;
-    __shared__ uint32_t blk_min[OIFT_WARPS];
-    __shared__ uint32_t s_level;
+    uint32_t *blk_min = cs.blk_min;
     long long cyc_tile[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    __shared__ uint32_t s_wl[OIFT_WARPS][OIFT_WORKLIST];
-    __shared__ int s_wcount[OIFT_WARPS];
-    __shared__ uint32_t s_rmask[OIFT_WARPS];
-    uint32_t *rmask = &s_rmask[warp];
+    uint32_t *rmask = &cs.rmask[warp];
     if (lane == 0) *rmask = 0u;
     __syncwarp();
-    uint32_t *wl = s_wl[warp];
-    int *wcount = &s_wcount[warp];
+    uint32_t *wl = cs.wl[warp];
+    int *wcount = &cs.wcount[warp];
     OiftGlobals *g = A.g;
-    const int gwarp = blockIdx.x * OIFT_WARPS + warp;
-    const int nwarps = gridDim.x * OIFT_WARPS;
-
+    const int gwarp = team_cta * OIFT_WARPS + warp;
+    const int nwarps = team_ctas * OIFT_WARPS;
+    const bool leader_cta = team_cta == 0;
     uint32_t prev_level = 0;
     long long lvl_t0 = 0;
     long long cyc_levelsync = 0, cyc_owner = 0, cyc_busy = 0, cyc_drain = 0;
@@ -612,22 +620,22 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
             uint32_t bm = blk_min[0];
             for (int w = 1; w < OIFT_WARPS; w++) bm = blk_min[w] < bm ? blk_min[w] : bm;
             if (bm != OIFT_KEY_INF) atomicMin(&g->nextmin[par], bm);
-            if (blockIdx.x == 0) {
+            if (leader_cta) {
                 g->outstanding[par] = nwarps;
                 g->nextmin[par ^ 1] = OIFT_KEY_INF;
             }
         }
-        grid_barrier(g, A.spin_limit);
-        if (blockIdx.x == 0 && threadIdx.x == 0 && A.lprof && e > 0 && e - 1 < A.lprof_cap) {
+        team_barrier(g, A.spin_limit, team_ctas);
+        if (leader_cta && threadIdx.x == 0 && A.lprof && e > 0 && e - 1 < A.lprof_cap) {
             const long long now = clock64();
             A.lprof[2 * (e - 1)] = (unsigned int)min(now - lvl_t0, 0xffffffffll);
             lvl_t0 = now;
-        } else if (blockIdx.x == 0 && threadIdx.x == 0 && e == 0) {
+        } else if (leader_cta && threadIdx.x == 0 && e == 0) {
             lvl_t0 = clock64();
         }
-        if (threadIdx.x == 0) s_level = vload(&g->nextmin[par]);
+        if (threadIdx.x == 0) cs.level = vload(&g->nextmin[par]);
         __syncthreads();
-        const uint32_t kk = s_level;
+        const uint32_t kk = cs.level;
         if (kk == OIFT_KEY_INF || vload(&g->error)) break;
         // levels strictly increase; a repeat or a runaway level count is a fault
         if ((e > 0 && kk <= prev_level) || e >= A.max_levels) {
@@ -635,7 +643,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
             break;
         }
         prev_level = kk;
-        if (blockIdx.x == 0 && threadIdx.x == 0) g->levels = e + 1;
+        if (leader_cta && threadIdx.x == 0) g->levels = e + 1;
         const int c = key_cost(kk), l = key_label(kk);
         const double per = (double)polarity_of(A, l);
         const double fgt = 1.0 + per / 100.0, flt = 1.0 - per / 100.0;
@@ -729,6 +737,13 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
         atomicAdd(&g->cycles[3], (unsigned long long)cyc_drain);
         for (int i = 0; i < 12; i++) atomicAdd(&g->cycles[4 + i], (unsigned long long)cyc_tile[i]);
     }
+}
+
+template <int TY, int TZ>
+__global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(OiftArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ OiftCtaSmem cs;
+    oift_solve<TY, TZ>(A, blockIdx.x, gridDim.x, cs, smem_raw);
 }
 
 __global__ void oift_seed_kernel(uint32_t *key, uint32_t *tpend, const int32_t *seeds,

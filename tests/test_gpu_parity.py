@@ -187,3 +187,46 @@ def test_relax_tile_skipping_exact(roift, oracle_lib, size):
     assert np.array_equal(lab, lab32)
     tiles = ((X + 31) // 32) * ((Y + 7) // 8) * ((Z + 3) // 4)
     assert st.relax_active_voxel_sweeps < 0.8 * K * tiles * 1024
+
+
+def _batch_jobs(rb, cases, torch, dev):
+    bufs, jobs = [], (rb.Job * len(cases))()
+    for i, c in enumerate(cases):
+        img = torch.from_numpy(c.image.astype(np.int16)).to(dev)
+        sd = torch.from_numpy(c.seeds).to(dev)
+        sl = torch.from_numpy(c.seed_labels).to(dev)
+        lab = torch.full((c.n,), -5, dtype=torch.int32, device=dev)
+        mask = torch.zeros(c.n, dtype=torch.uint8, device=dev)
+        Z, Y, X = c.shape
+        jobs[i] = rb.Job(img.data_ptr(), X, Y, Z, sd.data_ptr(), sl.data_ptr(), len(c.seeds),
+                         float(np.float32(c.pol * 100.0)), None, lab.data_ptr(), mask.data_ptr(), 0)
+        bufs.append((img, sd, sl, lab, mask))
+    return jobs, bufs
+
+
+@pytest.mark.parametrize("lanes", [1, 3, 0])
+def test_batch_matches_single_runs(roift, lanes):
+    """Concurrent lanes (and the autotuner, lanes=0) give the labels of one-at-a-time runs."""
+    import torch
+    dev = torch.device("cuda:0")
+    cases = []
+    for i, size in enumerate([40, 56, 48, 64, 40, 52]):
+        c = synth.ellipsoid3d(seed=20 + i, size=size, sweeps=6, pol=[-0.3, 0.2, 0.4][i % 3])
+        cases.append(c)
+    p = roift.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=6)
+    jobs, bufs = _batch_jobs(roift, cases, torch, dev)
+    ctx = roift.Context(0)
+    st = ctx.run_batch(p, jobs, lanes=lanes)
+    torch.cuda.synchronize()
+    assert st.jobs == len(cases)
+    for c, (img, sd, sl, lab, mask), job in zip(cases, bufs, jobs):
+        assert job.status == 0
+        single = roift.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095,
+                                   pol=c.pol, sweeps=6)
+        lab1 = torch.empty(c.n, dtype=torch.int32, device=dev)
+        roift._ctx().run_device(single, img.data_ptr(), sd.data_ptr(), sl.data_ptr(),
+                                len(c.seeds), label=lab1.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(lab, lab1)
+        assert torch.equal(mask, (lab1 != 0).to(torch.uint8))
+    ctx.close()
