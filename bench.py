@@ -177,9 +177,10 @@ def read_traffic(kernel: str, workload: str):
 
 
 def run_batch_workload(args):
-    """Configuration 4: 64 int16 volumes (axes from {96..256}), 2-8 seed sets each, 6-adj
-    uint16 gradient weights, alpha ~ U(-0.5, 0.5), 20 sweeps.  Times the per-volume path
-    (one job at a time on the whole GPU) and the batched driver (autotuned lanes)."""
+    """Many-volume batch: `nvol` int16 volumes (axes from {96..256}), 2-8 seed sets each,
+    6-adj uint16 gradient weights, alpha ~ U(-0.5, 0.5), 20 sweeps, a mask per seed set.
+    Times the per-volume path (run_device on one job at a time, whole GPU) and the batched
+    driver (team-batched OIFT) at its autotuned and at each scanned team count."""
     import torch
     import roift_b200 as rb
     from roift_b200 import synth
@@ -204,31 +205,48 @@ def run_batch_workload(args):
     vox = sum(j[0].n for j in jobs_py)
     common = rb.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=20)
     ctx = rb.Context(0)
-    ctx.run_batch(common, jobs, lanes=0)            # warm-up; the autotuner picks its lanes
-    tuned = ctx.run_batch(common, jobs, lanes=0).lanes
-    scan = {}
-    for lanes in (1, 2, 4, 8):
+    ctx.run_batch(common, jobs, teams=0)            # warm-up; the autotuner picks its teams
+    tuned = ctx.run_batch(common, jobs, teams=0).teams
+
+    def timed(fn):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ctx.run_batch(common, jobs, lanes=lanes)
+        r = fn()
         torch.cuda.synchronize()
-        scan[lanes] = time.perf_counter() - t0
-    per_volume_s = scan[1]
-    batched_s = scan[tuned]
-    out = {"metric": "batched vol/s (config 4: 64-volume mix, OIFT + 20 sweeps per seed set)",
+        return time.perf_counter() - t0, r
+
+    scan, parts = {}, {}
+    for teams in [int(t) for t in args.team_scan.split(",")]:
+        scan[teams], st = timed(lambda: ctx.run_batch(common, jobs, teams=teams))
+        parts[teams] = {"oift_ms": st.ms_oift, "relax_ms": st.ms_relax}
+    batched_s, _ = timed(lambda: ctx.run_batch(common, jobs, teams=tuned))
+    # the per-volume path: the single-volume API, one job after the other on the whole GPU
+    single = rb.Context(0)
+
+    def per_volume():
+        for case, img, st, lt, mask, ns in jobs_py:
+            prm = rb.make_params(case.shape, adjacency=6, weight_mode="grad_q", wq=4095,
+                                 pol=case.pol, sweeps=20)
+            single.run_device(prm, img.data_ptr(), st.data_ptr(), lt.data_ptr(), ns,
+                              mask=mask.data_ptr())
+    per_volume()                                     # warm-up (scratch growth)
+    per_volume_s, _ = timed(per_volume)
+    out = {"metric": "batched vol/s (64-volume mix, OIFT + 20 sweeps per seed set)",
            "value": args.nvol / batched_s, "unit": "vol/s", "n_gpus": 1,
            "higher_is_better": True, "data": "synthetic", "dtype": "int32/fp32",
            "config": {"workload": f"{args.nvol} int16 volumes, axes from {{96..256}}, "
                                   f"{len(jobs_py)} seed sets, 6-adj uint16 gradient weights, "
                                   "20 FP32 sweeps", "voxels_per_pass": vox},
-           "jobs": len(jobs_py), "lanes": tuned,
-           "lane_scan_s": {str(k): v for k, v in scan.items()},
+           "jobs": len(jobs_py), "teams": tuned,
+           "team_scan_s": {str(k): v for k, v in scan.items()},
+           "team_scan_parts_ms": {str(k): v for k, v in parts.items()},
            "per_volume_path": {"s": per_volume_s, "vol_s": args.nvol / per_volume_s,
                                "gvox_s": vox / per_volume_s / 1e9},
            "batched": {"s": batched_s, "vol_s": args.nvol / batched_s,
                        "gvox_s": vox / batched_s / 1e9},
            "speedup_vs_per_volume": per_volume_s / batched_s}
     print(json.dumps(out))
+    single.close()
     ctx.close()
 
 
@@ -243,6 +261,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain-gpu", action="store_true")
     ap.add_argument("--workload", default="ellipsoid256", choices=["ellipsoid256", "batch64"])
+    ap.add_argument("--team-scan", default="1,2,4,8,16,32,64",
+                    help="team counts timed by the batch64 workload")
     ap.add_argument("--nvol", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -137,26 +137,30 @@ typedef struct {
     int nseeds;
     float per;          /* polarity x100 of this job (global mode) */
     int32_t *cost;      /* device outputs, each may be NULL */
-    int32_t *label;
+    int32_t *label;     /* final (relaxed) labels */
     uint8_t *mask;
     int status;         /* out: oift_status of this job */
 } oift_b200_job;
 
 typedef struct {
-    int lanes;          /* concurrent lanes used for the timed part */
+    int teams;          /* OIFT teams of the timed part */
     int jobs;
-    int tuned_jobs;     /* jobs run while the autotuner measured lane counts */
+    int tuned_jobs;     /* jobs run while the autotuner measured team counts */
     float ms_wall;      /* host wall time of the jobs after tuning */
+    float ms_oift;      /* device time of weights + batched OIFT */
+    float ms_relax;     /* host wall time of the relaxation phase */
 } oift_b200_batch_stats;
 
-/* Batched driver (configuration-4 style work: many volumes of uneven sizes, several seed
- * sets per volume).  Runs the full pipeline of `common` (adjacency, weights, sweeps) for
- * every job; jobs run concurrently on `lanes` GPU partitions, each with its own stream,
- * scratch and a persistent OIFT grid of sms/lanes CTAs.  lanes = 0 lets an autotuner
- * measure 1, 2, 4 and 8 lanes on the first jobs (once per context) and keep the fastest.
- * Returns the first failing job status, OIFT_OK otherwise. */
+/* Batched driver for many volumes of uneven sizes with several seed sets per volume.  Runs
+ * the pipeline of `common` (adjacency 6 or 4, weights, sweeps; the job gives extents and
+ * polarity) for every job.  Edge codes are built once per distinct image; the OIFT of all
+ * jobs runs in one persistent launch split into `teams` teams of sms/teams CTAs, each team
+ * taking the next job (largest first) from a device counter; relaxation then runs on
+ * several streams.  teams = 0 lets an autotuner measure 1, 2, 4, ..., 64 teams on the
+ * first jobs (once per context) and keep the fastest.  Writes each job's status; returns
+ * the first failing one, OIFT_OK otherwise. */
 OIFT_API int oift_b200_run_batch(oift_b200_ctx *ctx, const oift_b200_params *common,
-                                 oift_b200_job *jobs, int njobs, int lanes,
+                                 oift_b200_job *jobs, int njobs, int teams,
                                  oift_b200_batch_stats *stats);
 /* CTAs of the persistent OIFT grid of this context (0 = one per SM, the default). */
 OIFT_API int oift_b200_set_oift_grid(oift_b200_ctx *ctx, int ctas);

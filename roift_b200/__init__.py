@@ -26,6 +26,8 @@ NIL = -1
 OK = 0
 STATUS = {0: "OK", -1: "BAD_ARG", -2: "NO_SEEDS", -3: "OOM", -4: "NOT_CONVERGED",
           -5: "QUEUE_OVERFLOW", -6: "CUDA", -7: "RANGE", -8: "UNSUPPORTED", -9: "SEED_RANGE"}
+E_BAD_ARG, E_NO_SEEDS, E_OOM, E_NOT_CONVERGED, E_QUEUE_OVERFLOW = -1, -2, -3, -4, -5
+E_CUDA, E_RANGE, E_UNSUPPORTED, E_SEED_RANGE = -6, -7, -8, -9
 W_MODES = {"grad": 0, "grad_q": 1, "rbf_q": 2, "blend_q": 3}
 
 
@@ -71,8 +73,8 @@ class Job(C.Structure):
 
 
 class BatchStats(C.Structure):
-    _fields_ = [("lanes", C.c_int), ("jobs", C.c_int), ("tuned_jobs", C.c_int),
-                ("ms_wall", C.c_float)]
+    _fields_ = [("teams", C.c_int), ("jobs", C.c_int), ("tuned_jobs", C.c_int),
+                ("ms_wall", C.c_float), ("ms_oift", C.c_float), ("ms_relax", C.c_float)]
 
 
 EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
@@ -218,11 +220,11 @@ class Context:
             memb = memb[: st.nclasses * N].reshape(st.nclasses, N)
         return lab, cost, memb, mask, st
 
-    def run_batch(self, params, jobs, lanes=0) -> BatchStats:
-        """Batched driver: `jobs` is a ctypes array of Job (device pointers); lanes = 0
-        autotunes the number of concurrent GPU partitions."""
+    def run_batch(self, params, jobs, teams=0) -> BatchStats:
+        """Batched driver: `jobs` is a ctypes array of Job (device pointers); teams = 0
+        autotunes the number of OIFT teams the GPU is split into."""
         st = BatchStats()
-        rc = lib().oift_b200_run_batch(self._h, C.byref(params), jobs, len(jobs), int(lanes),
+        rc = lib().oift_b200_run_batch(self._h, C.byref(params), jobs, len(jobs), int(teams),
                                        C.byref(st))
         if rc != OK:
             raise OiftError(rc, "oift_b200_run_batch")

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <mutex>
@@ -27,14 +28,17 @@ struct oift_b200_ctx {
     int device = 0;
     int sms = 148;
     int oift_ctas = 0;  // CTAs of the persistent OIFT grid (0 = one per SM)
-    std::vector<oift_b200_ctx *> lanes;  // sub-contexts of the batched driver
-    int tuned_lanes = 0;                 // lane count chosen by the batch autotuner
+    std::vector<oift_b200_ctx *> lanes;  // sub-contexts (relaxation streams) of the batched driver
+    int tuned_teams = 0;                 // team count chosen by the batch autotuner
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev[8];
     // scratch (grow-only)
     DevBuf img32, img16, W, key, tpend, inq, queue, glob, flag, minmax, seeds, slabels, cost,
         olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8, ctaq, lprof, rtdist;
+    // batched driver: job descriptors, per-image min/max + clamp counters, per-team OIFT
+    // state, job counter + abort flag, OIFT labels of jobs that only want a mask
+    DevBuf bjobs, bmm, bkey, btpend, bmbox, bglob, bctl, bolab;
     size_t total = 0;
     unsigned long long oift_cycles[16] = {0};
 };
@@ -127,7 +131,8 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->queue, &c->glob,   &c->flag,   &c->minmax,  &c->seeds,   &c->slabels,
                       &c->cost,  &c->olabel, &c->flabel, &c->memb,    &c->seedc,   &c->l2c,
                       &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8, &c->ctaq,
-                      &c->lprof, &c->rtdist};
+                      &c->lprof, &c->rtdist, &c->bjobs, &c->bmm,  &c->bkey,  &c->btpend,
+                      &c->bmbox, &c->bglob, &c->bctl, &c->bolab};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -136,7 +141,12 @@ int oift_b200_destroy(oift_b200_ctx *c) {
     return OIFT_OK;
 }
 
-size_t oift_b200_scratch_bytes(const oift_b200_ctx *c) { return c ? c->total : 0; }
+size_t oift_b200_scratch_bytes(const oift_b200_ctx *c) {
+    if (!c) return 0;
+    size_t t = c->total;
+    for (const oift_b200_ctx *l : c->lanes) t += l->total;
+    return t;
+}
 
 int oift_b200_set_oift_grid(oift_b200_ctx *c, int ctas) {
     if (!c || ctas < 0) return OIFT_E_BAD_ARG;
@@ -213,6 +223,155 @@ static int upload_polarity(oift_b200_ctx *c, const oift_b200_params *p, int *npo
     CU(cudaMemcpyAsync(c->pol.p, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice,
                        c->stream));
     *npol = (int)t.size();
+    return OIFT_OK;
+}
+
+struct RelaxResult {
+    int nclasses = 0;
+    long long active_voxel_sweeps = 0;
+    int dilations = 0;
+};
+
+// Relaxation of one job on the context's stream: classes from the seed labels, one-hot
+// start from the OIFT labels d_olab, K tile sweeps, argmax into out->label / out->mask (and
+// the membership copy).  hmm = intensity min / max of the image.  d_olab is not read after
+// the argmax kernel starts, so it may alias out->label.
+template <typename T>
+static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_img,
+                       const int32_t *d_seeds, const int32_t *d_slabels, int nseeds,
+                       const int32_t *d_olab, const int hmm[2], const oift_b200_outputs *out,
+                       RelaxResult *rr) {
+    cudaStream_t s = c->stream;
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    const size_t N = (size_t)X * Y * Z;
+    Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
+    const int K = p->relax_sweeps;
+    TRY(grow(c, c->presence, 1024 * sizeof(uint32_t)));
+    std::vector<int> classes;
+    int nclasses = 0;
+    long long relax_active = 0;
+    int relax_dilations = 0;
+    // classes = labels present among seeds, plus 0 (gft_ift.cpp:8684-8712)
+    CU(cudaMemsetAsync(c->presence.p, 0, 1024 * sizeof(uint32_t), s));
+    if (nseeds > 0)
+        seed_presence_kernel<<<std::min((nseeds + 255) / 256, c->sms * 4), 256, 0, s>>>(
+            d_slabels, nseeds, (uint32_t *)c->presence.p);
+    std::vector<uint32_t> bits(1024);
+    CU(cudaMemcpyAsync(bits.data(), c->presence.p, 1024 * sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    bits[0] |= 1u;
+    for (int l = 0; l <= OIFT_MAX_LABEL; l++)
+        if ((bits[l >> 5] >> (l & 31)) & 1u) classes.push_back(l);
+    nclasses = (int)classes.size();
+    if (nclasses > 8) return OIFT_E_UNSUPPORTED;
+    int maxl = classes.back();
+    std::vector<int> l2c(maxl + 1, -1);
+    for (int k = 0; k < nclasses; k++) l2c[classes[k]] = k;
+    int bg = l2c[0] < 0 ? 0 : l2c[0];
+    // Wmax (gft_ift.cpp:8733-8734) on the image shifted to >= 0 as the CLI does
+    float max_abs_per = 0.0f;
+    std::vector<float> pcm(nclasses, 0.0f);
+    if (p->per_class) {
+        for (int k = 0; k < nclasses; k++) {
+            float v = (classes[k] <= p->max_label) ? p->per_class[classes[k]] : 0.0f;
+            pcm[k] = v;
+            if (std::fabs(v) > max_abs_per) max_abs_per = std::fabs(v);
+        }
+    } else {
+        max_abs_per = std::fabs(p->per);
+    }
+    long long imax = hmm[1], imin = hmm[0];
+    long long shifted_max = imin < 0 ? imax - imin : imax;
+    float Wmax = (float)shifted_max;
+    Wmax = (float)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));
+    double deg = (p->adjacency == 26) ? 26 : (p->adjacency == 8 ? 8 : (p->adjacency == 6 ? 6 : 4));
+    if ((double)Wmax > std::pow(3.0e38 / deg, 0.125)) return OIFT_E_RANGE;
+
+    RelaxArgs ra;
+    ra.X = X;
+    ra.Y = Y;
+    ra.Z = Z;
+    ra.N = N;
+    ra.nadj = adj.n;
+    for (int i = 0; i < adj.n; i++) {
+        ra.dx[i] = adj.dx[i];
+        ra.dy[i] = adj.dy[i];
+        ra.dz[i] = adj.dz[i];
+        // Dpq = sqrtf(dx^2 + dy^2 + dz^2) / dmin with unit spacing (gft_ift.cpp:8723-8731)
+        ra.dpq[i] = sqrtf((float)(adj.dx[i] * adj.dx[i]) + (float)(adj.dy[i] * adj.dy[i]) +
+                          (float)(adj.dz[i] * adj.dz[i])) /
+                    1.0f;
+    }
+    ra.Wmax = Wmax;
+    ra.per = p->per;
+    ra.bg = bg;
+    for (int k = 0; k < 8; k++) ra.pcm[k] = k < nclasses ? pcm[k] : 0.0f;
+
+    TRY(grow(c, c->memb, 2 * (size_t)nclasses * N * sizeof(float)));
+    TRY(grow(c, c->seedc, N));
+    TRY(grow(c, c->l2c, (maxl + 1) * sizeof(int)));
+    TRY(grow(c, c->classes, nclasses * sizeof(int)));
+    CU(cudaMemcpyAsync(c->l2c.p, l2c.data(), (maxl + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->classes.p, classes.data(), nclasses * sizeof(int), cudaMemcpyHostToDevice, s));
+    float *m0 = (float *)c->memb.p, *m1 = m0 + (size_t)nclasses * N;
+    int blocks = (int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16);
+    // both ping-pong buffers start one-hot: tiles skipped at a sweep keep that value
+    relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m0);
+    relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m1);
+    CU(cudaMemsetAsync(c->seedc.p, 0xFF, N, s));
+    if (nseeds > 0)
+        relax_seed_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(d_seeds, nseeds, d_olab, N,
+                                                               (const int *)c->l2c.p, maxl, bg,
+                                                               (uint8_t *)c->seedc.p);
+    // block distance of every relaxation tile to the label boundary (exact skipping)
+    const int rtx = (X + 31) / 32, rty = (Y + 7) / 8, rtz = (Z + 3) / 4;
+    const int rnt = rtx * rty * rtz;
+    TRY(grow(c, c->rtdist, 2 * (size_t)rnt * sizeof(uint16_t) + (size_t)(K + 1) * sizeof(unsigned)));
+    uint16_t *td0 = (uint16_t *)c->rtdist.p, *td1 = td0 + rnt;
+    unsigned *hist = (unsigned *)(td1 + rnt);  // byte offset 4 * rnt
+    CU(cudaMemsetAsync(td0, 0xFF, 2 * (size_t)rnt * sizeof(uint16_t), s));
+    relax_boundary_tiles_kernel<<<dim3((X + 31) / 32, (Y + 7) / 8, Z), dim3(32, 8), 0, s>>>(
+        d_olab, X, Y, Z, adj.n, ra, td0, rtx, rty);
+    const int cheb = (adj.n == 26);
+    // exact lower bound of the voxel distance to the mask: three separable passes
+    relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 0, 32, cheb);
+    relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td1, td0, rtx, rty, rtz, 1, 8, cheb);
+    relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 2, 4, cheb);
+    std::swap(td0, td1);
+    long long active_vs = 0;
+    if (K > 0) {
+        CU(cudaMemsetAsync(hist, 0, (size_t)(K + 1) * sizeof(unsigned), s));
+        relax_tile_hist_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, rnt, K, hist);
+    }
+    float *cur = m0, *nxt = m1;
+    cudaEventRecord(c->ev[6], s);
+    for (int it = 0; it < K; it++) {
+        CU(launch_relax_tiles<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, td0,
+                                 it + 1, ra, p->per_class != nullptr, rnt, rtx, rty, s));
+        std::swap(cur, nxt);
+    }
+    if (K > 0) {
+        std::vector<unsigned> h(K);
+        CU(cudaMemcpyAsync(h.data(), hist, K * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        long long run = 0;
+        for (int t = 1; t <= K; t++) {  // tiles with distance <= t-1 run at sweep t
+            run += h[t - 1];
+            active_vs += run * 1024;
+        }
+    }
+    relax_active = active_vs;
+    relax_dilations = 3;
+    cudaEventRecord(c->ev[7], s);
+    relax_argmax_kernel<<<(int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16), 256, 0, s>>>(cur, N, nclasses, (const int *)c->classes.p,
+                                               out->label, out->mask);
+    if (out->membership)
+        CU(cudaMemcpyAsync(out->membership, cur, (size_t)nclasses * N * sizeof(float),
+                           cudaMemcpyDeviceToDevice, s));
+    rr->nclasses = nclasses;
+    rr->active_voxel_sweeps = relax_active;
+    rr->dilations = relax_dilations;
     return OIFT_OK;
 }
 
@@ -316,131 +475,12 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
 
     // ---- relaxation ----
     const int K = p->relax_sweeps;
-    int nclasses = 0;
-    long long relax_active = 0;
-    int relax_dilations = 0;
-    std::vector<int> classes;
+    RelaxResult rr;
     bool want_relax = out && (out->label || out->mask || out->membership);
-    if (want_relax) {
-        // classes = labels present among seeds, plus 0 (gft_ift.cpp:8684-8712)
-        CU(cudaMemsetAsync(c->presence.p, 0, 1024 * sizeof(uint32_t), s));
-        if (nseeds > 0)
-            seed_presence_kernel<<<std::min((nseeds + 255) / 256, c->sms * 4), 256, 0, s>>>(
-                d_slabels, nseeds, (uint32_t *)c->presence.p);
-        std::vector<uint32_t> bits(1024);
-        CU(cudaMemcpyAsync(bits.data(), c->presence.p, 1024 * sizeof(uint32_t),
-                           cudaMemcpyDeviceToHost, s));
-        CU(cudaStreamSynchronize(s));
-        bits[0] |= 1u;
-        for (int l = 0; l <= OIFT_MAX_LABEL; l++)
-            if ((bits[l >> 5] >> (l & 31)) & 1u) classes.push_back(l);
-        nclasses = (int)classes.size();
-        if (nclasses > 8) return OIFT_E_UNSUPPORTED;
-        int maxl = classes.back();
-        std::vector<int> l2c(maxl + 1, -1);
-        for (int k = 0; k < nclasses; k++) l2c[classes[k]] = k;
-        int bg = l2c[0] < 0 ? 0 : l2c[0];
-        // Wmax (gft_ift.cpp:8733-8734) on the image shifted to >= 0 as the CLI does
-        float max_abs_per = 0.0f;
-        std::vector<float> pcm(nclasses, 0.0f);
-        if (p->per_class) {
-            for (int k = 0; k < nclasses; k++) {
-                float v = (classes[k] <= p->max_label) ? p->per_class[classes[k]] : 0.0f;
-                pcm[k] = v;
-                if (std::fabs(v) > max_abs_per) max_abs_per = std::fabs(v);
-            }
-        } else {
-            max_abs_per = std::fabs(p->per);
-        }
-        long long imax = hmm[1], imin = hmm[0];
-        long long shifted_max = imin < 0 ? imax - imin : imax;
-        float Wmax = (float)shifted_max;
-        Wmax = (float)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));
-        double deg = (p->adjacency == 26) ? 26 : (p->adjacency == 8 ? 8 : (p->adjacency == 6 ? 6 : 4));
-        if ((double)Wmax > std::pow(3.0e38 / deg, 0.125)) return OIFT_E_RANGE;
-
-        RelaxArgs ra;
-        ra.X = X;
-        ra.Y = Y;
-        ra.Z = Z;
-        ra.N = N;
-        ra.nadj = adj.n;
-        for (int i = 0; i < adj.n; i++) {
-            ra.dx[i] = adj.dx[i];
-            ra.dy[i] = adj.dy[i];
-            ra.dz[i] = adj.dz[i];
-            // Dpq = sqrtf(dx^2 + dy^2 + dz^2) / dmin with unit spacing (gft_ift.cpp:8723-8731)
-            ra.dpq[i] = sqrtf((float)(adj.dx[i] * adj.dx[i]) + (float)(adj.dy[i] * adj.dy[i]) +
-                              (float)(adj.dz[i] * adj.dz[i])) /
-                        1.0f;
-        }
-        ra.Wmax = Wmax;
-        ra.per = p->per;
-        ra.bg = bg;
-        for (int k = 0; k < 8; k++) ra.pcm[k] = k < nclasses ? pcm[k] : 0.0f;
-
-        TRY(grow(c, c->memb, 2 * (size_t)nclasses * N * sizeof(float)));
-        TRY(grow(c, c->seedc, N));
-        TRY(grow(c, c->l2c, (maxl + 1) * sizeof(int)));
-        TRY(grow(c, c->classes, nclasses * sizeof(int)));
-        CU(cudaMemcpyAsync(c->l2c.p, l2c.data(), (maxl + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
-        CU(cudaMemcpyAsync(c->classes.p, classes.data(), nclasses * sizeof(int), cudaMemcpyHostToDevice, s));
-        float *m0 = (float *)c->memb.p, *m1 = m0 + (size_t)nclasses * N;
-        int blocks = (int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16);
-        // both ping-pong buffers start one-hot: tiles skipped at a sweep keep that value
-        relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m0);
-        relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m1);
-        CU(cudaMemsetAsync(c->seedc.p, 0xFF, N, s));
-        if (nseeds > 0)
-            relax_seed_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(d_seeds, nseeds, d_olab, N,
-                                                                   (const int *)c->l2c.p, maxl, bg,
-                                                                   (uint8_t *)c->seedc.p);
-        // block distance of every relaxation tile to the label boundary (exact skipping)
-        const int rtx = (X + 31) / 32, rty = (Y + 7) / 8, rtz = (Z + 3) / 4;
-        const int rnt = rtx * rty * rtz;
-        TRY(grow(c, c->rtdist, 2 * (size_t)rnt * sizeof(uint16_t) + (size_t)(K + 1) * sizeof(unsigned)));
-        uint16_t *td0 = (uint16_t *)c->rtdist.p, *td1 = td0 + rnt;
-        unsigned *hist = (unsigned *)(td1 + rnt);  // byte offset 4 * rnt
-        CU(cudaMemsetAsync(td0, 0xFF, 2 * (size_t)rnt * sizeof(uint16_t), s));
-        relax_boundary_tiles_kernel<<<dim3((X + 31) / 32, (Y + 7) / 8, Z), dim3(32, 8), 0, s>>>(
-            d_olab, X, Y, Z, adj.n, ra, td0, rtx, rty);
-        const int cheb = (adj.n == 26);
-        // exact lower bound of the voxel distance to the mask: three separable passes
-        relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 0, 32, cheb);
-        relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td1, td0, rtx, rty, rtz, 1, 8, cheb);
-        relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 2, 4, cheb);
-        std::swap(td0, td1);
-        long long active_vs = 0;
-        if (K > 0) {
-            CU(cudaMemsetAsync(hist, 0, (size_t)(K + 1) * sizeof(unsigned), s));
-            relax_tile_hist_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, rnt, K, hist);
-        }
-        float *cur = m0, *nxt = m1;
-        cudaEventRecord(c->ev[6], s);
-        for (int it = 0; it < K; it++) {
-            CU(launch_relax_tiles<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, td0,
-                                     it + 1, ra, p->per_class != nullptr, rnt, rtx, rty, s));
-            std::swap(cur, nxt);
-        }
-        if (K > 0) {
-            std::vector<unsigned> h(K);
-            CU(cudaMemcpyAsync(h.data(), hist, K * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-            CU(cudaStreamSynchronize(s));
-            long long run = 0;
-            for (int t = 1; t <= K; t++) {  // tiles with distance <= t-1 run at sweep t
-                run += h[t - 1];
-                active_vs += run * 1024;
-            }
-        }
-        relax_active = active_vs;
-        relax_dilations = 3;
-        cudaEventRecord(c->ev[7], s);
-        relax_argmax_kernel<<<(int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16), 256, 0, s>>>(cur, N, nclasses, (const int *)c->classes.p,
-                                                   out->label, out->mask);
-        if (out->membership)
-            CU(cudaMemcpyAsync(out->membership, cur, (size_t)nclasses * N * sizeof(float),
-                               cudaMemcpyDeviceToDevice, s));
-    }
+    if (want_relax) TRY(relax_stage<T>(c, p, d_img, d_seeds, d_slabels, nseeds, d_olab, hmm, out, &rr));
+    const int nclasses = rr.nclasses;
+    const long long relax_active = rr.active_voxel_sweeps;
+    const int relax_dilations = rr.dilations;
     cudaEventRecord(c->ev[3], s);
     CU(cudaStreamSynchronize(s));
     CU(cudaGetLastError());
@@ -655,11 +695,16 @@ int oift_fmax_gpu_run(const int *h_image, int *h_labels, int n, int xsize, int y
 
 
 // ----------------------------------------------------------------- batched driver ----
-// Jobs (volume, seed set) run concurrently on `lanes` partitions of the GPU: each lane is a
-// sub-context with its own stream and scratch whose persistent OIFT grid has sms/lanes
-// CTAs, so that several latency-bound OIFT launches are resident at once; relaxation
-// sweeps of all lanes share the whole device.  One host thread per lane pulls the next
-// job index from a shared counter.
+// The OIFT of one volume is bound by the latency of its level loop (grid reduction, team
+// barrier, a few tile steps per level), not by the SM count: halving its CTAs slows one job
+// by only a few percent.  So the driver runs the OIFT of all jobs of a call in ONE
+// cooperative launch of `teams` teams of sms/teams CTAs (oift_team_run), each team pulling
+// jobs from a device counter, largest volume first.  Edge codes and intensity ranges are
+// computed once per distinct image before that launch; the relaxation of the jobs follows
+// on RELAX_LANES sub-context streams, one host thread each (its host reads of the class set
+// and the sweep histogram would otherwise serialise the jobs).
+static constexpr int RELAX_LANES = 4;
+
 static int ensure_lanes(oift_b200_ctx *c, int lanes) {
     while ((int)c->lanes.size() < lanes) {
         oift_b200_ctx *l = nullptr;
@@ -667,95 +712,328 @@ static int ensure_lanes(oift_b200_ctx *c, int lanes) {
         if (rc != OIFT_OK) return rc;
         c->lanes.push_back(l);
     }
-    for (int i = 0; i < lanes; i++) c->lanes[i]->oift_ctas = c->sms / lanes;
     return OIFT_OK;
 }
 
-static int run_jobs(oift_b200_ctx *c, const oift_b200_params *common, oift_b200_job *jobs,
-                    int first, int count, int lanes, double *wall_ms) {
-    int rc = ensure_lanes(c, lanes);
-    if (rc != OIFT_OK) return rc;
-    std::atomic<int> next(first);
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct BatchTimes {
+    double wall_ms = 0, oift_ms = 0, relax_ms = 0;
+};
+
+static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
+                           oift_b200_job *jobs, int first, int count, int teams,
+                           BatchTimes *bt) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    cudaStream_t s = c->stream;
     const int end = first + count;
-    auto worker = [&](int lane) {
-        cudaSetDevice(c->device);
-        oift_b200_ctx *l = c->lanes[lane];
-        for (;;) {
-            const int j = next.fetch_add(1);
-            if (j >= end) break;
-            oift_b200_job &job = jobs[j];
-            oift_b200_params p = *common;
-            p.xsize = job.xsize;
-            p.ysize = job.ysize;
-            p.zsize = job.zsize;
-            p.per = job.per;
-            p.per_class = nullptr;
-            p.max_label = 0;
-            int st = check_params(&p);
-            if (st == OIFT_OK && job.nseeds <= 0) st = OIFT_E_NO_SEEDS;
-            if (st == OIFT_OK) {
-                oift_b200_outputs o{};
-                o.cost = job.cost;
-                o.label = job.label;
-                o.mask = job.mask;
-                if (!o.label && !o.mask) o.oift_label = nullptr;
-                st = run_pipeline<int16_t>(l, &p, job.image, job.seeds, job.seed_labels,
-                                           job.nseeds, &o, nullptr);
-            }
-            job.status = st;
-        }
+    const int team_ctas = c->sms / teams;
+    if (team_ctas < 1) return OIFT_E_BAD_ARG;
+
+    // ---- per-job checks; distinct images (pointer + extents) ----
+    struct Img {
+        const int16_t *p;
+        int X, Y, Z;
+        size_t woff;  // element offset of its edge codes in c->W
     };
-    const auto t0 = std::chrono::steady_clock::now();
-    std::vector<std::thread> ths;
-    for (int i = 0; i < lanes; i++) ths.emplace_back(worker, i);
-    for (auto &t : ths) t.join();
-    const auto t1 = std::chrono::steady_clock::now();
-    if (wall_ms) *wall_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    std::vector<Img> imgs;
+    std::vector<int> job_img(count, -1);
+    size_t wtotal = 0;
+    for (int j = first; j < end; j++) {
+        oift_b200_job &jb = jobs[j];
+        oift_b200_params p = *common;
+        p.xsize = jb.xsize;
+        p.ysize = jb.ysize;
+        p.zsize = jb.zsize;
+        p.per = jb.per;
+        p.per_class = nullptr;
+        p.max_label = 0;
+        int st = check_params(&p);
+        if (st == OIFT_OK && (!jb.image || !jb.seeds || !jb.seed_labels)) st = OIFT_E_BAD_ARG;
+        if (st == OIFT_OK && jb.nseeds <= 0) st = OIFT_E_NO_SEEDS;
+        jb.status = st;
+        if (st != OIFT_OK) continue;
+        int k = -1;
+        for (size_t i = 0; i < imgs.size(); i++)
+            if (imgs[i].p == jb.image && imgs[i].X == jb.xsize && imgs[i].Y == jb.ysize &&
+                imgs[i].Z == jb.zsize) {
+                k = (int)i;
+                break;
+            }
+        if (k < 0) {
+            k = (int)imgs.size();
+            imgs.push_back({jb.image, jb.xsize, jb.ysize, jb.zsize, wtotal});
+            const size_t n = (size_t)jb.xsize * jb.ysize * jb.zsize;
+            wtotal += align_up(3 * n, 128);  // 256-byte aligned planes blocks
+        }
+        job_img[j - first] = k;
+    }
+    const int nimg = (int)imgs.size();
+    if (nimg == 0) {
+        for (int j = first; j < end; j++)
+            if (jobs[j].status != OIFT_OK) return jobs[j].status;
+        return OIFT_OK;
+    }
+
+    // ---- intensity range and edge codes, once per image ----
+    TRY(grow(c, c->W, wtotal * sizeof(uint16_t)));
+    TRY(grow(c, c->bmm, (size_t)nimg * (2 * sizeof(int) + sizeof(unsigned long long))));
+    int *d_mm = (int *)c->bmm.p;
+    unsigned long long *d_clamp = (unsigned long long *)((char *)c->bmm.p + (size_t)nimg * 2 * sizeof(int));
+    {
+        std::vector<int> mm_init(2 * (size_t)nimg);
+        for (int i = 0; i < nimg; i++) {
+            mm_init[2 * i] = 0x7fffffff;
+            mm_init[2 * i + 1] = (int)0x80000000;
+        }
+        CU(cudaMemcpyAsync(d_mm, mm_init.data(), mm_init.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, s));
+        CU(cudaMemsetAsync(d_clamp, 0, (size_t)nimg * sizeof(unsigned long long), s));
+    }
+    cudaEventRecord(c->ev[0], s);
+    for (int i = 0; i < nimg; i++) {
+        const size_t n = (size_t)imgs[i].X * imgs[i].Y * imgs[i].Z;
+        CU(launch_minmax<int16_t>(imgs[i].p, n, d_mm + 2 * i, c->sms, s));
+    }
+    std::vector<int> hmm(2 * (size_t)nimg);
+    CU(cudaMemcpyAsync(hmm.data(), d_mm, hmm.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const uint16_t *lut = nullptr;
+    int lut_len = 0;
+    if (common->weight_mode == OIFT_W_RBF_Q) {
+        // the table depends on |I_p - I_q| only: one table for the widest range serves all
+        long long range = 0;
+        for (int i = 0; i < nimg; i++)
+            range = std::max(range, (long long)hmm[2 * i + 1] - (long long)hmm[2 * i]);
+        lut_len = (int)(range + 1);
+        std::vector<uint16_t> t(lut_len);
+        const double sg = common->rbf_sigma;
+        for (int d = 0; d < lut_len; d++) {
+            double a = std::exp(-((double)d * (double)d) / (2.0 * sg * sg));
+            double v = std::floor((double)common->wq * (1.0 - a) + 0.5);
+            t[d] = (uint16_t)(v < 0 ? 0 : (v > common->wq ? common->wq : v));
+        }
+        TRY(grow(c, c->lut, lut_len * sizeof(uint16_t)));
+        CU(cudaMemcpyAsync(c->lut.p, t.data(), lut_len * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        lut = (const uint16_t *)c->lut.p;
+    }
+    const Adjacency adj = make_adjacency(6);
+    for (int i = 0; i < nimg; i++) {
+        BuildArgs ba;
+        ba.X = imgs[i].X;
+        ba.Y = imgs[i].Y;
+        ba.Z = imgs[i].Z;
+        ba.planes = 3;
+        ba.mode = common->weight_mode;
+        ba.cap = (common->weight_mode == OIFT_W_GRAD) ? OIFT_MAX_BASE : common->wq;
+        for (int k = 0; k < 3; k++) {
+            ba.dx[k] = adj.dx[adj.n / 2 + k];
+            ba.dy[k] = adj.dy[adj.n / 2 + k];
+            ba.dz[k] = adj.dz[adj.n / 2 + k];
+        }
+        ba.lut = lut;
+        ba.lut_len = lut_len;
+        ba.grad = nullptr;
+        ba.blend_a = common->blend_a;
+        ba.clamped = d_clamp + i;
+        CU(launch_build_weights<int16_t>(imgs[i].p, (uint16_t *)c->W.p + imgs[i].woff, ba,
+                                         c->sms, s));
+    }
+
+    // ---- job descriptors: 3D jobs then 2D jobs, each group largest volume first ----
+    std::vector<int> order;
+    for (int j = first; j < end; j++)
+        if (jobs[j].status == OIFT_OK) order.push_back(j);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const bool pa = jobs[a].zsize == 1, pb = jobs[b].zsize == 1;
+        if (pa != pb) return pb;  // 3D first
+        return (size_t)jobs[a].xsize * jobs[a].ysize * jobs[a].zsize >
+               (size_t)jobs[b].xsize * jobs[b].ysize * jobs[b].zsize;
+    });
+    const int nj = (int)order.size();
+    std::vector<OiftTeamJob> dj(nj);
+    size_t max_n = 0, max_tiles = 0, max_mbox = 0, olab_total = 0;
+    std::vector<size_t> olab_off(nj, (size_t)-1);
+    for (int i = 0; i < nj; i++) {
+        // a job with a label output relaxes in place; one with only a mask needs room for
+        // its OIFT labels
+        const oift_b200_job &jb = jobs[order[i]];
+        const size_t n = (size_t)jb.xsize * jb.ysize * jb.zsize;
+        if (!jb.label && jb.mask) {
+            olab_off[i] = olab_total;
+            olab_total += align_up(n, 64);
+        }
+    }
+    if (olab_total) TRY(grow(c, c->bolab, olab_total * sizeof(int32_t)));
+    std::vector<int32_t *> olab(nj, nullptr);
+    int n3d = 0;
+    for (int i = 0; i < nj; i++) {
+        const oift_b200_job &jb = jobs[order[i]];
+        const OiftPlan P = oift_plan(jb.xsize, jb.ysize, jb.zsize);
+        const size_t n = (size_t)jb.xsize * jb.ysize * jb.zsize;
+        OiftTeamJob &d = dj[i];
+        d.W = (const uint16_t *)c->W.p + imgs[job_img[order[i] - first]].woff;
+        d.seeds = jb.seeds;
+        d.seed_labels = jb.seed_labels;
+        d.cost = jb.cost;
+        olab[i] = jb.label ? jb.label
+                           : (olab_off[i] != (size_t)-1 ? (int32_t *)c->bolab.p + olab_off[i] : nullptr);
+        d.label = olab[i];
+        d.X = jb.xsize;
+        d.Y = jb.ysize;
+        d.Z = jb.zsize;
+        d.nseeds = jb.nseeds;
+        d.ntx = P.ntx;
+        d.nty = P.nty;
+        d.ntz = P.ntz;
+        d.ntiles = P.ntiles;
+        d.mbox_words = oift_mbox_words(P, team_ctas);
+        d.pol0 = -jb.per;  // label 0 takes -per (gft_ift.cpp:968)
+        d.pol_default = jb.per;
+        d.status = OIFT_TEAM_NOT_RUN;
+        d.levels = 0;
+        d.steps = 0;
+        max_n = std::max(max_n, n);
+        max_tiles = std::max(max_tiles, (size_t)P.ntiles);
+        max_mbox = std::max(max_mbox, (size_t)team_ctas * OIFT_WARPS_PER_CTA * d.mbox_words);
+        if (jb.zsize > 1) n3d++;
+    }
+    OiftTeamScratch S;
+    S.key_stride = align_up(max_n, 64);
+    S.tpend_stride = align_up(max_tiles, 64);
+    S.mbox_stride = align_up(max_mbox, 32);
+    TRY(grow(c, c->bjobs, (size_t)nj * sizeof(OiftTeamJob)));
+    TRY(grow(c, c->bkey, (size_t)teams * S.key_stride * sizeof(uint32_t)));
+    TRY(grow(c, c->btpend, (size_t)teams * S.tpend_stride * sizeof(uint32_t)));
+    TRY(grow(c, c->bmbox, (size_t)teams * S.mbox_stride * sizeof(unsigned long long)));
+    TRY(grow(c, c->bglob, (size_t)teams * sizeof(OiftGlobals)));
+    TRY(grow(c, c->bctl, 2 * sizeof(unsigned int)));
+    S.key = (uint32_t *)c->bkey.p;
+    S.tpend = (uint32_t *)c->btpend.p;
+    S.mbox = (unsigned long long *)c->bmbox.p;
+    S.g = (OiftGlobals *)c->bglob.p;
+    S.next_job = (unsigned int *)c->bctl.p;
+    S.abort = (int *)c->bctl.p + 1;
+    OiftTeamJob *d_jobs = (OiftTeamJob *)c->bjobs.p;
+    CU(cudaMemcpyAsync(d_jobs, dj.data(), (size_t)nj * sizeof(OiftTeamJob), cudaMemcpyHostToDevice, s));
+
+    // ---- the OIFT of every job: one team launch per group ----
+    if (n3d > 0) TRY(oift_team_run(d_jobs, n3d, false, teams, team_ctas, S, s));
+    if (nj - n3d > 0) TRY(oift_team_run(d_jobs + n3d, nj - n3d, true, teams, team_ctas, S, s));
+    cudaEventRecord(c->ev[1], s);
+    std::vector<unsigned long long> hclamp(nimg);
+    CU(cudaMemcpyAsync(dj.data(), d_jobs, (size_t)nj * sizeof(OiftTeamJob), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(hclamp.data(), d_clamp, nimg * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    float oift_ms = 0;
+    cudaEventElapsedTime(&oift_ms, c->ev[0], c->ev[1]);
+    for (int i = 0; i < nj; i++) {
+        oift_b200_job &jb = jobs[order[i]];
+        int st = dj[i].status;
+        if (st == OIFT_TEAM_NOT_RUN) st = OIFT_E_NOT_CONVERGED;
+        if (st == OIFT_OK && common->weight_mode == OIFT_W_GRAD && hclamp[job_img[order[i] - first]])
+            st = OIFT_E_RANGE;
+        jb.status = st;
+    }
+    const auto t1 = clk::now();
+
+    // ---- relaxation of the jobs that want labels or a mask ----
+    std::vector<int> rjobs;
+    for (int i = 0; i < nj; i++) {
+        const oift_b200_job &jb = jobs[order[i]];
+        if (jb.status == OIFT_OK && (jb.label || jb.mask)) rjobs.push_back(i);
+    }
+    const int nl = std::min<int>(RELAX_LANES, (int)rjobs.size());
+    if (nl > 0) {
+        TRY(ensure_lanes(c, nl));
+        std::atomic<int> next(0);
+        auto worker = [&](int lane) {
+            cudaSetDevice(c->device);
+            oift_b200_ctx *l = c->lanes[lane];
+            for (;;) {
+                const int r = next.fetch_add(1);
+                if (r >= (int)rjobs.size()) break;
+                const int i = rjobs[r];
+                oift_b200_job &jb = jobs[order[i]];
+                oift_b200_params p = *common;
+                p.xsize = jb.xsize;
+                p.ysize = jb.ysize;
+                p.zsize = jb.zsize;
+                p.per = jb.per;
+                p.per_class = nullptr;
+                p.max_label = 0;
+                oift_b200_outputs o{};
+                o.label = jb.label;
+                o.mask = jb.mask;
+                RelaxResult rr;
+                const int k = job_img[order[i] - first];
+                int st = relax_stage<int16_t>(l, &p, jb.image, jb.seeds, jb.seed_labels,
+                                              jb.nseeds, olab[i], &hmm[2 * k], &o, &rr);
+                if (st == OIFT_OK && cudaStreamSynchronize(l->stream) != cudaSuccess) st = OIFT_E_CUDA;
+                jb.status = st;
+            }
+        };
+        std::vector<std::thread> ths;
+        for (int i = 0; i < nl; i++) ths.emplace_back(worker, i);
+        for (auto &t : ths) t.join();
+    }
+    const auto t2 = clk::now();
+    if (bt) {
+        bt->oift_ms = oift_ms;
+        bt->relax_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        bt->wall_ms = std::chrono::duration<double, std::milli>(t2 - t0).count();
+    }
     for (int j = first; j < end; j++)
         if (jobs[j].status != OIFT_OK) return jobs[j].status;
     return OIFT_OK;
 }
 
 int oift_b200_run_batch(oift_b200_ctx *c, const oift_b200_params *common, oift_b200_job *jobs,
-                        int njobs, int lanes, oift_b200_batch_stats *stats) {
-    if (!c || !common || !jobs || njobs < 0 || lanes < 0 || lanes > 16) return OIFT_E_BAD_ARG;
+                        int njobs, int teams, oift_b200_batch_stats *stats) {
+    if (!c || !common || !jobs || njobs < 0 || teams < 0 || teams > c->sms) return OIFT_E_BAD_ARG;
     if (njobs == 0) return OIFT_OK;
     cudaSetDevice(c->device);
     int first = 0;
-    if (lanes == 0) {
-        // autotune once per context: time each candidate lane count on a few jobs (those
-        // jobs are then done) and keep the fastest in voxels per second
-        if (c->tuned_lanes == 0) {
-            const int cands[] = {1, 2, 4, 8};
+    if (teams == 0) {
+        // autotune once per context: time each candidate team count on its own slice of
+        // 2 * teams jobs (those jobs are then done) and keep the fastest in voxels per ms
+        if (c->tuned_teams == 0) {
+            const int cands[] = {1, 2, 4, 8, 16, 32, 64};
             double best = -1.0;
-            int best_l = 1;
-            for (int ci = 0; ci < 4 && first < njobs; ci++) {
-                const int l = cands[ci];
-                const int cnt = std::min(njobs - first, 2 * l);
-                double ms = 0;
-                int rc = run_jobs(c, common, jobs, first, cnt, l, &ms);
+            int best_t = 1;
+            for (int ci = 0; ci < 7 && first < njobs; ci++) {
+                const int t = cands[ci];
+                if (t > c->sms) break;
+                const int cnt = std::min(njobs - first, 2 * t);
+                BatchTimes bt;
+                int rc = run_batch_teams(c, common, jobs, first, cnt, t, &bt);
                 if (rc != OIFT_OK) return rc;
                 double vox = 0;
                 for (int j = first; j < first + cnt; j++)
                     vox += (double)jobs[j].xsize * jobs[j].ysize * jobs[j].zsize;
-                const double rate = vox / std::max(ms, 1e-3);
+                const double rate = vox / std::max(bt.wall_ms, 1e-3);
                 if (rate > best) {
                     best = rate;
-                    best_l = l;
+                    best_t = t;
                 }
                 first += cnt;
             }
-            c->tuned_lanes = best_l;
+            c->tuned_teams = best_t;
         }
-        lanes = c->tuned_lanes;
+        teams = c->tuned_teams;
     }
-    double ms = 0;
-    int rc = run_jobs(c, common, jobs, first, njobs - first, lanes, &ms);
+    BatchTimes bt;
+    int rc = OIFT_OK;
+    if (first < njobs) rc = run_batch_teams(c, common, jobs, first, njobs - first, teams, &bt);
     if (stats) {
-        stats->lanes = lanes;
+        stats->teams = teams;
         stats->jobs = njobs;
         stats->tuned_jobs = first;
-        stats->ms_wall = (float)ms;
+        stats->ms_wall = (float)bt.wall_ms;
+        stats->ms_oift = (float)bt.oift_ms;
+        stats->ms_relax = (float)bt.relax_ms;
     }
     return rc;
 }

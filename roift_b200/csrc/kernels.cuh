@@ -47,7 +47,9 @@ struct OiftGlobals {
                                     // tiles, drain; key staging, sparse tiles, dense tiles,
                                     // #stale, #sparse, #dense; dense: masks, flood, flood
                                     // iterations, expansion, faces, pending
-    unsigned int pad4[26];
+    int job;       // job of the batched kernel this team works on
+    int bad_seed;  // OIFT_E_* of an invalid seed of the team's current job, else 0
+    unsigned int pad4[24];
 };
 
 
@@ -94,6 +96,44 @@ OiftPlan oift_plan(int X, int Y, int Z);
 size_t oift_globals_bytes();
 int oift_mbox_words(const OiftPlan &P, int ctas);
 size_t oift_mbox_bytes(const OiftPlan &P, int ctas);
+// One job (volume + seed set) of the batched OIFT kernel; the device copy is read by
+// the team that draws it and receives the job's status.
+struct OiftTeamJob {
+    const uint16_t *W;  // edge codes of the job's volume, built before the launch
+    const int32_t *seeds, *seed_labels;
+    int32_t *cost, *label;  // device outputs, each may be null
+    int X, Y, Z, nseeds;
+    int ntx, nty, ntz, ntiles;
+    int mbox_words;      // re-activation words per warp for the team size of the launch
+    float pol0;          // polarity (x100) of label 0
+    float pol_default;   // polarity (x100) of every other label
+    int status;          // out: OIFT_OK or OIFT_E_*; OIFT_TEAM_NOT_RUN until a team ends it
+    int levels;          // out
+    unsigned long long steps;  // out
+};
+#define OIFT_TEAM_NOT_RUN 1
+
+// Per-team state of the batched kernel: team t uses key + t * key_stride and so on.
+struct OiftTeamScratch {
+    uint32_t *key;
+    size_t key_stride;
+    uint32_t *tpend;
+    size_t tpend_stride;
+    unsigned long long *mbox;
+    size_t mbox_stride;
+    OiftGlobals *g;           // [teams]
+    unsigned int *next_job;   // job counter shared by the teams
+    int *abort;               // set when a team stops on an error; others take no new job
+};
+
+// Batched OIFT: one cooperative launch of teams * team_ctas CTAs; each team of team_ctas
+// CTAs repeatedly draws the next job from d_jobs (in array order), clears its state, seeds,
+// runs the level loop with a team barrier and writes cost / label.  All jobs of one call
+// must be 2D (Z == 1) when planar, else 3D.  Returns OIFT_OK once the launch completed;
+// per-job results are in d_jobs[].status.
+int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int team_ctas,
+                  const OiftTeamScratch &S, cudaStream_t st);
+
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,

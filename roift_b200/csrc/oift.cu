@@ -64,11 +64,13 @@ __device__ __forceinline__ unsigned long long vload(const volatile unsigned long
 }
 
 // Barrier over the `nctas` CTAs that share `g` (the whole cooperative grid, or one team of
-// the batched kernel), with a bounded wait.
+// the batched kernel), with a bounded wait.  Returns false, in every thread of the CTA, when
+// the wait ended on an error flag or on the spin limit instead of the last arrival.
 __device__ bool team_barrier(OiftGlobals *g, long long limit, unsigned int nctas) {
+    __shared__ int s_ok;
     __syncthreads();
-    bool ok = true;
     if (threadIdx.x == 0) {
+        int ok = 1;
         unsigned int gen = vload(&g->bar_gen);
         __threadfence();
         if (atomicAdd(&g->bar_count, 1u) == nctas - 1) {
@@ -78,18 +80,23 @@ __device__ bool team_barrier(OiftGlobals *g, long long limit, unsigned int nctas
         } else {
             long long spins = 0;
             while (vload(&g->bar_gen) == gen) {
-                if (vload(&g->error)) break;
+                if (vload(&g->error)) {
+                    ok = 0;
+                    break;
+                }
                 if (++spins > limit) {
                     atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
+                    ok = 0;
                     break;
                 }
                 __nanosleep(64);
             }
         }
         __threadfence();
+        s_ok = ok;
     }
     __syncthreads();
-    return ok;
+    return s_ok != 0;
 }
 
 __device__ __forceinline__ float polarity_of(const OiftArgs &A, int l) {
@@ -223,15 +230,15 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         const int yr = y0 + (lane % TY), zr = z0 + (lane / TY);
         uint16_t hx = 0, hy[TZ], hz[TY];
         if (x0 > 0 && yr < Y && zr < Z)
-            hx = __ldcg(&A.W[(size_t)(x0 - 1) + (size_t)yr * X + (size_t)zr * XY]);
+            hx = __ldg(&A.W[(size_t)(x0 - 1) + (size_t)yr * X + (size_t)zr * XY]);
 #pragma unroll
         for (int zl = 0; zl < TZ; zl++)
             hy[zl] = (y0 > 0 && x < X && z0 + zl < Z)
-                ? __ldcg(&A.W[N + (size_t)x + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY]) : 0;
+                ? __ldg(&A.W[N + (size_t)x + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY]) : 0;
 #pragma unroll
         for (int yl = 0; yl < TY; yl++)
             hz[yl] = (TZ > 1 && has_z && z0 > 0 && x < X && y0 + yl < Y)
-                ? __ldcg(&A.W[2 * N + (size_t)x + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY]) : 0;
+                ? __ldg(&A.W[2 * N + (size_t)x + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY]) : 0;
         if (full) {
             uint4 cv[12];
 #pragma unroll
@@ -240,7 +247,7 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
                 const size_t p0 =
                     (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
                 if (pl < 2 || has_z)
-                    cv[m] = __ldcg(reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
+                    cv[m] = __ldg(reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
                 else
                     cv[m] = make_uint4(0, 0, 0, 0);
             }
@@ -251,9 +258,9 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
                 const int y = y0 + (r % TY), z = z0 + (r / TY);
                 const bool valid = (x < X) && (y < Y) && (z < Z);
                 const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
-                sw[r * 32 + lane] = valid ? __ldcg(&A.W[p]) : 0;
-                sw[1024 + r * 32 + lane] = valid ? __ldcg(&A.W[N + p]) : 0;
-                sw[2048 + r * 32 + lane] = (valid && has_z) ? __ldcg(&A.W[2 * N + p]) : 0;
+                sw[r * 32 + lane] = valid ? __ldg(&A.W[p]) : 0;
+                sw[1024 + r * 32 + lane] = valid ? __ldg(&A.W[N + p]) : 0;
+                sw[2048 + r * 32 + lane] = (valid && has_z) ? __ldg(&A.W[2 * N + p]) : 0;
             }
         }
         shx[lane] = hx;
@@ -746,6 +753,125 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
     oift_solve<TY, TZ>(A, blockIdx.x, gridDim.x, cs, smem_raw);
 }
 
+// Batched OIFT: CTA b belongs to team b / team_ctas.  A team draws jobs from a shared
+// counter until none is left; per job it clears its key / pending / mailbox arrays, places
+// the seeds, runs the level loop of oift_solve over its own CTAs and writes cost and label.
+// Five team barriers per job separate the phases.  An error inside the level loop (a
+// bounded wait that expired, a worklist overflow) leaves the team's barrier state
+// unusable, so the team records it in the job, sets the abort flag and stops; jobs that no
+// team ended keep status OIFT_TEAM_NOT_RUN.
+template <int TY, int TZ>
+__global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
+    oift_team_kernel(OiftTeamJob *jobs, int njobs, int team_ctas, OiftTeamScratch S,
+                     long long spin_limit, int max_levels) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ OiftCtaSmem cs;
+    __shared__ OiftArgs sA;
+    __shared__ int s_job, s_bad;
+    const int team = blockIdx.x / team_ctas, tc = blockIdx.x - team * team_ctas;
+    OiftGlobals *g = S.g + team;
+    uint32_t *key = S.key + (size_t)team * S.key_stride;
+    uint32_t *tpend = S.tpend + (size_t)team * S.tpend_stride;
+    unsigned long long *mbox = S.mbox + (size_t)team * S.mbox_stride;
+    const size_t tid = (size_t)tc * blockDim.x + threadIdx.x;
+    const size_t nthr = (size_t)team_ctas * blockDim.x;
+    const bool leader = tc == 0 && threadIdx.x == 0;
+    for (;;) {
+        // ---- the leader draws a job and clears the per-job globals ----
+        if (leader) {
+            g->job = vload(S.abort) ? njobs : (int)atomicAdd(S.next_job, 1u);
+            g->nextmin[0] = g->nextmin[1] = OIFT_KEY_INF;
+            g->levels = 0;
+            g->tile_steps = 0;
+            g->bad_seed = 0;
+        }
+        if (!team_barrier(g, spin_limit, team_ctas)) break;
+        if (threadIdx.x == 0) s_job = vload(&g->job);
+        __syncthreads();
+        const int j = s_job;
+        if (j >= njobs) break;
+        OiftTeamJob *J = jobs + j;
+        const int X = J->X, Y = J->Y, Z = J->Z, ntx = J->ntx, nty = J->nty;
+        const int ntiles = J->ntiles, mbox_words = J->mbox_words;
+        const size_t N = (size_t)X * Y * Z;
+        if (threadIdx.x == 0) {
+            sA.key = key;
+            sA.W = J->W;
+            sA.tpend = tpend;
+            sA.mbox = mbox;
+            sA.lprof = nullptr;
+            sA.lprof_cap = 0;
+            sA.mbox_words = mbox_words;
+            sA.nwarps = team_ctas * OIFT_WARPS;
+            sA.X = X;
+            sA.Y = Y;
+            sA.Z = Z;
+            sA.N = N;
+            sA.ntx = ntx;
+            sA.nty = nty;
+            sA.ntz = J->ntz;
+            sA.ntiles = ntiles;
+            sA.pol_table = &J->pol0;
+            sA.npol = 1;
+            sA.pol_default = J->pol_default;
+            sA.g = g;
+            sA.spin_limit = spin_limit;
+            sA.max_levels = max_levels;
+        }
+        // ---- clear the team's state for this volume ----
+        for (size_t i = tid; i < N; i += nthr) key[i] = OIFT_KEY_INF;
+        for (size_t i = tid; i < (size_t)ntiles; i += nthr) tpend[i] = OIFT_KEY_INF;
+        const size_t nmb = (size_t)team_ctas * OIFT_WARPS * mbox_words;
+        for (size_t i = tid; i < nmb; i += nthr) mbox[i] = 0ull;
+        if (!team_barrier(g, spin_limit, team_ctas)) break;
+        // ---- seeds (as oift_seed_kernel) ----
+        for (size_t i = tid; i < (size_t)J->nseeds; i += nthr) {
+            const int p = J->seeds[i];
+            const int lb0 = J->seed_labels[i];
+            const int lb = lb0 < 0 ? 0 : lb0;
+            if (p < 0 || (size_t)p >= N) {
+                atomicExch(&g->bad_seed, OIFT_E_SEED_RANGE);
+                continue;
+            }
+            if (lb > OIFT_MAX_LABEL) {
+                atomicExch(&g->bad_seed, OIFT_E_BAD_ARG);
+                continue;
+            }
+            const uint32_t k = make_key(0, lb, 1);
+            atomicMin(&key[p], k);
+            const int x = p % X, y = (p / X) % Y, z = (int)(p / ((size_t)X * Y));
+            atomicMin(&tpend[(x >> 5) + (y / TY) * ntx + (z / TZ) * ntx * nty], k);
+        }
+        if (!team_barrier(g, spin_limit, team_ctas)) break;
+        if (threadIdx.x == 0) s_bad = vload(&g->bad_seed);
+        __syncthreads();
+        const int bad = s_bad;
+        if (!bad) oift_solve<TY, TZ>(sA, tc, team_ctas, cs, smem_raw);
+        const bool ok = team_barrier(g, spin_limit, team_ctas);
+        const int err = vload(&g->error);
+        if (!ok || err) {
+            if (leader)
+                J->status = err == OIFT_DEV_QUEUE ? OIFT_E_QUEUE_OVERFLOW : OIFT_E_NOT_CONVERGED;
+            if (threadIdx.x == 0) atomicExch(S.abort, 1);
+            break;
+        }
+        // ---- cost and label (as oift_finalize_kernel) ----
+        if (!bad) {
+            int32_t *cost = J->cost, *label = J->label;
+            for (size_t i = tid; i < N; i += nthr) {
+                const uint32_t k = __ldcg(&key[i]);
+                if (cost) cost[i] = (k == OIFT_KEY_INF) ? 0x7fffffff : key_cost(k);
+                if (label) label[i] = (k == OIFT_KEY_INF) ? -1 : key_label(k);
+            }
+        }
+        if (leader) {
+            J->levels = g->levels;
+            J->steps = g->tile_steps;
+            J->status = bad ? bad : OIFT_OK;
+        }
+    }
+}
+
 __global__ void oift_seed_kernel(uint32_t *key, uint32_t *tpend, const int32_t *seeds,
                                  const int32_t *labels, int nseeds, int X, int Y, int Z,
                                  int ntx, int nty, int TY, int TZ, int *bad) {
@@ -893,6 +1019,41 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
         for (int i = 0; i < 16; i++) cycles_out[i] = hg.cycles[i];
     if (hg.error == OIFT_DEV_TIMEOUT) return OIFT_E_NOT_CONVERGED;
     if (hg.error == OIFT_DEV_QUEUE) return OIFT_E_QUEUE_OVERFLOW;
+    return OIFT_OK;
+}
+
+int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int team_ctas,
+                  const OiftTeamScratch &S, cudaStream_t st) {
+    if (njobs <= 0) return OIFT_OK;
+    if (teams <= 0 || team_ctas <= 0) return OIFT_E_BAD_ARG;
+    if (cudaMemsetAsync(S.g, 0, (size_t)teams * sizeof(OiftGlobals), st) != cudaSuccess ||
+        cudaMemsetAsync(S.next_job, 0, sizeof(unsigned int), st) != cudaSuccess ||
+        cudaMemsetAsync(S.abort, 0, sizeof(int), st) != cudaSuccess) {
+        cudaGetLastError();
+        return OIFT_E_CUDA;
+    }
+    long long spin_limit = 20000000LL;
+    int max_levels = 4000000;
+    int tc = team_ctas;
+    OiftTeamScratch sc = S;
+    void *args[] = {&d_jobs, &njobs, &tc, &sc, &spin_limit, &max_levels};
+    const size_t smem = oift_smem_bytes();
+    cudaError_t err;
+    if (planar) {
+        auto kfn = oift_team_kernel<32, 1>;
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(teams * team_ctas),
+                                          dim3(OIFT_WARPS * 32), args, smem, st);
+    } else {
+        auto kfn = oift_team_kernel<8, 4>;
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(teams * team_ctas),
+                                          dim3(OIFT_WARPS * 32), args, smem, st);
+    }
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return OIFT_E_CUDA;
+    }
     return OIFT_OK;
 }
 

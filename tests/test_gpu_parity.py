@@ -8,6 +8,8 @@ of ORelax_1_Multi and within 1e-5 of the FP64 oracle):
     OIFT_Multi labels exactly; label differences to OIFT_Multi only at equal-cost ties;
   * relaxed membership == R3-FP32 bitwise, |m - m64| <= 1e-5, labels == ORelax_1_Multi.
 """
+import copy
+
 import numpy as np
 import pytest
 
@@ -189,38 +191,102 @@ def test_relax_tile_skipping_exact(roift, oracle_lib, size):
     assert st.relax_active_voxel_sweeps < 0.8 * K * tiles * 1024
 
 
-def _batch_jobs(rb, cases, torch, dev):
+def _batch_jobs(rb, cases, torch, dev, outs=None):
+    """Job array over `cases`; outs[i] names the outputs of job i ("label", "mask", "cost").
+    Cases that share an image object share one device image (one edge-code build)."""
     bufs, jobs = [], (rb.Job * len(cases))()
+    imgs = {}
     for i, c in enumerate(cases):
-        img = torch.from_numpy(c.image.astype(np.int16)).to(dev)
+        want = outs[i] if outs else ("label", "mask")
+        if id(c.image) not in imgs:
+            imgs[id(c.image)] = torch.from_numpy(c.image.astype(np.int16)).to(dev)
+        img = imgs[id(c.image)]
         sd = torch.from_numpy(c.seeds).to(dev)
         sl = torch.from_numpy(c.seed_labels).to(dev)
         lab = torch.full((c.n,), -5, dtype=torch.int32, device=dev)
         mask = torch.zeros(c.n, dtype=torch.uint8, device=dev)
+        cost = torch.full((c.n,), -5, dtype=torch.int32, device=dev)
         Z, Y, X = c.shape
         jobs[i] = rb.Job(img.data_ptr(), X, Y, Z, sd.data_ptr(), sl.data_ptr(), len(c.seeds),
-                         float(np.float32(c.pol * 100.0)), None, lab.data_ptr(), mask.data_ptr(), 0)
-        bufs.append((img, sd, sl, lab, mask))
+                         float(np.float32(c.pol * 100.0)),
+                         cost.data_ptr() if "cost" in want else None,
+                         lab.data_ptr() if "label" in want else None,
+                         mask.data_ptr() if "mask" in want else None, 0)
+        bufs.append((img, sd, sl, lab, mask, cost))
     return jobs, bufs
 
 
-@pytest.mark.parametrize("lanes", [1, 3, 0])
-def test_batch_matches_single_runs(roift, lanes):
-    """Concurrent lanes (and the autotuner, lanes=0) give the labels of one-at-a-time runs."""
-    import torch
-    dev = torch.device("cuda:0")
+def _batch_cases():
+    """Uneven 3D volumes, a second seed set on one of them (shared image), a 2D slice."""
     cases = []
     for i, size in enumerate([40, 56, 48, 64, 40, 52]):
-        c = synth.ellipsoid3d(seed=20 + i, size=size, sweeps=6, pol=[-0.3, 0.2, 0.4][i % 3])
-        cases.append(c)
+        cases.append(synth.ellipsoid3d(seed=20 + i, size=size, sweeps=6,
+                                       pol=[-0.3, 0.2, 0.4][i % 3]))
+    base = cases[1]
+    rng = np.random.default_rng(3)
+    keep = rng.random(len(base.seeds)) < 0.7
+    alt = copy.copy(base)
+    alt.seeds, alt.seed_labels = base.seeds[keep], base.seed_labels[keep]
+    alt.pol = -0.45
+    cases.append(alt)
+    d = synth.disc2d(seed=9, size=96)
+    d.image = d.image.astype(np.int16)
+    cases.append(d)
+    return cases
+
+
+@pytest.mark.parametrize("teams", [1, 3, 16, 0])
+def test_batch_matches_single_runs(roift, teams):
+    """The team-batched OIFT (and the autotuner, teams=0) gives, per job, the labels, mask
+    and costs of one-at-a-time runs, for every mix of requested outputs."""
+    import torch
+    dev = torch.device("cuda:0")
+    cases = _batch_cases()
+    outs = [("label", "mask"), ("label",), ("mask",), ("cost", "label"), ("cost",),
+            ("label", "mask", "cost"), ("label", "mask"), ("label", "cost")]
+    p = roift.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=6)
+    jobs, bufs = _batch_jobs(roift, cases, torch, dev, outs)
+    ctx = roift.Context(0)
+    st = ctx.run_batch(p, jobs, teams=teams)
+    torch.cuda.synchronize()
+    assert st.jobs == len(cases) and st.teams >= 1
+    for c, (img, sd, sl, lab, mask, cost), job, want in zip(cases, bufs, jobs, outs):
+        assert job.status == 0
+        single = roift.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095,
+                                   pol=c.pol, sweeps=6)
+        lab1 = torch.empty(c.n, dtype=torch.int32, device=dev)
+        cost1 = torch.empty(c.n, dtype=torch.int32, device=dev)
+        roift._ctx().run_device(single, img.data_ptr(), sd.data_ptr(), sl.data_ptr(),
+                                len(c.seeds), label=lab1.data_ptr(), cost=cost1.data_ptr())
+        torch.cuda.synchronize()
+        if "label" in want:
+            assert torch.equal(lab, lab1)
+        if "mask" in want:
+            assert torch.equal(mask, (lab1 != 0).to(torch.uint8))
+        if "cost" in want:
+            assert torch.equal(cost, cost1)
+    ctx.close()
+
+
+def test_batch_bad_seed_is_reported_per_job(roift):
+    """A job whose seed lies outside its volume ends with OIFT_E_SEED_RANGE; the other
+    jobs of the same launch still complete with the labels of single runs."""
+    import torch
+    dev = torch.device("cuda:0")
+    cases = _batch_cases()[:4]
+    bad = copy.copy(cases[2])
+    bad.seeds = bad.seeds.copy()
+    bad.seeds[len(bad.seeds) // 2] = bad.n + 5
+    cases[2] = bad
     p = roift.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=6)
     jobs, bufs = _batch_jobs(roift, cases, torch, dev)
     ctx = roift.Context(0)
-    st = ctx.run_batch(p, jobs, lanes=lanes)
+    with pytest.raises(roift.OiftError):
+        ctx.run_batch(p, jobs, teams=2)
     torch.cuda.synchronize()
-    assert st.jobs == len(cases)
-    for c, (img, sd, sl, lab, mask), job in zip(cases, bufs, jobs):
-        assert job.status == 0
+    assert [j.status for j in jobs] == [0, 0, roift.E_SEED_RANGE, 0]
+    for i in (0, 1, 3):
+        c, (img, sd, sl, lab, mask, cost) = cases[i], bufs[i]
         single = roift.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095,
                                    pol=c.pol, sweeps=6)
         lab1 = torch.empty(c.n, dtype=torch.int32, device=dev)
@@ -228,5 +294,4 @@ def test_batch_matches_single_runs(roift, lanes):
                                 len(c.seeds), label=lab1.data_ptr())
         torch.cuda.synchronize()
         assert torch.equal(lab, lab1)
-        assert torch.equal(mask, (lab1 != 0).to(torch.uint8))
     ctx.close()
