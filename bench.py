@@ -205,7 +205,8 @@ def run_batch_workload(args):
     vox = sum(j[0].n for j in jobs_py)
     common = rb.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=20)
     ctx = rb.Context(0)
-    ctx.run_batch(common, jobs, teams=0)            # warm-up; the autotuner picks its teams
+    while ctx.run_batch(common, jobs, teams=0).tuning:   # warm-up: the autotuner explores
+        pass
     tuned = ctx.run_batch(common, jobs, teams=0).teams
 
     def timed(fn):
@@ -219,7 +220,7 @@ def run_batch_workload(args):
     for teams in [int(t) for t in args.team_scan.split(",")]:
         scan[teams], st = timed(lambda: ctx.run_batch(common, jobs, teams=teams))
         parts[teams] = {"oift_ms": st.ms_oift, "relax_ms": st.ms_relax}
-    batched_s, _ = timed(lambda: ctx.run_batch(common, jobs, teams=tuned))
+    batched_s, _ = timed(lambda: ctx.run_batch(common, jobs, teams=0))
     # the per-volume path: the single-volume API, one job after the other on the whole GPU
     single = rb.Context(0)
 
@@ -261,7 +262,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain-gpu", action="store_true")
     ap.add_argument("--workload", default="ellipsoid256", choices=["ellipsoid256", "batch64"])
-    ap.add_argument("--team-scan", default="1,2,4,8,16,32,64",
+    ap.add_argument("--team-scan", default="1,4,16,37,74,148",
                     help="team counts timed by the batch64 workload")
     ap.add_argument("--nvol", type=int, default=64)
     args = ap.parse_args()
@@ -393,6 +394,9 @@ def main():
               "oift_cycles_stage_sparse_dense": list(stats[-1].oift_cycles)[4:7],
               "oift_dense_cycles_masks_flood_iters_expand_faces_pending":
                   list(stats[-1].oift_cycles)[10:16],
+              "oift_sparse_cycles_worklist_rounds_push_publish_pending":
+                  list(stats[-1].oift_cycles)[16:21],
+              "oift_sparse_rounds_voxels_publications": list(stats[-1].oift_cycles)[21:24],
               "oift_gbs": oift_bytes / (ms_oiftk * 1e-3) / 1e9,
               "relax_sweep_gbs": relax_bytes / (ms_sweep * 1e-3) / 1e9}
 

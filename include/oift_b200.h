@@ -94,11 +94,13 @@ typedef struct {
     int kernels;          /* kernel launches issued by the call */
     float ms_oift_kernel; /* persistent OIFT kernel alone (CUDA events around the launch) */
     float ms_sweeps;      /* the K relaxation sweep launches alone */
-    long long oift_cycles[16]; /* OIFT SM cycles summed over warps: level switch, owner
+    long long oift_cycles[24]; /* OIFT SM cycles summed over warps: level switch, owner
                                   phase, queued tiles, drain; key staging, sparse tiles,
                                   dense tiles; counts of stale, sparse, dense tiles; dense
                                   tiles: masks, flood, flood iterations, expansion, faces,
-                                  pending */
+                                  pending; sparse tiles: worklist, flood rounds, face
+                                  pushes, publication, pending, counts of rounds, voxels,
+                                  publications */
     long long relax_active_voxel_sweeps; /* voxels computed over all sweeps (tiles outside
                                             the reference's growing mask are skipped) */
 } oift_b200_stats;
@@ -145,7 +147,7 @@ typedef struct {
 typedef struct {
     int teams;          /* OIFT teams of the timed part */
     int jobs;
-    int tuned_jobs;     /* jobs run while the autotuner measured team counts */
+    int tuning;         /* 1 when this call measured a team count for the autotuner */
     float ms_wall;      /* host wall time of the jobs after tuning */
     float ms_oift;      /* device time of weights + batched OIFT */
     float ms_relax;     /* host wall time of the relaxation phase */
@@ -154,11 +156,11 @@ typedef struct {
 /* Batched driver for many volumes of uneven sizes with several seed sets per volume.  Runs
  * the pipeline of `common` (adjacency 6 or 4, weights, sweeps; the job gives extents and
  * polarity) for every job.  Edge codes are built once per distinct image; the OIFT of all
- * jobs runs in one persistent launch split into `teams` teams of sms/teams CTAs, each team
+ * jobs runs in one persistent launch over all SMs split into `teams` teams, each team
  * taking the next job (largest first) from a device counter; relaxation then runs on
- * several streams.  teams = 0 lets an autotuner measure 1, 2, 4, ..., 64 teams on the
- * first jobs (once per context) and keep the fastest.  Writes each job's status; returns
- * the first failing one, OIFT_OK otherwise. */
+ * several streams.  teams = 0 selects the context's autotuner: its first calls try
+ * sms/2, sms/4, sms and sms/8 teams, one per call, and later calls use the fastest.  Writes
+ * each job's status; returns the first failing one, OIFT_OK otherwise. */
 OIFT_API int oift_b200_run_batch(oift_b200_ctx *ctx, const oift_b200_params *common,
                                  oift_b200_job *jobs, int njobs, int teams,
                                  oift_b200_batch_stats *stats);

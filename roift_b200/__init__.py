@@ -55,7 +55,7 @@ class Stats(C.Structure):
                 ("nclasses", C.c_int), ("ms_weights", C.c_float), ("ms_oift", C.c_float),
                 ("ms_relax", C.c_float), ("ms_total", C.c_float), ("kernels", C.c_int),
                 ("ms_oift_kernel", C.c_float), ("ms_sweeps", C.c_float),
-                ("oift_cycles", C.c_longlong * 16),
+                ("oift_cycles", C.c_longlong * 24),
                 ("relax_active_voxel_sweeps", C.c_longlong)]
 
     def as_dict(self):
@@ -73,7 +73,7 @@ class Job(C.Structure):
 
 
 class BatchStats(C.Structure):
-    _fields_ = [("teams", C.c_int), ("jobs", C.c_int), ("tuned_jobs", C.c_int),
+    _fields_ = [("teams", C.c_int), ("jobs", C.c_int), ("tuning", C.c_int),
                 ("ms_wall", C.c_float), ("ms_oift", C.c_float), ("ms_relax", C.c_float)]
 
 
@@ -222,7 +222,8 @@ class Context:
 
     def run_batch(self, params, jobs, teams=0) -> BatchStats:
         """Batched driver: `jobs` is a ctypes array of Job (device pointers); teams = 0
-        autotunes the number of OIFT teams the GPU is split into."""
+        autotunes the number of OIFT teams the GPU is split into (the first calls of a
+        context measure one candidate each; stats.tuning is 1 for those calls)."""
         st = BatchStats()
         rc = lib().oift_b200_run_batch(self._h, C.byref(params), jobs, len(jobs), int(teams),
                                        C.byref(st))

@@ -29,7 +29,7 @@ struct oift_b200_ctx {
     int sms = 148;
     int oift_ctas = 0;  // CTAs of the persistent OIFT grid (0 = one per SM)
     std::vector<oift_b200_ctx *> lanes;  // sub-contexts (relaxation streams) of the batched driver
-    int tuned_teams = 0;                 // team count chosen by the batch autotuner
+    std::vector<std::pair<int, double>> tune_cands;  // batch autotuner: (teams, rate)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev[8];
@@ -40,7 +40,7 @@ struct oift_b200_ctx {
     // state, job counter + abort flag, OIFT labels of jobs that only want a mask
     DevBuf bjobs, bmm, bkey, btpend, bmbox, bglob, bctl, bolab;
     size_t total = 0;
-    unsigned long long oift_cycles[16] = {0};
+    unsigned long long oift_cycles[24] = {0};
 };
 
 static thread_local int g_last_status = OIFT_OK;
@@ -502,7 +502,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         st->relax_active_voxel_sweeps = relax_active;
         cudaEventElapsedTime(&st->ms_oift_kernel, c->ev[4], c->ev[5]);
         st->ms_sweeps = 0.0f;
-        for (int i = 0; i < 16; i++) st->oift_cycles[i] = (long long)c->oift_cycles[i];
+        for (int i = 0; i < 24; i++) st->oift_cycles[i] = (long long)c->oift_cycles[i];
         if (want_relax) cudaEventElapsedTime(&st->ms_sweeps, c->ev[6], c->ev[7]);
     }
     return OIFT_OK;
@@ -728,8 +728,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     const auto t0 = clk::now();
     cudaStream_t s = c->stream;
     const int end = first + count;
-    const int team_ctas = c->sms / teams;
-    if (team_ctas < 1) return OIFT_E_BAD_ARG;
+    if (teams < 1 || teams > c->sms) return OIFT_E_BAD_ARG;
+    const int ctas_lo = c->sms / teams, ctas_hi = (c->sms + teams - 1) / teams;
 
     // ---- per-job checks; distinct images (pointer + extents) ----
     struct Img {
@@ -888,7 +888,6 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
         d.nty = P.nty;
         d.ntz = P.ntz;
         d.ntiles = P.ntiles;
-        d.mbox_words = oift_mbox_words(P, team_ctas);
         d.pol0 = -jb.per;  // label 0 takes -per (gft_ift.cpp:968)
         d.pol_default = jb.per;
         d.status = OIFT_TEAM_NOT_RUN;
@@ -896,7 +895,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
         d.steps = 0;
         max_n = std::max(max_n, n);
         max_tiles = std::max(max_tiles, (size_t)P.ntiles);
-        max_mbox = std::max(max_mbox, (size_t)team_ctas * OIFT_WARPS_PER_CTA * d.mbox_words);
+        max_mbox = std::max(max_mbox, std::max(oift_mbox_bytes(P, ctas_lo), oift_mbox_bytes(P, ctas_hi)) /
+                                          sizeof(unsigned long long));
         if (jb.zsize > 1) n3d++;
     }
     OiftTeamScratch S;
@@ -919,8 +919,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     CU(cudaMemcpyAsync(d_jobs, dj.data(), (size_t)nj * sizeof(OiftTeamJob), cudaMemcpyHostToDevice, s));
 
     // ---- the OIFT of every job: one team launch per group ----
-    if (n3d > 0) TRY(oift_team_run(d_jobs, n3d, false, teams, team_ctas, S, s));
-    if (nj - n3d > 0) TRY(oift_team_run(d_jobs + n3d, nj - n3d, true, teams, team_ctas, S, s));
+    if (n3d > 0) TRY(oift_team_run(d_jobs, n3d, false, teams, c->sms, S, s));
+    if (nj - n3d > 0) TRY(oift_team_run(d_jobs + n3d, nj - n3d, true, teams, c->sms, S, s));
     cudaEventRecord(c->ev[1], s);
     std::vector<unsigned long long> hclamp(nimg);
     CU(cudaMemcpyAsync(dj.data(), d_jobs, (size_t)nj * sizeof(OiftTeamJob), cudaMemcpyDeviceToHost, s));
@@ -995,42 +995,44 @@ int oift_b200_run_batch(oift_b200_ctx *c, const oift_b200_params *common, oift_b
     if (!c || !common || !jobs || njobs < 0 || teams < 0 || teams > c->sms) return OIFT_E_BAD_ARG;
     if (njobs == 0) return OIFT_OK;
     cudaSetDevice(c->device);
-    int first = 0;
+    // teams = 0: the context's autotuner.  While exploring, each call runs with the next
+    // untried candidate and records its rate (voxels per wall millisecond of the call);
+    // once every candidate has a rate, calls use the fastest.
+    int cand = -1;
     if (teams == 0) {
-        // autotune once per context: time each candidate team count on its own slice of
-        // 2 * teams jobs (those jobs are then done) and keep the fastest in voxels per ms
-        if (c->tuned_teams == 0) {
-            const int cands[] = {1, 2, 4, 8, 16, 32, 64};
-            double best = -1.0;
-            int best_t = 1;
-            for (int ci = 0; ci < 7 && first < njobs; ci++) {
-                const int t = cands[ci];
-                if (t > c->sms) break;
-                const int cnt = std::min(njobs - first, 2 * t);
-                BatchTimes bt;
-                int rc = run_batch_teams(c, common, jobs, first, cnt, t, &bt);
-                if (rc != OIFT_OK) return rc;
-                double vox = 0;
-                for (int j = first; j < first + cnt; j++)
-                    vox += (double)jobs[j].xsize * jobs[j].ysize * jobs[j].zsize;
-                const double rate = vox / std::max(bt.wall_ms, 1e-3);
-                if (rate > best) {
-                    best = rate;
-                    best_t = t;
-                }
-                first += cnt;
-            }
-            c->tuned_teams = best_t;
+        if (c->tune_cands.empty()) {
+            const int G = c->sms;
+            for (int t : {G / 2, G / 4, G, G / 8})
+                if (t >= 1) c->tune_cands.push_back({t, -1.0});
         }
-        teams = c->tuned_teams;
+        for (size_t i = 0; i < c->tune_cands.size(); i++)
+            if (c->tune_cands[i].second < 0) {
+                cand = (int)i;
+                break;
+            }
+        if (cand >= 0) {
+            teams = c->tune_cands[cand].first;
+        } else {
+            double best = -1.0;
+            for (auto &tc : c->tune_cands)
+                if (tc.second > best) {
+                    best = tc.second;
+                    teams = tc.first;
+                }
+        }
     }
+    const int used = std::min(teams, njobs);  // more teams than jobs would idle
     BatchTimes bt;
-    int rc = OIFT_OK;
-    if (first < njobs) rc = run_batch_teams(c, common, jobs, first, njobs - first, teams, &bt);
+    const int rc = run_batch_teams(c, common, jobs, 0, njobs, used, &bt);
+    if (cand >= 0 && rc == OIFT_OK) {
+        double vox = 0;
+        for (int j = 0; j < njobs; j++) vox += (double)jobs[j].xsize * jobs[j].ysize * jobs[j].zsize;
+        c->tune_cands[cand].second = vox / std::max(bt.wall_ms, 1e-3);
+    }
     if (stats) {
-        stats->teams = teams;
+        stats->teams = used;
         stats->jobs = njobs;
-        stats->tuned_jobs = first;
+        stats->tuning = cand >= 0 ? 1 : 0;
         stats->ms_wall = (float)bt.wall_ms;
         stats->ms_oift = (float)bt.oift_ms;
         stats->ms_relax = (float)bt.relax_ms;

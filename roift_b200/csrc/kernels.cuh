@@ -43,13 +43,15 @@ struct OiftGlobals {
     int levels;
     unsigned long long tile_steps;
     unsigned long long pushes;
-    unsigned long long cycles[16];  // summed warp cycles: level sync, owner phase, queued
+    unsigned long long cycles[24];  // summed warp cycles: level sync, owner phase, queued
                                     // tiles, drain; key staging, sparse tiles, dense tiles,
                                     // #stale, #sparse, #dense; dense: masks, flood, flood
-                                    // iterations, expansion, faces, pending
+                                    // iterations, expansion, faces, pending; sparse:
+                                    // worklist, flood rounds, face pushes, publication,
+                                    // pending, #rounds, #voxels, #publications
     int job;       // job of the batched kernel this team works on
     int bad_seed;  // OIFT_E_* of an invalid seed of the team's current job, else 0
-    unsigned int pad4[24];
+    unsigned int pad4[8];
 };
 
 
@@ -104,7 +106,6 @@ struct OiftTeamJob {
     int32_t *cost, *label;  // device outputs, each may be null
     int X, Y, Z, nseeds;
     int ntx, nty, ntz, ntiles;
-    int mbox_words;      // re-activation words per warp for the team size of the launch
     float pol0;          // polarity (x100) of label 0
     float pol_default;   // polarity (x100) of every other label
     int status;          // out: OIFT_OK or OIFT_E_*; OIFT_TEAM_NOT_RUN until a team ends it
@@ -126,12 +127,13 @@ struct OiftTeamScratch {
     int *abort;               // set when a team stops on an error; others take no new job
 };
 
-// Batched OIFT: one cooperative launch of teams * team_ctas CTAs; each team of team_ctas
-// CTAs repeatedly draws the next job from d_jobs (in array order), clears its state, seeds,
-// runs the level loop with a team barrier and writes cost / label.  All jobs of one call
-// must be 2D (Z == 1) when planar, else 3D.  Returns OIFT_OK once the launch completed;
-// per-job results are in d_jobs[].status.
-int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int team_ctas,
+// Batched OIFT: one cooperative launch of `ctas` CTAs split into `teams` teams of
+// ctas/teams or ctas/teams + 1 CTAs; each team repeatedly draws the next job from d_jobs
+// (in array order), clears its state, seeds, runs the level loop with a team barrier and
+// writes cost / label.  All jobs of one call must be 2D (Z == 1) when planar, else 3D.
+// The mailbox stride must hold oift_mbox_bytes for both team sizes.  Returns OIFT_OK once
+// the launch is queued; per-job results are in d_jobs[].status.
+int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ctas,
                   const OiftTeamScratch &S, cudaStream_t st);
 
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,

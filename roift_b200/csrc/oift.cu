@@ -63,6 +63,19 @@ __device__ __forceinline__ unsigned long long vload(const volatile unsigned long
     return *p;
 }
 
+// Asynchronous global -> shared copies (cp.async): 16 bytes through L2 only, 4 bytes.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // Barrier over the `nctas` CTAs that share `g` (the whole cooperative grid, or one team of
 // the batched kernel), with a bounded wait.  Returns false, in every thread of the CTA, when
 // the wait ended on an error flag or on the spin limit instead of the last arrival.
@@ -129,7 +142,7 @@ template <int TY, int TZ>
 __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
                              double fgt, double flt, int bgt, int blt, uint32_t *skey,
                              uint16_t *sw, uint16_t *shx, uint16_t *shy, uint16_t *shz,
-                             uint32_t *wl, int *wcount, uint32_t *rmask, long long *cyc) {
+                             uint32_t *wl, uint32_t *nfm, uint32_t *rmask, long long *cyc) {
     long long tc0 = clock64();
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -193,10 +206,13 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
     };
     auto pending = [&]() {
         uint32_t m = OIFT_KEY_INF;
-#pragma unroll 8
-        for (int r = 0; r < 32; r++) {
-            uint32_t v = skey[r * 32 + lane];
-            if (v > kk && v < m) m = v;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint4 v = reinterpret_cast<const uint4 *>(skey)[lane + 32 * i];
+            if (v.x > kk && v.x < m) m = v.x;
+            if (v.y > kk && v.y < m) m = v.y;
+            if (v.z > kk && v.z < m) m = v.z;
+            if (v.w > kk && v.w < m) m = v.w;
         }
         for (int o = 16; o > 0; o >>= 1) {
             uint32_t v = __shfl_xor_sync(FULL, m, o);
@@ -204,18 +220,53 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         }
         if (lane == 0 && m != OIFT_KEY_INF) atomicMin(&A.tpend[t], m);
     };
-    // ---- stage the keys of the tile in shared memory ----
+    // ---- stage keys, edge codes and the -x/-y/-z halo codes in shared memory ----
+    // shx holds the -x halo as 32-bit pairs (codes of x0-2, x0-1): entry 2r+1 is row r's.
     const bool full = (x0 + 32 <= X) && (y0 + TY <= Y) && (z0 + TZ <= Z) && ((X & 7) == 0);
     if (full) {
-        uint4 kv[8];
+        // one round trip: every lane queues its 16-byte chunks as asynchronous copies and
+        // waits for all of them (rows start 16-byte aligned since X % 8 == 0, x0 % 32 == 0)
 #pragma unroll
         for (int m = 0; m < 8; m++) {
             const int j = lane + 32 * m, r = j >> 3, col = j & 7;
             const size_t p0 = (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
-            kv[m] = __ldcg(reinterpret_cast<const uint4 *>(A.key + p0) + col);
+            cp_async16(reinterpret_cast<uint4 *>(skey) + j,
+                       reinterpret_cast<const uint4 *>(A.key + p0) + col);
         }
 #pragma unroll
-        for (int m = 0; m < 8; m++) reinterpret_cast<uint4 *>(skey)[lane + 32 * m] = kv[m];
+        for (int m = 0; m < 12; m++) {
+            const int j = lane + 32 * m, pl = j >> 7, r = (j >> 2) & 31, col = j & 3;
+            const size_t p0 = (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
+            if (pl < 2 || has_z)
+                cp_async16(reinterpret_cast<uint4 *>(sw) + j,
+                           reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
+            else
+                reinterpret_cast<uint4 *>(sw)[j] = make_uint4(0, 0, 0, 0);
+        }
+        {
+            const int yr = y0 + (lane % TY), zr = z0 + (lane / TY);
+            if (x0 > 0)
+                cp_async4(shx + 2 * lane, A.W + (size_t)(x0 - 2) + (size_t)yr * X + (size_t)zr * XY);
+            else
+                shx[2 * lane + 1] = 0;
+        }
+        if (lane < 4 * TZ) {
+            const int zl = lane >> 2, col = lane & 3;
+            if (y0 > 0)
+                cp_async16(shy + zl * 32 + col * 8,
+                           A.W + N + (size_t)(x0 + col * 8) + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY);
+            else
+                *reinterpret_cast<uint4 *>(shy + zl * 32 + col * 8) = make_uint4(0, 0, 0, 0);
+        }
+        if (TZ > 1) {
+            const int yl = lane >> 2, col = lane & 3;
+            if (z0 > 0)
+                cp_async16(shz + yl * 32 + col * 8,
+                           A.W + 2 * N + (size_t)(x0 + col * 8) + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY);
+            else
+                *reinterpret_cast<uint4 *>(shz + yl * 32 + col * 8) = make_uint4(0, 0, 0, 0);
+        }
+        cp_async_wait_all();
     } else {
 #pragma unroll 4
         for (int r = 0; r < 32; r++) {
@@ -224,9 +275,6 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
             skey[r * 32 + lane] =
                 valid ? __ldcg(&A.key[(size_t)x + (size_t)y * X + (size_t)z * XY]) : 0u;
         }
-    }
-    // ---- stage the edge codes of the tile and of its -x/-y/-z halo faces ----
-    {
         const int yr = y0 + (lane % TY), zr = z0 + (lane / TY);
         uint16_t hx = 0, hy[TZ], hz[TY];
         if (x0 > 0 && yr < Y && zr < Z)
@@ -239,31 +287,15 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         for (int yl = 0; yl < TY; yl++)
             hz[yl] = (TZ > 1 && has_z && z0 > 0 && x < X && y0 + yl < Y)
                 ? __ldg(&A.W[2 * N + (size_t)x + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY]) : 0;
-        if (full) {
-            uint4 cv[12];
-#pragma unroll
-            for (int m = 0; m < 12; m++) {
-                const int j = lane + 32 * m, pl = j >> 7, r = (j >> 2) & 31, col = j & 3;
-                const size_t p0 =
-                    (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
-                if (pl < 2 || has_z)
-                    cv[m] = __ldg(reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
-                else
-                    cv[m] = make_uint4(0, 0, 0, 0);
-            }
-#pragma unroll
-            for (int m = 0; m < 12; m++) reinterpret_cast<uint4 *>(sw)[lane + 32 * m] = cv[m];
-        } else {
-            for (int r = 0; r < 32; r++) {
-                const int y = y0 + (r % TY), z = z0 + (r / TY);
-                const bool valid = (x < X) && (y < Y) && (z < Z);
-                const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
-                sw[r * 32 + lane] = valid ? __ldg(&A.W[p]) : 0;
-                sw[1024 + r * 32 + lane] = valid ? __ldg(&A.W[N + p]) : 0;
-                sw[2048 + r * 32 + lane] = (valid && has_z) ? __ldg(&A.W[2 * N + p]) : 0;
-            }
+        for (int r = 0; r < 32; r++) {
+            const int y = y0 + (r % TY), z = z0 + (r / TY);
+            const bool valid = (x < X) && (y < Y) && (z < Z);
+            const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+            sw[r * 32 + lane] = valid ? __ldg(&A.W[p]) : 0;
+            sw[1024 + r * 32 + lane] = valid ? __ldg(&A.W[N + p]) : 0;
+            sw[2048 + r * 32 + lane] = (valid && has_z) ? __ldg(&A.W[2 * N + p]) : 0;
         }
-        shx[lane] = hx;
+        shx[2 * lane + 1] = hx;
 #pragma unroll
         for (int zl = 0; zl < TZ; zl++) shy[zl * 32 + lane] = hy[zl];
         if (TZ > 1) {
@@ -272,10 +304,20 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         }
     }
     __syncwarp();
-    // ---- how many voxels of the tile sit at this level? ----
-    int nf0 = 0;
+    // ---- level rows: lane r keeps row r's voxels at this level (rowF) and those at or
+    // below it, i.e. at this level or expanded before (rowV) ----
+    uint32_t rowF = 0, rowV = 0;
 #pragma unroll 8
-    for (int r = 0; r < 32; r++) nf0 += (skey[r * 32 + lane] == kk);
+    for (int r = 0; r < 32; r++) {
+        const uint32_t k = skey[r * 32 + lane];
+        const uint32_t bF = __ballot_sync(FULL, k == kk);
+        const uint32_t bV = __ballot_sync(FULL, k <= kk);
+        if (lane == r) {
+            rowF = bF;
+            rowV = bV;
+        }
+    }
+    int nf0 = __popc(rowF);
     for (int o = 16; o > 0; o >>= 1) nf0 += __shfl_xor_sync(FULL, nf0, o);
     const long long tcount = clock64();
     cyc[0] += tcount - tc0;
@@ -287,27 +329,93 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
     bool dense = nf0 > OIFT_SPARSE_MAX;
     if (!dense) {
         // ---- sparse mode: flood and expand from a voxel worklist ----
-        if (lane == 0) *wcount = 0;
+        // append_rows(m, base): the voxels of row `lane` in m join the worklist after `base`
+        // entries (a warp prefix sum places them) and are marked at this level; returns the
+        // new count.  Entries past OIFT_WORKLIST are not stored: the caller switches to the
+        // dense path, which finds them through their key.
+        auto append_rows = [&](uint32_t m, int base) -> int {
+            const int n = __popc(m);
+            int incl = n;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(FULL, incl, 31);
+            int pos = base + incl - n;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                const uint32_t li = (uint32_t)(lane << 5 | b);
+                if (pos < OIFT_WORKLIST) wl[pos] = li;
+                skey[li] = kk;
+                pos++;
+            }
+            return base + total;
+        };
+        const long long ts0 = clock64();
+        nfm[lane] = 0u;
+        int cnt = append_rows(rowF, 0);
         __syncwarp();
-        for (int r = 0; r < 32; r++) {
-            const bool isf = skey[r * 32 + lane] == kk;
-            const uint32_t b = __ballot_sync(FULL, isf);
-            if (!b) continue;
-            int base = 0;
-            if (lane == 0) base = atomicAdd(wcount, __popc(b));
-            base = __shfl_sync(FULL, base, 0);
-            if (isf) wl[base + __popc(b & ((1u << lane) - 1u))] = (uint32_t)(r << 5 | lane);
-        }
-        int done = 0;
+        // Pushes across the tile faces from the expanded voxels wl[0, n), all lanes at once:
+        // the flood rounds stay in shared memory and the global atomics of the tile step
+        // share one round trip.
+        auto push_out = [&](int n) {
+            for (int base = 0; base < n; base += 32) {
+                const int idx = base + lane;
+                // one slot per axis: a voxel leaves the tile at most once along each axis
+                uint32_t nk[3] = {OIFT_KEY_INF, OIFT_KEY_INF, OIFT_KEY_INF}, old[3] = {0, 0, 0};
+                int qx[3] = {0, 0, 0}, qy[3] = {0, 0, 0}, qz[3] = {0, 0, 0};
+                if (idx < n) {
+                    const uint32_t li = wl[idx];
+                    const int r = (int)(li >> 5), xl = (int)(li & 31);
+                    const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
+                    if (xl == 0 && xg > 0) {
+                        nk[0] = arc_key(shx[2 * r + 1], false);
+                        qx[0] = xg - 1; qy[0] = y; qz[0] = z;
+                    } else if (xl == 31 && xg + 1 < X) {
+                        nk[0] = arc_key(sw[r * 32 + xl], true);
+                        qx[0] = xg + 1; qy[0] = y; qz[0] = z;
+                    }
+                    if ((r % TY) == 0 && y > 0) {
+                        nk[1] = arc_key(shy[(r / TY) * 32 + xl], false);
+                        qx[1] = xg; qy[1] = y - 1; qz[1] = z;
+                    } else if ((r % TY) == TY - 1 && y + 1 < Y) {
+                        nk[1] = arc_key(sw[1024 + r * 32 + xl], true);
+                        qx[1] = xg; qy[1] = y + 1; qz[1] = z;
+                    }
+                    if (has_z) {
+                        if (r < TY && z > 0) {
+                            nk[2] = arc_key(TZ > 1 ? shz[(r % TY) * 32 + xl] : 0u, false);
+                            qx[2] = xg; qy[2] = y; qz[2] = z - 1;
+                        } else if (r + TY >= 32 && z + 1 < Z) {
+                            nk[2] = arc_key(sw[2048 + r * 32 + xl], true);
+                            qx[2] = xg; qy[2] = y; qz[2] = z + 1;
+                        }
+                    }
+#pragma unroll
+                    for (int a = 0; a < 3; a++)
+                        if (nk[a] != OIFT_KEY_INF)
+                            old[a] = atomicMin(&A.key[(size_t)qx[a] + (size_t)qy[a] * X +
+                                                      (size_t)qz[a] * XY], nk[a]);
+                }
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                    if (nk[a] != OIFT_KEY_INF) settle(nk[a], old[a], qx[a], qy[a], qz[a]);
+            }
+        };
+        int done = 0, rounds = 0;
+        const long long ts1 = clock64();
+        cyc[12] += ts1 - ts0;
         for (;;) {
-            __syncwarp();
-            const int cnt = *(volatile int *)wcount;
             if (cnt > OIFT_WORKLIST) {  // overflow: the dense path finishes the level
+                push_out(done);
                 dense = true;
                 break;
             }
             if (done >= cnt) break;
-
+            // ---- one flood round: expand up to 32 worklist voxels, one per lane; open arcs
+            // mark their in-tile heads in nfm, other arcs lower the heads' keys ----
             const int idx = done + lane;
             if (idx < cnt) {
                 const uint32_t li = wl[idx];
@@ -315,83 +423,78 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
                 const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
                 const size_t p = (size_t)xg + (size_t)y * X + (size_t)z * XY;
                 const uint32_t cxp = sw[r * 32 + xl];
-                const uint32_t cxm = xl > 0 ? sw[r * 32 + xl - 1] : shx[r];
+                const uint32_t cxm = xl > 0 ? sw[r * 32 + xl - 1] : 0u;
                 const uint32_t cyp = sw[1024 + r * 32 + xl];
-                const uint32_t cym = (r % TY) > 0 ? sw[1024 + (r - 1) * 32 + xl]
-                                                  : shy[(r / TY) * 32 + xl];
+                const uint32_t cym = (r % TY) > 0 ? sw[1024 + (r - 1) * 32 + xl] : 0u;
                 const uint32_t czp = sw[2048 + r * 32 + xl];
-                const uint32_t czm = r >= TY ? sw[2048 + (r - TY) * 32 + xl]
-                                             : (TZ > 1 ? shz[(r % TY) * 32 + xl] : 0u);
+                const uint32_t czm = r >= TY ? sw[2048 + (r - TY) * 32 + xl] : 0u;
                 A.key[p] = kexp;
                 skey[li] = kexp;
-                uint32_t onk[6], oold[6];
-                int oq[6];
 #pragma unroll
                 for (int d = 0; d < 6; d++) {
-                    onk[d] = OIFT_KEY_INF;
-                    oold[d] = 0;
-                    oq[d] = -1;
-                    int qx = xg, qy = y, qz = z, rq = r, xq = xl;
+                    int rq = r, xq = xl;
                     uint32_t code;
-                    bool tail_low, ok, in_tile;
+                    bool tail_low, in_tile;
                     if (d == 0) {  // -z
-                        ok = has_z && z > 0; qz = z - 1; rq = r - TY; in_tile = r >= TY;
-                        code = czm; tail_low = false;
+                        rq = r - TY; in_tile = r >= TY; code = czm; tail_low = false;
                     } else if (d == 1) {  // -y
-                        ok = y > 0; qy = y - 1; rq = r - 1; in_tile = (r % TY) > 0;
-                        code = cym; tail_low = false;
+                        rq = r - 1; in_tile = (r % TY) > 0; code = cym; tail_low = false;
                     } else if (d == 2) {  // -x
-                        ok = xg > 0; qx = xg - 1; xq = xl - 1; in_tile = xl > 0;
-                        code = cxm; tail_low = false;
+                        xq = xl - 1; in_tile = xl > 0; code = cxm; tail_low = false;
                     } else if (d == 3) {  // +x
-                        ok = xg + 1 < X; qx = xg + 1; xq = xl + 1; in_tile = xl < 31;
-                        code = cxp; tail_low = true;
+                        xq = xl + 1; in_tile = xl < 31 && xg + 1 < X; code = cxp; tail_low = true;
                     } else if (d == 4) {  // +y
-                        ok = y + 1 < Y; qy = y + 1; rq = r + 1; in_tile = (r % TY) < TY - 1;
-                        code = cyp; tail_low = true;
+                        rq = r + 1; in_tile = (r % TY) < TY - 1 && y + 1 < Y; code = cyp;
+                        tail_low = true;
                     } else {  // +z
-                        ok = has_z && z + 1 < Z; qz = z + 1; rq = r + TY; in_tile = r + TY < 32;
-                        code = czp; tail_low = true;
+                        rq = r + TY; in_tile = r + TY < 32 && has_z && z + 1 < Z; code = czp;
+                        tail_low = true;
                     }
-                    if (!ok) continue;
-                    const size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * XY;
-                    if (in_tile) {
-                        const int lq = rq * 32 + xq;
-                        const uint32_t sk = *(volatile uint32_t *)&skey[lq];
-                        if (sk <= kk) continue;  // already at this level or expanded
-                        if (arc_ok(code, tail_low, c, bgt, blt)) {
-                            const uint32_t old = atomicMin(&skey[lq], kk);
-                            if (old > kk) {
-                                const int pos = atomicAdd(wcount, 1);
-                                if (pos < OIFT_WORKLIST) wl[pos] = (uint32_t)lq;
-                            }
-                        } else {
-                            const uint32_t nk = arc_key(code, tail_low);
-                            const uint32_t old = atomicMin(&skey[lq], nk);
-                            if (nk < old) atomicMin(&A.key[q], nk);
-                        }
+                    if (!in_tile) continue;  // across a face: push_out
+                    const int lq = rq * 32 + xq;
+                    // keys only decrease, so a stale read costs at most a redundant push
+                    const uint32_t sk = skey[lq];
+                    if (sk <= kk) continue;  // at this level or expanded
+                    if (arc_ok(code, tail_low, c, bgt, blt)) {
+                        atomicOr(&nfm[rq], 1u << xq);
                     } else {
-                        onk[d] = arc_key(code, tail_low);
-                        oold[d] = atomicMin(&A.key[q], onk[d]);
-                        oq[d] = d;
+                        const uint32_t nk = arc_key(code, tail_low);
+                        if (nk < sk) {
+                            atomicMin(&skey[lq], nk);
+                            atomicMin(&A.key[(size_t)(x0 + xq) + (size_t)(y0 + rq % TY) * X +
+                                             (size_t)(z0 + rq / TY) * XY], nk);
+                        }
                     }
-                }
-#pragma unroll
-                for (int d = 0; d < 6; d++) {
-                    if (oq[d] < 0) continue;
-                    const int qx = xg + (d == 2 ? -1 : d == 3 ? 1 : 0);
-                    const int qy = y + (d == 1 ? -1 : d == 4 ? 1 : 0);
-                    const int qz = z + (d == 0 ? -1 : d == 5 ? 1 : 0);
-                    settle(onk[d], oold[d], qx, qy, qz);
                 }
             }
             done = (done + 32 < cnt) ? done + 32 : cnt;
+            rounds++;
+            __syncwarp();
+            // ---- the next flood layer: heads reached in this round and not visited ----
+            const uint32_t m = nfm[lane] & ~rowV;
+            nfm[lane] = 0u;
+            rowV |= m;
+            cnt = append_rows(m, cnt);
+            __syncwarp();
         }
         __syncwarp();
         if (!dense) {
+            const long long ts2 = clock64();
+            push_out(done);
+            __syncwarp();
+            const long long ts3 = clock64();
+            cyc[19] += (*(volatile uint32_t *)rmask != 0u);
             flush_reactivations();
+            const long long ts4 = clock64();
             pending();
-            cyc[1] += clock64() - tcount;
+            const long long ts5 = clock64();
+            cyc[13] += ts2 - ts1;
+            cyc[14] += ts3 - ts2;
+            cyc[15] += ts4 - ts3;
+            cyc[16] += ts5 - ts4;
+            cyc[17] += rounds;
+            cyc[18] += done;
+            cyc[1] += ts5 - tcount;
             cyc[4] += 1;
             return;
         }
@@ -502,7 +605,7 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
         const bool px = ((F >> 31) & 1u) && x0 + 32 < X;
         uint32_t nkm = OIFT_KEY_INF, nkp = OIFT_KEY_INF, om = 0, op = 0;
         if (mx) {
-            nkm = arc_key(shx[lane], false);
+            nkm = arc_key(shx[2 * lane + 1], false);
             om = atomicMin(&A.key[prow + x0 - 1], nkm);
         }
         if (px) {
@@ -573,12 +676,17 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
     cyc[5] += 1;
 }
 
+// Re-activation bitmask words per warp when `nwarps` warps own `ntiles` tiles round-robin.
+__host__ __device__ __forceinline__ int oift_mbox_words_for(int ntiles, int nwarps) {
+    return ((ntiles + nwarps - 1) / nwarps + 63) / 64;
+}
+
 // Shared-memory working set of one CTA of the persistent kernels.
 struct OiftCtaSmem {
     uint32_t blk_min[OIFT_WARPS];
     uint32_t level;
     uint32_t wl[OIFT_WARPS][OIFT_WORKLIST];
-    int wcount[OIFT_WARPS];
+    uint32_t nfm[OIFT_WARPS][32];  // per row: voxels reached by open arcs in a flood round
     uint32_t rmask[OIFT_WARPS];
 };
 
@@ -591,16 +699,18 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *skey = reinterpret_cast<uint32_t *>(smem_raw) + warp * 1024;
     uint16_t *sw = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * 4096) + warp * 3072;
-    uint16_t *shx = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * (4096 + 6144)) + warp * 416;
-    uint16_t *shy = shx + 32;
-    uint16_t *shz = shx + 32 + 4 * 32;
+    uint16_t *shx = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * (4096 + 6144)) + warp * 448;
+    uint16_t *shy = shx + 64;
+    uint16_t *shz = shx + 64 + 4 * 32;
     uint32_t *blk_min = cs.blk_min;
-    long long cyc_tile[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    long long cyc_tile[20];
+#pragma unroll
+    for (int i = 0; i < 20; i++) cyc_tile[i] = 0;
     uint32_t *rmask = &cs.rmask[warp];
     if (lane == 0) *rmask = 0u;
     __syncwarp();
     uint32_t *wl = cs.wl[warp];
-    int *wcount = &cs.wcount[warp];
+    uint32_t *nfm = cs.nfm[warp];
     OiftGlobals *g = A.g;
     const int gwarp = team_cta * OIFT_WARPS + warp;
     const int nwarps = team_ctas * OIFT_WARPS;
@@ -670,7 +780,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 if (lane == 0) A.tpend[th] = OIFT_KEY_INF;
                 __syncwarp();
                 process_tile<TY, TZ>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey, sw,
-                                     shx, shy, shz, wl, wcount, rmask, cyc_tile);
+                                     shx, shy, shz, wl, nfm, rmask, cyc_tile);
                 steps++;
             }
         }
@@ -705,7 +815,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                         b &= b - 1;
                         const int t = gwarp + j * nwarps;
                         process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey,
-                                             sw, shx, shy, shz, wl, wcount, rmask, cyc_tile);
+                                             sw, shx, shy, shz, wl, nfm, rmask, cyc_tile);
                         steps++;
                         __threadfence();
                         __syncwarp();
@@ -742,7 +852,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         atomicAdd(&g->cycles[1], (unsigned long long)cyc_owner);
         atomicAdd(&g->cycles[2], (unsigned long long)cyc_busy);
         atomicAdd(&g->cycles[3], (unsigned long long)cyc_drain);
-        for (int i = 0; i < 12; i++) atomicAdd(&g->cycles[4 + i], (unsigned long long)cyc_tile[i]);
+        for (int i = 0; i < 20; i++) atomicAdd(&g->cycles[4 + i], (unsigned long long)cyc_tile[i]);
     }
 }
 
@@ -762,13 +872,18 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
 // team ended keep status OIFT_TEAM_NOT_RUN.
 template <int TY, int TZ>
 __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
-    oift_team_kernel(OiftTeamJob *jobs, int njobs, int team_ctas, OiftTeamScratch S,
+    oift_team_kernel(OiftTeamJob *jobs, int njobs, int teams, OiftTeamScratch S,
                      long long spin_limit, int max_levels) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ OiftCtaSmem cs;
     __shared__ OiftArgs sA;
     __shared__ int s_job, s_bad;
-    const int team = blockIdx.x / team_ctas, tc = blockIdx.x - team * team_ctas;
+    // team t owns CTAs [t*G/T, (t+1)*G/T): sizes differ by at most one CTA
+    const unsigned G = gridDim.x, T = (unsigned)teams;
+    const int team = (int)(((blockIdx.x + 1) * T - 1) / G);
+    const int cta0 = (int)((unsigned long long)team * G / T);
+    const int team_ctas = (int)((unsigned long long)(team + 1) * G / T) - cta0;
+    const int tc = blockIdx.x - cta0;
     OiftGlobals *g = S.g + team;
     uint32_t *key = S.key + (size_t)team * S.key_stride;
     uint32_t *tpend = S.tpend + (size_t)team * S.tpend_stride;
@@ -792,7 +907,8 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
         if (j >= njobs) break;
         OiftTeamJob *J = jobs + j;
         const int X = J->X, Y = J->Y, Z = J->Z, ntx = J->ntx, nty = J->nty;
-        const int ntiles = J->ntiles, mbox_words = J->mbox_words;
+        const int ntiles = J->ntiles;
+        const int mbox_words = oift_mbox_words_for(ntiles, team_ctas * OIFT_WARPS);
         const size_t N = (size_t)X * Y * Z;
         if (threadIdx.x == 0) {
             sA.key = key;
@@ -924,14 +1040,12 @@ OiftPlan oift_plan(int X, int Y, int Z) {
     return P;
 }
 
-size_t oift_smem_bytes() { return (size_t)OIFT_WARPS * (4096 + 6144 + 832); }
+size_t oift_smem_bytes() { return (size_t)OIFT_WARPS * (4096 + 6144 + 896); }
 
 
 size_t oift_globals_bytes() { return sizeof(OiftGlobals); }
 int oift_mbox_words(const OiftPlan &P, int ctas) {
-    const int nw = ctas * OIFT_WARPS;
-    const int per_warp = (P.ntiles + nw - 1) / nw;
-    return (per_warp + 63) / 64;
+    return oift_mbox_words_for(P.ntiles, ctas * OIFT_WARPS);
 }
 size_t oift_mbox_bytes(const OiftPlan &P, int ctas) {
     return (size_t)ctas * OIFT_WARPS * oift_mbox_words(P, ctas) * sizeof(unsigned long long);
@@ -1016,16 +1130,16 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     if (levels_out) *levels_out = hg.levels;
     if (steps_out) *steps_out = (long long)hg.tile_steps;
     if (cycles_out)
-        for (int i = 0; i < 16; i++) cycles_out[i] = hg.cycles[i];
+        for (int i = 0; i < 24; i++) cycles_out[i] = hg.cycles[i];
     if (hg.error == OIFT_DEV_TIMEOUT) return OIFT_E_NOT_CONVERGED;
     if (hg.error == OIFT_DEV_QUEUE) return OIFT_E_QUEUE_OVERFLOW;
     return OIFT_OK;
 }
 
-int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int team_ctas,
+int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ctas,
                   const OiftTeamScratch &S, cudaStream_t st) {
     if (njobs <= 0) return OIFT_OK;
-    if (teams <= 0 || team_ctas <= 0) return OIFT_E_BAD_ARG;
+    if (teams <= 0 || ctas < teams) return OIFT_E_BAD_ARG;
     if (cudaMemsetAsync(S.g, 0, (size_t)teams * sizeof(OiftGlobals), st) != cudaSuccess ||
         cudaMemsetAsync(S.next_job, 0, sizeof(unsigned int), st) != cudaSuccess ||
         cudaMemsetAsync(S.abort, 0, sizeof(int), st) != cudaSuccess) {
@@ -1034,21 +1148,21 @@ int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int te
     }
     long long spin_limit = 20000000LL;
     int max_levels = 4000000;
-    int tc = team_ctas;
+    int nt = teams;
     OiftTeamScratch sc = S;
-    void *args[] = {&d_jobs, &njobs, &tc, &sc, &spin_limit, &max_levels};
+    void *args[] = {&d_jobs, &njobs, &nt, &sc, &spin_limit, &max_levels};
     const size_t smem = oift_smem_bytes();
     cudaError_t err;
     if (planar) {
         auto kfn = oift_team_kernel<32, 1>;
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(teams * team_ctas),
-                                          dim3(OIFT_WARPS * 32), args, smem, st);
+        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(ctas), dim3(OIFT_WARPS * 32), args,
+                                          smem, st);
     } else {
         auto kfn = oift_team_kernel<8, 4>;
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(teams * team_ctas),
-                                          dim3(OIFT_WARPS * 32), args, smem, st);
+        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(ctas), dim3(OIFT_WARPS * 32), args,
+                                          smem, st);
     }
     if (err != cudaSuccess) {
         cudaGetLastError();
