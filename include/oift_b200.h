@@ -167,6 +167,32 @@ OIFT_API int oift_b200_run_batch(oift_b200_ctx *ctx, const oift_b200_params *com
 /* CTAs of the persistent OIFT grid of this context (0 = one per SM, the default). */
 OIFT_API int oift_b200_set_oift_grid(oift_b200_ctx *ctx, int ctas);
 
+/* Steps around the path in the reference CLI (oiftrelax.cpp main). */
+/* `passes` Gaussian blurs (Scene32::GaussianBlur, gft_filtering3.cpp:385-397) of a device
+ * int32 volume; in == out allowed. */
+OIFT_API int oift_b200_gaussian_blur_i32(oift_b200_ctx *ctx, const int32_t *in, int32_t *out,
+                                         int xsize, int ysize, int zsize, int passes);
+/* Conditional dilation (oiftrelax.cpp:87-169) of a device label map: label-0 voxels within
+ * Spheric(radius) of a label-1 voxel whose `image` value ranks within the percentile become
+ * 1.  *added (may be NULL) receives the count. */
+OIFT_API int oift_b200_conditional_dilation(oift_b200_ctx *ctx, const int32_t *image,
+                                            int32_t *label, int xsize, int ysize, int zsize,
+                                            float radius, float percentile, long long *added);
+/* Boundary seeds (oiftrelax.cpp:175-224) on host arrays: face voxels on the stride grid
+ * whose label is NIL (-1) become background (0) and are appended to seeds_out.  Returns the
+ * number of seeds (with seeds_out == NULL: counts only, changes nothing), OIFT_E_RANGE if
+ * cap is too small. */
+OIFT_API int oift_b200_inject_boundary_seeds(int32_t *label, int xsize, int ysize, int zsize,
+                                             int stride, int32_t *seeds_out, int cap);
+/* The CLI's processing chain on host buffers: shift the unshifted int32 `image` to >= 0,
+ * `blur_passes` Gaussian blurs (the CLI uses 2), OIFT + relax_sweeps sweeps as run_host,
+ * then, if percentile >= 0 and the result is binary, the conditional dilation with
+ * Spheric(1).  `label` holds the seed labels on entry and the result on return. */
+OIFT_API int oift_b200_run_cli_host(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                                    const int32_t *image, int32_t *label, const int32_t *seeds,
+                                    int nseeds, int blur_passes, float percentile,
+                                    oift_b200_stats *stats);
+
 /* Stage entry points on device pointers (used by the batched driver and tests). */
 OIFT_API int oift_b200_build_weights_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
                                 const int16_t *image, uint16_t *weights /* [planes][N] */,

@@ -73,6 +73,12 @@ def lib():
         L.or_relax_f64.restype = C.c_int
         L.or_relax_f64.argtypes = L.or_relax_f32.argtypes
         L.or_gaussian_blur.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        L.or_conditional_dilation.restype = C.c_longlong
+        L.or_conditional_dilation.argtypes = [_i32p, _i32p, C.c_int, C.c_int, C.c_int,
+                                              C.c_float, C.c_float]
+        L.or_inject_boundary_seeds.restype = C.c_int
+        L.or_inject_boundary_seeds.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                               _i32p, C.c_int]
         _lib = L
     return _lib
 
@@ -99,6 +105,13 @@ def ref():
         R.ref_energy_min_graph.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, _i32p,
                                            C.c_int]
         R.ref_gaussian_blur.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        R.ref_dilation_conditional.argtypes = [_i32p, _i32p, C.c_int, C.c_int, C.c_int,
+                                               C.c_float, C.c_float]
+        R.ref_inject_boundary_seeds.restype = C.c_int
+        R.ref_inject_boundary_seeds.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                _i32p, C.c_int, _i32p, C.c_int]
+        R.ref_oiftrelax_chain.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                          C.c_int, C.c_float, _i32p, C.c_int, _i32p]
         _ref = R
     return _ref
 
@@ -216,6 +229,46 @@ def relax(img, adj, seeds, label, ntimes, pol=None, per_class=None, fp64=False):
     return lab, mem.reshape(nc, N), nc
 
 
+def conditional_dilation(img, label, radius=1.0, percentile=50.0):
+    """R-restatement of oiftrelax.cpp:87-169 on copies: (label after, voxels added)."""
+    X, Y, Z = _dims(img)
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    n = lib().or_conditional_dilation(as_i32(img), lab, X, Y, Z, radius, percentile)
+    return lab, n
+
+
+def inject_boundary_seeds(label, shape_zyx, stride):
+    """Restatement of oiftrelax.cpp:175-224: (label after, new seeds)."""
+    Z, Y, X = shape_zyx
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    out = np.empty(X * Y * Z, np.int32)
+    n = lib().or_inject_boundary_seeds(lab, X, Y, Z, stride, out, len(out))
+    return lab, out[:n].copy()
+
+
+def oiftrelax_chain(img, pol, niter, percentile, seeds, seed_labels, oift="r2", blur=2):
+    """The CLI chain restated (oiftrelax.cpp main 263-268, 368-414): shift to >= 0, `blur`
+    Gaussian blurs, exact-gradient OIFT (R2, or R1 = OIFT_Multi's Prim order), R3-FP32
+    relaxation with niter sweeps, conditional dilation (Spheric(1)) when binary.
+    Returns (label, blurred image)."""
+    shape = img.shape
+    X, Y, Z = _dims(img)
+    b = np.asarray(img, np.int64)
+    b = (b - min(0, int(b.min()))).astype(np.int32)
+    for _ in range(blur):
+        b = gaussian_blur(b.reshape(shape)).reshape(shape)
+    W, _ = build_weights(b, 6 if Z > 1 else 4, "grad")
+    adj = 6 if Z > 1 else 4
+    if oift == "r2":
+        _, lab, _ = oift_fmax(W, (X, Y, Z), adj, seeds, seed_labels, pol=pol)
+    else:
+        lab = oift_prim(W, (X, Y, Z), adj, seeds, seed_labels, pol=pol)[0]
+    out, _, _ = relax(b, adj, seeds, lab, niter, pol=pol)
+    if out.max() <= 1:
+        out, _ = conditional_dilation(b, out, 1.0, percentile)
+    return out, b
+
+
 def gaussian_blur(img):
     X, Y, Z = _dims(img)
     out = np.empty(X * Y * Z, np.int32)
@@ -295,6 +348,33 @@ def ref_oift_fmax_gpu_run(img, seeds, seed_labels, per_class):
         os.close(saved)
         os.close(devnull)
     return lab, waves
+
+
+def ref_dilation_conditional(img, label, radius=1.0, percentile=50.0):
+    """Reference dilation_conditional (oiftrelax.cpp:149-165) on copies; returns the label."""
+    X, Y, Z = _dims(img)
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    ref().ref_dilation_conditional(as_i32(img), lab, X, Y, Z, radius, percentile)
+    return lab
+
+
+def ref_inject_boundary_seeds(label, shape_zyx, stride, seeds):
+    """Reference inject_boundary_seeds: (label after, seeds after)."""
+    Z, Y, X = shape_zyx
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    sd = np.ascontiguousarray(seeds, np.int32)
+    out = np.empty(len(sd) + X * Y * Z, np.int32)
+    n = ref().ref_inject_boundary_seeds(lab, X, Y, Z, stride, sd, len(sd), out, len(out))
+    return lab, out[:n].copy()
+
+
+def ref_oiftrelax_chain(img, pol, niter, percentile, seeds, label):
+    """The reference CLI chain (shift, blur x2, OIFT_Multi, ORelax_1_Multi, dilation)."""
+    X, Y, Z = _dims(img)
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    ref().ref_oiftrelax_chain(as_i32(img), X, Y, Z, float(pol), int(niter), float(percentile),
+                              np.ascontiguousarray(seeds, np.int32), len(seeds), lab)
+    return lab
 
 
 def ref_gaussian_blur(img):

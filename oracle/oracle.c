@@ -616,3 +616,78 @@ void or_gaussian_blur(const int *img, int X, int Y, int Z, int *out) {
                 out[x + y * X + z * X * Y] = (conv < 0) ? (int)(conv - 0.5) : (int)(conv + 0.5);
             }
 }
+
+/* ------------------------------------------------------ conditional dilation --- */
+/* oiftrelax.cpp:87-169 (get_dilation_border, condition_percentil, dilation_conditional):
+ * border = label-0 voxels with a label-1 voxel within Spheric(radius); the border voxels
+ * sorted by image value (stable: address order among equal values) up to index
+ * (int)(float)((percentile / 100.0) * (n - 1)) become 1.  Returns the voxels relabelled.
+ * n == 0 changes nothing (the reference indexes out of range there). */
+typedef struct {
+    int value, position;
+} or_vp;
+
+static int or_vp_cmp(const void *a, const void *b) {
+    const or_vp *u = (const or_vp *)a, *v = (const or_vp *)b;
+    if (u->value != v->value) return u->value < v->value ? -1 : 1;
+    return u->position < v->position ? -1 : (u->position > v->position);
+}
+
+long long or_conditional_dilation(const int *img, int *label, int X, int Y, int Z,
+                                  float radius, float percentile) {
+    const long long N = (long long)X * Y * Z;
+    const int r0 = (int)radius, r2 = (int)(radius * radius);
+    or_vp *bv = (or_vp *)malloc(sizeof(or_vp) * (size_t)(N > 0 ? N : 1));
+    long long n = 0;
+    for (long long p = 0; p < N; p++) {
+        if (label[p] != 0) continue;
+        const int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / ((long long)X * Y));
+        int hit = 0;
+        for (int dz = -r0; dz <= r0 && !hit; dz++)
+            for (int dy = -r0; dy <= r0 && !hit; dy++)
+                for (int dx = -r0; dx <= r0 && !hit; dx++) {
+                    if (dx * dx + dy * dy + dz * dz > r2) continue;
+                    if (!in_bounds(x + dx, y + dy, z + dz, X, Y, Z)) continue;
+                    if (label[(x + dx) + (long long)(y + dy) * X + (long long)(z + dz) * X * Y] == 1)
+                        hit = 1;
+                }
+        if (hit) {
+            bv[n].value = img[p];
+            bv[n].position = (int)p;
+            n++;
+        }
+    }
+    long long added = 0;
+    if (n > 0) {
+        qsort(bv, (size_t)n, sizeof(or_vp), or_vp_cmp);
+        const float index_percentile = (float)((percentile / 100.0) * (double)(n - 1));
+        const double ipd = (double)index_percentile;
+        long long vp = ipd >= 2147483647.0 ? 2147483647LL
+                       : ipd <= -2147483648.0 ? -2147483648LL : (long long)(int)index_percentile;
+        long long keep = vp + 1;
+        if (keep < 0) keep = 0;
+        if (keep > n) keep = n;
+        for (long long i = 0; i < keep; i++) label[bv[i].position] = 1;
+        added = keep;
+    }
+    free(bv);
+    return added;
+}
+
+/* oiftrelax.cpp:175-224: face voxels on the stride grid (z, y, x order) whose label is
+ * NIL become background seeds.  Returns how many were appended to out (cap entries). */
+int or_inject_boundary_seeds(int *label, int X, int Y, int Z, int stride, int *out, int cap) {
+    int n = 0;
+    for (int z = 0; z < Z; z += stride)
+        for (int y = 0; y < Y; y += stride)
+            for (int x = 0; x < X; x += stride) {
+                if (!(x == 0 || x == X - 1 || y == 0 || y == Y - 1 || z == 0 || z == Z - 1))
+                    continue;
+                const long long p = x + (long long)y * X + (long long)z * X * Y;
+                if (label[p] != -1) continue;
+                label[p] = 0;
+                if (n < cap) out[n] = (int)p;
+                n++;
+            }
+    return n;
+}

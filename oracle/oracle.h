@@ -104,6 +104,12 @@ int or_relax_f64(const int *img, int X, int Y, int Z, int adj, float per,
 /* GaussianBlur restatement (gft_filtering3.cpp:106-126,321-346,385-397). */
 void or_gaussian_blur(const int *img, int X, int Y, int Z, int *out);
 
+/* oiftrelax.cpp:87-169 conditional dilation (label in/out); returns voxels relabelled. */
+long long or_conditional_dilation(const int *img, int *label, int X, int Y, int Z,
+                                  float radius, float percentile);
+/* oiftrelax.cpp:175-224 boundary seeds; returns the count (out holds up to cap). */
+int or_inject_boundary_seeds(int *label, int X, int Y, int Z, int stride, int *out, int cap);
+
 #ifdef __cplusplus
 }
 #endif

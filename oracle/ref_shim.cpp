@@ -13,6 +13,12 @@
 //                                (gft/src/gft_ift.cpp:4753-4809, gft/src/gft_graph.cpp:126-155)
 //   ref_gaussian_blur         -> gft::Scene32::GaussianBlur      (gft/src/gft_filtering3.cpp:385-397)
 //   ref_energy_min_graph      -> gft::ift::GetEnergy_Min(sGraph*) (gft/src/gft_ift.cpp:4xx)
+//   ref_dilation_conditional  -> dilation_conditional             (oiftrelax.cpp:149-165)
+//   ref_inject_boundary_seeds -> inject_boundary_seeds            (oiftrelax.cpp:175-224)
+//   ref_oiftrelax_chain       -> the processing chain of the CLI main (oiftrelax.cpp:
+//                                263-268, 368-414): shift, GaussianBlur x2, OIFT_Multi,
+//                                ORelax_1_Multi, conditional dilation when binary
+// The two CLI helpers come from oiftrelax.cpp itself, compiled with its main renamed.
 //
 // Seeds are passed 0-based without a count; the 1-based S[0]=count list the
 // reference expects is built here.  Adjacency radius: 6-adj = Spheric(1.0),
@@ -43,6 +49,11 @@ static sAdjRel3 *make_adj(int adj) {
 }
 
 #define REF_API __attribute__((visibility("default")))
+
+// defined in oiftrelax.cpp (compiled into the same library with main renamed)
+void dilation_conditional(gft::sScene32 *scn, gft::sScene32 *label, float radius_sphere,
+                          float percentile);
+int inject_boundary_seeds(gft::sScene32 *label, int *&S, int current_count, int stride);
 
 extern "C" {
 
@@ -138,4 +149,55 @@ REF_API void ref_gaussian_blur(const int *img, int X, int Y, int Z, int *out) {
     Scene32::Destroy(&scn);
 }
 
+
+REF_API void ref_dilation_conditional(const int *img, int *label, int X, int Y, int Z,
+                                      float radius, float percentile) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    sScene32 *lab = make_scene(label, X, Y, Z);
+    dilation_conditional(scn, lab, radius, percentile);
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y * Z);
+    Scene32::Destroy(&lab);
+    Scene32::Destroy(&scn);
+}
+
+// Appends the boundary seeds to `seeds` (nseeds entries) into out[0, cap); returns the new
+// total count.
+REF_API int ref_inject_boundary_seeds(int *label, int X, int Y, int Z, int stride,
+                                      const int *seeds, int nseeds, int *out, int cap) {
+    sScene32 *lab = make_scene(label, X, Y, Z);
+    int *S = make_S(seeds, nseeds);
+    inject_boundary_seeds(lab, S, nseeds, stride);
+    const int total = S[0];
+    for (int i = 0; i < total && i < cap; i++) out[i] = S[i + 1];
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y * Z);
+    free(S);
+    Scene32::Destroy(&lab);
+    return total;
+}
+
+// The CLI chain on an unshifted image; label holds the seed labels (NIL elsewhere) and
+// receives the result.  pol in [-1, 1] as on the command line.
+REF_API void ref_oiftrelax_chain(const int *img, int X, int Y, int Z, double pol, int niter,
+                                 float percentile, const int *seeds, int nseeds, int *label) {
+    sScene32 *scn = make_scene(img, X, Y, Z);
+    sScene32 *lab = make_scene(label, X, Y, Z);
+    sAdjRel3 *A = AdjRel3::Spheric(1.0);
+    int *S = make_S(seeds, nseeds);
+    const int Imin = Scene32::GetMinimumValue(scn);
+    if (Imin < 0)
+        for (int p = 0; p < scn->n; p++) scn->data[p] += (-Imin);
+    sScene32 *fscn = Scene32::GaussianBlur(scn);
+    Scene32::Destroy(&scn);
+    scn = fscn;
+    fscn = Scene32::GaussianBlur(scn);
+    Scene32::Destroy(&scn);
+    ift::OIFT_Multi(A, fscn, pol * 100.0, S, lab);
+    ift::ORelax_1_Multi(A, fscn, pol * 100.0, S, lab, niter);
+    if (Scene32::GetMaximumValue(lab) <= 1) dilation_conditional(fscn, lab, 1, percentile);
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y * Z);
+    free(S);
+    AdjRel3::Destroy(&A);
+    Scene32::Destroy(&lab);
+    Scene32::Destroy(&fscn);
+}
 }  // extern "C"

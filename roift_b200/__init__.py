@@ -83,7 +83,9 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status",
            "oift_b200_level_profile", "oift_b200_selftest_div100",
            "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes",
-           "oift_b200_run_batch", "oift_b200_set_oift_grid"]
+           "oift_b200_run_batch", "oift_b200_set_oift_grid", "oift_b200_gaussian_blur_i32",
+           "oift_b200_conditional_dilation", "oift_b200_inject_boundary_seeds",
+           "oift_b200_run_cli_host"]
 
 _lib = None
 
@@ -122,6 +124,15 @@ def lib():
                                         np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"),
                                         C.c_int, i32p, C.c_int]
         L.oift_gpu_run.argtypes = [C.c_int] + L.oift_fmax_gpu_run.argtypes
+        L.oift_b200_gaussian_blur_i32.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int,
+                                                  C.c_int]
+        L.oift_b200_conditional_dilation.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int,
+                                                     C.c_float, C.c_float,
+                                                     C.POINTER(C.c_longlong)]
+        L.oift_b200_inject_boundary_seeds.argtypes = [i32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                      vp, C.c_int]
+        L.oift_b200_run_cli_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
+                                             C.c_int, C.c_float, C.POINTER(Stats)]
         _lib = L
     return _lib
 
@@ -236,6 +247,39 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_set_oift_grid")
 
+    def gaussian_blur(self, in_ptr, out_ptr, shape_zyx, passes=1):
+        """`passes` Gaussian blurs of a device int32 volume (in == out allowed)."""
+        Z, Y, X = shape_zyx
+        rc = lib().oift_b200_gaussian_blur_i32(self._h, C.c_void_p(in_ptr), C.c_void_p(out_ptr),
+                                               X, Y, Z, int(passes))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_gaussian_blur_i32")
+
+    def conditional_dilation(self, image_ptr, label_ptr, shape_zyx, radius=1.0,
+                             percentile=50.0) -> int:
+        """Conditional dilation of a device int32 label map; returns the voxels added."""
+        Z, Y, X = shape_zyx
+        added = C.c_longlong(0)
+        rc = lib().oift_b200_conditional_dilation(self._h, C.c_void_p(image_ptr),
+                                                  C.c_void_p(label_ptr), X, Y, Z, float(radius),
+                                                  float(percentile), C.byref(added))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_conditional_dilation")
+        return added.value
+
+    def run_cli_host(self, params, image, label, seeds, blur_passes=2, percentile=50.0):
+        """The CLI chain (shift, blur, OIFT, relaxation, conditional dilation) on host
+        arrays; `label` (seed labels in) receives the result."""
+        img = np.ascontiguousarray(np.asarray(image).reshape(-1), np.int32)
+        lab = np.ascontiguousarray(label, np.int32)
+        sd = np.ascontiguousarray(seeds, np.int32)
+        st = Stats()
+        rc = lib().oift_b200_run_cli_host(self._h, C.byref(params), img, lab, sd, len(sd),
+                                          int(blur_passes), float(percentile), C.byref(st))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_run_cli_host")
+        return lab, st
+
     def level_profile(self, cap=8192):
         """(cycles, tile activations) per OIFT level of the last run."""
         buf = np.zeros(2 * cap, np.uint32)
@@ -251,6 +295,20 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_build_weights_i16")
         return cl.value
+
+
+def inject_boundary_seeds(label, shape_zyx, stride):
+    """Boundary seeds of the CLI (host-only): returns the new seeds; `label` (int32, NIL =
+    -1) is updated in place."""
+    Z, Y, X = shape_zyx
+    n = lib().oift_b200_inject_boundary_seeds(label, X, Y, Z, int(stride), None, 0)
+    if n < 0:
+        raise OiftError(n, "oift_b200_inject_boundary_seeds")
+    out = np.empty(max(n, 1), np.int32)
+    n = lib().oift_b200_inject_boundary_seeds(label, X, Y, Z, int(stride), out.ctypes.data, n)
+    if n < 0:
+        raise OiftError(n, "oift_b200_inject_boundary_seeds")
+    return out[:n].copy()
 
 
 def oift_noalloc(image_ptr, shape_zyx, seeds_ptr, labels_ptr, nseeds, cost_ptr=None,

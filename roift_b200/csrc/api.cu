@@ -39,6 +39,8 @@ struct oift_b200_ctx {
     // batched driver: job descriptors, per-image min/max + clamp counters, per-team OIFT
     // state, job counter + abort flag, OIFT labels of jobs that only want a mask
     DevBuf bjobs, bmm, bkey, btpend, bmbox, bglob, bctl, bolab;
+    // CLI steps: shifted / blurred images, dilation border, histograms and tie counts
+    DevBuf cimg0, cimg1, dborder, dhist, daux, dlabel;
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -132,7 +134,8 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->cost,  &c->olabel, &c->flabel, &c->memb,    &c->seedc,   &c->l2c,
                       &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8, &c->ctaq,
                       &c->lprof, &c->rtdist, &c->bjobs, &c->bmm,  &c->bkey,  &c->btpend,
-                      &c->bmbox, &c->bglob, &c->bctl, &c->bolab};
+                      &c->bmbox, &c->bglob, &c->bctl, &c->bolab, &c->cimg0, &c->cimg1,
+                      &c->dborder, &c->dhist, &c->daux, &c->dlabel};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -693,6 +696,256 @@ int oift_fmax_gpu_run(const int *h_image, int *h_labels, int n, int xsize, int y
     return rc == OIFT_OK ? st.levels : -1;
 }
 
+
+// --------------------------------------------------------- steps of the CLI ----
+// oiftrelax.cpp main: shift to >= 0 (263-268), GaussianBlur twice (368-377), OIFT +
+// relaxation (379-401), conditional dilation of a binary result (403-414).
+
+// Kernel3::SphericalGaussian(R = 1, s = 10, f = 1) + Normalize (gft_filtering3.cpp:106-126,
+// 72-83), evaluated in float exactly as the C++ source: val = s * exp(-f * (r2 / R2)) with
+// the float overload of exp, wt = float sum in Spheric order, val /= wt.
+static void blur_weights(float *w0, float *w1) {
+    const float R = 1.0f, sg = 10.0f, f = 1.0f, R2 = R * R;
+    float val[7];
+    for (int i = 0; i < 7; i++) {
+        const float r2 = i == 0 ? 0.0f : 1.0f;
+        val[i] = sg * std::exp(-f * (r2 / R2));
+    }
+    float wt = 0.0f;
+    for (int i = 0; i < 7; i++) wt += val[i];
+    *w0 = val[0] / wt;
+    *w1 = val[1] / wt;
+}
+
+// `passes` blurs of the device int32 volume `in` into `out` (in == out allowed).
+static int blur_passes_i32(oift_b200_ctx *c, const int32_t *in, int32_t *out, int X, int Y,
+                           int Z, int passes) {
+    const size_t N = (size_t)X * Y * Z;
+    float w0, w1;
+    blur_weights(&w0, &w1);
+    TRY(grow(c, c->cimg1, N * sizeof(int32_t)));
+    const int32_t *src = in;
+    for (int i = 0; i < passes; i++) {
+        // the last pass lands in `out`; earlier ones alternate so that no pass reads its
+        // own output
+        int32_t *dst = ((passes - 1 - i) % 2 == 0) ? out : (int32_t *)c->cimg1.p;
+        if (dst == src) dst = (dst == out) ? (int32_t *)c->cimg1.p : out;
+        CU(launch_gaussian_blur<int32_t>(src, dst, X, Y, Z, w0, w1, c->stream));
+        src = dst;
+    }
+    if (src != out)
+        CU(cudaMemcpyAsync(out, src, N * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+    return OIFT_OK;
+}
+
+// Spheric(r) offsets (gft_adjrel3.cpp:47-85), centre included.
+static std::vector<int> spheric_offsets(float r) {
+    std::vector<int> off;
+    const int r0 = (int)r, r2 = (int)(r * r);
+    for (int dz = -r0; dz <= r0; dz++)
+        for (int dy = -r0; dy <= r0; dy++)
+            for (int dx = -r0; dx <= r0; dx++)
+                if (dx * dx + dy * dy + dz * dz <= r2) {
+                    off.push_back(dx);
+                    off.push_back(dy);
+                    off.push_back(dz);
+                }
+    return off;
+}
+
+// Conditional dilation (oiftrelax.cpp:87-169) of the device label map by the border voxels
+// whose intensity in `img` is within the percentile.  *added = voxels relabelled.
+static int conditional_dilation(oift_b200_ctx *c, const int32_t *img, int32_t *label, int X,
+                                int Y, int Z, float radius, float percentile, long long *added) {
+    cudaStream_t s = c->stream;
+    const size_t N = (size_t)X * Y * Z;
+    if (added) *added = 0;
+    const std::vector<int> off = spheric_offsets(radius);
+    const int noff = (int)off.size() / 3;
+    const size_t chunk = 8192;
+    const size_t nchunks = (N + chunk - 1) / chunk;
+    TRY(grow(c, c->dborder, N));
+    TRY(grow(c, c->dhist, (65536 + 16) * sizeof(unsigned)));
+    TRY(grow(c, c->daux, std::max((size_t)noff * 3 * sizeof(int), 2 * nchunks * sizeof(unsigned))));
+    unsigned *hist = (unsigned *)c->dhist.p, *d_count = hist + 65536;
+    int *d_off = (int *)c->daux.p;
+    CU(cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(hist, 0, (65536 + 16) * sizeof(unsigned), s));
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16));
+    dilation_border_kernel<<<blocks, 256, 0, s>>>(label, img, (uint8_t *)c->dborder.p, X, Y, Z,
+                                                  d_off, noff, hist, d_count);
+    CU(cudaGetLastError());
+    std::vector<unsigned> h(65537);
+    CU(cudaMemcpyAsync(h.data(), hist, 65537 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const long long n = h[65536];
+    if (n == 0) return OIFT_OK;  // the reference indexes out of range here; nothing to add
+    // float index_percentile = (percentil / 100.0) * (size - 1); int value_position = (int)
+    const float index_percentile = (percentile / 100.0) * (double)(size_t)(n - 1);
+    const double ipd = (double)index_percentile;
+    const long long vp = ipd >= 2147483647.0 ? 2147483647LL
+                         : ipd <= -2147483648.0 ? -2147483648LL
+                                                : (long long)static_cast<int>(index_percentile);
+    const long long keep = std::min<long long>(std::max<long long>(vp + 1, 0), n);
+    if (keep == 0) return OIFT_OK;
+    const long long k = keep - 1;  // rank of the last voxel kept
+    long long cum = 0;
+    uint32_t hi = 0;
+    for (; hi < 65536; hi++) {
+        if (cum + h[hi] > (unsigned long long)k) break;
+        cum += h[hi];
+    }
+    CU(cudaMemsetAsync(hist, 0, 65536 * sizeof(unsigned), s));
+    dilation_hist_lo_kernel<<<blocks, 256, 0, s>>>((const uint8_t *)c->dborder.p, img, N, hi, hist);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(h.data(), hist, 65536 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    uint32_t lo = 0;
+    for (; lo < 65536; lo++) {
+        if (cum + h[lo] > (unsigned long long)k) break;
+        cum += h[lo];
+    }
+    const uint32_t pivot = (hi << 16) | lo;
+    const unsigned take = (unsigned)(keep - cum);  // pivot-valued voxels kept, in address order
+    unsigned *d_counts = (unsigned *)c->daux.p, *d_base = d_counts + nchunks;
+    dilation_tie_count_kernel<<<(unsigned)nchunks, 256, 0, s>>>((const uint8_t *)c->dborder.p,
+                                                                img, N, chunk, pivot, d_counts);
+    CU(cudaGetLastError());
+    std::vector<unsigned> cnt(nchunks);
+    CU(cudaMemcpyAsync(cnt.data(), d_counts, nchunks * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    unsigned run = 0;
+    for (size_t i = 0; i < nchunks; i++) {
+        const unsigned v = cnt[i];
+        cnt[i] = run;
+        run += v;
+    }
+    CU(cudaMemcpyAsync(d_base, cnt.data(), nchunks * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+    dilation_apply_kernel<<<(unsigned)nchunks, 256, 0, s>>>((const uint8_t *)c->dborder.p, img,
+                                                            label, N, chunk, pivot, d_base, take);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s));
+    if (added) *added = keep;
+    return OIFT_OK;
+}
+
+extern "C" {
+
+int oift_b200_gaussian_blur_i32(oift_b200_ctx *c, const int32_t *in, int32_t *out, int xsize,
+                                int ysize, int zsize, int passes) {
+    if (!c || !in || !out || xsize <= 0 || ysize <= 0 || zsize <= 0 || passes < 0)
+        return OIFT_E_BAD_ARG;
+    if (ysize > 65535 || zsize > 65535) return OIFT_E_RANGE;
+    cudaSetDevice(c->device);
+    const size_t N = (size_t)xsize * ysize * zsize;
+    if (passes == 0) {
+        if (in != out)
+            CU(cudaMemcpyAsync(out, in, N * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        TRY(blur_passes_i32(c, in, out, xsize, ysize, zsize, passes));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return OIFT_OK;
+}
+
+int oift_b200_conditional_dilation(oift_b200_ctx *c, const int32_t *image, int32_t *label,
+                                   int xsize, int ysize, int zsize, float radius,
+                                   float percentile, long long *added) {
+    if (!c || !image || !label || xsize <= 0 || ysize <= 0 || zsize <= 0) return OIFT_E_BAD_ARG;
+    if (!(radius >= 0.0f && radius < 6.0f) || !(std::fabs(percentile) < 1e9f)) return OIFT_E_BAD_ARG;
+    cudaSetDevice(c->device);
+    return conditional_dilation(c, image, label, xsize, ysize, zsize, radius, percentile, added);
+}
+
+int oift_b200_inject_boundary_seeds(int32_t *label, int xsize, int ysize, int zsize, int stride,
+                                    int32_t *seeds_out, int cap) {
+    // oiftrelax.cpp:175-224: voxels on the six faces, visited in z, y, x order with the
+    // stride on every axis, that carry no label yet become background seeds.  With
+    // seeds_out == NULL the count is returned and nothing is changed.
+    if (!label || xsize <= 0 || ysize <= 0 || zsize <= 0 || stride <= 0) return OIFT_E_BAD_ARG;
+    int n = 0;
+    for (int z = 0; z < zsize; z += stride)
+        for (int y = 0; y < ysize; y += stride)
+            for (int x = 0; x < xsize; x += stride) {
+                const bool face = x == 0 || x == xsize - 1 || y == 0 || y == ysize - 1 ||
+                                  z == 0 || z == zsize - 1;
+                if (!face) continue;
+                const size_t p = (size_t)x + (size_t)y * xsize + (size_t)z * xsize * ysize;
+                if (label[p] != -1) continue;
+                if (seeds_out) {
+                    if (n >= cap) return OIFT_E_RANGE;
+                    label[p] = 0;
+                    seeds_out[n] = (int32_t)p;
+                }
+                n++;
+            }
+    return n;
+}
+
+int oift_b200_run_cli_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *image,
+                           int32_t *label, const int32_t *seeds, int nseeds, int blur_passes,
+                           float percentile, oift_b200_stats *stats) {
+    if (!c || !image || !label || (nseeds > 0 && !seeds) || blur_passes < 0) return OIFT_E_BAD_ARG;
+    TRY(check_params(p));
+    if (nseeds <= 0) return OIFT_E_NO_SEEDS;
+    cudaSetDevice(c->device);
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    if (Y > 65535 || Z > 65535) return OIFT_E_RANGE;
+    const size_t N = (size_t)X * Y * Z;
+    cudaStream_t s = c->stream;
+    std::vector<int32_t> slab(nseeds);
+    for (int i = 0; i < nseeds; i++) {
+        if (seeds[i] < 0 || (size_t)seeds[i] >= N) return OIFT_E_SEED_RANGE;
+        const int lb = label[seeds[i]];
+        slab[i] = lb < 0 ? 0 : lb;
+        if (slab[i] > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
+    }
+    TRY(grow(c, c->img32, N * sizeof(int32_t)));
+    TRY(grow(c, c->cimg0, N * sizeof(int32_t)));
+    TRY(grow(c, c->seeds, (size_t)nseeds * sizeof(int32_t)));
+    TRY(grow(c, c->slabels, (size_t)nseeds * sizeof(int32_t)));
+    TRY(grow(c, c->dlabel, N * sizeof(int32_t)));
+    TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
+    CU(cudaMemcpyAsync(c->img32.p, image, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->seeds.p, seeds, (size_t)nseeds * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->slabels.p, slab.data(), (size_t)nseeds * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, s));
+    // ---- shift to >= 0, blur ----
+    int *d_mm = (int *)c->minmax.p;
+    const int mm_init[2] = {0x7fffffff, (int)0x80000000};
+    CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+    CU(launch_minmax<int32_t>((const int32_t *)c->img32.p, N, d_mm, c->sms, s));
+    CU(launch_shift_to_i32<int32_t>((const int32_t *)c->img32.p, (int32_t *)c->cimg0.p, N, d_mm,
+                                    c->sms, s));
+    if (blur_passes > 0)
+        TRY(blur_passes_i32(c, (const int32_t *)c->cimg0.p, (int32_t *)c->cimg0.p, X, Y, Z, blur_passes));
+    // ---- OIFT + relaxation on the blurred image ----
+    oift_b200_outputs o{};
+    const bool relax = p->relax_sweeps > 0;
+    if (relax)
+        o.label = (int32_t *)c->dlabel.p;
+    else
+        o.oift_label = (int32_t *)c->dlabel.p;
+    oift_b200_stats lst{};
+    TRY(run_pipeline<int32_t>(c, p, (const int32_t *)c->cimg0.p, (const int32_t *)c->seeds.p,
+                              (const int32_t *)c->slabels.p, nseeds, &o, stats ? stats : &lst));
+    // ---- conditional dilation of a binary result ----
+    if (percentile >= 0.0f) {
+        CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+        CU(launch_minmax<int32_t>((const int32_t *)c->dlabel.p, N, d_mm, c->sms, s));
+        int hmm[2];
+        CU(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (hmm[1] <= 1)
+            TRY(conditional_dilation(c, (const int32_t *)c->cimg0.p, (int32_t *)c->dlabel.p, X, Y,
+                                     Z, 1.0f, percentile, nullptr));
+    }
+    CU(cudaMemcpyAsync(label, c->dlabel.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    return OIFT_OK;
+}
+
+}  // extern "C"
 
 // ----------------------------------------------------------------- batched driver ----
 // The OIFT of one volume is bound by the latency of its level loop (grid reduction, team

@@ -136,6 +136,24 @@ struct OiftTeamScratch {
 int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ctas,
                   const OiftTeamScratch &S, cudaStream_t st);
 
+// ---- steps around the path (prepost.cu) ----
+template <typename T>
+cudaError_t launch_shift_to_i32(const T *in, int32_t *out, size_t n, const int *d_mm, int sms,
+                                cudaStream_t s);
+template <typename T>
+cudaError_t launch_gaussian_blur(const T *in, int32_t *out, int X, int Y, int Z, float w0,
+                                 float w1, cudaStream_t s);
+__global__ void dilation_border_kernel(const int32_t *label, const int32_t *img, uint8_t *border,
+                                       int X, int Y, int Z, const int *off, int noff,
+                                       unsigned *hist_hi, unsigned *count);
+__global__ void dilation_hist_lo_kernel(const uint8_t *border, const int32_t *img, size_t N,
+                                        uint32_t hi, unsigned *hist_lo);
+__global__ void dilation_tie_count_kernel(const uint8_t *border, const int32_t *img, size_t N,
+                                          size_t chunk, uint32_t pivot, unsigned *counts);
+__global__ void dilation_apply_kernel(const uint8_t *border, const int32_t *img, int32_t *label,
+                                      size_t N, size_t chunk, uint32_t pivot,
+                                      const unsigned *tie_base, unsigned take);
+
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,

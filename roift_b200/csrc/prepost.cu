@@ -1,0 +1,188 @@
+// prepost.cu -- the device steps around OIFT + relaxation in the reference CLI
+// (oiftrelax.cpp main): intensity shift, Gaussian blur, and the conditional dilation of
+// a binary result.  All kernels are HBM-bound integer / FP32 stencils or scans.
+#include "kernels.cuh"
+
+namespace oiftb {
+
+// ---------------------------------------------------------------- shift ----
+// oiftrelax.cpp:263-268: when min(I) < 0 every voxel gets -min(I) added.
+template <typename T>
+__global__ void shift_to_i32_kernel(const T *__restrict__ in, int32_t *__restrict__ out,
+                                    size_t n, const int *__restrict__ mm) {
+    const int lo = mm[0];
+    const int add = lo < 0 ? -lo : 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (int32_t)in[i] + add;
+}
+
+template <typename T>
+cudaError_t launch_shift_to_i32(const T *in, int32_t *out, size_t n, const int *d_mm, int sms,
+                                cudaStream_t s) {
+    int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)sms * 16);
+    if (blocks < 1) blocks = 1;
+    shift_to_i32_kernel<T><<<blocks, 256, 0, s>>>(in, out, n, d_mm);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------- blur ----
+// Scene32::GaussianBlur (gft_filtering3.cpp:385-397): Convolution (321-346) with the
+// normalised SphericalGaussian(R = 1, s = 10, f = 1) kernel (106-126, 72-83) over
+// Spheric(1.0): the centre first, then -z, -y, -x, +x, +y, +z.  Neighbours outside the
+// volume are skipped without renormalising; the sum is FP32 in that order with separate
+// multiply and add; the result is ROUND (gft_common.h:120) evaluated in double.
+// One thread per voxel, x fastest: the six neighbour reads of a warp are coalesced rows
+// and the +-y / +-z rows are re-read from L2.
+template <typename T>
+__global__ void gaussian_blur_kernel(const T *__restrict__ in, int32_t *__restrict__ out,
+                                     int X, int Y, int Z, float w0, float w1) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (x >= X) return;
+    const size_t XY = (size_t)X * Y;
+    const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+    float conv = __fmul_rn((float)in[p], w0);
+    if (z > 0) conv = __fadd_rn(conv, __fmul_rn((float)in[p - XY], w1));
+    if (y > 0) conv = __fadd_rn(conv, __fmul_rn((float)in[p - X], w1));
+    if (x > 0) conv = __fadd_rn(conv, __fmul_rn((float)in[p - 1], w1));
+    if (x + 1 < X) conv = __fadd_rn(conv, __fmul_rn((float)in[p + 1], w1));
+    if (y + 1 < Y) conv = __fadd_rn(conv, __fmul_rn((float)in[p + X], w1));
+    if (z + 1 < Z) conv = __fadd_rn(conv, __fmul_rn((float)in[p + XY], w1));
+    out[p] = conv < 0.0f ? (int32_t)((double)conv - 0.5) : (int32_t)((double)conv + 0.5);
+}
+
+template <typename T>
+cudaError_t launch_gaussian_blur(const T *in, int32_t *out, int X, int Y, int Z, float w0,
+                                 float w1, cudaStream_t s) {
+    if (Y > 65535 || Z > 65535) return cudaErrorInvalidValue;
+    dim3 grid((X + 127) / 128, Y, Z);
+    gaussian_blur_kernel<T><<<grid, 128, 0, s>>>(in, out, X, Y, Z, w0, w1);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------- conditional dilation ----
+// oiftrelax.cpp:87-169.  The border is every voxel labelled 0 that has a voxel labelled 1
+// within Spheric(radius); the border voxels whose blurred intensity ranks at or below the
+// percentile index (ties in address order, as std::stable_sort keeps them) become 1.
+//
+// On the device: (1) border mask + a 65536-bin histogram of the high half of the
+// order-preserving key (I ^ 0x80000000); (2) the host finds the bin of rank k; a second
+// histogram of the low half inside that bin gives the exact value v and the count below
+// it; (3) per-block counts of border voxels equal to v, (4) after a host prefix over the
+// blocks, voxels below v, and the first ones equal to v in address order, are relabelled.
+
+__device__ __forceinline__ uint32_t order_key(int v) { return (uint32_t)v ^ 0x80000000u; }
+
+__global__ void dilation_border_kernel(const int32_t *__restrict__ label,
+                                       const int32_t *__restrict__ img, uint8_t *border, int X,
+                                       int Y, int Z, const int *__restrict__ off, int noff,
+                                       unsigned *hist_hi, unsigned *count) {
+    const size_t N = (size_t)X * Y * Z, XY = (size_t)X * Y;
+    unsigned local = 0;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        uint8_t b = 0;
+        if (label[p] == 0) {
+            const int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / XY);
+            for (int i = 0; i < noff; i++) {
+                const int qx = x + off[3 * i], qy = y + off[3 * i + 1], qz = z + off[3 * i + 2];
+                if (qx < 0 || qy < 0 || qz < 0 || qx >= X || qy >= Y || qz >= Z) continue;
+                if (label[(size_t)qx + (size_t)qy * X + (size_t)qz * XY] == 1) {
+                    b = 1;
+                    break;
+                }
+            }
+        }
+        border[p] = b;
+        if (b) {
+            atomicAdd(&hist_hi[order_key(img[p]) >> 16], 1u);
+            local++;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+__global__ void dilation_hist_lo_kernel(const uint8_t *__restrict__ border,
+                                        const int32_t *__restrict__ img, size_t N,
+                                        uint32_t hi, unsigned *hist_lo) {
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        if (!border[p]) continue;
+        const uint32_t k = order_key(img[p]);
+        if ((k >> 16) == hi) atomicAdd(&hist_lo[k & 0xffffu], 1u);
+    }
+}
+
+// Count of border voxels equal to the pivot in each chunk of `chunk` addresses.
+__global__ void dilation_tie_count_kernel(const uint8_t *__restrict__ border,
+                                          const int32_t *__restrict__ img, size_t N,
+                                          size_t chunk, uint32_t pivot, unsigned *counts) {
+    const size_t b0 = (size_t)blockIdx.x * chunk;
+    const size_t b1 = min(N, b0 + chunk);
+    unsigned c = 0;
+    for (size_t p = b0 + threadIdx.x; p < b1; p += blockDim.x)
+        c += (border[p] && order_key(img[p]) == pivot) ? 1u : 0u;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    __shared__ unsigned ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// Relabel: border voxels below the pivot, and pivot-valued ones whose rank among equal
+// values (address order) is below `take`.  tie_base[b] = pivot-valued border voxels in the
+// chunks before b.  A block walks its chunk in rounds of blockDim addresses, ranking the
+// pivot-valued voxels of each round with a block prefix sum.
+__global__ void dilation_apply_kernel(const uint8_t *__restrict__ border,
+                                      const int32_t *__restrict__ img, int32_t *label, size_t N,
+                                      size_t chunk, uint32_t pivot,
+                                      const unsigned *__restrict__ tie_base, unsigned take) {
+    __shared__ unsigned ws[33];
+    const size_t b0 = (size_t)blockIdx.x * chunk;
+    const size_t b1 = min(N, b0 + chunk);
+    unsigned base = tie_base[blockIdx.x];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (size_t r = b0; r < b1; r += blockDim.x) {
+        const size_t p = r + threadIdx.x;
+        bool eq = false, lt = false;
+        if (p < b1 && border[p]) {
+            const uint32_t k = order_key(img[p]);
+            eq = k == pivot;
+            lt = k < pivot;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, eq);
+        if (lane == 0) ws[wid] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned s = 0;
+            for (int w = 0; w < nw; w++) {
+                const unsigned v = ws[w];
+                ws[w] = s;
+                s += v;
+            }
+            ws[32] = s;
+        }
+        __syncthreads();
+        const unsigned rank = base + ws[wid] + __popc(bal & ((1u << lane) - 1u));
+        if (lt || (eq && rank < take)) label[p] = 1;
+        base += ws[32];
+        __syncthreads();
+    }
+}
+
+template cudaError_t launch_shift_to_i32<int16_t>(const int16_t *, int32_t *, size_t,
+                                                  const int *, int, cudaStream_t);
+template cudaError_t launch_shift_to_i32<int32_t>(const int32_t *, int32_t *, size_t,
+                                                  const int *, int, cudaStream_t);
+template cudaError_t launch_gaussian_blur<int16_t>(const int16_t *, int32_t *, int, int, int,
+                                                   float, float, cudaStream_t);
+template cudaError_t launch_gaussian_blur<int32_t>(const int32_t *, int32_t *, int, int, int,
+                                                   float, float, cudaStream_t);
+
+}  // namespace oiftb

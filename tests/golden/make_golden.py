@@ -47,6 +47,19 @@ def make(name, shape, pol, adj, nl, per_class, seed):
                per_class=pc if pc is not None else np.zeros(0, np.float32),
                ref_oift_label=lab_oift, ref_relax_label=lab_relax,
                ref_blur=O.ref_gaussian_blur(img))
+    # the CLI steps: conditional dilation of the binary relaxed labels on the blurred image,
+    # boundary seeds (stride 2), and the whole CLI chain on an image shifted below zero
+    if nl == 1 and pc is None:
+        out["ref_dilated_p50"] = O.ref_dilation_conditional(out["ref_blur"].reshape(img.shape),
+                                                            lab_relax, 1.0, 50.0)
+        chain_img = (img - 500).astype(np.int32)
+        chain_lab = np.full(img.size, -1, np.int32)
+        chain_lab[c.seeds] = c.seed_labels
+        bl, bs = O.ref_inject_boundary_seeds(chain_lab, shape, 2, c.seeds)
+        out["ref_boundary_label"], out["ref_boundary_seeds"] = bl, bs
+        out["chain_image"] = chain_img.reshape(shape)
+        out["ref_chain_label"] = O.ref_oiftrelax_chain(chain_img.reshape(shape), pol, SWEEPS,
+                                                       50.0, c.seeds, chain_lab)
     if pol == 0.0 and pc is None:
         cost, lab = O.ref_ift_fmax(img, adj, c.seeds, c.seed_labels)
         out["ref_ift_fmax_cost"] = cost

@@ -79,3 +79,17 @@ def test_dropin_rejects_bad_arguments_before_touching_a_gpu(roift):
     # additive cost mode is not provided
     assert L.oift_gpu_run(1, img, lab, 8, 2, 2, 2, pc, 1, sd, 1) == -1
     assert L.oift_b200_last_status() == -8
+
+
+def test_boundary_seed_injection_is_host_logic(roift, oracle_lib):
+    """The CLI's boundary seeds are computed on the host by the library itself; they match
+    the restatement of oiftrelax.cpp:175-224 (pinned against the reference)."""
+    import oracle as O
+    rng = np.random.default_rng(11)
+    for stride in (1, 2, 3):
+        shape = (5, 9, 12)
+        lab = rng.choice([-1, -1, 0, 1], size=5 * 9 * 12).astype(np.int32)
+        exp_lab, exp_seeds = O.inject_boundary_seeds(lab, shape, stride)
+        got = lab.copy()
+        seeds = roift.inject_boundary_seeds(got, shape, stride)
+        assert np.array_equal(seeds, exp_seeds) and np.array_equal(got, exp_lab)

@@ -9,6 +9,8 @@ of ORelax_1_Multi and within 1e-5 of the FP64 oracle):
   * relaxed membership == R3-FP32 bitwise, |m - m64| <= 1e-5, labels == ORelax_1_Multi.
 """
 import copy
+import glob
+import os
 
 import numpy as np
 import pytest
@@ -295,3 +297,80 @@ def test_batch_bad_seed_is_reported_per_job(roift):
         torch.cuda.synchronize()
         assert torch.equal(lab, lab1)
     ctx.close()
+
+
+# ------------------------------------------------------------ steps of the CLI ----
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_gaussian_blur_matches_reference(roift, path):
+    """GPU blur == Scene32::GaussianBlur outputs (golden), and two passes == two oracle
+    passes, on the image and on it shifted below zero."""
+    import torch
+    d = np.load(path)
+    img = d["image"].astype(np.int32)
+    dev = torch.device("cuda:0")
+    ctx = roift._ctx()
+    src = torch.from_numpy(img.reshape(-1).copy()).to(dev)
+    out = torch.empty_like(src)
+    ctx.gaussian_blur(src.data_ptr(), out.data_ptr(), img.shape, 1)
+    assert np.array_equal(out.cpu().numpy(), d["ref_blur"])
+    neg = (img - 700).astype(np.int32)
+    src = torch.from_numpy(neg.reshape(-1).copy()).to(dev)
+    ctx.gaussian_blur(src.data_ptr(), src.data_ptr(), img.shape, 2)   # in place
+    exp = O.gaussian_blur(O.gaussian_blur(neg).reshape(img.shape))
+    assert np.array_equal(src.cpu().numpy(), exp)
+
+
+def test_gaussian_blur_large_matches_oracle(roift):
+    import torch
+    rng = np.random.default_rng(8)
+    img = rng.integers(-30000, 30000, size=(37, 61, 130)).astype(np.int32)
+    src = torch.from_numpy(img.reshape(-1).copy()).to("cuda:0")
+    out = torch.empty_like(src)
+    roift._ctx().gaussian_blur(src.data_ptr(), out.data_ptr(), img.shape, 1)
+    assert np.array_equal(out.cpu().numpy(), O.gaussian_blur(img))
+
+
+@pytest.mark.parametrize("trial", range(12))
+def test_conditional_dilation_matches_oracle(roift, trial):
+    """Border detection, percentile rank and address-order ties (few distinct values)."""
+    import torch
+    rng = np.random.default_rng(900 + trial)
+    shape = [(1, 40, 52), (9, 23, 31), (24, 40, 70)][trial % 3]
+    n = int(np.prod(shape))
+    img = rng.integers(0, 4 if trial % 2 else 50000, size=shape).astype(np.int32) - 100
+    lab = rng.choice([-1, 0, 0, 0, 1, 1], size=n).astype(np.int32)
+    r = [1.0, 1.0, 1.5, 2.0][trial % 4]
+    pc = [50.0, 0.0, 100.0, 37.5, 99.9, 150.0][trial % 6]
+    exp, added = O.conditional_dilation(img, lab, r, pc)
+    d_img = torch.from_numpy(img.reshape(-1).copy()).to("cuda:0")
+    d_lab = torch.from_numpy(lab.copy()).to("cuda:0")
+    got = roift._ctx().conditional_dilation(d_img.data_ptr(), d_lab.data_ptr(), shape, r, pc)
+    assert got == added
+    assert np.array_equal(d_lab.cpu().numpy(), exp)
+
+
+CLI_GOLDEN = [p for p in GOLDEN if "ref_chain_label" in np.load(p).files]
+
+
+@pytest.mark.parametrize("path", CLI_GOLDEN, ids=[os.path.basename(p)[:-4] for p in CLI_GOLDEN])
+def test_cli_chain_matches_oracle_and_reference(roift, path):
+    """run_cli_host (shift, blur x2, OIFT, relaxation, dilation) == the oracle chain on the
+    lexicographic OIFT labels, bit for bit; == the reference chain wherever the oracle's
+    OIFT_Multi restatement and the lexicographic labels agree (no equal-cost ties)."""
+    d = np.load(path)
+    img = d["chain_image"]
+    seeds, sl = d["seeds"], d["seed_labels"]
+    pol, K = float(d["pol"]), int(d["sweeps"])
+    lab = np.full(img.size, -1, np.int32)
+    lab[seeds] = sl
+    adj = 4 if img.shape[0] == 1 else 6
+    p = roift.make_params(img.shape, adjacency=adj, weight_mode="grad", pol=pol, sweeps=K)
+    got, _ = roift._ctx().run_cli_host(p, img, lab.copy(), seeds, blur_passes=2, percentile=50.0)
+    exp2, _ = O.oiftrelax_chain(img, pol, K, 50.0, seeds, sl, oift="r2")
+    assert np.array_equal(got, exp2)
+    exp1, _ = O.oiftrelax_chain(img, pol, K, 50.0, seeds, sl, oift="r1")
+    if np.array_equal(exp1, exp2):
+        assert np.array_equal(got, d["ref_chain_label"])

@@ -100,3 +100,45 @@ def test_weight_builder_modes(oracle_lib):
     assert ncl == 1
     W, _ = O.build_weights(img, 6, "rbf_q", wq=4095, rbf_sigma=150.0)
     assert (W[1] & 0x3FFF) == 4095 and (W[0] & 0x3FFF) == round(4095 * (1 - np.exp(-100 / 45000)))
+
+
+CLI_GOLDEN = [p for p in GOLDEN if "ref_chain_label" in np.load(p).files]
+
+
+@pytest.mark.parametrize("path", CLI_GOLDEN, ids=[os.path.basename(p)[:-4] for p in CLI_GOLDEN])
+def test_cli_steps_match_golden(oracle_lib, path):
+    """Conditional dilation, boundary seeds and the whole CLI chain (shift, blur x2,
+    OIFT_Multi, ORelax_1_Multi, dilation) restated against the reference's outputs."""
+    d = np.load(path)
+    img = d["image"]
+    shape = img.shape
+    seeds, sl = d["seeds"], d["seed_labels"]
+    lab, n = O.conditional_dilation(d["ref_blur"].reshape(shape), d["ref_relax_label"], 1.0, 50.0)
+    assert np.array_equal(lab, d["ref_dilated_p50"]) and n > 0
+    chain_lab = np.full(img.size, -1, np.int32)
+    chain_lab[seeds] = sl
+    bl, bs = O.inject_boundary_seeds(chain_lab, shape, 2)
+    assert np.array_equal(bl, d["ref_boundary_label"])
+    assert np.array_equal(np.concatenate([seeds, bs]), d["ref_boundary_seeds"])
+    out, _ = O.oiftrelax_chain(d["chain_image"], float(d["pol"]), int(d["sweeps"]), 50.0,
+                               seeds, sl, oift="r1")
+    assert np.array_equal(out, d["ref_chain_label"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("trial", range(24))
+def test_dilation_and_boundary_seeds_match_live_reference(oracle_lib, trial):
+    """Random label maps with NIL / 0 / 1, heavy ties in the intensities, several radii
+    and percentiles (including the 0 and 100 ends and past 100)."""
+    rng = np.random.default_rng(500 + trial)
+    Z, Y, X = int(rng.integers(1, 9)), int(rng.integers(2, 14)), int(rng.integers(2, 14))
+    img = rng.integers(0, 6 if trial % 2 else 3000, size=(Z, Y, X)).astype(np.int32)
+    lab = rng.choice([-1, 0, 0, 0, 1], size=Z * Y * X).astype(np.int32)
+    r = [1.0, 1.5, 2.0][trial % 3]
+    pc = [0.0, 37.5, 50.0, 99.0, 100.0, 150.0][trial % 6]
+    a, _ = O.conditional_dilation(img, lab, r, pc)
+    assert np.array_equal(a, O.ref_dilation_conditional(img, lab, r, pc))
+    stride = [1, 2, 3][trial % 3]
+    la, sa = O.inject_boundary_seeds(lab, (Z, Y, X), stride)
+    lb, sb = O.ref_inject_boundary_seeds(lab, (Z, Y, X), stride, np.zeros(0, np.int32))
+    assert np.array_equal(la, lb) and np.array_equal(sa, sb)
