@@ -205,8 +205,6 @@ static int check_params(const oift_b200_params *p) {
     }
     if (p->weight_mode == OIFT_W_BLEND_Q) return OIFT_E_UNSUPPORTED;
     if (p->weight_mode == OIFT_W_RBF_Q && !(p->rbf_sigma > 0.0f)) return OIFT_E_BAD_ARG;
-    // the tile OIFT handles the 6 / 4 neighbourhoods
-    if (p->adjacency == 26 || p->adjacency == 8) return OIFT_E_UNSUPPORTED;
     return OIFT_OK;
 }
 
@@ -387,9 +385,11 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     const size_t N = (size_t)X * Y * Z;
     const int planes = oift_b200_weight_planes(p->adjacency);
     Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
-    OiftPlan plan = oift_plan(X, Y, Z);
+    // 26 / 8: the full-neighbourhood OIFT evaluates arc weights from the image itself
+    const bool fulln = p->adjacency == 26 || p->adjacency == 8;
+    OiftPlan plan = fulln ? oift_plan_full(X, Y, Z) : oift_plan(X, Y, Z);
 
-    TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
+    if (!fulln) TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
     TRY(grow(c, c->key, N * sizeof(uint32_t)));
     TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
     const int octas = (c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms;
@@ -449,7 +449,22 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         ba.lut = (const uint16_t *)c->lut.p;
         ba.lut_len = len;
     }
-    CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
+    if (!fulln) {
+        CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
+    } else if (p->weight_mode == OIFT_W_GRAD &&
+               (long long)hmm[1] - (long long)hmm[0] > OIFT_MAX_BASE) {
+        // exact gradient weights must fit 14 bits: count the arcs that do not (the planes
+        // are built only for that count)
+        TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
+        CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
+    }
+    OiftFullN fn{};
+    fn.img = d_img;
+    fn.img_i16 = sizeof(T) == 2;
+    fn.wmode = p->weight_mode;
+    fn.wcap = ba.cap;
+    fn.lut = ba.lut;
+    fn.lut_len = ba.lut_len;
     cudaEventRecord(c->ev[1], s);
 
     // ---- OIFT ----
@@ -470,7 +485,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     long long steps = 0;
     int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
                       (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
-                      octas, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles);
+                      octas, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles,
+                      fulln ? &fn : nullptr);
     if (rc != OIFT_OK) return rc;
     unsigned long long hclamp = 0;
     CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));
@@ -982,6 +998,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     cudaStream_t s = c->stream;
     const int end = first + count;
     if (teams < 1 || teams > c->sms) return OIFT_E_BAD_ARG;
+    // the team kernel is the 6 / 4-neighbourhood tile step on prebuilt edge codes
+    if (common->adjacency != 6 && common->adjacency != 4) return OIFT_E_UNSUPPORTED;
     const int ctas_lo = c->sms / teams, ctas_hi = (c->sms + teams - 1) / teams;
 
     // ---- per-job checks; distinct images (pointer + extents) ----

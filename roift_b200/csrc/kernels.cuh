@@ -154,12 +154,23 @@ __global__ void dilation_apply_kernel(const uint8_t *border, const int32_t *img,
                                       size_t N, size_t chunk, uint32_t pivot,
                                       const unsigned *tie_base, unsigned take);
 
+// Full 3x3(x3) neighbourhood OIFT (26 / 8): arc weights from the image on the fly.
+struct OiftFullN {
+    const void *img;
+    bool img_i16;
+    int wmode, wcap;
+    const uint16_t *lut;
+    int lut_len;
+};
+// Tiling of the full-neighbourhood kernel: 32 x 4 x 4 (3D) or 32 x 16 (2D).
+OiftPlan oift_plan_full(int X, int Y, int Z);
+
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
              long long *steps_out, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr,
-             unsigned long long *cycles_out = nullptr);
+             unsigned long long *cycles_out = nullptr, const OiftFullN *fn = nullptr);
 constexpr int OIFT_WARPS_PER_CTA = 16;
 
 }  // namespace oiftb

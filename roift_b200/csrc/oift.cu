@@ -51,6 +51,12 @@ struct OiftArgs {
     OiftGlobals *g;
     long long spin_limit;
     int max_levels;
+    // 26 / 8 neighbourhoods: arc weights from the image on the fly (process_tile_full)
+    const void *img;       // int16 or int32 [N]
+    int wmode;             // OIFT_W_GRAD, OIFT_W_GRAD_Q or OIFT_W_RBF_Q
+    int wcap;              // base weight ceiling (wq, or OIFT_MAX_BASE)
+    const uint16_t *lut;   // RBF_Q table over |dI|
+    int lut_len;
 };
 
 constexpr int OIFT_WARPS = 16;
@@ -139,7 +145,7 @@ __device__ __forceinline__ int tile_of(const OiftArgs &A, int x, int y, int z) {
 
 // Process one tile at level kk (cost c, label l).  All 32 lanes of the warp call it.
 template <int TY, int TZ>
-__device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
+__device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
                              double fgt, double flt, int bgt, int blt, uint32_t *skey,
                              uint16_t *sw, uint16_t *shx, uint16_t *shy, uint16_t *shz,
                              uint32_t *wl, uint32_t *nfm, uint32_t *rmask, long long *cyc) {
@@ -676,6 +682,273 @@ __device__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int
     cyc[5] += 1;
 }
 
+
+// ------------------------------------------------------ 26 / 8 neighbourhoods ----
+// Tile step for the full 3x3(x3) neighbourhood (Spheric(1.75): 26 in 3D, 8 in 2D).  The
+// 13 (4) edge planes of a tile would not fit in shared memory next to the keys, so the
+// tile stages its intensities with a one-voxel halo instead and evaluates the base weight
+// of every arc from |I_p - I_q| as the builder does (GRAD: |dI|, GRAD_Q: min(|dI|, wq),
+// RBF_Q: lut[|dI|]); the orientation is the sign of I_tail - I_head.  Tiles are 32 x TY x TZ
+// with TY * TZ <= 16 rows, the level's voxels are flooded in rounds from a worklist that
+// holds every voxel of the tile (no overflow), and pushes across the 26 faces, edges and
+// corners of the tile go out together after the flood.
+template <typename TI>
+__device__ __forceinline__ int gen_base(const OiftArgs &A, int ip, int iq) {
+    const int d = ip - iq;
+    const int ad = d < 0 ? -d : d;
+    int b = ad;
+    if (A.wmode == OIFT_W_RBF_Q) b = A.lut[ad < A.lut_len ? ad : A.lut_len - 1];
+    return b > A.wcap ? A.wcap : b;
+}
+
+template <int TY, int TZ, typename TI>
+__device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
+                                  double fgt, double flt, int bgt, int blt, uint32_t *skey,
+                                  int32_t *simg, uint16_t *wl, uint32_t *nfm, uint32_t *rmask,
+                                  long long *cyc) {
+    constexpr int NR = TY * TZ;           // rows of 32 voxels
+    constexpr int HY = TY + 2;
+    constexpr int HZ = TZ > 1 ? TZ + 2 : 1;
+    constexpr int ZO = TZ > 1 ? 1 : 0;    // halo offset along z
+    static_assert(NR <= 16, "full-neighbourhood tiles hold at most 16 rows");
+    long long tc0 = clock64();
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int X = A.X, Y = A.Y, Z = A.Z;
+    const size_t XY = (size_t)X * Y;
+    const int tx = t % A.ntx, ty = (t / A.ntx) % A.nty, tz = t / (A.ntx * A.nty);
+    const int x0 = tx * 32, y0 = ty * TY, z0 = tz * TZ;
+    const int x = x0 + lane;
+    const uint32_t kexp = kk - 1u;
+    const uint32_t lab_bits = ((uint32_t)l << 1) | 1u;
+    const TI *img = static_cast<const TI *>(A.img);
+    auto himg = [&](int xl, int yl, int zl) -> int {  // tile-local coordinates, -1 .. 32
+        return simg[(zl + ZO) * (HY * 34) + (yl + 1) * 34 + (xl + 1)];
+    };
+    // arc p -> q with tail p: open at this cost, or the key it offers q
+    auto arc_open = [&](int ip, int iq) -> bool {
+        const int b = gen_base<TI>(A, ip, iq);
+        return ip > iq ? b <= bgt : (ip < iq ? b <= blt : b <= c);
+    };
+    auto arc_key = [&](int ip, int iq) -> uint32_t {
+        const int b = gen_base<TI>(A, ip, iq);
+        const int w = oriented_weight((uint32_t)b, ip > iq, ip < iq, fgt, flt);
+        const int nc = w > c ? w : c;
+        return ((uint32_t)nc << 17) | lab_bits;
+    };
+    auto pending = [&]() {
+        uint32_t m = OIFT_KEY_INF;
+#pragma unroll
+        for (int i = 0; i < NR / 4; i++) {
+            const uint4 v = reinterpret_cast<const uint4 *>(skey)[lane + 32 * i];
+            if (v.x > kk && v.x < m) m = v.x;
+            if (v.y > kk && v.y < m) m = v.y;
+            if (v.z > kk && v.z < m) m = v.z;
+            if (v.w > kk && v.w < m) m = v.w;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            uint32_t v = __shfl_xor_sync(FULL, m, o);
+            m = v < m ? v : m;
+        }
+        if (lane == 0 && m != OIFT_KEY_INF) atomicMin(&A.tpend[t], m);
+    };
+    // ---- stage keys and the intensities with a one-voxel halo ----
+    const bool full = (x0 + 32 <= X) && (y0 + TY <= Y) && (z0 + TZ <= Z) && ((X & 7) == 0);
+    if (full) {
+#pragma unroll
+        for (int m = 0; m < NR / 4; m++) {
+            const int j = lane + 32 * m, r = j >> 3, col = j & 7;
+            const size_t p0 = (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
+            cp_async16(reinterpret_cast<uint4 *>(skey) + j,
+                       reinterpret_cast<const uint4 *>(A.key + p0) + col);
+        }
+    } else {
+#pragma unroll 4
+        for (int r = 0; r < NR; r++) {
+            const int y = y0 + (r % TY), z = z0 + (r / TY);
+            const bool valid = (x < X) && (y < Y) && (z < Z);
+            skey[r * 32 + lane] =
+                valid ? __ldcg(&A.key[(size_t)x + (size_t)y * X + (size_t)z * XY]) : 0u;
+        }
+    }
+    for (int i = lane; i < 34 * HY * HZ; i += 32) {
+        const int hx = i % 34, hy = (i / 34) % HY, hz = i / (34 * HY);
+        const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - ZO + hz;
+        const bool ok = gx >= 0 && gx < X && gy >= 0 && gy < Y && gz >= 0 && gz < Z;
+        simg[i] = ok ? (int32_t)__ldg(&img[(size_t)gx + (size_t)gy * X + (size_t)gz * XY]) : 0;
+    }
+    if (full) cp_async_wait_all();
+    __syncwarp();
+    // ---- level rows (lane r < NR keeps row r): at this level, at or below it ----
+    uint32_t rowF = 0, rowV = 0;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const uint32_t k = skey[r * 32 + lane];
+        const uint32_t bF = __ballot_sync(FULL, k == kk);
+        const uint32_t bV = __ballot_sync(FULL, k <= kk);
+        if (lane == r) {
+            rowF = bF;
+            rowV = bV;
+        }
+    }
+    int nf0 = __popc(rowF);
+    for (int o = 16; o > 0; o >>= 1) nf0 += __shfl_xor_sync(FULL, nf0, o);
+    const long long tcount = clock64();
+    cyc[0] += tcount - tc0;
+    if (nf0 == 0) {
+        pending();
+        cyc[3] += 1;
+        return;
+    }
+    auto append_rows = [&](uint32_t m, int base) -> int {
+        const int n = __popc(m);
+        int incl = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        int pos = base + incl - n;
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            const int li = (lane << 5) | b;
+            wl[pos++] = (uint16_t)li;
+            skey[li] = kk;
+        }
+        return base + total;
+    };
+    if (lane < NR) nfm[lane] = 0u;
+    int cnt = append_rows(rowF, 0);
+    __syncwarp();
+    int done = 0, rounds = 0;
+    while (done < cnt) {
+        // ---- one flood round over up to 32 worklist voxels ----
+        const int idx = done + lane;
+        if (idx < cnt) {
+            const int li = wl[idx];
+            const int r = li >> 5, xl = li & 31, yl = r % TY, zl = r / TY;
+            const int xg = x0 + xl, y = y0 + yl, z = z0 + zl;
+            A.key[(size_t)xg + (size_t)y * X + (size_t)z * XY] = kexp;
+            skey[li] = kexp;
+            const int ip = himg(xl, yl, zl);
+#pragma unroll
+            for (int dz = (TZ > 1 ? -1 : 0); dz <= (TZ > 1 ? 1 : 0); dz++)
+#pragma unroll
+                for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                    for (int dx = -1; dx <= 1; dx++) {
+                        if (dx == 0 && dy == 0 && dz == 0) continue;
+                        const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
+                        if (qxl < 0 || qxl >= 32 || qyl < 0 || qyl >= TY || qzl < 0 || qzl >= TZ)
+                            continue;  // across the tile boundary: after the flood
+                        if (xg + dx >= X || y + dy >= Y || z + dz >= Z) continue;
+                        const int lq = (qyl + TY * qzl) * 32 + qxl;
+                        const uint32_t sk = skey[lq];
+                        if (sk <= kk) continue;
+                        const int iq = himg(qxl, qyl, qzl);
+                        if (arc_open(ip, iq)) {
+                            atomicOr(&nfm[qyl + TY * qzl], 1u << qxl);
+                        } else {
+                            const uint32_t nk = arc_key(ip, iq);
+                            if (nk < sk) {
+                                atomicMin(&skey[lq], nk);
+                                atomicMin(&A.key[(size_t)(xg + dx) + (size_t)(y + dy) * X +
+                                                 (size_t)(z + dz) * XY], nk);
+                            }
+                        }
+                    }
+        }
+        done = (done + 32 < cnt) ? done + 32 : cnt;
+        rounds++;
+        __syncwarp();
+        uint32_t m = 0;
+        if (lane < NR) {
+            m = nfm[lane] & ~rowV;
+            nfm[lane] = 0u;
+            rowV |= m;
+        }
+        cnt = append_rows(m, cnt);
+        __syncwarp();
+    }
+    // ---- pushes across the tile boundary from every voxel expanded in this step ----
+    for (int base = 0; base < cnt; base += 32) {
+        const int idx = base + lane;
+        if (idx >= cnt) continue;
+        const int li = wl[idx];
+        const int r = li >> 5, xl = li & 31, yl = r % TY, zl = r / TY;
+        const bool edge = xl == 0 || xl == 31 || yl == 0 || yl == TY - 1 ||
+                          (TZ > 1 && (zl == 0 || zl == TZ - 1));
+        if (!edge) continue;
+        const int xg = x0 + xl, y = y0 + yl, z = z0 + zl;
+        const int ip = himg(xl, yl, zl);
+#pragma unroll
+        for (int dz = (TZ > 1 ? -1 : 0); dz <= (TZ > 1 ? 1 : 0); dz++) {
+            uint32_t nk[9], old[9];
+#pragma unroll
+            for (int j = 0; j < 9; j++) {
+                const int dy = j / 3 - 1, dx = j % 3 - 1;
+                nk[j] = OIFT_KEY_INF;
+                const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
+                const bool out = qxl < 0 || qxl >= 32 || qyl < 0 || qyl >= TY || qzl < 0 || qzl >= TZ;
+                const int qx = xg + dx, qy = y + dy, qz = z + dz;
+                if (!out || qx < 0 || qy < 0 || qz < 0 || qx >= X || qy >= Y || qz >= Z) continue;
+                nk[j] = arc_key(ip, himg(qxl, qyl, qzl));
+                old[j] = atomicMin(&A.key[(size_t)qx + (size_t)qy * X + (size_t)qz * XY], nk[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 9; j++) {
+                if (nk[j] == OIFT_KEY_INF || !(nk[j] < old[j])) continue;
+                const int dy = j / 3 - 1, dx = j % 3 - 1;
+                const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
+                const int ox = qxl < 0 ? -1 : (qxl >= 32 ? 1 : 0);
+                const int oy = qyl < 0 ? -1 : (qyl >= TY ? 1 : 0);
+                const int oz = qzl < 0 ? -1 : (qzl >= TZ ? 1 : 0);
+                if (nk[j] == kk) {
+                    atomicOr(rmask, 1u << ((oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)));
+                } else {
+                    const int tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
+                    atomicMin(&A.tpend[tq], nk[j]);
+                }
+            }
+        }
+    }
+    __syncwarp();
+    // ---- publish the same-level re-activations of the neighbour tiles ----
+    {
+        const uint32_t m = *(volatile uint32_t *)rmask;
+        if (m != 0u) {
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) {
+                atomicAdd(&A.g->outstanding[par], __popc(m));
+                __threadfence();
+                *rmask = 0u;
+            }
+            __syncwarp();
+            bool dup = false;
+            if (lane < 27 && ((m >> lane) & 1u)) {
+                const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
+                const int tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
+                const int w = tq % A.nwarps, j = tq / A.nwarps;
+                const unsigned long long bit = 1ull << (j & 63);
+                const unsigned long long o =
+                    atomicOr(&A.mbox[(size_t)w * A.mbox_words + (j >> 6)], bit);
+                dup = (o & bit) != 0ull;
+            }
+            const uint32_t dups = __ballot_sync(FULL, dup);
+            if (lane == 0 && dups) atomicSub(&A.g->outstanding[par], __popc(dups));
+        }
+    }
+    __syncwarp();
+    pending();
+    cyc[1] += clock64() - tcount;
+    cyc[4] += 1;
+    cyc[17] += rounds;
+    cyc[18] += cnt;
+}
+
 // Re-activation bitmask words per warp when `nwarps` warps own `ntiles` tiles round-robin.
 __host__ __device__ __forceinline__ int oift_mbox_words_for(int ntiles, int nwarps) {
     return ((ntiles + nwarps - 1) / nwarps + 63) / 64;
@@ -692,7 +965,7 @@ struct OiftCtaSmem {
 
 // The level loop of one OIFT job, run by the `team_ctas` CTAs starting at team CTA index
 // `team_cta` (0 .. team_ctas-1).  A.nwarps must equal team_ctas * OIFT_WARPS.
-template <int TY, int TZ>
+template <int TY, int TZ, bool FULLN = false, typename TI = int16_t>
 __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftCtaSmem &cs,
                            unsigned char *smem_raw) {
     const unsigned FULL = 0xffffffffu;
@@ -779,8 +1052,14 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 const int th = gwarp + (j0 + b) * nwarps;
                 if (lane == 0) A.tpend[th] = OIFT_KEY_INF;
                 __syncwarp();
-                process_tile<TY, TZ>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey, sw,
-                                     shx, shy, shz, wl, nfm, rmask, cyc_tile);
+                if constexpr (FULLN)
+                    process_tile_full<TY, TZ, TI>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey,
+                                                  reinterpret_cast<int32_t *>(sw),
+                                                  reinterpret_cast<uint16_t *>(wl), nfm, rmask,
+                                                  cyc_tile);
+                else
+                    process_tile<TY, TZ>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey, sw,
+                                         shx, shy, shz, wl, nfm, rmask, cyc_tile);
                 steps++;
             }
         }
@@ -814,8 +1093,15 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                         const int j = wd * 64 + __ffsll((long long)b) - 1;
                         b &= b - 1;
                         const int t = gwarp + j * nwarps;
-                        process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey,
-                                             sw, shx, shy, shz, wl, nfm, rmask, cyc_tile);
+                        if constexpr (FULLN)
+                            process_tile_full<TY, TZ, TI>(A, t, par, kk, c, l, fgt, flt, bgt,
+                                                          blt, skey,
+                                                          reinterpret_cast<int32_t *>(sw),
+                                                          reinterpret_cast<uint16_t *>(wl), nfm,
+                                                          rmask, cyc_tile);
+                        else
+                            process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey,
+                                                 sw, shx, shy, shz, wl, nfm, rmask, cyc_tile);
                         steps++;
                         __threadfence();
                         __syncwarp();
@@ -856,11 +1142,11 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     }
 }
 
-template <int TY, int TZ>
+template <int TY, int TZ, bool FULLN = false, typename TI = int16_t>
 __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(OiftArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ OiftCtaSmem cs;
-    oift_solve<TY, TZ>(A, blockIdx.x, gridDim.x, cs, smem_raw);
+    oift_solve<TY, TZ, FULLN, TI>(A, blockIdx.x, gridDim.x, cs, smem_raw);
 }
 
 // Batched OIFT: CTA b belongs to team b / team_ctas.  A team draws jobs from a shared
@@ -1023,6 +1309,23 @@ __global__ void oift_finalize_kernel(const uint32_t *key, size_t n, int32_t *cos
 
 // ------------------------------------------------------------------ host side ----
 
+OiftPlan oift_plan_full(int X, int Y, int Z) {
+    OiftPlan P;
+    if (Z == 1) {
+        P.TY = 16;
+        P.TZ = 1;
+    } else {
+        P.TY = 4;
+        P.TZ = 4;
+    }
+    P.ntx = (X + 31) / 32;
+    P.nty = (Y + P.TY - 1) / P.TY;
+    P.ntz = (Z + P.TZ - 1) / P.TZ;
+    P.ntiles = P.ntx * P.nty * P.ntz;
+    P.qcap = 0;
+    return P;
+}
+
 OiftPlan oift_plan(int X, int Y, int Z) {
     OiftPlan P;
     if (Z == 1) {
@@ -1057,7 +1360,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
              long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end,
-             unsigned long long *cycles_out) {
+             unsigned long long *cycles_out, const OiftFullN *fn) {
     size_t N = (size_t)X * Y * Z;
     cudaMemsetAsync(S.key, 0xFF, N * sizeof(uint32_t), st);
     cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
@@ -1102,20 +1405,30 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.g = S.g;
     A.spin_limit = 20000000LL;  // ~1-2 s of polling at ~64 ns per spin
     A.max_levels = 4000000;
+    A.img = fn ? fn->img : nullptr;
+    A.wmode = fn ? fn->wmode : 0;
+    A.wcap = fn ? fn->wcap : OIFT_MAX_BASE;
+    A.lut = fn ? fn->lut : nullptr;
+    A.lut_len = fn ? fn->lut_len : 0;
     size_t smem = oift_smem_bytes();
     void *args[] = {&A};
     cudaError_t err;
     if (ev_begin) cudaEventRecord(ev_begin, st);
-    if (P.TZ == 1) {
-        auto kfn = oift_persistent_kernel<32, 1>;
+    auto launch = [&](const void *kfn) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(sms), dim3(OIFT_WARPS * 32), args,
-                                          smem, st);
+        return cudaLaunchCooperativeKernel(kfn, dim3(sms), dim3(OIFT_WARPS * 32), args, smem, st);
+    };
+    if (fn) {
+        if (P.TZ == 1)
+            err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<16, 1, true, int16_t>)
+                              : launch((const void *)oift_persistent_kernel<16, 1, true, int32_t>);
+        else
+            err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<4, 4, true, int16_t>)
+                              : launch((const void *)oift_persistent_kernel<4, 4, true, int32_t>);
+    } else if (P.TZ == 1) {
+        err = launch((const void *)oift_persistent_kernel<32, 1>);
     } else {
-        auto kfn = oift_persistent_kernel<8, 4>;
-        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(sms), dim3(OIFT_WARPS * 32), args,
-                                          smem, st);
+        err = launch((const void *)oift_persistent_kernel<8, 4>);
     }
     if (err != cudaSuccess) return OIFT_E_CUDA;
     if (ev_end) cudaEventRecord(ev_end, st);

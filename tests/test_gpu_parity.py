@@ -30,6 +30,13 @@ CASES = [
     ((1, 67, 45), -0.2, 4, 2, "grad"),
     ((20, 24, 64), -0.3, 6, 1, "grad_q"),
     ((12, 16, 40), 0.3, 6, 2, "rbf_q"),
+    # full 3x3(x3) neighbourhoods: partial tiles along every axis, exact / quantised / RBF
+    ((10, 14, 40), -0.3, 26, 1, "grad"),
+    ((9, 21, 70), 0.4, 26, 2, "grad"),
+    ((1, 45, 67), 0.5, 8, 1, "grad"),
+    ((1, 40, 48), -0.2, 8, 2, "grad"),
+    ((12, 16, 40), 0.3, 26, 2, "rbf_q"),
+    ((8, 12, 64), -0.4, 26, 1, "grad_q"),
 ]
 
 
@@ -374,3 +381,27 @@ def test_cli_chain_matches_oracle_and_reference(roift, path):
     exp1, _ = O.oiftrelax_chain(img, pol, K, 50.0, seeds, sl, oift="r1")
     if np.array_equal(exp1, exp2):
         assert np.array_equal(got, d["ref_chain_label"])
+
+
+@pytest.mark.parametrize("adj", [26, 6])
+def test_device_path_int16_full_neighbourhood(roift, oracle_lib, adj):
+    """int16 device images through the full-neighbourhood kernel (and 6-adj beside it):
+    three objects, RBF weights, cost and labels == R2."""
+    import torch
+    c = synth.three_ellipsoids(seed=31, shape=(40, 48, 56))
+    dev = torch.device("cuda:0")
+    img16 = c.image.astype(np.int16)
+    Z, Y, X = c.shape
+    p = roift.make_params(c.shape, adjacency=adj, weight_mode="rbf_q", wq=4095, rbf_sigma=150.0,
+                          pol=c.pol, sweeps=0)
+    d_img = torch.from_numpy(img16.reshape(-1).copy()).to(dev)
+    sd = torch.from_numpy(c.seeds).to(dev)
+    sl = torch.from_numpy(c.seed_labels).to(dev)
+    cost = torch.empty(c.n, dtype=torch.int32, device=dev)
+    lab = torch.empty(c.n, dtype=torch.int32, device=dev)
+    roift._ctx().run_device(p, d_img.data_ptr(), sd.data_ptr(), sl.data_ptr(), len(c.seeds),
+                            cost=cost.data_ptr(), oift_label=lab.data_ptr())
+    W, _ = O.build_weights(img16.astype(np.int32), adj, "rbf_q", wq=4095, rbf_sigma=150.0)
+    cost_r2, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
+    assert np.array_equal(cost.cpu().numpy(), cost_r2)
+    assert np.array_equal(lab.cpu().numpy(), lab_r2)
