@@ -193,6 +193,24 @@ OIFT_API int oift_b200_run_cli_host(oift_b200_ctx *ctx, const oift_b200_params *
                                     int nseeds, int blur_passes, float percentile,
                                     oift_b200_stats *stats);
 
+/* Two-level coarse-to-fine cascade (experiments/exp_coarse_to_fine.cpp:327-414): shift,
+ * `blur_passes` blurs, Subsampling to odd half extents, seeds at (x/2, y/2, z/2) (first
+ * seed wins), coarse OIFT + relaxation, nearest ScaleLabel, labels that touch another value
+ * become NIL, the caller's labels kept, every labelled voxel a seed of the fine OIFT +
+ * relaxation, conditional dilation (percentile >= 0) of a binary result.  Host flavour:
+ * `label` holds the seed labels on entry (NIL = -1 elsewhere) and the result on return. */
+OIFT_API int oift_b200_run_pyramid_host(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                                        const int32_t *image, int32_t *label,
+                                        const int32_t *seeds, int nseeds, int blur_passes,
+                                        float percentile, oift_b200_stats *stats);
+/* Device flavour: int16 image, label_in (seed labels, NIL elsewhere), seeds and label_out
+ * are device arrays. */
+OIFT_API int oift_b200_run_pyramid_device_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                                              const int16_t *image, const int32_t *label_in,
+                                              const int32_t *seeds, int nseeds, int blur_passes,
+                                              float percentile, int32_t *label_out,
+                                              oift_b200_stats *stats);
+
 /* Stage entry points on device pointers (used by the batched driver and tests). */
 OIFT_API int oift_b200_build_weights_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
                                 const int16_t *image, uint16_t *weights /* [planes][N] */,

@@ -73,6 +73,8 @@ def lib():
         L.or_relax_f64.restype = C.c_int
         L.or_relax_f64.argtypes = L.or_relax_f32.argtypes
         L.or_gaussian_blur.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        L.or_adjacency.restype = C.c_int
+        L.or_adjacency.argtypes = [C.c_int, _i32p, _i32p, _i32p]
         L.or_conditional_dilation.restype = C.c_longlong
         L.or_conditional_dilation.argtypes = [_i32p, _i32p, C.c_int, C.c_int, C.c_int,
                                               C.c_float, C.c_float]
@@ -110,6 +112,8 @@ def ref():
         R.ref_inject_boundary_seeds.restype = C.c_int
         R.ref_inject_boundary_seeds.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int,
                                                 _i32p, C.c_int, _i32p, C.c_int]
+        R.ref_coarse_to_fine.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                         C.c_int, C.c_float, _i32p, C.c_int, _i32p]
         R.ref_oiftrelax_chain.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_double,
                                           C.c_int, C.c_float, _i32p, C.c_int, _i32p]
         _ref = R
@@ -269,6 +273,100 @@ def oiftrelax_chain(img, pol, niter, percentile, seeds, seed_labels, oift="r2", 
     return out, b
 
 
+def coarse_size(n):
+    """Scene32::Subsampling extent (gft_filtering3.cpp:449-455): n/2 + n%2, made odd."""
+    c = n // 2 + n % 2
+    return c + 1 if c % 2 == 0 else c
+
+
+def subsample(fscn):
+    """Scene32::Subsampling (gft_filtering3.cpp:445-476): coarse voxel v takes the fine
+    voxel (v - c/2) * 2 + n/2 (integer halves) when inside, else 0."""
+    Z, Y, X = fscn.shape
+    cz, cy, cx = coarse_size(Z), coarse_size(Y), coarse_size(X)
+    out = np.zeros((cz, cy, cx), np.int32)
+    ux = (np.arange(cx) - cx // 2) * 2 + X // 2
+    uy = (np.arange(cy) - cy // 2) * 2 + Y // 2
+    uz = (np.arange(cz) - cz // 2) * 2 + Z // 2
+    vx, vy, vz = (ux >= 0) & (ux < X), (uy >= 0) & (uy < Y), (uz >= 0) & (uz < Z)
+    out[np.ix_(vz, vy, vx)] = fscn[np.ix_(uz[vz], uy[vy], ux[vx])]
+    return out
+
+
+def scale_label_nn(lab_c, coarse_shape, fine_shape):
+    """Scene32::ScaleLabel(..., none) = Scale nearest (gft_scene32.cpp:1091-1120,
+    1240-1262): x = (u - n/2.) * 0.5 + c/2. in double stored as float, index
+    (int)(x + 0.5) truncated toward zero, clamped to the coarse extent."""
+    def axis(n, c):
+        u = np.arange(n, dtype=np.float64)
+        x = ((u - n / 2.0) * np.float64(np.float32(0.5)) + c / 2.0).astype(np.float32)
+        i = np.trunc(x.astype(np.float64) + 0.5).astype(np.int64)
+        return np.clip(i, 0, c - 1)
+    (Z, Y, X), (cz, cy, cx) = fine_shape, coarse_shape
+    lc = lab_c.reshape(coarse_shape)
+    return lc[np.ix_(axis(Z, cz), axis(Y, cy), axis(X, cx))].reshape(-1)
+
+
+def mark_boundary_nil(label, shape, adj):
+    """Labelled voxels with a neighbour (adjacency without the centre) of another value,
+    NIL included, become NIL (exp_coarse_to_fine.cpp:216-249)."""
+    Z, Y, X = shape
+    lab = label.reshape(shape)
+    dx, dy, dz = (np.zeros(26, np.int32) for _ in range(3))
+    n = lib().or_adjacency(adj, dx, dy, dz)
+    pad = np.pad(lab, 1, constant_values=-2)  # -2: outside the volume
+    bnd = np.zeros(shape, bool)
+    for i in range(n):
+        sz, sy, sx = int(dz[i]), int(dy[i]), int(dx[i])
+        nb = pad[1 + sz:1 + sz + Z, 1 + sy:1 + sy + Y, 1 + sx:1 + sx + X]
+        bnd |= (nb != -2) & (nb != lab)
+    out = lab.copy()
+    out[bnd & (lab != NIL)] = NIL
+    return out.reshape(-1)
+
+
+def coarse_to_fine(fscn, adj, pol, niter, percentile, seeds, label, mode="grad", wq=4095,
+                   rbf_sigma=150.0, oift="r2"):
+    """The two-level cascade (exp_coarse_to_fine.cpp:327-414) restated on the blurred,
+    shifted volume with the oracle's OIFT (R2, or R1 = OIFT_Multi's order) and R3-FP32
+    relaxation.  label: seed labels (NIL elsewhere).  Returns the label map."""
+    shape = fscn.shape
+    Z, Y, X = shape
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    coarse = subsample(fscn)
+    cshape = coarse.shape
+    cz, cy, cx = cshape
+    lab_c = np.full(coarse.size, NIL, np.int32)
+    cs = []
+    for pp in np.asarray(seeds, np.int64):
+        x, y, z = int(pp % X), int((pp // X) % Y), int(pp // (X * Y))
+        q = x // 2 + (y // 2) * cx + (z // 2) * cx * cy
+        if x // 2 < cx and y // 2 < cy and z // 2 < cz and lab_c[q] == NIL:
+            lab_c[q] = lab[pp]
+            cs.append(q)
+    cs = np.array(cs, np.int32)
+
+    def solve(img, sd, lab_in):
+        X_, Y_, Z_ = img.shape[2], img.shape[1], img.shape[0]
+        W, _ = build_weights(img, adj, mode, wq=wq, rbf_sigma=rbf_sigma)
+        sl = lab_in[sd]
+        if oift == "r2":
+            _, lo, _ = oift_fmax(W, (X_, Y_, Z_), adj, sd, sl, pol=pol)
+        else:
+            lo = oift_prim(W, (X_, Y_, Z_), adj, sd, sl, pol=pol)[0]
+        out, _, _ = relax(img, adj, sd, lo, niter, pol=pol)
+        return out
+
+    lab_c = solve(coarse, cs, lab_c)
+    up = mark_boundary_nil(scale_label_nn(lab_c, cshape, shape), shape, adj)
+    merged = np.where((up != NIL) & (lab == NIL), up, lab).astype(np.int32)
+    fs = np.nonzero(merged != NIL)[0].astype(np.int32)
+    out = solve(fscn, fs, merged)
+    if out.max() <= 1:
+        out, _ = conditional_dilation(fscn, out, 1.0, percentile)
+    return out
+
+
 def gaussian_blur(img):
     X, Y, Z = _dims(img)
     out = np.empty(X * Y * Z, np.int32)
@@ -374,6 +472,17 @@ def ref_oiftrelax_chain(img, pol, niter, percentile, seeds, label):
     lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
     ref().ref_oiftrelax_chain(as_i32(img), X, Y, Z, float(pol), int(niter), float(percentile),
                               np.ascontiguousarray(seeds, np.int32), len(seeds), lab)
+    return lab
+
+
+def ref_coarse_to_fine(fscn, adj, pol, niter, percentile, seeds, label):
+    """The reference coarse-to-fine cascade (experiments/exp_coarse_to_fine.cpp:327-414) on
+    the blurred, shifted volume; label holds the seed labels.  Returns the label map."""
+    X, Y, Z = _dims(fscn)
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    ref().ref_coarse_to_fine(as_i32(fscn), X, Y, Z, adj, float(pol), int(niter),
+                             float(percentile), np.ascontiguousarray(seeds, np.int32),
+                             len(seeds), lab)
     return lab
 
 

@@ -85,7 +85,8 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes",
            "oift_b200_run_batch", "oift_b200_set_oift_grid", "oift_b200_gaussian_blur_i32",
            "oift_b200_conditional_dilation", "oift_b200_inject_boundary_seeds",
-           "oift_b200_run_cli_host"]
+           "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
+           "oift_b200_run_pyramid_device_i16"]
 
 _lib = None
 
@@ -133,6 +134,10 @@ def lib():
                                                       vp, C.c_int]
         L.oift_b200_run_cli_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
                                              C.c_int, C.c_float, C.POINTER(Stats)]
+        L.oift_b200_run_pyramid_host.argtypes = L.oift_b200_run_cli_host.argtypes
+        L.oift_b200_run_pyramid_device_i16.argtypes = [vp, C.POINTER(Params), vp, vp, vp, C.c_int,
+                                                       C.c_int, C.c_float, vp,
+                                                       C.POINTER(Stats)]
         _lib = L
     return _lib
 
@@ -279,6 +284,31 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_run_cli_host")
         return lab, st
+
+    def run_pyramid_host(self, params, image, label, seeds, blur_passes=2, percentile=50.0):
+        """Two-level coarse-to-fine cascade on host arrays (unshifted int32 image; `label`
+        holds the seed labels, NIL elsewhere, and receives the result)."""
+        img = np.ascontiguousarray(np.asarray(image).reshape(-1), np.int32)
+        lab = np.ascontiguousarray(label, np.int32)
+        sd = np.ascontiguousarray(seeds, np.int32)
+        st = Stats()
+        rc = lib().oift_b200_run_pyramid_host(self._h, C.byref(params), img, lab, sd, len(sd),
+                                              int(blur_passes), float(percentile), C.byref(st))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_run_pyramid_host")
+        return lab, st
+
+    def run_pyramid_device(self, params, image_ptr, label_in_ptr, seeds_ptr, nseeds,
+                           label_out_ptr, blur_passes=2, percentile=50.0) -> Stats:
+        """The cascade on device arrays (int16 image, int32 labels and seeds)."""
+        st = Stats()
+        rc = lib().oift_b200_run_pyramid_device_i16(
+            self._h, C.byref(params), C.c_void_p(image_ptr), C.c_void_p(label_in_ptr),
+            C.c_void_p(seeds_ptr), int(nseeds), int(blur_passes), float(percentile),
+            C.c_void_p(label_out_ptr), C.byref(st))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_run_pyramid_device_i16")
+        return st
 
     def level_profile(self, cap=8192):
         """(cycles, tile activations) per OIFT level of the last run."""

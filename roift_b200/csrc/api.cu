@@ -32,7 +32,7 @@ struct oift_b200_ctx {
     std::vector<std::pair<int, double>> tune_cands;  // batch autotuner: (teams, rate)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    cudaEvent_t ev[8];
+    cudaEvent_t ev[10];
     // scratch (grow-only)
     DevBuf img32, img16, W, key, tpend, inq, queue, glob, flag, minmax, seeds, slabels, cost,
         olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8, ctaq, lprof, rtdist;
@@ -41,6 +41,9 @@ struct oift_b200_ctx {
     DevBuf bjobs, bmm, bkey, btpend, bmbox, bglob, bctl, bolab;
     // CLI steps: shifted / blurred images, dilation border, histograms and tie counts
     DevBuf cimg0, cimg1, dborder, dhist, daux, dlabel;
+    // coarse-to-fine cascade: coarse image / labels / seeds, first-seed map, upscaled and
+    // merged labels, fine seeds, axis tables and chunk counts
+    DevBuf yimg, ylab, yseeds, yslab, yfirst, yup, ymerge, yfseeds, yfslab, yaux;
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -135,7 +138,9 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->classes, &c->pol,  &c->presence, &c->lut,   &c->mask8, &c->ctaq,
                       &c->lprof, &c->rtdist, &c->bjobs, &c->bmm,  &c->bkey,  &c->btpend,
                       &c->bmbox, &c->bglob, &c->bctl, &c->bolab, &c->cimg0, &c->cimg1,
-                      &c->dborder, &c->dhist, &c->daux, &c->dlabel};
+                      &c->dborder, &c->dhist, &c->daux, &c->dlabel, &c->yimg, &c->ylab,
+                      &c->yseeds, &c->yslab, &c->yfirst, &c->yup, &c->ymerge, &c->yfseeds,
+                      &c->yfslab, &c->yaux};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -845,6 +850,171 @@ static int conditional_dilation(oift_b200_ctx *c, const int32_t *img, int32_t *l
     return OIFT_OK;
 }
 
+extern "C++" {
+
+// Every labelled voxel (!= NIL) of the device map `lab` as a seed, in address order.
+static int seeds_from_labels(oift_b200_ctx *c, const int32_t *lab, size_t N, DevBuf &seeds,
+                             DevBuf &slabels, int *nout) {
+    cudaStream_t s = c->stream;
+    const size_t chunk = 8192, nch = (N + chunk - 1) / chunk;
+    TRY(grow(c, c->yaux, 2 * nch * sizeof(unsigned)));
+    unsigned *d_cnt = (unsigned *)c->yaux.p, *d_base = d_cnt + nch;
+    seeds_count_kernel<<<(unsigned)nch, 256, 0, s>>>(lab, N, chunk, d_cnt);
+    CU(cudaGetLastError());
+    std::vector<unsigned> h(nch);
+    CU(cudaMemcpyAsync(h.data(), d_cnt, nch * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    unsigned long long run = 0;
+    for (size_t i = 0; i < nch; i++) {
+        const unsigned v = h[i];
+        h[i] = (unsigned)run;
+        run += v;
+    }
+    if (run > 0x7fffffffULL) return OIFT_E_RANGE;
+    TRY(grow(c, seeds, std::max<size_t>(run, 1) * sizeof(int32_t)));
+    TRY(grow(c, slabels, std::max<size_t>(run, 1) * sizeof(int32_t)));
+    CU(cudaMemcpyAsync(d_base, h.data(), nch * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+    seeds_scatter_kernel<<<(unsigned)nch, 256, 0, s>>>(lab, N, chunk, d_base, (int32_t *)seeds.p,
+                                                       (int32_t *)slabels.p);
+    CU(cudaGetLastError());
+    *nout = (int)run;
+    return OIFT_OK;
+}
+
+// ScaleLabel(.., none) index of fine coordinate u along an axis of n fine / nc coarse
+// voxels (gft_scene32.cpp:1108-1116, 1240-1262): x = (u - n/2.) * (1/2.f) + nc/2. in
+// double, stored as float; (int)(x + 0.5); clamped to [0, nc - 1].
+static int nn_index(int u, int n, int nc) {
+    const float ratio = 1.0f / 2.0f;  // ref->dx / scn->dx, fine spacing over coarse
+    const float x = (float)(((double)u - n / 2.) * (double)ratio + nc / 2.);
+    int v = (int)((double)x + 0.5);
+    if (v > nc - 1)
+        v = nc - 1;
+    else if (v < 0)
+        v = 0;
+    return v;
+}
+
+static int coarse_extent(int n) {  // Subsampling (gft_filtering3.cpp:449-455)
+    const int c = n / 2 + n % 2;
+    return c % 2 == 0 ? c + 1 : c;
+}
+
+// The two-level cascade (exp_coarse_to_fine.cpp:327-414) on the device: d_fscn is the
+// blurred volume shifted to >= 0; d_label_in holds the seed labels (NIL elsewhere) of the
+// nseeds device seeds.  The result goes to d_label_out.
+static int run_pyramid(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *d_fscn,
+                       const int32_t *d_label_in, const int32_t *d_seeds, int nseeds,
+                       float percentile, int32_t *d_label_out, oift_b200_stats *st) {
+    cudaStream_t s = c->stream;
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    const size_t N = (size_t)X * Y * Z;
+    const int cx = coarse_extent(X), cy = coarse_extent(Y), cz = coarse_extent(Z);
+    const size_t cn = (size_t)cx * cy * cz;
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16));
+    const int cblocks = (int)std::max<size_t>(1, std::min<size_t>((cn + 255) / 256, (size_t)c->sms * 16));
+    cudaEventRecord(c->ev[8], s);
+    // ---- coarse pass ----
+    TRY(grow(c, c->yimg, cn * sizeof(int32_t)));
+    TRY(grow(c, c->ylab, cn * sizeof(int32_t)));
+    TRY(grow(c, c->yfirst, cn * sizeof(unsigned)));
+    pyr_subsample_kernel<<<cblocks, 256, 0, s>>>(d_fscn, (int32_t *)c->yimg.p, X, Y, Z, cx, cy, cz);
+    CU(cudaMemsetAsync(c->yfirst.p, 0xFF, cn * sizeof(unsigned), s));
+    if (nseeds > 0)
+        pyr_coarse_first_kernel<<<std::min((nseeds + 255) / 256, c->sms * 16), 256, 0, s>>>(
+            d_seeds, nseeds, X, Y, Z, cx, cy, cz, (unsigned *)c->yfirst.p);
+    pyr_coarse_labels_kernel<<<cblocks, 256, 0, s>>>((const unsigned *)c->yfirst.p, d_seeds,
+                                                     d_label_in, cn, (int32_t *)c->ylab.p);
+    CU(cudaGetLastError());
+    int ncs = 0;
+    TRY(seeds_from_labels(c, (const int32_t *)c->ylab.p, cn, c->yseeds, c->yslab, &ncs));
+    if (ncs == 0) return OIFT_E_NO_SEEDS;
+    oift_b200_params pc = *p;
+    pc.xsize = cx;
+    pc.ysize = cy;
+    pc.zsize = cz;
+    oift_b200_outputs oc{};
+    oc.label = (int32_t *)c->ylab.p;  // the coarse seed map is no longer needed
+    oift_b200_stats stc{};
+    TRY(run_pipeline<int32_t>(c, &pc, (const int32_t *)c->yimg.p, (const int32_t *)c->yseeds.p,
+                              (const int32_t *)c->yslab.p, ncs, &oc, &stc));
+    // ---- upscale, band around the coarse boundaries to NIL, merge ----
+    TRY(grow(c, c->yup, N * sizeof(int32_t)));
+    TRY(grow(c, c->ymerge, N * sizeof(int32_t)));
+    {
+        std::vector<int> tab((size_t)X + Y + Z);
+        for (int u = 0; u < X; u++) tab[u] = nn_index(u, X, cx);
+        for (int u = 0; u < Y; u++) tab[X + u] = nn_index(u, Y, cy);
+        for (int u = 0; u < Z; u++) tab[X + Y + u] = nn_index(u, Z, cz);
+        const Adjacency adj =
+            make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
+        std::vector<int> off;
+        for (int i = 0; i < adj.n; i++) {
+            off.push_back(adj.dx[i]);
+            off.push_back(adj.dy[i]);
+            off.push_back(adj.dz[i]);
+        }
+        TRY(grow(c, c->dhist, (tab.size() + off.size()) * sizeof(int)));
+        int *d_tab = (int *)c->dhist.p, *d_off = d_tab + tab.size();
+        CU(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        pyr_upscale_kernel<<<blocks, 256, 0, s>>>((const int32_t *)c->ylab.p, (int32_t *)c->ymerge.p,
+                                                  X, Y, Z, cx, cy, d_tab, d_tab + X, d_tab + X + Y);
+        pyr_boundary_nil_kernel<<<blocks, 256, 0, s>>>((const int32_t *)c->ymerge.p,
+                                                       (int32_t *)c->yup.p, X, Y, Z, d_off, adj.n);
+        pyr_merge_kernel<<<blocks, 256, 0, s>>>(d_label_in, (const int32_t *)c->yup.p,
+                                                (int32_t *)c->ymerge.p, N);
+        CU(cudaGetLastError());
+        // the tables must stay valid until the kernels above have read them
+        CU(cudaStreamSynchronize(s));
+    }
+    // ---- fine pass: every labelled voxel is a seed ----
+    int nfs = 0;
+    TRY(seeds_from_labels(c, (const int32_t *)c->ymerge.p, N, c->yfseeds, c->yfslab, &nfs));
+    oift_b200_outputs of{};
+    of.label = d_label_out;
+    TRY(run_pipeline<int32_t>(c, p, d_fscn, (const int32_t *)c->yfseeds.p,
+                              (const int32_t *)c->yfslab.p, nfs, &of, st));
+    if (percentile >= 0.0f) {
+        int *d_mm = (int *)c->minmax.p;
+        const int mm_init[2] = {0x7fffffff, (int)0x80000000};
+        CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+        CU(launch_minmax<int32_t>(d_label_out, N, d_mm, c->sms, s));
+        int hmm[2];
+        CU(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (hmm[1] <= 1)
+            TRY(conditional_dilation(c, d_fscn, d_label_out, X, Y, Z, 1.0f, percentile, nullptr));
+    }
+    cudaEventRecord(c->ev[9], s);
+    CU(cudaStreamSynchronize(s));
+    if (st) {
+        // stage figures of the fine pass; the total covers both passes and the glue
+        cudaEventElapsedTime(&st->ms_total, c->ev[8], c->ev[9]);
+        st->levels += stc.levels;
+        st->tile_steps += stc.tile_steps;
+        st->kernels += stc.kernels + 9;
+    }
+    return OIFT_OK;
+}
+
+// Shift to >= 0 and blur: the device int32 volume the cascade and the CLI chain work on.
+template <typename T>
+static int shift_and_blur(oift_b200_ctx *c, const T *d_img, size_t N, int X, int Y, int Z,
+                          int blur_passes, int32_t *d_out) {
+    cudaStream_t s = c->stream;
+    TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
+    int *d_mm = (int *)c->minmax.p;
+    const int mm_init[2] = {0x7fffffff, (int)0x80000000};
+    CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+    CU(launch_minmax<T>(d_img, N, d_mm, c->sms, s));
+    CU(launch_shift_to_i32<T>(d_img, d_out, N, d_mm, c->sms, s));
+    if (blur_passes > 0) TRY(blur_passes_i32(c, d_out, d_out, X, Y, Z, blur_passes));
+    return OIFT_OK;
+}
+
+}  // extern "C++"
+
 extern "C" {
 
 int oift_b200_gaussian_blur_i32(oift_b200_ctx *c, const int32_t *in, int32_t *out, int xsize,
@@ -960,6 +1130,61 @@ int oift_b200_run_cli_host(oift_b200_ctx *c, const oift_b200_params *p, const in
     CU(cudaStreamSynchronize(s));
     return OIFT_OK;
 }
+
+int oift_b200_run_pyramid_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *image,
+                               int32_t *label, const int32_t *seeds, int nseeds, int blur_passes,
+                               float percentile, oift_b200_stats *stats) {
+    if (!c || !image || !label || (nseeds > 0 && !seeds) || blur_passes < 0) return OIFT_E_BAD_ARG;
+    TRY(check_params(p));
+    if (nseeds <= 0) return OIFT_E_NO_SEEDS;
+    cudaSetDevice(c->device);
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    if (Y > 65535 || Z > 65535) return OIFT_E_RANGE;
+    const size_t N = (size_t)X * Y * Z;
+    cudaStream_t s = c->stream;
+    for (int i = 0; i < nseeds; i++) {
+        if (seeds[i] < 0 || (size_t)seeds[i] >= N) return OIFT_E_SEED_RANGE;
+        if (label[seeds[i]] > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
+    }
+    TRY(grow(c, c->img32, N * sizeof(int32_t)));
+    TRY(grow(c, c->cimg0, N * sizeof(int32_t)));
+    TRY(grow(c, c->seeds, (size_t)nseeds * sizeof(int32_t)));
+    TRY(grow(c, c->dlabel, N * sizeof(int32_t)));
+    TRY(grow(c, c->flabel, N * sizeof(int32_t)));
+    CU(cudaMemcpyAsync(c->img32.p, image, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->seeds.p, seeds, (size_t)nseeds * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->flabel.p, label, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    TRY(shift_and_blur<int32_t>(c, (const int32_t *)c->img32.p, N, X, Y, Z, blur_passes,
+                                (int32_t *)c->cimg0.p));
+    oift_b200_stats lst{};
+    TRY(run_pyramid(c, p, (const int32_t *)c->cimg0.p, (const int32_t *)c->flabel.p,
+                    (const int32_t *)c->seeds.p, nseeds, percentile, (int32_t *)c->dlabel.p,
+                    stats ? stats : &lst));
+    CU(cudaMemcpyAsync(label, c->dlabel.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    return OIFT_OK;
+}
+
+int oift_b200_run_pyramid_device_i16(oift_b200_ctx *c, const oift_b200_params *p,
+                                     const int16_t *image, const int32_t *label_in,
+                                     const int32_t *seeds, int nseeds, int blur_passes,
+                                     float percentile, int32_t *label_out,
+                                     oift_b200_stats *stats) {
+    if (!c || !image || !label_in || !label_out || (nseeds > 0 && !seeds) || blur_passes < 0)
+        return OIFT_E_BAD_ARG;
+    TRY(check_params(p));
+    if (nseeds <= 0) return OIFT_E_NO_SEEDS;
+    cudaSetDevice(c->device);
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    if (Y > 65535 || Z > 65535) return OIFT_E_RANGE;
+    const size_t N = (size_t)X * Y * Z;
+    TRY(grow(c, c->cimg0, N * sizeof(int32_t)));
+    TRY(shift_and_blur<int16_t>(c, image, N, X, Y, Z, blur_passes, (int32_t *)c->cimg0.p));
+    oift_b200_stats lst{};
+    return run_pyramid(c, p, (const int32_t *)c->cimg0.p, label_in, seeds, nseeds, percentile,
+                       label_out, stats ? stats : &lst);
+}
+
 
 }  // extern "C"
 

@@ -165,6 +165,23 @@ struct OiftFullN {
 // Tiling of the full-neighbourhood kernel: 32 x 4 x 4 (3D) or 32 x 16 (2D).
 OiftPlan oift_plan_full(int X, int Y, int Z);
 
+__global__ void pyr_subsample_kernel(const int32_t *fine, int32_t *coarse, int X, int Y, int Z,
+                                     int cx, int cy, int cz);
+__global__ void pyr_coarse_first_kernel(const int32_t *seeds, int nseeds, int X, int Y, int Z,
+                                        int cx, int cy, int cz, unsigned *first);
+__global__ void pyr_coarse_labels_kernel(const unsigned *first, const int32_t *seeds,
+                                         const int32_t *fine_label, size_t cn, int32_t *clab);
+__global__ void pyr_upscale_kernel(const int32_t *clab, int32_t *up, int X, int Y, int Z, int cx,
+                                   int cy, const int *ix, const int *iy, const int *iz);
+__global__ void pyr_boundary_nil_kernel(const int32_t *lab, int32_t *out, int X, int Y, int Z,
+                                        const int *off, int noff);
+__global__ void pyr_merge_kernel(const int32_t *label, const int32_t *up, int32_t *merged,
+                                 size_t N);
+__global__ void seeds_count_kernel(const int32_t *lab, size_t N, size_t chunk, unsigned *counts);
+__global__ void seeds_scatter_kernel(const int32_t *lab, size_t N, size_t chunk,
+                                     const unsigned *base_of, int32_t *seeds,
+                                     int32_t *seed_labels);
+
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,

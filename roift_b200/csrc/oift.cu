@@ -1277,24 +1277,30 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
 __global__ void oift_seed_kernel(uint32_t *key, uint32_t *tpend, const int32_t *seeds,
                                  const int32_t *labels, int nseeds, int X, int Y, int Z,
                                  int ntx, int nty, int TY, int TZ, int *bad) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nseeds) return;
-    int p = seeds[i];
-    size_t N = (size_t)X * Y * Z;
-    if (p < 0 || (size_t)p >= N) {
-        atomicExch(bad, 1);
-        return;
+    // every lane of the warp reaches the tile aggregation below (no early return)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t N = (size_t)X * Y * Z;
+    int t = -1;
+    uint32_t k = OIFT_KEY_INF;
+    if (i < nseeds) {
+        const int p = seeds[i];
+        const int lb = labels[i] < 0 ? 0 : labels[i];
+        if (p < 0 || (size_t)p >= N) {
+            atomicExch(bad, 1);
+        } else if (lb > OIFT_MAX_LABEL) {
+            atomicExch(bad, 2);
+        } else {
+            k = make_key(0, lb, 1);
+            atomicMin(&key[p], k);
+            const int x = p % X, y = (p / X) % Y, z = (int)(p / ((size_t)X * Y));
+            t = (x >> 5) + (y / TY) * ntx + (z / TZ) * ntx * nty;
+        }
     }
-    int lb = labels[i] < 0 ? 0 : labels[i];
-    if (lb > OIFT_MAX_LABEL) {
-        atomicExch(bad, 2);
-        return;
-    }
-    uint32_t k = make_key(0, lb, 1);
-    atomicMin(&key[p], k);
-    int x = p % X, y = (p / X) % Y, z = (int)(p / ((size_t)X * Y));
-    int t = (x >> 5) + (y / TY) * ntx + (z / TZ) * ntx * nty;
-    atomicMin(&tpend[t], k);
+    // seed lists in address order put many seeds of a warp in one tile: one pending-key
+    // update per tile and warp
+    const unsigned peers = __match_any_sync(0xffffffffu, t);
+    const uint32_t km = __reduce_min_sync(peers, k);
+    if (t >= 0 && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicMin(&tpend[t], km);
 }
 
 __global__ void oift_finalize_kernel(const uint32_t *key, size_t n, int32_t *cost,

@@ -186,3 +186,154 @@ template cudaError_t launch_gaussian_blur<int32_t>(const int32_t *, int32_t *, i
                                                    float, float, cudaStream_t);
 
 }  // namespace oiftb
+
+namespace oiftb {
+
+// ------------------------------------------------------ coarse-to-fine cascade ----
+// experiments/exp_coarse_to_fine.cpp:327-414 on the device.
+
+// Scene32::Subsampling (gft_filtering3.cpp:445-476): coarse voxel v takes the fine voxel
+// (v - c/2) * 2 + n/2 (integer halves) when it lies inside, else 0.
+__global__ void pyr_subsample_kernel(const int32_t *__restrict__ fine, int32_t *__restrict__ coarse,
+                                     int X, int Y, int Z, int cx, int cy, int cz) {
+    const size_t cn = (size_t)cx * cy * cz;
+    for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < cn;
+         v += (size_t)gridDim.x * blockDim.x) {
+        const int vx = (int)(v % cx), vy = (int)((v / cx) % cy), vz = (int)(v / ((size_t)cx * cy));
+        const int ux = (vx - cx / 2) * 2 + X / 2, uy = (vy - cy / 2) * 2 + Y / 2,
+                  uz = (vz - cz / 2) * 2 + Z / 2;
+        const bool in = ux >= 0 && ux < X && uy >= 0 && uy < Y && uz >= 0 && uz < Z;
+        coarse[v] = in ? fine[(size_t)ux + (size_t)uy * X + (size_t)uz * X * Y] : 0;
+    }
+}
+
+// Seeds at (x/2, y/2, z/2); the first seed of the list that lands on a coarse voxel gives
+// it its label (first[cq] = smallest seed index).
+__global__ void pyr_coarse_first_kernel(const int32_t *__restrict__ seeds, int nseeds, int X,
+                                        int Y, int Z, int cx, int cy, int cz, unsigned *first) {
+    const size_t N = (size_t)X * Y * Z;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nseeds; i += gridDim.x * blockDim.x) {
+        const int p = seeds[i];
+        if (p < 0 || (size_t)p >= N) continue;
+        const int x = p % X, y = (p / X) % Y, z = (int)(p / ((size_t)X * Y));
+        const int qx = x / 2, qy = y / 2, qz = z / 2;
+        if (qx >= cx || qy >= cy || qz >= cz) continue;
+        atomicMin(&first[(size_t)qx + (size_t)qy * cx + (size_t)qz * cx * cy], (unsigned)i);
+    }
+}
+
+__global__ void pyr_coarse_labels_kernel(const unsigned *__restrict__ first,
+                                         const int32_t *__restrict__ seeds,
+                                         const int32_t *__restrict__ fine_label, size_t cn,
+                                         int32_t *__restrict__ clab) {
+    for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < cn;
+         v += (size_t)gridDim.x * blockDim.x) {
+        const unsigned f = first[v];
+        clab[v] = f == 0xFFFFFFFFu ? -1 : fine_label[seeds[f]];
+    }
+}
+
+// Scene32::ScaleLabel(.., none) (gft_scene32.cpp:1145-1161, 1091-1120): fine voxel u takes
+// coarse voxel (ix[x], iy[y], iz[z]); the per-axis tables are computed on the host with
+// the reference's float / double expression.
+__global__ void pyr_upscale_kernel(const int32_t *__restrict__ clab, int32_t *__restrict__ up,
+                                   int X, int Y, int Z, int cx, int cy,
+                                   const int *__restrict__ ix, const int *__restrict__ iy,
+                                   const int *__restrict__ iz) {
+    const size_t N = (size_t)X * Y * Z;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / ((size_t)X * Y));
+        up[p] = clab[(size_t)ix[x] + (size_t)iy[y] * cx + (size_t)iz[z] * cx * cy];
+    }
+}
+
+// mark_boundary_voxels_nil (exp_coarse_to_fine.cpp:216-249): a labelled voxel with a
+// neighbour of another value (NIL included) becomes NIL; out-of-volume neighbours are
+// ignored.  off: the adjacency without its centre.
+__global__ void pyr_boundary_nil_kernel(const int32_t *__restrict__ lab, int32_t *__restrict__ out,
+                                        int X, int Y, int Z, const int *__restrict__ off,
+                                        int noff) {
+    const size_t N = (size_t)X * Y * Z, XY = (size_t)X * Y;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        const int l = lab[p];
+        int o = l;
+        if (l != -1) {
+            const int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / XY);
+            for (int i = 0; i < noff; i++) {
+                const int qx = x + off[3 * i], qy = y + off[3 * i + 1], qz = z + off[3 * i + 2];
+                if (qx < 0 || qy < 0 || qz < 0 || qx >= X || qy >= Y || qz >= Z) continue;
+                if (lab[(size_t)qx + (size_t)qy * X + (size_t)qz * XY] != l) {
+                    o = -1;
+                    break;
+                }
+            }
+        }
+        out[p] = o;
+    }
+}
+
+// Fine labels before the second pass: the caller's label where set, else the upscaled
+// interior label (exp_coarse_to_fine.cpp:376-383).
+__global__ void pyr_merge_kernel(const int32_t *__restrict__ label, const int32_t *__restrict__ up,
+                                 int32_t *__restrict__ merged, size_t N) {
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < N;
+         p += (size_t)gridDim.x * blockDim.x) {
+        const int l = label[p];
+        merged[p] = (l == -1) ? up[p] : l;
+    }
+}
+
+// Every labelled voxel becomes a seed, in address order (build_seeds_from_label,
+// exp_coarse_to_fine.cpp:197-212): per-chunk counts, then an ordered scatter.
+__global__ void seeds_count_kernel(const int32_t *__restrict__ lab, size_t N, size_t chunk,
+                                   unsigned *counts) {
+    const size_t b0 = (size_t)blockIdx.x * chunk, b1 = min(N, b0 + chunk);
+    unsigned c = 0;
+    for (size_t p = b0 + threadIdx.x; p < b1; p += blockDim.x) c += lab[p] != -1;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    __shared__ unsigned ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+__global__ void seeds_scatter_kernel(const int32_t *__restrict__ lab, size_t N, size_t chunk,
+                                     const unsigned *__restrict__ base_of, int32_t *seeds,
+                                     int32_t *seed_labels) {
+    __shared__ unsigned ws[33];
+    const size_t b0 = (size_t)blockIdx.x * chunk, b1 = min(N, b0 + chunk);
+    unsigned base = base_of[blockIdx.x];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (size_t r = b0; r < b1; r += blockDim.x) {
+        const size_t p = r + threadIdx.x;
+        const int l = p < b1 ? lab[p] : -1;
+        const unsigned bal = __ballot_sync(0xffffffffu, l != -1);
+        if (lane == 0) ws[wid] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned s = 0;
+            for (int w = 0; w < nw; w++) {
+                const unsigned v = ws[w];
+                ws[w] = s;
+                s += v;
+            }
+            ws[32] = s;
+        }
+        __syncthreads();
+        if (l != -1) {
+            const unsigned pos = base + ws[wid] + __popc(bal & ((1u << lane) - 1u));
+            seeds[pos] = (int32_t)p;
+            seed_labels[pos] = l < 0 ? 0 : l;
+        }
+        base += ws[32];
+        __syncthreads();
+    }
+}
+
+}  // namespace oiftb

@@ -60,6 +60,13 @@ def make(name, shape, pol, adj, nl, per_class, seed):
         out["chain_image"] = chain_img.reshape(shape)
         out["ref_chain_label"] = O.ref_oiftrelax_chain(chain_img.reshape(shape), pol, SWEEPS,
                                                        50.0, c.seeds, chain_lab)
+    # the coarse-to-fine cascade on the twice-blurred volume (global polarity cases)
+    if pc is None and adj in (6, 26):
+        f = O.ref_gaussian_blur(O.ref_gaussian_blur(img).reshape(shape)).reshape(shape)
+        lab0 = np.full(img.size, -1, np.int32)
+        lab0[c.seeds] = c.seed_labels
+        out["c2f_image"] = f
+        out["ref_c2f_label"] = O.ref_coarse_to_fine(f, adj, pol, SWEEPS, 50.0, c.seeds, lab0)
     if pol == 0.0 and pc is None:
         cost, lab = O.ref_ift_fmax(img, adj, c.seeds, c.seed_labels)
         out["ref_ift_fmax_cost"] = cost

@@ -405,3 +405,55 @@ def test_device_path_int16_full_neighbourhood(roift, oracle_lib, adj):
     cost_r2, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
     assert np.array_equal(cost.cpu().numpy(), cost_r2)
     assert np.array_equal(lab.cpu().numpy(), lab_r2)
+
+
+# ------------------------------------------------------ coarse-to-fine cascade ----
+C2F_GOLDEN = [p for p in GOLDEN if "ref_c2f_label" in np.load(p).files]
+
+
+def _c2f_expected(img, adj, pol, K, seeds, lab0, mode="grad", oift="r2"):
+    b = np.asarray(img, np.int64)
+    b = (b - min(0, int(b.min()))).astype(np.int32)
+    f = O.gaussian_blur(O.gaussian_blur(b).reshape(img.shape)).reshape(img.shape)
+    return O.coarse_to_fine(f, adj, pol, K, 50.0, seeds, lab0, mode=mode, oift=oift)
+
+
+@pytest.mark.parametrize("path", C2F_GOLDEN, ids=[os.path.basename(p)[:-4] for p in C2F_GOLDEN])
+def test_pyramid_matches_oracle_and_reference(roift, path):
+    """run_pyramid_host == the restated cascade on the lexicographic OIFT bit for bit, and
+    == the reference experiment where OIFT_Multi's order gives the same labels."""
+    d = np.load(path)
+    img = d["image"].astype(np.int32)
+    seeds, sl = d["seeds"], d["seed_labels"]
+    adj, pol, K = int(d["adjacency"]), float(d["pol"]), int(d["sweeps"])
+    lab0 = np.full(img.size, -1, np.int32)
+    lab0[seeds] = sl
+    p = roift.make_params(img.shape, adjacency=adj, weight_mode="grad", pol=pol, sweeps=K)
+    got, st = roift._ctx().run_pyramid_host(p, img, lab0.copy(), seeds, 2, 50.0)
+    assert np.array_equal(got, _c2f_expected(img, adj, pol, K, seeds, lab0))
+    if np.array_equal(_c2f_expected(img, adj, pol, K, seeds, lab0, oift="r1"),
+                      _c2f_expected(img, adj, pol, K, seeds, lab0)):
+        assert np.array_equal(got, d["ref_c2f_label"])
+
+
+@pytest.mark.parametrize("adj,mode", [(26, "rbf_q"), (6, "grad_q")])
+def test_pyramid_device_int16(roift, adj, mode):
+    """Device flavour on an int16 volume with negative intensities, odd extents, three
+    objects and a boundary shell (the configuration of the large three-object workload
+    at a small size)."""
+    import torch
+    c = synth.three_ellipsoids(seed=7, shape=(37, 45, 51))
+    img16 = (c.image.astype(np.int32) - 300).astype(np.int16)
+    lab0 = np.full(c.n, -1, np.int32)
+    lab0[c.seeds] = c.seed_labels
+    dev = torch.device("cuda:0")
+    d_img = torch.from_numpy(img16.reshape(-1).copy()).to(dev)
+    d_lab = torch.from_numpy(lab0).to(dev)
+    d_sd = torch.from_numpy(c.seeds).to(dev)
+    out = torch.empty(c.n, dtype=torch.int32, device=dev)
+    p = roift.make_params(c.shape, adjacency=adj, weight_mode=mode, wq=4095, rbf_sigma=150.0,
+                          pol=0.2, sweeps=4)
+    roift._ctx().run_pyramid_device(p, d_img.data_ptr(), d_lab.data_ptr(), d_sd.data_ptr(),
+                                    len(c.seeds), out.data_ptr(), 2, 50.0)
+    exp = _c2f_expected(img16.astype(np.int32), adj, 0.2, 4, c.seeds, lab0, mode=mode)
+    assert np.array_equal(out.cpu().numpy(), exp)

@@ -142,3 +142,35 @@ def test_dilation_and_boundary_seeds_match_live_reference(oracle_lib, trial):
     la, sa = O.inject_boundary_seeds(lab, (Z, Y, X), stride)
     lb, sb = O.ref_inject_boundary_seeds(lab, (Z, Y, X), stride, np.zeros(0, np.int32))
     assert np.array_equal(la, lb) and np.array_equal(sa, sb)
+
+
+C2F_GOLDEN = [p for p in GOLDEN if "ref_c2f_label" in np.load(p).files]
+
+
+@pytest.mark.parametrize("path", C2F_GOLDEN, ids=[os.path.basename(p)[:-4] for p in C2F_GOLDEN])
+def test_coarse_to_fine_matches_golden(oracle_lib, path):
+    """The restated cascade (Subsampling, first-seed coarse map, coarse OIFT + relaxation,
+    nearest ScaleLabel, NIL band, merge, all-labelled fine seeds, fine OIFT + relaxation,
+    dilation) with OIFT_Multi's order reproduces the reference experiment's labels."""
+    d = np.load(path)
+    f = d["c2f_image"]
+    seeds, sl = d["seeds"], d["seed_labels"]
+    lab0 = np.full(f.size, -1, np.int32)
+    lab0[seeds] = sl
+    out = O.coarse_to_fine(f, int(d["adjacency"]), float(d["pol"]), int(d["sweeps"]), 50.0,
+                           seeds, lab0, oift="r1")
+    assert np.array_equal(out, d["ref_c2f_label"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("shape,adj,pol", [((12, 20, 26), 6, -0.3), ((11, 17, 23), 6, 0.5),
+                                           ((10, 14, 18), 26, 0.2), ((1, 40, 52), 6, 0.4)])
+def test_coarse_to_fine_matches_live_reference(oracle_lib, shape, adj, pol):
+    c = synth.small_case(seed=40 + shape[1], shape=shape, pol=pol, adjacency=adj,
+                         nlabels=2 if adj == 26 else 1, noise=120, contrast=400)
+    img = c.image.astype(np.int32)
+    f = O.gaussian_blur(O.gaussian_blur(img).reshape(shape)).reshape(shape)
+    lab = np.full(img.size, -1, np.int32)
+    lab[c.seeds] = c.seed_labels
+    ref = O.ref_coarse_to_fine(f, adj, pol, 5, 50.0, c.seeds, lab)
+    assert np.array_equal(O.coarse_to_fine(f, adj, pol, 5, 50.0, c.seeds, lab, oift="r1"), ref)
