@@ -211,6 +211,34 @@ OIFT_API int oift_b200_run_pyramid_device_i16(oift_b200_ctx *ctx, const oift_b20
                                               float percentile, int32_t *label_out,
                                               oift_b200_stats *stats);
 
+/* Gradient of a soft-Dice loss through K relaxation sweeps (config-5 style training).
+ * Forward model per updated voxel p and neighbour q:
+ *   d = beta |I_p - I_q| + (1 - beta)(g_p + g_q)/2,  w = d (1 + sign(I_p - I_q) alpha (2 m_bg(q) - 1)),
+ *   W = exp(-w^2/sigma^2)/Dpq (OIFT_ADJ_RBF) or max(0, max(I)(1 + |alpha|) - w)^8/Dpq (OIFT_ADJ_POW8),
+ *   m'(p) = sum W m(q) / sum W on the mask that grows one ring per sweep from the boundary of
+ *   the OIFT labels; seeds stay one-hot.  Loss 1 - (2 sum p t + eps)/(sum p + sum t + eps)
+ *   with p = 1 - m_bg.  The OIFT labels are held fixed; states are checkpointed every
+ *   `checkpoint` sweeps (0 = ceil(sqrt(K))) and recomputed on the way back. */
+typedef enum { OIFT_ADJ_RBF = 0, OIFT_ADJ_POW8 = 1 } oift_adjoint_kernel;
+
+typedef struct {
+    int xsize, ysize, zsize;
+    int adjacency;        /* 4, 6, 8 or 26 */
+    int sweeps;           /* K >= 1 */
+    int checkpoint;       /* 0 = ceil(sqrt(K)) */
+    int kernel;           /* oift_adjoint_kernel */
+    float sigma, alpha, beta, eps;
+} oift_b200_adjoint_params;
+
+/* Device inputs: int16 image (shifted to >= 0 for POW8), optional float gradient map,
+ * OIFT labels, seeds with their labels, uint8 truth; membership_out [classes][N] may be
+ * NULL.  loss receives L; grad (may be NULL: forward only) receives dL/d(sigma, alpha, beta). */
+OIFT_API int oift_b200_adjoint(oift_b200_ctx *ctx, const oift_b200_adjoint_params *ap,
+                               const int16_t *image, const float *grad_map,
+                               const int32_t *labels0, const int32_t *seeds,
+                               const int32_t *seed_labels, int nseeds, const uint8_t *truth,
+                               float *membership_out, double *loss, double *grad);
+
 /* Stage entry points on device pointers (used by the batched driver and tests). */
 OIFT_API int oift_b200_build_weights_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
                                 const int16_t *image, uint16_t *weights /* [planes][N] */,

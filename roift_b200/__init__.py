@@ -72,6 +72,17 @@ class Job(C.Structure):
                 ("label", C.c_void_p), ("mask", C.c_void_p), ("status", C.c_int)]
 
 
+class AdjointParams(C.Structure):
+    """oift_b200_adjoint_params."""
+    _fields_ = [("xsize", C.c_int), ("ysize", C.c_int), ("zsize", C.c_int),
+                ("adjacency", C.c_int), ("sweeps", C.c_int), ("checkpoint", C.c_int),
+                ("kernel", C.c_int), ("sigma", C.c_float), ("alpha", C.c_float),
+                ("beta", C.c_float), ("eps", C.c_float)]
+
+
+ADJ_KERNELS = {"rbf": 0, "pow8": 1}
+
+
 class BatchStats(C.Structure):
     _fields_ = [("teams", C.c_int), ("jobs", C.c_int), ("tuning", C.c_int),
                 ("ms_wall", C.c_float), ("ms_oift", C.c_float), ("ms_relax", C.c_float)]
@@ -86,7 +97,7 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_run_batch", "oift_b200_set_oift_grid", "oift_b200_gaussian_blur_i32",
            "oift_b200_conditional_dilation", "oift_b200_inject_boundary_seeds",
            "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
-           "oift_b200_run_pyramid_device_i16"]
+           "oift_b200_run_pyramid_device_i16", "oift_b200_adjoint"]
 
 _lib = None
 
@@ -135,6 +146,8 @@ def lib():
         L.oift_b200_run_cli_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
                                              C.c_int, C.c_float, C.POINTER(Stats)]
         L.oift_b200_run_pyramid_host.argtypes = L.oift_b200_run_cli_host.argtypes
+        L.oift_b200_adjoint.argtypes = [vp, C.POINTER(AdjointParams), vp, vp, vp, vp, vp, C.c_int,
+                                        vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.oift_b200_run_pyramid_device_i16.argtypes = [vp, C.POINTER(Params), vp, vp, vp, C.c_int,
                                                        C.c_int, C.c_float, vp,
                                                        C.POINTER(Stats)]
@@ -309,6 +322,28 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_run_pyramid_device_i16")
         return st
+
+    def adjoint(self, shape_zyx, image_ptr, labels0_ptr, seeds_ptr, seed_labels_ptr, nseeds,
+                truth_ptr, sigma=150.0, alpha=0.0, beta=1.0, sweeps=10, checkpoint=0,
+                kernel="rbf", adjacency=6, eps=1.0, grad_map_ptr=None, membership_ptr=None,
+                want_grad=True):
+        """Soft-Dice loss after `sweeps` relaxation sweeps and its gradient with respect to
+        (sigma, alpha, beta).  Returns (loss, np.array([dL/dsigma, dL/dalpha, dL/dbeta]))."""
+        Z, Y, X = shape_zyx
+        ap = AdjointParams(X, Y, Z, adjacency, int(sweeps), int(checkpoint), ADJ_KERNELS[kernel],
+                           float(sigma), float(alpha), float(beta), float(eps))
+        loss = C.c_double(0.0)
+        g = (C.c_double * 3)()
+        rc = lib().oift_b200_adjoint(self._h, C.byref(ap), C.c_void_p(image_ptr),
+                                     C.c_void_p(grad_map_ptr) if grad_map_ptr else None,
+                                     C.c_void_p(labels0_ptr), C.c_void_p(seeds_ptr),
+                                     C.c_void_p(seed_labels_ptr), int(nseeds),
+                                     C.c_void_p(truth_ptr),
+                                     C.c_void_p(membership_ptr) if membership_ptr else None,
+                                     C.byref(loss), g if want_grad else None)
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_adjoint")
+        return loss.value, np.array(list(g))
 
     def level_profile(self, cap=8192):
         """(cycles, tile activations) per OIFT level of the last run."""

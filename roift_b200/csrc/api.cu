@@ -44,6 +44,8 @@ struct oift_b200_ctx {
     // coarse-to-fine cascade: coarse image / labels / seeds, first-seed map, upscaled and
     // merged labels, fine seeds, axis tables and chunk counts
     DevBuf yimg, ylab, yseeds, yslab, yfirst, yup, ymerge, yfseeds, yfslab, yaux;
+    // adjoint: checkpoints / segment / lambdas / weight sums, mask rings, seed classes, sums
+    DevBuf awork, adist, aseedc, asmall, al2c;
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -140,7 +142,8 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->bmbox, &c->bglob, &c->bctl, &c->bolab, &c->cimg0, &c->cimg1,
                       &c->dborder, &c->dhist, &c->daux, &c->dlabel, &c->yimg, &c->ylab,
                       &c->yseeds, &c->yslab, &c->yfirst, &c->yup, &c->ymerge, &c->yfseeds,
-                      &c->yfslab, &c->yaux};
+                      &c->yfslab, &c->yaux, &c->awork, &c->adist, &c->aseedc, &c->asmall,
+                      &c->al2c};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -1129,6 +1132,96 @@ int oift_b200_run_cli_host(oift_b200_ctx *c, const oift_b200_params *p, const in
     CU(cudaMemcpyAsync(label, c->dlabel.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     return OIFT_OK;
+}
+
+int oift_b200_adjoint(oift_b200_ctx *c, const oift_b200_adjoint_params *ap, const int16_t *image,
+                      const float *grad_map, const int32_t *labels0, const int32_t *seeds,
+                      const int32_t *seed_labels, int nseeds, const uint8_t *truth,
+                      float *membership_out, double *loss, double *grad) {
+    if (!c || !ap || !image || !labels0 || !truth || !loss || (nseeds > 0 && (!seeds || !seed_labels)))
+        return OIFT_E_BAD_ARG;
+    const int X = ap->xsize, Y = ap->ysize, Z = ap->zsize;
+    if (X <= 0 || Y <= 0 || Z <= 0 || ap->sweeps < 1 || ap->sweeps > 60000 || ap->checkpoint < 0)
+        return OIFT_E_BAD_ARG;
+    if (ap->adjacency == 4 || ap->adjacency == 8) {
+        if (Z != 1) return OIFT_E_BAD_ARG;
+    } else if (ap->adjacency != 6 && ap->adjacency != 26) {
+        return OIFT_E_BAD_ARG;
+    }
+    if (ap->kernel != OIFT_ADJ_RBF && ap->kernel != OIFT_ADJ_POW8) return OIFT_E_BAD_ARG;
+    if (ap->kernel == OIFT_ADJ_RBF && !(ap->sigma > 0.0f)) return OIFT_E_BAD_ARG;
+    if (!(std::fabs(ap->alpha) <= 1.0f) || !(ap->beta >= 0.0f && ap->beta <= 1.0f) || !(ap->eps >= 0.0f))
+        return OIFT_E_BAD_ARG;
+    if (nseeds <= 0) return OIFT_E_NO_SEEDS;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    const size_t N = (size_t)X * Y * Z;
+    const int K = ap->sweeps;
+    int cp = ap->checkpoint;
+    if (cp == 0) cp = (int)std::ceil(std::sqrt((double)K));
+    if (cp > K) cp = K;
+    // ---- classes: 0 and the seed labels (gft_ift.cpp:8684-8712) ----
+    TRY(grow(c, c->presence, 1024 * sizeof(uint32_t)));
+    CU(cudaMemsetAsync(c->presence.p, 0, 1024 * sizeof(uint32_t), s));
+    seed_presence_kernel<<<std::min((nseeds + 255) / 256, c->sms * 4), 256, 0, s>>>(
+        seed_labels, nseeds, (uint32_t *)c->presence.p);
+    std::vector<uint32_t> bits(1024);
+    CU(cudaMemcpyAsync(bits.data(), c->presence.p, 1024 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
+    int *d_mm = (int *)c->minmax.p;
+    const int mm_init[2] = {0x7fffffff, (int)0x80000000};
+    CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+    CU(launch_minmax<int16_t>(image, N, d_mm, c->sms, s));
+    int hmm[2];
+    CU(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    bits[0] |= 1u;
+    std::vector<int> classes;
+    for (int l = 0; l <= OIFT_MAX_LABEL; l++)
+        if ((bits[l >> 5] >> (l & 31)) & 1u) classes.push_back(l);
+    const int C = (int)classes.size();
+    if (C > 8) return OIFT_E_UNSUPPORTED;
+    const int maxl = classes.back();
+    std::vector<int> l2c(maxl + 1, -1);
+    for (int k = 0; k < C; k++) l2c[classes[k]] = k;
+    const int bg = l2c[0];
+    TRY(grow(c, c->al2c, (maxl + 1) * sizeof(int)));
+    TRY(grow(c, c->aseedc, N));
+    TRY(grow(c, c->adist, N * sizeof(uint16_t)));
+    TRY(grow(c, c->asmall, 8 * sizeof(double)));
+    const size_t wf = adjoint_work_floats(N, C, K, cp);
+    TRY(grow(c, c->awork, wf * sizeof(float)));
+    CU(cudaMemcpyAsync(c->al2c.p, l2c.data(), (maxl + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(c->aseedc.p, 0xFF, N, s));
+    relax_seed_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(seeds, nseeds, labels0, N,
+                                                           (const int *)c->al2c.p, maxl, bg,
+                                                           (uint8_t *)c->aseedc.p);
+    CU(cudaGetLastError());
+    AdjointJob J{};
+    J.X = X;
+    J.Y = Y;
+    J.Z = Z;
+    J.adjacency = ap->adjacency;
+    J.sweeps = K;
+    J.checkpoint = cp;
+    J.C = C;
+    J.bg = bg;
+    J.kernel = ap->kernel;
+    J.sigma = ap->sigma;
+    J.alpha = ap->alpha;
+    J.beta = ap->beta;
+    J.eps = ap->eps;
+    J.imax = hmm[1];
+    J.img = image;
+    J.g = grad_map;
+    J.dist = (uint16_t *)c->adist.p;
+    J.seedc = (const uint8_t *)c->aseedc.p;
+    J.labels0 = labels0;
+    J.l2c = (const int *)c->al2c.p;
+    J.maxl = maxl;
+    J.truth = truth;
+    J.membership_out = membership_out;
+    return adjoint_run(J, s, c->sms, (float *)c->awork.p, wf, c->asmall.p, loss, grad);
 }
 
 int oift_b200_run_pyramid_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *image,

@@ -182,6 +182,29 @@ __global__ void seeds_scatter_kernel(const int32_t *lab, size_t N, size_t chunk,
                                      const unsigned *base_of, int32_t *seeds,
                                      int32_t *seed_labels);
 
+// ---- adjoint of the relaxation (adjoint.cu) ----
+struct AdjointJob {
+    int X, Y, Z, adjacency;
+    int sweeps, checkpoint;   // K, sweeps between stored states (>= 1)
+    int C, bg;                // classes, background class
+    int kernel;               // 0 RBF, 1 POW8
+    float sigma, alpha, beta;
+    double eps;               // soft-Dice smoothing
+    int imax;                 // max of the image (POW8 Wmax)
+    const int16_t *img;
+    const float *g;           // gradient map for the blend (may be null)
+    uint16_t *dist;           // [N] scratch: sweep at which a voxel joins the mask
+    const uint8_t *seedc;     // [N] seed class or 0xFF
+    const int32_t *labels0;   // [N] OIFT labels
+    const int *l2c;           // label -> class (-1 if none), labels 0..maxl
+    int maxl;
+    const uint8_t *truth;     // [N] 0 / 1
+    float *membership_out;    // [C][N] final membership, may be null
+};
+size_t adjoint_work_floats(size_t N, int C, int K, int c);
+int adjoint_run(const AdjointJob &J, cudaStream_t s, int sms, float *work, size_t work_floats,
+                void *small, double *loss_out, double *grad_out);
+
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,

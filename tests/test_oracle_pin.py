@@ -174,3 +174,30 @@ def test_coarse_to_fine_matches_live_reference(oracle_lib, shape, adj, pol):
     lab[c.seeds] = c.seed_labels
     ref = O.ref_coarse_to_fine(f, adj, pol, 5, 50.0, c.seeds, lab)
     assert np.array_equal(O.coarse_to_fine(f, adj, pol, 5, 50.0, c.seeds, lab, oift="r1"), ref)
+
+
+@pytest.mark.parametrize("kernel,adj", [("rbf", 6), ("pow8", 6), ("rbf", 26)])
+def test_fp64_adjoint_matches_central_differences(kernel, adj):
+    """The FP64 reverse-mode gradient of the relaxation (the checker of the CUDA adjoint)
+    equals central differences of its own FP64 forward."""
+    from oracle import adjoint as A
+    rng = np.random.default_rng(0)
+    Z, Y, X = 6, 9, 11
+    img = rng.integers(0, 400, size=(Z, Y, X)).astype(float)
+    img[2:5, 3:7, 3:9] += 600
+    lab = np.zeros(Z * Y * X, np.int64)
+    lab.reshape(Z, Y, X)[2:5, 3:7, 3:9] = 1
+    seeds = np.array([0, 1, 2, np.ravel_multi_index((3, 5, 5), (Z, Y, X))])
+    sl = np.array([0, 0, 0, 1])
+    truth = lab.copy()
+    truth.reshape(Z, Y, X)[2, 3, 3] = 0
+    g = rng.integers(0, 300, size=(Z, Y, X)).astype(float)
+    P = A.Problem(img, lab, seeds, sl, truth, adj=adj, grad=g, K=6, kernel=kernel)
+    th = np.array([150.0, 0.3, 0.7])
+    _, gr = P.gradient(*th)
+    for i, h in enumerate([1e-3 * th[0], 1e-5, 1e-5]):
+        tp, tm = th.copy(), th.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (P.forward(*tp)[0] - P.forward(*tm)[0]) / (2 * h)
+        assert abs(gr[i] - fd) <= 1e-6 * max(abs(fd), 1e-9), (i, gr[i], fd)
