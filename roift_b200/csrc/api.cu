@@ -241,26 +241,21 @@ struct RelaxResult {
     int dilations = 0;
 };
 
-// Relaxation of one job on the context's stream: classes from the seed labels, one-hot
-// start from the OIFT labels d_olab, K tile sweeps, argmax into out->label / out->mask (and
-// the membership copy).  hmm = intensity min / max of the image.  d_olab is not read after
-// the argmax kernel starts, so it may alias out->label.
-template <typename T>
-static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_img,
-                       const int32_t *d_seeds, const int32_t *d_slabels, int nseeds,
-                       const int32_t *d_olab, const int hmm[2], const oift_b200_outputs *out,
-                       RelaxResult *rr) {
+// Class set and sweep constants of one relaxation: classes = 0 and the labels present among
+// the seeds (gft_ift.cpp:8684-8712, read back to the host); Wmax (8733-8734) from hmm.
+struct RelaxPlan {
+    int nclasses = 0, maxl = 0, bg = 0;
+    std::vector<int> classes, l2c;
+    RelaxArgs ra;
+};
+
+static int relax_plan(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *d_slabels,
+                      int nseeds, const int hmm[2], RelaxPlan *pl) {
     cudaStream_t s = c->stream;
     const int X = p->xsize, Y = p->ysize, Z = p->zsize;
     const size_t N = (size_t)X * Y * Z;
     Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
-    const int K = p->relax_sweeps;
     TRY(grow(c, c->presence, 1024 * sizeof(uint32_t)));
-    std::vector<int> classes;
-    int nclasses = 0;
-    long long relax_active = 0;
-    int relax_dilations = 0;
-    // classes = labels present among seeds, plus 0 (gft_ift.cpp:8684-8712)
     CU(cudaMemsetAsync(c->presence.p, 0, 1024 * sizeof(uint32_t), s));
     if (nseeds > 0)
         seed_presence_kernel<<<std::min((nseeds + 255) / 256, c->sms * 4), 256, 0, s>>>(
@@ -270,20 +265,22 @@ static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_i
                        cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     bits[0] |= 1u;
+    pl->classes.clear();
     for (int l = 0; l <= OIFT_MAX_LABEL; l++)
-        if ((bits[l >> 5] >> (l & 31)) & 1u) classes.push_back(l);
-    nclasses = (int)classes.size();
+        if ((bits[l >> 5] >> (l & 31)) & 1u) pl->classes.push_back(l);
+    const int nclasses = (int)pl->classes.size();
     if (nclasses > 8) return OIFT_E_UNSUPPORTED;
-    int maxl = classes.back();
-    std::vector<int> l2c(maxl + 1, -1);
-    for (int k = 0; k < nclasses; k++) l2c[classes[k]] = k;
-    int bg = l2c[0] < 0 ? 0 : l2c[0];
+    pl->nclasses = nclasses;
+    pl->maxl = pl->classes.back();
+    pl->l2c.assign(pl->maxl + 1, -1);
+    for (int k = 0; k < nclasses; k++) pl->l2c[pl->classes[k]] = k;
+    pl->bg = pl->l2c[0] < 0 ? 0 : pl->l2c[0];
     // Wmax (gft_ift.cpp:8733-8734) on the image shifted to >= 0 as the CLI does
     float max_abs_per = 0.0f;
     std::vector<float> pcm(nclasses, 0.0f);
     if (p->per_class) {
         for (int k = 0; k < nclasses; k++) {
-            float v = (classes[k] <= p->max_label) ? p->per_class[classes[k]] : 0.0f;
+            float v = (pl->classes[k] <= p->max_label) ? p->per_class[pl->classes[k]] : 0.0f;
             pcm[k] = v;
             if (std::fabs(v) > max_abs_per) max_abs_per = std::fabs(v);
         }
@@ -297,7 +294,7 @@ static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_i
     double deg = (p->adjacency == 26) ? 26 : (p->adjacency == 8 ? 8 : (p->adjacency == 6 ? 6 : 4));
     if ((double)Wmax > std::pow(3.0e38 / deg, 0.125)) return OIFT_E_RANGE;
 
-    RelaxArgs ra;
+    RelaxArgs &ra = pl->ra;
     ra.X = X;
     ra.Y = Y;
     ra.Z = Z;
@@ -314,73 +311,116 @@ static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_i
     }
     ra.Wmax = Wmax;
     ra.per = p->per;
-    ra.bg = bg;
+    ra.bg = pl->bg;
     for (int k = 0; k < 8; k++) ra.pcm[k] = k < nclasses ? pcm[k] : 0.0f;
+    return OIFT_OK;
+}
 
-    TRY(grow(c, c->memb, 2 * (size_t)nclasses * N * sizeof(float)));
+// Scratch a relaxation of N voxels with C classes and K sweeps needs in the context.
+static int relax_reserve(oift_b200_ctx *c, size_t N, int C, int maxl, int X, int Y, int Z, int K) {
+    TRY(grow(c, c->memb, 2 * (size_t)C * N * sizeof(float)));
     TRY(grow(c, c->seedc, N));
     TRY(grow(c, c->l2c, (maxl + 1) * sizeof(int)));
-    TRY(grow(c, c->classes, nclasses * sizeof(int)));
-    CU(cudaMemcpyAsync(c->l2c.p, l2c.data(), (maxl + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(c->classes.p, classes.data(), nclasses * sizeof(int), cudaMemcpyHostToDevice, s));
+    TRY(grow(c, c->classes, C * sizeof(int)));
+    const size_t rnt = (size_t)((X + 31) / 32) * ((Y + 7) / 8) * ((Z + 3) / 4);
+    TRY(grow(c, c->rtdist, 2 * rnt * sizeof(uint16_t) + (size_t)(K + 1) * sizeof(unsigned)));
+    return OIFT_OK;
+}
+
+// The sweeps of one planned relaxation: kernel launches and device-side memsets only (the
+// context's scratch must already be reserved), so the sequence can also be captured in a
+// CUDA graph.  With `active` non-null the sweep histogram is read back (a host sync) to
+// count the voxel-sweeps computed, and the sweep loop is bracketed by the context's events.
+template <typename T>
+static int relax_launch(oift_b200_ctx *c, const oift_b200_params *p, const T *d_img,
+                        const int32_t *d_seeds, int nseeds, const int32_t *d_olab,
+                        const RelaxPlan &pl, const int *d_l2c, const int *d_classes,
+                        const oift_b200_outputs *out, long long *active) {
+    cudaStream_t s = c->stream;
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    const size_t N = (size_t)X * Y * Z;
+    const int K = p->relax_sweeps;
+    const int nclasses = pl.nclasses, maxl = pl.maxl, bg = pl.bg;
+    const RelaxArgs &ra = pl.ra;
+    TRY(relax_reserve(c, N, nclasses, maxl, X, Y, Z, K));
     float *m0 = (float *)c->memb.p, *m1 = m0 + (size_t)nclasses * N;
     int blocks = (int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16);
     // both ping-pong buffers start one-hot: tiles skipped at a sweep keep that value
-    relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m0);
-    relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, (const int *)c->l2c.p, maxl, bg, m1);
+    relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, d_l2c, maxl, bg, m0);
+    relax_init_kernel<<<blocks, 256, 0, s>>>(d_olab, N, nclasses, d_l2c, maxl, bg, m1);
     CU(cudaMemsetAsync(c->seedc.p, 0xFF, N, s));
     if (nseeds > 0)
         relax_seed_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(d_seeds, nseeds, d_olab, N,
-                                                               (const int *)c->l2c.p, maxl, bg,
+                                                               d_l2c, maxl, bg,
                                                                (uint8_t *)c->seedc.p);
     // block distance of every relaxation tile to the label boundary (exact skipping)
     const int rtx = (X + 31) / 32, rty = (Y + 7) / 8, rtz = (Z + 3) / 4;
     const int rnt = rtx * rty * rtz;
-    TRY(grow(c, c->rtdist, 2 * (size_t)rnt * sizeof(uint16_t) + (size_t)(K + 1) * sizeof(unsigned)));
     uint16_t *td0 = (uint16_t *)c->rtdist.p, *td1 = td0 + rnt;
     unsigned *hist = (unsigned *)(td1 + rnt);  // byte offset 4 * rnt
     CU(cudaMemsetAsync(td0, 0xFF, 2 * (size_t)rnt * sizeof(uint16_t), s));
     relax_boundary_tiles_kernel<<<dim3((X + 31) / 32, (Y + 7) / 8, Z), dim3(32, 8), 0, s>>>(
-        d_olab, X, Y, Z, adj.n, ra, td0, rtx, rty);
-    const int cheb = (adj.n == 26);
+        d_olab, X, Y, Z, ra.nadj, ra, td0, rtx, rty);
+    const int cheb = (ra.nadj == 26);
     // exact lower bound of the voxel distance to the mask: three separable passes
     relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 0, 32, cheb);
     relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td1, td0, rtx, rty, rtz, 1, 8, cheb);
     relax_tile_gap_pass_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, td1, rtx, rty, rtz, 2, 4, cheb);
     std::swap(td0, td1);
-    long long active_vs = 0;
-    if (K > 0) {
+    if (K > 0 && active) {
         CU(cudaMemsetAsync(hist, 0, (size_t)(K + 1) * sizeof(unsigned), s));
         relax_tile_hist_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, rnt, K, hist);
     }
     float *cur = m0, *nxt = m1;
-    cudaEventRecord(c->ev[6], s);
+    if (active) cudaEventRecord(c->ev[6], s);
     for (int it = 0; it < K; it++) {
         CU(launch_relax_tiles<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, td0,
                                  it + 1, ra, p->per_class != nullptr, rnt, rtx, rty, s));
         std::swap(cur, nxt);
     }
-    if (K > 0) {
+    if (K > 0 && active) {
         std::vector<unsigned> h(K);
         CU(cudaMemcpyAsync(h.data(), hist, K * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
-        long long run = 0;
+        long long run = 0, active_vs = 0;
         for (int t = 1; t <= K; t++) {  // tiles with distance <= t-1 run at sweep t
             run += h[t - 1];
             active_vs += run * 1024;
         }
+        *active = active_vs;
     }
-    relax_active = active_vs;
-    relax_dilations = 3;
-    cudaEventRecord(c->ev[7], s);
-    relax_argmax_kernel<<<(int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16), 256, 0, s>>>(cur, N, nclasses, (const int *)c->classes.p,
-                                               out->label, out->mask);
+    if (active) cudaEventRecord(c->ev[7], s);
+    relax_argmax_kernel<<<(int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16), 256, 0, s>>>(
+        cur, N, nclasses, d_classes, out->label, out->mask);
     if (out->membership)
         CU(cudaMemcpyAsync(out->membership, cur, (size_t)nclasses * N * sizeof(float),
                            cudaMemcpyDeviceToDevice, s));
-    rr->nclasses = nclasses;
-    rr->active_voxel_sweeps = relax_active;
-    rr->dilations = relax_dilations;
+    return OIFT_OK;
+}
+
+// Relaxation of one job on the context's stream: classes from the seed labels, one-hot
+// start from the OIFT labels d_olab, K tile sweeps, argmax into out->label / out->mask (and
+// the membership copy).  hmm = intensity min / max of the image.  d_olab is not read after
+// the argmax kernel starts, so it may alias out->label.
+template <typename T>
+static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_img,
+                       const int32_t *d_seeds, const int32_t *d_slabels, int nseeds,
+                       const int32_t *d_olab, const int hmm[2], const oift_b200_outputs *out,
+                       RelaxResult *rr) {
+    RelaxPlan pl;
+    TRY(relax_plan(c, p, d_slabels, nseeds, hmm, &pl));
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    TRY(relax_reserve(c, (size_t)X * Y * Z, pl.nclasses, pl.maxl, X, Y, Z, p->relax_sweeps));
+    CU(cudaMemcpyAsync(c->l2c.p, pl.l2c.data(), (pl.maxl + 1) * sizeof(int),
+                       cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(c->classes.p, pl.classes.data(), pl.nclasses * sizeof(int),
+                       cudaMemcpyHostToDevice, c->stream));
+    long long act = 0;
+    TRY(relax_launch<T>(c, p, d_img, d_seeds, nseeds, d_olab, pl, (const int *)c->l2c.p,
+                        (const int *)c->classes.p, out, &act));
+    rr->nclasses = pl.nclasses;
+    rr->active_voxel_sweeps = act;
+    rr->dilations = 3;
     return OIFT_OK;
 }
 
@@ -1308,11 +1348,31 @@ struct BatchTimes {
     double wall_ms = 0, oift_ms = 0, relax_ms = 0;
 };
 
-static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
-                           oift_b200_job *jobs, int first, int count, int teams,
-                           BatchTimes *bt) {
-    using clk = std::chrono::steady_clock;
-    const auto t0 = clk::now();
+struct BatchImg {
+    const int16_t *p;
+    int X, Y, Z;
+    size_t woff;  // element offset of its edge codes in c->W
+};
+
+// Everything of a batched call that needs the host: per-job checks, distinct images and
+// their intensity ranges, the RBF table, the weight builds to launch, job descriptors
+// (uploaded), per-team scratch.  Jobs that fail a check get their status here.
+struct BatchPrep {
+    std::vector<BatchImg> imgs;
+    std::vector<int> job_img;  // per job (from `first`): its image, -1 if the job failed a check
+    std::vector<int> hmm;      // intensity min / max per image
+    std::vector<BuildArgs> builds;
+    std::vector<int> order;    // launch slot -> job index
+    std::vector<int32_t *> olab;
+    std::vector<OiftTeamJob> dj;
+    int nj = 0, n3d = 0, nimg = 0;
+    OiftTeamScratch S;
+    OiftTeamJob *d_jobs = nullptr;
+    unsigned long long *d_clamp = nullptr;
+};
+
+static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_b200_job *jobs,
+                         int first, int count, int teams, BatchPrep *bp) {
     cudaStream_t s = c->stream;
     const int end = first + count;
     if (teams < 1 || teams > c->sms) return OIFT_E_BAD_ARG;
@@ -1321,13 +1381,9 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     const int ctas_lo = c->sms / teams, ctas_hi = (c->sms + teams - 1) / teams;
 
     // ---- per-job checks; distinct images (pointer + extents) ----
-    struct Img {
-        const int16_t *p;
-        int X, Y, Z;
-        size_t woff;  // element offset of its edge codes in c->W
-    };
-    std::vector<Img> imgs;
-    std::vector<int> job_img(count, -1);
+    std::vector<BatchImg> &imgs = bp->imgs;
+    std::vector<int> &job_img = bp->job_img;
+    job_img.assign(count, -1);
     size_t wtotal = 0;
     for (int j = first; j < end; j++) {
         oift_b200_job &jb = jobs[j];
@@ -1359,11 +1415,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
         job_img[j - first] = k;
     }
     const int nimg = (int)imgs.size();
-    if (nimg == 0) {
-        for (int j = first; j < end; j++)
-            if (jobs[j].status != OIFT_OK) return jobs[j].status;
-        return OIFT_OK;
-    }
+    bp->nimg = nimg;
+    if (nimg == 0) return OIFT_OK;
 
     // ---- intensity range and edge codes, once per image ----
     TRY(grow(c, c->W, wtotal * sizeof(uint16_t)));
@@ -1380,12 +1433,12 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
                            cudaMemcpyHostToDevice, s));
         CU(cudaMemsetAsync(d_clamp, 0, (size_t)nimg * sizeof(unsigned long long), s));
     }
-    cudaEventRecord(c->ev[0], s);
     for (int i = 0; i < nimg; i++) {
         const size_t n = (size_t)imgs[i].X * imgs[i].Y * imgs[i].Z;
         CU(launch_minmax<int16_t>(imgs[i].p, n, d_mm + 2 * i, c->sms, s));
     }
-    std::vector<int> hmm(2 * (size_t)nimg);
+    std::vector<int> &hmm = bp->hmm;
+    hmm.assign(2 * (size_t)nimg, 0);
     CU(cudaMemcpyAsync(hmm.data(), d_mm, hmm.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     const uint16_t *lut = nullptr;
@@ -1426,12 +1479,13 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
         ba.grad = nullptr;
         ba.blend_a = common->blend_a;
         ba.clamped = d_clamp + i;
-        CU(launch_build_weights<int16_t>(imgs[i].p, (uint16_t *)c->W.p + imgs[i].woff, ba,
-                                         c->sms, s));
+        bp->builds.push_back(ba);
     }
+    bp->d_clamp = d_clamp;
 
     // ---- job descriptors: 3D jobs then 2D jobs, each group largest volume first ----
-    std::vector<int> order;
+    std::vector<int> &order = bp->order;
+    order.clear();
     for (int j = first; j < end; j++)
         if (jobs[j].status == OIFT_OK) order.push_back(j);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -1441,7 +1495,9 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
                (size_t)jobs[b].xsize * jobs[b].ysize * jobs[b].zsize;
     });
     const int nj = (int)order.size();
-    std::vector<OiftTeamJob> dj(nj);
+    bp->nj = nj;
+    std::vector<OiftTeamJob> &dj = bp->dj;
+    dj.assign(nj, OiftTeamJob{});
     size_t max_n = 0, max_tiles = 0, max_mbox = 0, olab_total = 0;
     std::vector<size_t> olab_off(nj, (size_t)-1);
     for (int i = 0; i < nj; i++) {
@@ -1455,7 +1511,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
         }
     }
     if (olab_total) TRY(grow(c, c->bolab, olab_total * sizeof(int32_t)));
-    std::vector<int32_t *> olab(nj, nullptr);
+    std::vector<int32_t *> &olab = bp->olab;
+    olab.assign(nj, nullptr);
     int n3d = 0;
     for (int i = 0; i < nj; i++) {
         const oift_b200_job &jb = jobs[order[i]];
@@ -1488,7 +1545,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
                                           sizeof(unsigned long long));
         if (jb.zsize > 1) n3d++;
     }
-    OiftTeamScratch S;
+    bp->n3d = n3d;
+    OiftTeamScratch &S = bp->S;
     S.key_stride = align_up(max_n, 64);
     S.tpend_stride = align_up(max_tiles, 64);
     S.mbox_stride = align_up(max_mbox, 32);
@@ -1505,11 +1563,54 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     S.next_job = (unsigned int *)c->bctl.p;
     S.abort = (int *)c->bctl.p + 1;
     OiftTeamJob *d_jobs = (OiftTeamJob *)c->bjobs.p;
+    bp->d_jobs = d_jobs;
     CU(cudaMemcpyAsync(d_jobs, dj.data(), (size_t)nj * sizeof(OiftTeamJob), cudaMemcpyHostToDevice, s));
+    return OIFT_OK;
+}
 
-    // ---- the OIFT of every job: one team launch per group ----
-    if (n3d > 0) TRY(oift_team_run(d_jobs, n3d, false, teams, c->sms, S, s));
-    if (nj - n3d > 0) TRY(oift_team_run(d_jobs + n3d, nj - n3d, true, teams, c->sms, S, s));
+// The device work of the batched OIFT: weight builds, optionally the descriptors restored
+// from a pristine copy, one team launch per group.  Launches and device-side copies only,
+// so a stream capture can record it.
+static int batch_enqueue_oift(oift_b200_ctx *c, const BatchPrep &bp, int teams,
+                              const OiftTeamJob *d_pristine) {
+    cudaStream_t s = c->stream;
+    CU(cudaMemsetAsync(bp.d_clamp, 0, (size_t)bp.nimg * sizeof(unsigned long long), s));
+    for (int i = 0; i < bp.nimg; i++)
+        CU(launch_build_weights<int16_t>(bp.imgs[i].p, (uint16_t *)c->W.p + bp.imgs[i].woff,
+                                         bp.builds[i], c->sms, s));
+    if (d_pristine)
+        CU(cudaMemcpyAsync(bp.d_jobs, d_pristine, (size_t)bp.nj * sizeof(OiftTeamJob),
+                           cudaMemcpyDeviceToDevice, s));
+    if (bp.n3d > 0) TRY(oift_team_run(bp.d_jobs, bp.n3d, false, teams, c->sms, bp.S, s));
+    if (bp.nj - bp.n3d > 0)
+        TRY(oift_team_run(bp.d_jobs + bp.n3d, bp.nj - bp.n3d, true, teams, c->sms, bp.S, s));
+    return OIFT_OK;
+}
+
+static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
+                           oift_b200_job *jobs, int first, int count, int teams,
+                           BatchTimes *bt) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    cudaStream_t s = c->stream;
+    const int end = first + count;
+
+    BatchPrep bp;
+    TRY(batch_prepare(c, common, jobs, first, count, teams, &bp));
+    const int nimg = bp.nimg, nj = bp.nj;
+    if (nimg == 0) {
+        for (int j = first; j < end; j++)
+            if (jobs[j].status != OIFT_OK) return jobs[j].status;
+        return OIFT_OK;
+    }
+    const std::vector<int> &order = bp.order, &job_img = bp.job_img, &hmm = bp.hmm;
+    const std::vector<int32_t *> &olab = bp.olab;
+    std::vector<OiftTeamJob> &dj = bp.dj;
+    OiftTeamJob *d_jobs = bp.d_jobs;
+    unsigned long long *d_clamp = bp.d_clamp;
+    cudaEventRecord(c->ev[0], s);
+    // ---- the OIFT of every job: weight builds, one team launch per group ----
+    TRY(batch_enqueue_oift(c, bp, teams, nullptr));
     cudaEventRecord(c->ev[1], s);
     std::vector<unsigned long long> hclamp(nimg);
     CU(cudaMemcpyAsync(dj.data(), d_jobs, (size_t)nj * sizeof(OiftTeamJob), cudaMemcpyDeviceToHost, s));
@@ -1576,6 +1677,178 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     }
     for (int j = first; j < end; j++)
         if (jobs[j].status != OIFT_OK) return jobs[j].status;
+    return OIFT_OK;
+}
+
+// ------------------------------------------------------------ batch as a CUDA graph ----
+// A batch recorded once and replayed: the weight builds, the descriptor reset, the team
+// launches and every job's relaxation sweeps are captured from a private context (its
+// scratch cannot be reallocated by other calls), so a replay is one graph launch.  What the
+// host had to read to plan the batch -- job checks, intensity ranges (relaxation Wmax, RBF
+// table), each job's class set -- is fixed at recording: a replay is valid while the jobs'
+// buffers stay where they are, the images keep their intensity range and the seeds their
+// label set.
+struct oift_b200_batch_graph {
+    oift_b200_ctx *c = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BatchPrep bp;
+    int njobs = 0, weight_mode = 0, teams = 0;
+    void *pristine = nullptr;  // descriptors as uploaded
+    void *plans = nullptr;     // packed label -> class maps and class lists of the jobs
+};
+
+static void batch_graph_free(oift_b200_batch_graph *g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->pristine) cudaFree(g->pristine);
+    if (g->plans) cudaFree(g->plans);
+    if (g->c) oift_b200_destroy(g->c);
+    delete g;
+}
+
+int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_params *common,
+                                 oift_b200_job *jobs, int njobs, int teams,
+                                 oift_b200_batch_graph **out) {
+    if (!ctx || !common || !jobs || !out || njobs <= 0 || teams < 0 || teams > ctx->sms)
+        return OIFT_E_BAD_ARG;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    if (teams == 0) {
+        // the context's autotuned choice when it has one, else half the SMs
+        double best = -1.0;
+        teams = ctx->sms / 2;
+        for (auto &tc : ctx->tune_cands)
+            if (tc.second > best) {
+                best = tc.second;
+                teams = tc.first;
+            }
+    }
+    teams = std::max(1, std::min(teams, njobs));
+    oift_b200_batch_graph *g = new oift_b200_batch_graph();
+    g->njobs = njobs;
+    g->weight_mode = common->weight_mode;
+    g->teams = teams;
+    int rc = oift_b200_create(&g->c, ctx->device);
+    if (rc != OIFT_OK) {
+        batch_graph_free(g);
+        return rc;
+    }
+    oift_b200_ctx *c = g->c;
+    cudaStream_t s = c->stream;
+    BatchPrep &bp = g->bp;
+    rc = batch_prepare(c, common, jobs, 0, njobs, teams, &bp);
+    for (int j = 0; rc == OIFT_OK && j < njobs; j++)
+        if (jobs[j].status != OIFT_OK) rc = jobs[j].status;
+    if (rc == OIFT_OK && bp.nj == 0) rc = OIFT_E_BAD_ARG;
+    const size_t dbytes = (size_t)bp.nj * sizeof(OiftTeamJob);
+    if (rc == OIFT_OK && (cudaMalloc(&g->pristine, dbytes) != cudaSuccess ||
+                          cudaMemcpyAsync(g->pristine, bp.d_jobs, dbytes, cudaMemcpyDeviceToDevice,
+                                          s) != cudaSuccess)) {
+        cudaGetLastError();
+        rc = OIFT_E_CUDA;
+    }
+    // ---- relaxation plans (host reads) and the largest scratch any job needs ----
+    std::vector<RelaxPlan> plans(bp.nj);
+    std::vector<oift_b200_params> prm(bp.nj);
+    std::vector<size_t> off(bp.nj, 0);
+    std::vector<int> packed;
+    for (int i = 0; rc == OIFT_OK && i < bp.nj; i++) {
+        const oift_b200_job &jb = jobs[bp.order[i]];
+        if (!jb.label && !jb.mask) continue;
+        oift_b200_params &p = prm[i];
+        p = *common;
+        p.xsize = jb.xsize;
+        p.ysize = jb.ysize;
+        p.zsize = jb.zsize;
+        p.per = jb.per;
+        p.per_class = nullptr;
+        p.max_label = 0;
+        rc = relax_plan(c, &p, jb.seed_labels, jb.nseeds, &bp.hmm[2 * bp.job_img[bp.order[i]]],
+                        &plans[i]);
+        if (rc != OIFT_OK) break;
+        rc = relax_reserve(c, (size_t)jb.xsize * jb.ysize * jb.zsize, plans[i].nclasses,
+                           plans[i].maxl, jb.xsize, jb.ysize, jb.zsize, p.relax_sweeps);
+        off[i] = packed.size();
+        packed.insert(packed.end(), plans[i].l2c.begin(), plans[i].l2c.end());
+        packed.insert(packed.end(), plans[i].classes.begin(), plans[i].classes.end());
+    }
+    if (rc == OIFT_OK && !packed.empty() &&
+        (cudaMalloc(&g->plans, packed.size() * sizeof(int)) != cudaSuccess ||
+         cudaMemcpyAsync(g->plans, packed.data(), packed.size() * sizeof(int),
+                         cudaMemcpyHostToDevice, s) != cudaSuccess)) {
+        cudaGetLastError();
+        rc = OIFT_E_CUDA;
+    }
+    if (rc == OIFT_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = OIFT_E_CUDA;
+    if (rc != OIFT_OK) {
+        batch_graph_free(g);
+        return rc;
+    }
+    // ---- record ----
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGetLastError();
+        batch_graph_free(g);
+        return OIFT_E_CUDA;
+    }
+    rc = batch_enqueue_oift(c, bp, teams, (const OiftTeamJob *)g->pristine);
+    for (int i = 0; rc == OIFT_OK && i < bp.nj; i++) {
+        const oift_b200_job &jb = jobs[bp.order[i]];
+        if (!jb.label && !jb.mask) continue;
+        oift_b200_outputs o{};
+        o.label = jb.label;
+        o.mask = jb.mask;
+        const int *d_l2c = (const int *)g->plans + off[i];
+        rc = relax_launch<int16_t>(c, &prm[i], jb.image, jb.seeds, jb.nseeds, bp.olab[i], plans[i],
+                                   d_l2c, d_l2c + plans[i].l2c.size(), &o, nullptr);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    g->graph = graph;
+    if (rc == OIFT_OK && (ce != cudaSuccess || !graph)) rc = OIFT_E_CUDA;
+    if (rc == OIFT_OK && cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) rc = OIFT_E_CUDA;
+    if (rc != OIFT_OK) {
+        cudaGetLastError();
+        batch_graph_free(g);
+        return rc;
+    }
+    *out = g;
+    return OIFT_OK;
+}
+
+int oift_b200_batch_graph_launch(oift_b200_batch_graph *g, oift_b200_job *jobs, float *ms) {
+    if (!g || !g->exec) return OIFT_E_BAD_ARG;
+    oift_b200_ctx *c = g->c;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    BatchPrep &bp = g->bp;
+    std::vector<unsigned long long> hclamp(bp.nimg);
+    cudaEventRecord(c->ev[8], s);
+    CU(cudaGraphLaunch(g->exec, s));
+    cudaEventRecord(c->ev[9], s);
+    CU(cudaMemcpyAsync(bp.dj.data(), bp.d_jobs, (size_t)bp.nj * sizeof(OiftTeamJob),
+                       cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(hclamp.data(), bp.d_clamp, bp.nimg * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (ms) cudaEventElapsedTime(ms, c->ev[8], c->ev[9]);
+    int rc = OIFT_OK;
+    for (int i = 0; i < bp.nj; i++) {
+        int st = bp.dj[i].status;
+        if (st == OIFT_TEAM_NOT_RUN) st = OIFT_E_NOT_CONVERGED;
+        if (st == OIFT_OK && g->weight_mode == OIFT_W_GRAD && hclamp[bp.job_img[bp.order[i]]])
+            st = OIFT_E_RANGE;
+        if (jobs) jobs[bp.order[i]].status = st;
+        if (st != OIFT_OK && rc == OIFT_OK) rc = st;
+    }
+    return rc;
+}
+
+int oift_b200_batch_graph_destroy(oift_b200_batch_graph *g) {
+    if (!g) return OIFT_E_BAD_ARG;
+    cudaSetDevice(g->c ? g->c->device : 0);
+    batch_graph_free(g);
     return OIFT_OK;
 }
 

@@ -1471,18 +1471,24 @@ int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ct
     OiftTeamScratch sc = S;
     void *args[] = {&d_jobs, &njobs, &nt, &sc, &spin_limit, &max_levels};
     const size_t smem = oift_smem_bytes();
-    cudaError_t err;
-    if (planar) {
-        auto kfn = oift_team_kernel<32, 1>;
+    // cooperative launch through the launch-attribute API, which a stream capture records as
+    // a cooperative kernel node
+    auto launch = [&](const void *kfn) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(ctas), dim3(OIFT_WARPS * 32), args,
-                                          smem, st);
-    } else {
-        auto kfn = oift_team_kernel<8, 4>;
-        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        err = cudaLaunchCooperativeKernel((void *)kfn, dim3(ctas), dim3(OIFT_WARPS * 32), args,
-                                          smem, st);
-    }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ctas);
+        cfg.blockDim = dim3(OIFT_WARPS * 32);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelExC(&cfg, kfn, args);
+    };
+    cudaError_t err = planar ? launch((const void *)oift_team_kernel<32, 1>)
+                             : launch((const void *)oift_team_kernel<8, 4>);
     if (err != cudaSuccess) {
         cudaGetLastError();
         return OIFT_E_CUDA;

@@ -277,6 +277,42 @@ def test_batch_matches_single_runs(roift, teams):
     ctx.close()
 
 
+@pytest.mark.parametrize("teams", [3, 0])
+def test_batch_graph_replays_match_batch(roift, teams):
+    """A batch recorded into a CUDA graph gives, on two replays in a row, the labels, masks
+    and costs of the direct batched call."""
+    import torch
+    dev = torch.device("cuda:0")
+    cases = _batch_cases()
+    outs = [("label", "mask"), ("label",), ("mask",), ("cost", "label"), ("cost",),
+            ("label", "mask", "cost"), ("label", "mask"), ("label", "cost")]
+    p = roift.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=6)
+    ref_jobs, ref_bufs = _batch_jobs(roift, cases, torch, dev, outs)
+    ctx = roift.Context(0)
+    ctx.run_batch(p, ref_jobs, teams=3)
+    jobs, bufs = _batch_jobs(roift, cases, torch, dev, outs)
+    g = ctx.batch_graph(p, jobs, teams=teams)
+    for _ in range(2):
+        for (_, _, _, lab, mask, cost) in bufs:
+            lab.fill_(-7)
+            mask.fill_(9)
+            cost.fill_(-7)
+        ms = g.launch()
+        torch.cuda.synchronize()
+        assert ms > 0.0
+        for (_, _, _, lab, mask, cost), (_, _, _, rl, rm, rc), job, want in zip(bufs, ref_bufs,
+                                                                                  jobs, outs):
+            assert job.status == 0
+            if "label" in want:
+                assert torch.equal(lab, rl)
+            if "mask" in want:
+                assert torch.equal(mask, rm)
+            if "cost" in want:
+                assert torch.equal(cost, rc)
+    g.close()
+    ctx.close()
+
+
 def test_batch_bad_seed_is_reported_per_job(roift):
     """A job whose seed lies outside its volume ends with OIFT_E_SEED_RANGE; the other
     jobs of the same launch still complete with the labels of single runs."""
