@@ -199,6 +199,16 @@ OIFT_API int oift_b200_conditional_dilation(oift_b200_ctx *ctx, const int32_t *i
  * cap is too small. */
 OIFT_API int oift_b200_inject_boundary_seeds(int32_t *label, int xsize, int ysize, int zsize,
                                              int stride, int32_t *seeds_out, int cap);
+/* The CLI's text inputs (host-only).  Seeds file (oiftrelax.cpp:322-352): a count, then
+ * "x y z id label" per seed; negative labels become 0, seeds outside the volume are
+ * dropped, label[p] takes the seed's label.  Returns the number of in-volume seeds written
+ * to seeds_out (with seeds_out == NULL: counted only, nothing changed), OIFT_E_RANGE when
+ * cap is too small, OIFT_E_BAD_ARG when the file cannot be read. */
+OIFT_API int oift_b200_read_seeds(const char *path, int xsize, int ysize, int zsize,
+                                  int32_t *label, int32_t *seeds_out, int cap);
+/* Per-class polarity file (oiftrelax.cpp:280-300): a count n, then n values in [-1, 1],
+ * stored x100 in per_class (may be NULL to count).  Returns n. */
+OIFT_API int oift_b200_read_polarity(const char *path, float *per_class, int cap);
 /* The CLI's processing chain on host buffers: shift the unshifted int32 `image` to >= 0,
  * `blur_passes` Gaussian blurs (the CLI uses 2), OIFT + relax_sweeps sweeps as run_host,
  * then, if percentile >= 0 and the result is binary, the conditional dilation with

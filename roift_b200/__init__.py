@@ -99,7 +99,7 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
            "oift_b200_run_pyramid_device_i16", "oift_b200_adjoint",
            "oift_b200_batch_graph_create", "oift_b200_batch_graph_launch",
-           "oift_b200_batch_graph_destroy"]
+           "oift_b200_batch_graph_destroy", "oift_b200_read_seeds", "oift_b200_read_polarity"]
 
 _lib = None
 
@@ -131,6 +131,8 @@ def lib():
                                                    C.c_int, C.POINTER(vp)]
         L.oift_b200_batch_graph_launch.argtypes = [vp, C.POINTER(Job), C.POINTER(C.c_float)]
         L.oift_b200_batch_graph_destroy.argtypes = [vp]
+        L.oift_b200_read_seeds.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int]
+        L.oift_b200_read_polarity.argtypes = [C.c_char_p, vp, C.c_int]
         L.oift_b200_selftest_div100.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]
         L.oift_b200_oift_noalloc.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_int, C.c_float, vp, C.c_int, vp, vp, C.c_int,
@@ -401,6 +403,33 @@ class BatchGraph:
             self.close()
         except Exception:
             pass
+
+
+def read_seeds(path, shape_zyx, label):
+    """Seeds file of the CLI (host-only): returns the seed addresses; `label` (int32, NIL
+    elsewhere) receives the seed labels."""
+    Z, Y, X = shape_zyx
+    n = lib().oift_b200_read_seeds(os.fsencode(path), X, Y, Z, None, None, 0)
+    if n < 0:
+        raise OiftError(n, "oift_b200_read_seeds")
+    out = np.empty(max(n, 1), np.int32)
+    n = lib().oift_b200_read_seeds(os.fsencode(path), X, Y, Z, label.ctypes.data,
+                                   out.ctypes.data, n)
+    if n < 0:
+        raise OiftError(n, "oift_b200_read_seeds")
+    return out[:n].copy()
+
+
+def read_polarity(path):
+    """Per-class polarity file of the CLI: the values x100 (float32)."""
+    n = lib().oift_b200_read_polarity(os.fsencode(path), None, 0)
+    if n < 0:
+        raise OiftError(n, "oift_b200_read_polarity")
+    out = np.empty(n, np.float32)
+    n = lib().oift_b200_read_polarity(os.fsencode(path), out.ctypes.data, n)
+    if n < 0:
+        raise OiftError(n, "oift_b200_read_polarity")
+    return out
 
 
 def inject_boundary_seeds(label, shape_zyx, stride):

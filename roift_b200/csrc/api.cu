@@ -1111,6 +1111,73 @@ int oift_b200_inject_boundary_seeds(int32_t *label, int xsize, int ysize, int zs
     return n;
 }
 
+int oift_b200_read_seeds(const char *path, int xsize, int ysize, int zsize, int32_t *label,
+                         int32_t *seeds_out, int cap) {
+    // oiftrelax.cpp:322-352: a count, then "x y z id label" per seed; negative labels
+    // become 0 (background); seeds outside the volume are dropped; the label map takes the
+    // seed's label at its voxel.  With seeds_out == NULL only the in-volume count is
+    // returned and the label map is left alone.  A file with fewer entries than its count
+    // ends at the last complete entry.
+    if (!path || xsize <= 0 || ysize <= 0 || zsize <= 0 || (seeds_out && !label)) return OIFT_E_BAD_ARG;
+    FILE *fp = std::fopen(path, "r");
+    if (!fp) return OIFT_E_BAD_ARG;
+    int n = 0;
+    if (std::fscanf(fp, " %d", &n) != 1 || n < 0) {
+        std::fclose(fp);
+        return OIFT_E_BAD_ARG;
+    }
+    int count = 0;
+    for (int i = 0; i < n; i++) {
+        int x, y, z, id, lb;
+        if (std::fscanf(fp, " %d %d %d %d %d", &x, &y, &z, &id, &lb) != 5) break;
+        if (lb < 0) lb = 0;
+        if (x < 0 || y < 0 || z < 0 || x >= xsize || y >= ysize || z >= zsize) continue;
+        if (lb > OIFT_MAX_LABEL) {
+            std::fclose(fp);
+            return OIFT_E_BAD_ARG;
+        }
+        if (seeds_out) {
+            if (count >= cap) {
+                std::fclose(fp);
+                return OIFT_E_RANGE;
+            }
+            const size_t p = (size_t)x + (size_t)y * xsize + (size_t)z * xsize * ysize;
+            seeds_out[count] = (int32_t)p;
+            label[p] = lb;
+        }
+        count++;
+    }
+    std::fclose(fp);
+    return count;
+}
+
+int oift_b200_read_polarity(const char *path, float *per_class, int cap) {
+    // oiftrelax.cpp:280-300: a count n, then n polarities in [-1, 1]; each becomes x100 in
+    // float.  Returns n; OIFT_E_BAD_ARG when the file is unreadable or short.
+    if (!path) return OIFT_E_BAD_ARG;
+    FILE *fp = std::fopen(path, "r");
+    if (!fp) return OIFT_E_BAD_ARG;
+    int n = 0;
+    if (std::fscanf(fp, " %d", &n) != 1 || n <= 0) {
+        std::fclose(fp);
+        return OIFT_E_BAD_ARG;
+    }
+    if (per_class && n > cap) {
+        std::fclose(fp);
+        return OIFT_E_RANGE;
+    }
+    for (int i = 0; i < n; i++) {
+        float v;
+        if (std::fscanf(fp, " %f", &v) != 1) {
+            std::fclose(fp);
+            return OIFT_E_BAD_ARG;
+        }
+        if (per_class) per_class[i] = v * 100.0f;
+    }
+    std::fclose(fp);
+    return n;
+}
+
 int oift_b200_run_cli_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *image,
                            int32_t *label, const int32_t *seeds, int nseeds, int blur_passes,
                            float percentile, oift_b200_stats *stats) {

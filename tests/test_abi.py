@@ -93,3 +93,25 @@ def test_boundary_seed_injection_is_host_logic(roift, oracle_lib):
         got = lab.copy()
         seeds = roift.inject_boundary_seeds(got, shape, stride)
         assert np.array_equal(seeds, exp_seeds) and np.array_equal(got, exp_lab)
+
+
+def test_cli_text_inputs(roift, tmp_path):
+    """Seeds and per-class polarity files as the CLI reads them (oiftrelax.cpp:280-352):
+    negative labels become background, out-of-volume seeds are dropped, a later seed on the
+    same voxel wins, polarities are stored x100 in float."""
+    shape = (4, 5, 6)
+    f = tmp_path / "seeds.txt"
+    f.write_text("6\n1 2 3 0 1\n0 0 0 0 -2\n5 4 3 0 2\n6 0 0 0 1\n1 2 3 0 3\n2 1 0 7 1\n")
+    lab = np.full(4 * 5 * 6, -1, np.int32)
+    seeds = roift.read_seeds(str(f), shape, lab)
+    addr = lambda x, y, z: x + y * 6 + z * 30
+    assert list(seeds) == [addr(1, 2, 3), 0, addr(5, 4, 3), addr(1, 2, 3), addr(2, 1, 0)]
+    assert lab[addr(1, 2, 3)] == 3 and lab[0] == 0 and lab[addr(5, 4, 3)] == 2
+    assert (lab >= 0).sum() == 4
+    pf = tmp_path / "pol.txt"
+    pf.write_text("3\n-0.3 0.25 1\n")
+    assert np.array_equal(roift.read_polarity(str(pf)),
+                          np.array([np.float32(-0.3) * np.float32(100), 25.0, 100.0], np.float32))
+    (tmp_path / "short.txt").write_text("3\n0.1 0.2\n")
+    with pytest.raises(roift.OiftError):
+        roift.read_polarity(str(tmp_path / "short.txt"))
