@@ -73,6 +73,16 @@ def lib():
         L.or_relax_f64.restype = C.c_int
         L.or_relax_f64.argtypes = L.or_relax_f32.argtypes
         L.or_gaussian_blur.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        L.or_sobel_normalized.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        L.or_oift_fmax_blend.restype = C.c_int
+        L.or_oift_fmax_blend.argtypes = [_i32p, _i32p, C.c_float, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, _Polarity, _i32p, C.c_int, _i32p, _i32p, _i32p]
+        L.or_oift_prim_blend.argtypes = [_i32p, _i32p, C.c_float, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, _Polarity, C.c_int, _i32p, C.c_int, _i32p]
+        L.or_relax_blend_f32.restype = C.c_int
+        L.or_relax_blend_f32.argtypes = [_i32p, _i32p, C.c_float, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, C.c_float, _i32p, C.c_int, _i32p, C.c_int,
+                                         C.c_void_p]
         L.or_adjacency.restype = C.c_int
         L.or_adjacency.argtypes = [C.c_int, _i32p, _i32p, _i32p]
         L.or_conditional_dilation.restype = C.c_longlong
@@ -112,6 +122,9 @@ def ref():
         R.ref_inject_boundary_seeds.restype = C.c_int
         R.ref_inject_boundary_seeds.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int,
                                                 _i32p, C.c_int, _i32p, C.c_int]
+        R.ref_sobel_normalized.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
+        R.ref_gradweight.argtypes = [_i32p, _i32p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                     _i32p, C.c_int, _i32p, C.c_int]
         R.ref_coarse_to_fine.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_int, C.c_float, _i32p, C.c_int, _i32p]
         R.ref_oiftrelax_chain.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_double,
@@ -367,6 +380,60 @@ def coarse_to_fine(fscn, adj, pol, niter, percentile, seeds, label, mode="grad",
     return out
 
 
+def sobel_normalized(img):
+    """Scene32::SobelFilter normalised to the image maximum (exp_gradient_weight.cpp)."""
+    X, Y, Z = _dims(img)
+    out = np.empty(X * Y * Z, np.int32)
+    lib().or_sobel_normalized(as_i32(img), X, Y, Z, out)
+    return out
+
+
+def oift_fmax_blend(img, g, alpha, adj, seeds, seed_labels, pol=None):
+    """R2 with the blend weights of OIFT_Multi_GradWeight: (cost, label, levels)."""
+    X, Y, Z = _dims(img)
+    N = X * Y * Z
+    lab_in = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab_in[seeds] = seed_labels
+    cost = np.empty(N, np.int32)
+    label = np.empty(N, np.int32)
+    P, keep = polarity(pol)
+    levels = lib().or_oift_fmax_blend(as_i32(img), as_i32(g), float(alpha), X, Y, Z, adj, P,
+                                      seeds, len(seeds), lab_in, cost, label)
+    return cost, label, levels
+
+
+def oift_prim_blend(img, g, alpha, adj, seeds, seed_labels, pol=None):
+    """R1 with the blend weights (OIFT_Multi_GradWeight's Prim / FIFO order): labels."""
+    X, Y, Z = _dims(img)
+    N = X * Y * Z
+    lab = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    P, keep = polarity(pol)
+    gi = as_i32(g)
+    wmax = int(max(as_i32(img).max(), gi.max()) * 2) + 2
+    lib().or_oift_prim_blend(as_i32(img), gi, float(alpha), X, Y, Z, adj, P, wmax, seeds,
+                             len(seeds), lab)
+    return lab
+
+
+def relax_blend(img, g, alpha, adj, seeds, label, ntimes, pol):
+    """ORelax_1_Multi_GradWeight restated in FP32: (labels, membership [C, N])."""
+    X, Y, Z = _dims(img)
+    flat = as_i32(img)
+    N = flat.size
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab = np.ascontiguousarray(label, np.int32).copy()
+    nc = len({0} | {int(l) for l in lab[seeds] if l >= 0})
+    mem = np.empty(nc * N, np.float32)
+    got = lib().or_relax_blend_f32(flat, as_i32(g), float(alpha), X, Y, Z, adj,
+                                   float(np.float32((pol or 0.0) * 100.0)), seeds, len(seeds),
+                                   lab, int(ntimes), mem.ctypes.data)
+    assert got == nc
+    return lab, mem.reshape(nc, N)
+
+
 def gaussian_blur(img):
     X, Y, Z = _dims(img)
     out = np.empty(X * Y * Z, np.int32)
@@ -483,6 +550,24 @@ def ref_coarse_to_fine(fscn, adj, pol, niter, percentile, seeds, label):
     ref().ref_coarse_to_fine(as_i32(fscn), X, Y, Z, adj, float(pol), int(niter),
                              float(percentile), np.ascontiguousarray(seeds, np.int32),
                              len(seeds), lab)
+    return lab
+
+
+def ref_sobel_normalized(img):
+    X, Y, Z = _dims(img)
+    out = np.empty(X * Y * Z, np.int32)
+    ref().ref_sobel_normalized(as_i32(img), X, Y, Z, out)
+    return out
+
+
+def ref_gradweight(img, g, alpha, seeds, seed_labels, pol, ntimes):
+    """Reference OIFT_Multi_GradWeight (+ ORelax_1_Multi_GradWeight when ntimes > 0)."""
+    X, Y, Z = _dims(img)
+    lab = np.full(X * Y * Z, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    ref().ref_gradweight(as_i32(img), as_i32(g), X, Y, Z, float(np.float32(pol * 100.0)),
+                         float(alpha), seeds, len(seeds), lab, int(ntimes))
     return lab
 
 

@@ -116,11 +116,35 @@ static inline float polarity_of(or_polarity pol, int lb) {
     return pol.dflt;
 }
 
+/* Blend arc weight of OIFT_Multi_GradWeight (experiments/exp_gradient_weight.cpp:244-254):
+ * wf = alpha |I_p - I_q| + (1 - alpha) (g_p + g_q) * 0.5f in float, oriented by
+ * (int)(wf * (1 +/- per/100)) in float, (int)wf for equal intensities, at least 0. */
+static inline int blend_weight(const int *img, const int *g, float alpha, size_t p, size_t q,
+                               float pol) {
+    float intensity_diff = (float)abs(img[p] - img[q]);
+    float grad_avg = (g[p] + g[q]) * 0.5f;
+    float wf = alpha * intensity_diff + (1.0f - alpha) * grad_avg;
+    int w = (int)wf;
+    if (img[p] > img[q])
+        w = (int)(wf * (1.0f + pol / 100.0f));
+    else if (img[p] < img[q])
+        w = (int)(wf * (1.0f - pol / 100.0f));
+    if (w < 0) w = 0;
+    return w;
+}
+
+/* Where arc weights come from: edge-code planes W, or the blend of image and gradient. */
+typedef struct {
+    const uint16_t *W;
+    const int *img, *g;
+    float alpha;
+} wsrc;
+
 /* Arc weight p -> q where q = p + d_i.  For i in the positive half the edge lives in
  * plane (i - half) at p; otherwise in plane (n-1-i - half) at q with the bits read
  * from q's side, i.e. swapped. */
-static inline int arc_weight(const uint16_t *W, size_t N, int n, int i, size_t p, size_t q,
-                             float pol) {
+static inline int arc_weight_codes(const uint16_t *W, size_t N, int n, int i, size_t p, size_t q,
+                                   float pol) {
     int half = n / 2;
     uint16_t code;
     int gt, lt;
@@ -134,6 +158,12 @@ static inline int arc_weight(const uint16_t *W, size_t N, int n, int i, size_t p
         lt = (code >> 15) & 1;
     }
     return or_oriented((uint16_t)(code & 0x3fffu), gt, lt, pol);
+}
+
+static inline int arc_weight(const wsrc *ws, size_t N, int n, int i, size_t p, size_t q,
+                             float pol) {
+    if (ws->img) return blend_weight(ws->img, ws->g, ws->alpha, p, q, pol);
+    return arc_weight_codes(ws->W, N, n, i, p, q, pol);
 }
 
 /* ---------------------------------------------------------------- binary heap --- */
@@ -178,9 +208,9 @@ static uint64_t hpop(heap64 *h) {
  * (cost << 48 | label << 32 | voxel) with voxel < 2^32, cost < 2^16, label < 2^16.
  * Ties inside one (cost,label) level pop in any order: the set conquered at a level
  * is a reachability closure, so the result does not depend on that order. */
-int or_oift_fmax(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
-                 const int *seeds, int nseeds, const int *label_in,
-                 int *cost, int *label, int *pred) {
+static int fmax_core(const wsrc *ws, int X, int Y, int Z, int adj, or_polarity pol,
+                     const int *seeds, int nseeds, const int *label_in, int *cost, int *label,
+                     int *pred) {
     int dx[26], dy[26], dz[26];
     int n = or_adjacency(adj, dx, dy, dz);
     size_t N = (size_t)X * Y * Z;
@@ -219,7 +249,7 @@ int or_oift_fmax(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity po
             if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
             size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
             if (done[q]) continue;
-            int w = arc_weight(W, N, n, i, p, q, pl);
+            int w = arc_weight(ws, N, n, i, p, q, pl);
             int nc = MAX(c, w);
             if (nc < cost[q] || (nc == cost[q] && lb < label[q])) {
                 cost[q] = nc;
@@ -232,6 +262,21 @@ int or_oift_fmax(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity po
     free(h.k);
     free(done);
     return levels;
+}
+
+int or_oift_fmax(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
+                 const int *seeds, int nseeds, const int *label_in,
+                 int *cost, int *label, int *pred) {
+    wsrc ws = {W, NULL, NULL, 0.0f};
+    return fmax_core(&ws, X, Y, Z, adj, pol, seeds, nseeds, label_in, cost, label, pred);
+}
+
+/* R2 with the blend weights of OIFT_Multi_GradWeight. */
+int or_oift_fmax_blend(const int *img, const int *g, float alpha, int X, int Y, int Z, int adj,
+                       or_polarity pol, const int *seeds, int nseeds, const int *label_in,
+                       int *cost, int *label) {
+    wsrc ws = {NULL, img, g, alpha};
+    return fmax_core(&ws, X, Y, Z, adj, pol, seeds, nseeds, label_in, cost, label, NULL);
 }
 
 /* ------------------------------------------------------- R1: Prim / Dial queue --- */
@@ -295,9 +340,9 @@ static int dq_popmin(dialq *Q) {
     return e;
 }
 
-void or_oift_prim(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
-                  int wmax_buckets, const int *seeds, int nseeds, int *label,
-                  int *value_out, int *pred_out, int *fmax_out) {
+static void prim_core(const wsrc *ws, int X, int Y, int Z, int adj, or_polarity pol,
+                      int wmax_buckets, const int *seeds, int nseeds, int *label,
+                      int *value_out, int *pred_out, int *fmax_out) {
     int dx[26], dy[26], dz[26];
     int n = or_adjacency(adj, dx, dy, dz);
     size_t N = (size_t)X * Y * Z;
@@ -337,7 +382,7 @@ void or_oift_prim(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity p
             if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
             int q = qx + qy * X + qz * X * Y;
             if (Q.color[q] == BLACK) continue;
-            int w = arc_weight(W, N, n, i, (size_t)p, (size_t)q, pl);
+            int w = arc_weight(ws, N, n, i, (size_t)p, (size_t)q, pl);
             if (w < Q.value[q]) {
                 if (Q.color[q] == GRAY) {
                     dq_remove(&Q, q);
@@ -370,6 +415,22 @@ void or_oift_prim(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity p
     free(Q.value);
 }
 
+void or_oift_prim(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
+                  int wmax_buckets, const int *seeds, int nseeds, int *label,
+                  int *value_out, int *pred_out, int *fmax_out) {
+    wsrc ws = {W, NULL, NULL, 0.0f};
+    prim_core(&ws, X, Y, Z, adj, pol, wmax_buckets, seeds, nseeds, label, value_out, pred_out,
+              fmax_out);
+}
+
+/* R1 with the blend weights: OIFT_Multi_GradWeight (exp_gradient_weight.cpp:196-270). */
+void or_oift_prim_blend(const int *img, const int *g, float alpha, int X, int Y, int Z, int adj,
+                        or_polarity pol, int wmax_buckets, const int *seeds, int nseeds,
+                        int *label) {
+    wsrc ws = {NULL, img, g, alpha};
+    prim_core(&ws, X, Y, Z, adj, pol, wmax_buckets, seeds, nseeds, label, NULL, NULL, NULL);
+}
+
 /* R4: gft/src/gft_ift.cpp:287-319 (GetEnergy_Min) in 3D with OIFT_Multi's oriented
  * arc weights (gft_ift.cpp:965-973), tail label selecting the polarity. */
 int or_energy(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
@@ -390,7 +451,7 @@ int or_energy(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
                     if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
                     size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
                     if (label[q] == lp) continue;
-                    int w = arc_weight(W, N, n, i, p, q, pl);
+                    int w = arc_weight_codes(W, N, n, i, p, q, pl);
                     e = MIN(e, w);
                     if (lp >= 0 && lp < nl) energy_lb[lp] = MIN(energy_lb[lp], w);
                 }
@@ -460,7 +521,13 @@ int or_relax_classes(const int *seeds, int nseeds, const int *label, int n,
     int imax = img[0];                                                                      \
     for (int p = 1; p < n; p++) imax = MAX(imax, img[p]);                                   \
     T Wmax = (T)imax;                                                                       \
-    Wmax = (T)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));                         \
+    if (blend) { /* exp_gradient_weight.cpp:338-339, in float */                            \
+        float wm = (float)imax;                                                             \
+        wm *= (1.0f + fabsf(per) / 100.0f);                                                 \
+        Wmax = (T)wm;                                                                       \
+    } else {                                                                                \
+        Wmax = (T)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));                     \
+    }                                                                                       \
     size_t tot = (size_t)n * nc;                                                            \
     T *f1 = (T *)calloc(tot, sizeof(T)), *f2 = (T *)calloc(tot, sizeof(T));                 \
     int *mask_nodes = (int *)malloc(sizeof(int) * (n + 1));                                 \
@@ -497,6 +564,10 @@ int or_relax_classes(const int *seeds, int nseeds, const int *label, int n,
                 int q = qx + qy * X + qz * X * Y;                                           \
                 size_t qo = (size_t)q * nc;                                                 \
                 T w = FABS((T)(img[p] - img[q]));                                           \
+                if (blend) { /* exp_gradient_weight.cpp:403-405 */                          \
+                    T grad_avg = (T)(g[p] + g[q]) * (T)0.5f;                                \
+                    w = (T)alpha * w + ((T)1 - (T)alpha) * grad_avg;                        \
+                }                                                                           \
                 T per_pq;                                                                   \
                 if (per_class) {                                                            \
                     per_pq = (T)0;                                                          \
@@ -509,6 +580,7 @@ int or_relax_classes(const int *seeds, int nseeds, const int *label, int n,
                     w *= ((T)1 + per_pq / (T)100);                                          \
                 else if (img[p] < img[q])                                                   \
                     w *= ((T)1 - per_pq / (T)100);                                          \
+                if (blend && w < (T)0) w = (T)0;                                            \
                 w = Wmax - w;                                                               \
                 if (w < (T)0) w = (T)0;                                                     \
                 w = w * w;                                                                  \
@@ -580,13 +652,67 @@ int or_relax_classes(const int *seeds, int nseeds, const int *label, int n,
 int or_relax_f32(const int *img, int X, int Y, int Z, int adj, float per,
                  const float *per_class, int max_label,
                  const int *seeds, int nseeds, int *label, int ntimes, float *membership) {
+    const int blend = 0, *g = NULL;
+    const float alpha = 1.0f;
     RELAX_BODY(float, fabsf, sqrtf)
 }
 
 int or_relax_f64(const int *img, int X, int Y, int Z, int adj, float per,
                  const float *per_class, int max_label,
                  const int *seeds, int nseeds, int *label, int ntimes, double *membership) {
+    const int blend = 0, *g = NULL;
+    const float alpha = 1.0f;
     RELAX_BODY(double, fabs, sqrt)
+}
+
+/* ORelax_1_Multi_GradWeight (experiments/exp_gradient_weight.cpp:272-503): the relaxation
+ * with blend weights wf = alpha |dI| + (1 - alpha)(g_p + g_q) * 0.5f, oriented by the soft
+ * polarity and clamped at 0, and Wmax evaluated in float. */
+int or_relax_blend_f32(const int *img, const int *g, float alpha, int X, int Y, int Z, int adj,
+                       float per, const int *seeds, int nseeds, int *label, int ntimes,
+                       float *membership) {
+    const int blend = 1;
+    const float *per_class = NULL;
+    const int max_label = 0;
+    RELAX_BODY(float, fabsf, sqrtf)
+}
+
+/* ----------------------------------------------------------------- Sobel --- */
+/* Scene32::SobelFilter (gft/src/gft_filtering3.cpp:509-552): over the linear addresses
+ * i in [1 + X + XY, N - 1 - X - XY) (neighbours by address arithmetic, rows and planes wrap
+ * as in the reference), three 3x3 difference stencils with weights 1 2 1 / 2 4 2 / 1 2 1,
+ * each >> 4, then ROUND(sqrtf((a^2 + b^2 + c^2) / 3.0)); other voxels 0.  Then the
+ * normalisation of exp_gradient_weight.cpp:600-608: g = g * max(I) / max(g) in 64-bit
+ * integers when both maxima are positive. */
+void or_sobel_normalized(const int *img, int X, int Y, int Z, int *out) {
+    static const int n0[9] = {-1, 0, 1, -1, 0, 1, -1, 0, 1};
+    static const int n1[9] = {-1, -1, -1, 0, 0, 0, 1, 1, 1};
+    static const int we[9] = {1, 2, 1, 2, 4, 2, 1, 2, 1};
+    const long long N = (long long)X * Y * Z;
+    const long long dx = 1, dy = X, dz = (long long)X * Y, di = dx + dy + dz;
+    for (long long i = 0; i < N; i++) out[i] = 0;
+    for (long long i = di; i < N - di; i++) {
+        int acc[3] = {0, 0, 0};
+        for (int m = 0; m < 9; m++)
+            acc[0] += we[m] * (img[i + dz + dx * n0[m] + dy * n1[m]] - img[i - dz + dx * n0[m] + dy * n1[m]]);
+        for (int m = 0; m < 9; m++)
+            acc[1] += we[m] * (img[i + dx + dz * n0[m] + dy * n1[m]] - img[i - dx + dz * n0[m] + dy * n1[m]]);
+        for (int m = 0; m < 9; m++)
+            acc[2] += we[m] * (img[i + dy + dx * n0[m] + dz * n1[m]] - img[i - dy + dx * n0[m] + dz * n1[m]]);
+        acc[0] >>= 4;
+        acc[1] >>= 4;
+        acc[2] >>= 4;
+        float f0 = (float)acc[0], f1 = (float)acc[1], f2 = (float)acc[2];
+        float r = sqrtf((f0 * f0 + f1 * f1 + f2 * f2) / 3.0);
+        out[i] = (r < 0) ? (int)(r - 0.5) : (int)(r + 0.5);
+    }
+    int gmax = out[0], wmax = img[0];
+    for (long long i = 1; i < N; i++) {
+        gmax = MAX(gmax, out[i]);
+        wmax = MAX(wmax, img[i]);
+    }
+    if (gmax > 0 && wmax > 0)
+        for (long long i = 0; i < N; i++) out[i] = (int)((long long)out[i] * wmax / gmax);
 }
 
 /* ------------------------------------------------------------------- blur --- */

@@ -104,6 +104,19 @@ int or_relax_f64(const int *img, int X, int Y, int Z, int adj, float per,
 /* GaussianBlur restatement (gft_filtering3.cpp:106-126,321-346,385-397). */
 void or_gaussian_blur(const int *img, int X, int Y, int Z, int *out);
 
+/* Blend weights (experiments/exp_gradient_weight.cpp): Sobel gradient normalised to the
+ * image maximum; R2 and R1 with blend arc weights; the blend relaxation (FP32). */
+void or_sobel_normalized(const int *img, int X, int Y, int Z, int *out);
+int or_oift_fmax_blend(const int *img, const int *g, float alpha, int X, int Y, int Z, int adj,
+                       or_polarity pol, const int *seeds, int nseeds, const int *label_in,
+                       int *cost, int *label);
+void or_oift_prim_blend(const int *img, const int *g, float alpha, int X, int Y, int Z, int adj,
+                        or_polarity pol, int wmax_buckets, const int *seeds, int nseeds,
+                        int *label);
+int or_relax_blend_f32(const int *img, const int *g, float alpha, int X, int Y, int Z, int adj,
+                       float per, const int *seeds, int nseeds, int *label, int ntimes,
+                       float *membership);
+
 /* oiftrelax.cpp:87-169 conditional dilation (label in/out); returns voxels relabelled. */
 long long or_conditional_dilation(const int *img, int *label, int X, int Y, int Z,
                                   float radius, float percentile);

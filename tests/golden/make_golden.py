@@ -60,6 +60,15 @@ def make(name, shape, pol, adj, nl, per_class, seed):
         out["chain_image"] = chain_img.reshape(shape)
         out["ref_chain_label"] = O.ref_oiftrelax_chain(chain_img.reshape(shape), pol, SWEEPS,
                                                        50.0, c.seeds, chain_lab)
+    # the gradient-blend experiment on the twice-blurred volume (6 / 4-adj, global polarity)
+    if pc is None and adj in (6, 4):
+        f = O.ref_gaussian_blur(O.ref_gaussian_blur(img).reshape(shape)).reshape(shape)
+        g = O.ref_sobel_normalized(f)
+        out["blend_image"] = f
+        out["ref_sobel"] = g
+        out["ref_blend_oift_label"] = O.ref_gradweight(f, g, 0.6, c.seeds, c.seed_labels, pol, 0)
+        out["ref_blend_relax_label"] = O.ref_gradweight(f, g, 0.6, c.seeds, c.seed_labels, pol,
+                                                        SWEEPS)
     # the coarse-to-fine cascade on the twice-blurred volume (global polarity cases)
     if pc is None and adj in (6, 26):
         f = O.ref_gaussian_blur(O.ref_gaussian_blur(img).reshape(shape)).reshape(shape)

@@ -201,3 +201,40 @@ def test_fp64_adjoint_matches_central_differences(kernel, adj):
         tm[i] -= h
         fd = (P.forward(*tp)[0] - P.forward(*tm)[0]) / (2 * h)
         assert abs(gr[i] - fd) <= 1e-6 * max(abs(fd), 1e-9), (i, gr[i], fd)
+
+
+BLEND_GOLDEN = [p for p in GOLDEN if "ref_blend_oift_label" in np.load(p).files]
+
+
+@pytest.mark.parametrize("path", BLEND_GOLDEN, ids=[os.path.basename(p)[:-4] for p in BLEND_GOLDEN])
+def test_blend_weights_match_golden(oracle_lib, path):
+    """The Sobel gradient normalised to the image maximum, OIFT_Multi_GradWeight (R1 with
+    blend weights) and ORelax_1_Multi_GradWeight restated against the reference experiment."""
+    d = np.load(path)
+    f = d["blend_image"]
+    seeds, sl = d["seeds"], d["seed_labels"]
+    pol, K, adj = float(d["pol"]), int(d["sweeps"]), int(d["adjacency"])
+    g = O.sobel_normalized(f)
+    assert np.array_equal(g, d["ref_sobel"])
+    lab = O.oift_prim_blend(f, g, 0.6, adj, seeds, sl, pol=pol)
+    assert np.array_equal(lab, d["ref_blend_oift_label"])
+    out, _ = O.relax_blend(f, g, 0.6, adj, seeds, lab, K, pol)
+    assert np.array_equal(out, d["ref_blend_relax_label"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("i,shape,pol,alpha", [(0, (12, 16, 20), -0.3, 0.6),
+                                               (1, (10, 14, 18), 0.5, 0.3),
+                                               (2, (9, 13, 25), 0.0, 1.0),
+                                               (3, (8, 12, 16), 0.4, 0.0)])
+def test_blend_weights_match_live_reference(oracle_lib, i, shape, pol, alpha):
+    c = synth.small_case(seed=60 + i, shape=shape, pol=pol, adjacency=6,
+                         nlabels=1 if i % 2 == 0 else 2, noise=120, contrast=400)
+    img = c.image.astype(np.int32)
+    f = O.gaussian_blur(O.gaussian_blur(img).reshape(shape)).reshape(shape)
+    g = O.sobel_normalized(f)
+    assert np.array_equal(g, O.ref_sobel_normalized(f))
+    lr = O.ref_gradweight(f, g, alpha, c.seeds, c.seed_labels, pol, 0)
+    assert np.array_equal(O.oift_prim_blend(f, g, alpha, 6, c.seeds, c.seed_labels, pol=pol), lr)
+    out, _ = O.relax_blend(f, g, alpha, 6, c.seeds, lr, 7, pol)
+    assert np.array_equal(out, O.ref_gradweight(f, g, alpha, c.seeds, c.seed_labels, pol, 7))
