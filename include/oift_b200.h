@@ -56,7 +56,9 @@ typedef enum {
     OIFT_W_GRAD = 0,    /* |I_p - I_q| exactly (<= 16383, else OIFT_E_RANGE) */
     OIFT_W_GRAD_Q = 1,  /* min(|I_p - I_q|, wq); clamp events counted */
     OIFT_W_RBF_Q = 2,   /* floor(wq*(1 - exp(-d^2/(2 sigma^2))) + 0.5), host LUT */
-    OIFT_W_BLEND_Q = 3  /* (int)(a|dI| + (1-a)(g_p+g_q)/2) with a Sobel map g, clamped */
+    OIFT_W_BLEND_Q = 3  /* float a|dI| + (1-a)(g_p+g_q)/2, g = Sobel map scaled to max I
+                           (experiments/exp_gradient_weight.cpp:244-254, 596-608); 6 / 4
+                           adjacency, global polarity, image in 0..65535 */
 } oift_weight_mode;
 
 typedef struct oift_b200_ctx oift_b200_ctx;

@@ -46,6 +46,7 @@ struct oift_b200_ctx {
     DevBuf yimg, ylab, yseeds, yslab, yfirst, yup, ymerge, yfseeds, yfslab, yaux;
     // adjoint: checkpoints / segment / lambdas / weight sums, mask rings, seed classes, sums
     DevBuf awork, adist, aseedc, asmall, al2c;
+    DevBuf gmap;  // normalised Sobel gradient of the gradient-blend weights
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -143,7 +144,7 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->dborder, &c->dhist, &c->daux, &c->dlabel, &c->yimg, &c->ylab,
                       &c->yseeds, &c->yslab, &c->yfirst, &c->yup, &c->ymerge, &c->yfseeds,
                       &c->yfslab, &c->yaux, &c->awork, &c->adist, &c->aseedc, &c->asmall,
-                      &c->al2c};
+                      &c->al2c, &c->gmap};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -202,7 +203,9 @@ static int check_params(const oift_b200_params *p) {
         return OIFT_E_BAD_ARG;
     }
     if (p->weight_mode < 0 || p->weight_mode > 3) return OIFT_E_BAD_ARG;
-    if (p->weight_mode != OIFT_W_GRAD && (p->wq <= 0 || p->wq > OIFT_MAX_BASE)) return OIFT_E_BAD_ARG;
+    if ((p->weight_mode == OIFT_W_GRAD_Q || p->weight_mode == OIFT_W_RBF_Q) &&
+        (p->wq <= 0 || p->wq > OIFT_MAX_BASE))
+        return OIFT_E_BAD_ARG;
     if (p->relax_sweeps < 0) return OIFT_E_BAD_ARG;
     if (p->per_class) {
         if (p->max_label < 0 || p->max_label > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
@@ -211,7 +214,13 @@ static int check_params(const oift_b200_params *p) {
     } else if (!(std::fabs(p->per) <= 100.0f)) {
         return OIFT_E_BAD_ARG;
     }
-    if (p->weight_mode == OIFT_W_BLEND_Q) return OIFT_E_UNSUPPORTED;
+    if (p->weight_mode == OIFT_W_BLEND_Q) {
+        // the blend weights of exp_gradient_weight.cpp: face neighbourhood, global polarity,
+        // a mix weight in [0, 1]
+        if (p->adjacency != 6 && p->adjacency != 4) return OIFT_E_UNSUPPORTED;
+        if (p->per_class) return OIFT_E_UNSUPPORTED;
+        if (!(p->blend_a >= 0.0f && p->blend_a <= 1.0f)) return OIFT_E_BAD_ARG;
+    }
     if (p->weight_mode == OIFT_W_RBF_Q && !(p->rbf_sigma > 0.0f)) return OIFT_E_BAD_ARG;
     return OIFT_OK;
 }
@@ -246,7 +255,7 @@ struct RelaxResult {
 struct RelaxPlan {
     int nclasses = 0, maxl = 0, bg = 0;
     std::vector<int> classes, l2c;
-    RelaxArgs ra;
+    RelaxArgs ra{};
 };
 
 static int relax_plan(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *d_slabels,
@@ -290,7 +299,11 @@ static int relax_plan(oift_b200_ctx *c, const oift_b200_params *p, const int32_t
     long long imax = hmm[1], imin = hmm[0];
     long long shifted_max = imin < 0 ? imax - imin : imax;
     float Wmax = (float)shifted_max;
-    Wmax = (float)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));
+    const bool blend = p->weight_mode == OIFT_W_BLEND_Q;
+    if (blend)  // exp_gradient_weight.cpp:338-339, in float
+        Wmax *= (1.0f + std::fabs(p->per) / 100.0f);
+    else
+        Wmax = (float)((double)Wmax * (1.0 + (double)max_abs_per / 100.0));
     double deg = (p->adjacency == 26) ? 26 : (p->adjacency == 8 ? 8 : (p->adjacency == 6 ? 6 : 4));
     if ((double)Wmax > std::pow(3.0e38 / deg, 0.125)) return OIFT_E_RANGE;
 
@@ -312,6 +325,9 @@ static int relax_plan(oift_b200_ctx *c, const oift_b200_params *p, const int32_t
     ra.Wmax = Wmax;
     ra.per = p->per;
     ra.bg = pl->bg;
+    ra.blend = blend ? 1 : 0;
+    ra.alpha = p->blend_a;
+    ra.gmap = blend ? (const int32_t *)c->gmap.p : nullptr;
     for (int k = 0; k < 8; k++) ra.pcm[k] = k < nclasses ? pcm[k] : 0.0f;
     return OIFT_OK;
 }
@@ -434,7 +450,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     const int planes = oift_b200_weight_planes(p->adjacency);
     Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
     // 26 / 8: the full-neighbourhood OIFT evaluates arc weights from the image itself
-    const bool fulln = p->adjacency == 26 || p->adjacency == 8;
+    const bool blend = p->weight_mode == OIFT_W_BLEND_Q;
+    const bool fulln = p->adjacency == 26 || p->adjacency == 8 || blend;
     OiftPlan plan = fulln ? oift_plan_full(X, Y, Z) : oift_plan(X, Y, Z);
 
     if (!fulln) TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
@@ -513,6 +530,21 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     fn.wcap = ba.cap;
     fn.lut = ba.lut;
     fn.lut_len = ba.lut_len;
+    if (blend) {
+        // blend weights (exp_gradient_weight.cpp:244-254) from the image and its Sobel
+        // gradient normalised to the image maximum (596-608).  The tile stages both as 16-bit
+        // values, and an oriented weight must fit the 15-bit cost: wf <= max(I), so
+        // max(I) (1 + |per| / 100) must stay below 32767.
+        if (hmm[0] < 0 || hmm[1] > 65535 ||
+            (double)hmm[1] * (1.0 + std::fabs((double)p->per) / 100.0) >= 32767.0)
+            return OIFT_E_RANGE;
+        TRY(grow(c, c->gmap, N * sizeof(int32_t)));
+        int *d_mm_g = (int *)((char *)c->minmax.p + 2 * sizeof(int));
+        CU(launch_sobel_normalized<T>(d_img, (int32_t *)c->gmap.p, X, Y, Z, d_mm, d_mm_g, c->sms, s));
+        fn.blend = true;
+        fn.gmap = (const int32_t *)c->gmap.p;
+        fn.alpha = p->blend_a;
+    }
     cudaEventRecord(c->ev[1], s);
 
     // ---- OIFT ----
@@ -1445,6 +1477,7 @@ static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_
     if (teams < 1 || teams > c->sms) return OIFT_E_BAD_ARG;
     // the team kernel is the 6 / 4-neighbourhood tile step on prebuilt edge codes
     if (common->adjacency != 6 && common->adjacency != 4) return OIFT_E_UNSUPPORTED;
+    if (common->weight_mode == OIFT_W_BLEND_Q) return OIFT_E_UNSUPPORTED;
     const int ctas_lo = c->sms / teams, ctas_hi = (c->sms + teams - 1) / teams;
 
     // ---- per-job checks; distinct images (pointer + extents) ----

@@ -26,6 +26,10 @@ struct RelaxArgs {
     float per;
     int bg;
     float pcm[8];
+    // gradient blend (ORelax_1_Multi_GradWeight): normalised Sobel map and mix weight
+    int blend;
+    float alpha;
+    const int32_t *gmap;
 };
 
 // Hot scheduling counters of the persistent OIFT kernel, one 128-byte line each so
@@ -143,6 +147,11 @@ cudaError_t launch_shift_to_i32(const T *in, int32_t *out, size_t n, const int *
 template <typename T>
 cudaError_t launch_gaussian_blur(const T *in, int32_t *out, int X, int Y, int Z, float w0,
                                  float w1, cudaStream_t s);
+// Sobel gradient normalised to the image maximum (d_mm_img: image min / max on the device;
+// d_mm_g: 2 ints of scratch).
+template <typename T>
+cudaError_t launch_sobel_normalized(const T *img, int32_t *g, int X, int Y, int Z,
+                                    const int *d_mm_img, int *d_mm_g, int sms, cudaStream_t s);
 __global__ void dilation_border_kernel(const int32_t *label, const int32_t *img, uint8_t *border,
                                        int X, int Y, int Z, const int *off, int noff,
                                        unsigned *hist_hi, unsigned *count);
@@ -161,6 +170,10 @@ struct OiftFullN {
     int wmode, wcap;
     const uint16_t *lut;
     int lut_len;
+    // gradient blend: 6 / 4 face neighbourhood, weights from image + normalised Sobel map
+    bool blend;
+    const int32_t *gmap;
+    float alpha;
 };
 // Tiling of the full-neighbourhood kernel: 32 x 4 x 4 (3D) or 32 x 16 (2D).
 OiftPlan oift_plan_full(int X, int Y, int Z);

@@ -57,6 +57,9 @@ struct OiftArgs {
     int wcap;              // base weight ceiling (wq, or OIFT_MAX_BASE)
     const uint16_t *lut;   // RBF_Q table over |dI|
     int lut_len;
+    // gradient blend (BLEND_Q, 6 / 4 neighbourhoods): normalised Sobel map and mix weight
+    const int32_t *gmap;
+    float alpha;
 };
 
 constexpr int OIFT_WARPS = 16;
@@ -701,7 +704,7 @@ __device__ __forceinline__ int gen_base(const OiftArgs &A, int ip, int iq) {
     return b > A.wcap ? A.wcap : b;
 }
 
-template <int TY, int TZ, typename TI>
+template <int TY, int TZ, typename TI, bool BLEND>
 __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
                                   double fgt, double flt, int bgt, int blt, uint32_t *skey,
                                   int32_t *simg, uint16_t *wl, uint32_t *nfm, uint32_t *rmask,
@@ -722,17 +725,45 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     const uint32_t kexp = kk - 1u;
     const uint32_t lab_bits = ((uint32_t)l << 1) | 1u;
     const TI *img = static_cast<const TI *>(A.img);
-    auto himg = [&](int xl, int yl, int zl) -> int {  // tile-local coordinates, -1 .. 32
-        return simg[(zl + ZO) * (HY * 34) + (yl + 1) * 34 + (xl + 1)];
+    // staged halo: int32 intensities, or (BLEND) 16-bit intensities followed by 16-bit
+    // gradients; both index by halo position
+    constexpr int HN = 34 * HY * HZ;
+    uint16_t *simg16 = reinterpret_cast<uint16_t *>(simg);
+    auto hidx = [&](int xl, int yl, int zl) -> int {  // tile-local coordinates, -1 .. 32
+        return (zl + ZO) * (HY * 34) + (yl + 1) * 34 + (xl + 1);
+    };
+    auto hval = [&](int h) -> int { return BLEND ? (int)simg16[h] : simg[h]; };
+    // BLEND: per-label float factors of OIFT_Multi_GradWeight (exp_gradient_weight.cpp:249-252)
+    float bgtf = 1.0f, bltf = 1.0f;
+    if (BLEND) {
+        const float q = __fdiv_rn(polarity_of(A, l), 100.0f);
+        bgtf = __fadd_rn(1.0f, q);
+        bltf = __fsub_rn(1.0f, q);
+    }
+    // oriented weight of the arc p -> q (halo positions hp, hq) with tail p
+    auto arc_w = [&](int hp, int hq) -> int {
+        const int ip = hval(hp), iq = hval(hq);
+        if (BLEND) {
+            // wf = alpha |dI| + (1 - alpha)(g_p + g_q) * 0.5f, (int)(wf * factor), >= 0
+            const float idiff = (float)abs(ip - iq);
+            const float gavg = __fmul_rn((float)((int)simg16[HN + hp] + (int)simg16[HN + hq]), 0.5f);
+            const float wf = __fadd_rn(__fmul_rn(A.alpha, idiff),
+                                       __fmul_rn(__fsub_rn(1.0f, A.alpha), gavg));
+            const int w = ip > iq ? (int)__fmul_rn(wf, bgtf)
+                                  : (ip < iq ? (int)__fmul_rn(wf, bltf) : (int)wf);
+            return w < 0 ? 0 : w;
+        }
+        return oriented_weight((uint32_t)gen_base<TI>(A, ip, iq), ip > iq, ip < iq, fgt, flt);
     };
     // arc p -> q with tail p: open at this cost, or the key it offers q
-    auto arc_open = [&](int ip, int iq) -> bool {
+    auto arc_open = [&](int hp, int hq) -> bool {
+        if (BLEND) return arc_w(hp, hq) <= c;
+        const int ip = hval(hp), iq = hval(hq);
         const int b = gen_base<TI>(A, ip, iq);
         return ip > iq ? b <= bgt : (ip < iq ? b <= blt : b <= c);
     };
-    auto arc_key = [&](int ip, int iq) -> uint32_t {
-        const int b = gen_base<TI>(A, ip, iq);
-        const int w = oriented_weight((uint32_t)b, ip > iq, ip < iq, fgt, flt);
+    auto arc_key = [&](int hp, int hq) -> uint32_t {
+        const int w = arc_w(hp, hq);
         const int nc = w > c ? w : c;
         return ((uint32_t)nc << 17) | lab_bits;
     };
@@ -771,11 +802,17 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
                 valid ? __ldcg(&A.key[(size_t)x + (size_t)y * X + (size_t)z * XY]) : 0u;
         }
     }
-    for (int i = lane; i < 34 * HY * HZ; i += 32) {
+    for (int i = lane; i < HN; i += 32) {
         const int hx = i % 34, hy = (i / 34) % HY, hz = i / (34 * HY);
         const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - ZO + hz;
         const bool ok = gx >= 0 && gx < X && gy >= 0 && gy < Y && gz >= 0 && gz < Z;
-        simg[i] = ok ? (int32_t)__ldg(&img[(size_t)gx + (size_t)gy * X + (size_t)gz * XY]) : 0;
+        const size_t g = (size_t)gx + (size_t)gy * X + (size_t)gz * XY;
+        if (BLEND) {  // the host checked 0 <= I, g <= 65535
+            simg16[i] = ok ? (uint16_t)__ldg(&img[g]) : (uint16_t)0;
+            simg16[HN + i] = ok ? (uint16_t)__ldg(&A.gmap[g]) : (uint16_t)0;
+        } else {
+            simg[i] = ok ? (int32_t)__ldg(&img[g]) : 0;
+        }
     }
     if (full) cp_async_wait_all();
     __syncwarp();
@@ -832,7 +869,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
             const int xg = x0 + xl, y = y0 + yl, z = z0 + zl;
             A.key[(size_t)xg + (size_t)y * X + (size_t)z * XY] = kexp;
             skey[li] = kexp;
-            const int ip = himg(xl, yl, zl);
+            const int hp = hidx(xl, yl, zl);
 #pragma unroll
             for (int dz = (TZ > 1 ? -1 : 0); dz <= (TZ > 1 ? 1 : 0); dz++)
 #pragma unroll
@@ -840,6 +877,8 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
 #pragma unroll
                     for (int dx = -1; dx <= 1; dx++) {
                         if (dx == 0 && dy == 0 && dz == 0) continue;
+                        // the blend weights come with the 6 / 4 face neighbourhood
+                        if (BLEND && (dx != 0) + (dy != 0) + (dz != 0) != 1) continue;
                         const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
                         if (qxl < 0 || qxl >= 32 || qyl < 0 || qyl >= TY || qzl < 0 || qzl >= TZ)
                             continue;  // across the tile boundary: after the flood
@@ -847,11 +886,11 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
                         const int lq = (qyl + TY * qzl) * 32 + qxl;
                         const uint32_t sk = skey[lq];
                         if (sk <= kk) continue;
-                        const int iq = himg(qxl, qyl, qzl);
-                        if (arc_open(ip, iq)) {
+                        const int hq = hidx(qxl, qyl, qzl);
+                        if (arc_open(hp, hq)) {
                             atomicOr(&nfm[qyl + TY * qzl], 1u << qxl);
                         } else {
-                            const uint32_t nk = arc_key(ip, iq);
+                            const uint32_t nk = arc_key(hp, hq);
                             if (nk < sk) {
                                 atomicMin(&skey[lq], nk);
                                 atomicMin(&A.key[(size_t)(xg + dx) + (size_t)(y + dy) * X +
@@ -882,7 +921,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
                           (TZ > 1 && (zl == 0 || zl == TZ - 1));
         if (!edge) continue;
         const int xg = x0 + xl, y = y0 + yl, z = z0 + zl;
-        const int ip = himg(xl, yl, zl);
+        const int hp = hidx(xl, yl, zl);
 #pragma unroll
         for (int dz = (TZ > 1 ? -1 : 0); dz <= (TZ > 1 ? 1 : 0); dz++) {
             uint32_t nk[9], old[9];
@@ -890,11 +929,12 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
             for (int j = 0; j < 9; j++) {
                 const int dy = j / 3 - 1, dx = j % 3 - 1;
                 nk[j] = OIFT_KEY_INF;
+                if (BLEND && (dx != 0) + (dy != 0) + (dz != 0) != 1) continue;
                 const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
                 const bool out = qxl < 0 || qxl >= 32 || qyl < 0 || qyl >= TY || qzl < 0 || qzl >= TZ;
                 const int qx = xg + dx, qy = y + dy, qz = z + dz;
                 if (!out || qx < 0 || qy < 0 || qz < 0 || qx >= X || qy >= Y || qz >= Z) continue;
-                nk[j] = arc_key(ip, himg(qxl, qyl, qzl));
+                nk[j] = arc_key(hp, hidx(qxl, qyl, qzl));
                 old[j] = atomicMin(&A.key[(size_t)qx + (size_t)qy * X + (size_t)qz * XY], nk[j]);
             }
 #pragma unroll
@@ -965,7 +1005,7 @@ struct OiftCtaSmem {
 
 // The level loop of one OIFT job, run by the `team_ctas` CTAs starting at team CTA index
 // `team_cta` (0 .. team_ctas-1).  A.nwarps must equal team_ctas * OIFT_WARPS.
-template <int TY, int TZ, bool FULLN = false, typename TI = int16_t>
+template <int TY, int TZ, bool FULLN = false, typename TI = int16_t, bool BLEND = false>
 __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftCtaSmem &cs,
                            unsigned char *smem_raw) {
     const unsigned FULL = 0xffffffffu;
@@ -1053,7 +1093,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 if (lane == 0) A.tpend[th] = OIFT_KEY_INF;
                 __syncwarp();
                 if constexpr (FULLN)
-                    process_tile_full<TY, TZ, TI>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey,
+                    process_tile_full<TY, TZ, TI, BLEND>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey,
                                                   reinterpret_cast<int32_t *>(sw),
                                                   reinterpret_cast<uint16_t *>(wl), nfm, rmask,
                                                   cyc_tile);
@@ -1094,7 +1134,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                         b &= b - 1;
                         const int t = gwarp + j * nwarps;
                         if constexpr (FULLN)
-                            process_tile_full<TY, TZ, TI>(A, t, par, kk, c, l, fgt, flt, bgt,
+                            process_tile_full<TY, TZ, TI, BLEND>(A, t, par, kk, c, l, fgt, flt, bgt,
                                                           blt, skey,
                                                           reinterpret_cast<int32_t *>(sw),
                                                           reinterpret_cast<uint16_t *>(wl), nfm,
@@ -1142,11 +1182,11 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     }
 }
 
-template <int TY, int TZ, bool FULLN = false, typename TI = int16_t>
+template <int TY, int TZ, bool FULLN = false, typename TI = int16_t, bool BLEND = false>
 __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(OiftArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ OiftCtaSmem cs;
-    oift_solve<TY, TZ, FULLN, TI>(A, blockIdx.x, gridDim.x, cs, smem_raw);
+    oift_solve<TY, TZ, FULLN, TI, BLEND>(A, blockIdx.x, gridDim.x, cs, smem_raw);
 }
 
 // Batched OIFT: CTA b belongs to team b / team_ctas.  A team draws jobs from a shared
@@ -1416,6 +1456,8 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.wcap = fn ? fn->wcap : OIFT_MAX_BASE;
     A.lut = fn ? fn->lut : nullptr;
     A.lut_len = fn ? fn->lut_len : 0;
+    A.gmap = fn ? fn->gmap : nullptr;
+    A.alpha = fn ? fn->alpha : 1.0f;
     size_t smem = oift_smem_bytes();
     void *args[] = {&A};
     cudaError_t err;
@@ -1424,7 +1466,14 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return cudaLaunchCooperativeKernel(kfn, dim3(sms), dim3(OIFT_WARPS * 32), args, smem, st);
     };
-    if (fn) {
+    if (fn && fn->blend) {
+        if (P.TZ == 1)
+            err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<16, 1, true, int16_t, true>)
+                              : launch((const void *)oift_persistent_kernel<16, 1, true, int32_t, true>);
+        else
+            err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<4, 4, true, int16_t, true>)
+                              : launch((const void *)oift_persistent_kernel<4, 4, true, int32_t, true>);
+    } else if (fn) {
         if (P.TZ == 1)
             err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<16, 1, true, int16_t>)
                               : launch((const void *)oift_persistent_kernel<16, 1, true, int32_t>);

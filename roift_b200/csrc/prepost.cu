@@ -337,3 +337,75 @@ __global__ void seeds_scatter_kernel(const int32_t *__restrict__ lab, size_t N, 
 }
 
 }  // namespace oiftb
+
+namespace oiftb {
+
+// ------------------------------------------------------------- Sobel gradient ----
+// Scene32::SobelFilter (gft_filtering3.cpp:509-552) over the linear addresses
+// [1 + X + XY, N - 1 - X - XY): neighbours by address arithmetic (rows and planes wrap as in
+// the reference), three 3x3 difference stencils (1 2 1 / 2 4 2 / 1 2 1), each >> 4, then
+// ROUND(sqrtf((a^2 + b^2 + c^2) / 3.0)) with the float sum, the double division and the
+// float square root of the C++ expression; every other voxel 0.
+template <typename T>
+__global__ void sobel_kernel(const T *__restrict__ img, int32_t *__restrict__ out, long long N,
+                             long long dy, long long dz) {
+    const long long di = 1 + dy + dz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < di || i >= N - di) {
+            out[i] = 0;
+            continue;
+        }
+        int acc0 = 0, acc1 = 0, acc2 = 0;
+#pragma unroll
+        for (int m = 0; m < 9; m++) {
+            const int n0 = m % 3 - 1, n1 = m / 3 - 1;
+            const int we = (n0 == 0 ? 2 : 1) * (n1 == 0 ? 2 : 1);
+            acc0 += we * ((int)img[i + dz + n0 + dy * n1] - (int)img[i - dz + n0 + dy * n1]);
+            acc1 += we * ((int)img[i + 1 + dz * n0 + dy * n1] - (int)img[i - 1 + dz * n0 + dy * n1]);
+            acc2 += we * ((int)img[i + dy + n0 + dz * n1] - (int)img[i - dy + n0 + dz * n1]);
+        }
+        acc0 >>= 4;
+        acc1 >>= 4;
+        acc2 >>= 4;
+        const float f0 = (float)acc0, f1 = (float)acc1, f2 = (float)acc2;
+        const float s = __fadd_rn(__fadd_rn(__fmul_rn(f0, f0), __fmul_rn(f1, f1)), __fmul_rn(f2, f2));
+        const float q = __double2float_rn(__ddiv_rn((double)s, 3.0));
+        const float r = __fsqrt_rn(q);
+        out[i] = (int32_t)((double)r + 0.5);
+    }
+}
+
+// g = g * max(I) / max(g) in 64-bit integers when both maxima are positive
+// (exp_gradient_weight.cpp:600-608); mm_img / mm_g hold (min, max) of image and gradient.
+__global__ void sobel_normalize_kernel(int32_t *g, long long N, const int *__restrict__ mm_img,
+                                       const int *__restrict__ mm_g) {
+    const long long wmax = mm_img[1], gmax = mm_g[1];
+    if (!(gmax > 0 && wmax > 0)) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+        g[i] = (int32_t)((long long)g[i] * wmax / gmax);
+}
+
+template <typename T>
+cudaError_t launch_sobel_normalized(const T *img, int32_t *g, int X, int Y, int Z,
+                                    const int *d_mm_img, int *d_mm_g, int sms, cudaStream_t s) {
+    const long long N = (long long)X * Y * Z;
+    int blocks = (int)std::min<long long>((N + 255) / 256, (long long)sms * 16);
+    if (blocks < 1) blocks = 1;
+    sobel_kernel<T><<<blocks, 256, 0, s>>>(img, g, N, (long long)X, (long long)X * Y);
+    const int mm_init[2] = {0x7fffffff, (int)0x80000000};
+    cudaError_t e = cudaMemcpyAsync(d_mm_g, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    e = launch_minmax<int32_t>(g, (size_t)N, d_mm_g, sms, s);
+    if (e != cudaSuccess) return e;
+    sobel_normalize_kernel<<<blocks, 256, 0, s>>>(g, N, d_mm_img, d_mm_g);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_sobel_normalized<int16_t>(const int16_t *, int32_t *, int, int, int,
+                                                      const int *, int *, int, cudaStream_t);
+template cudaError_t launch_sobel_normalized<int32_t>(const int32_t *, int32_t *, int, int, int,
+                                                      const int *, int *, int, cudaStream_t);
+
+}  // namespace oiftb

@@ -4,11 +4,14 @@
 
 namespace oiftb {
 
-template <int C, bool PERCLASS>
-__device__ __forceinline__ void relax_accumulate(const RelaxArgs &a, int ip, int iq,
-                                                 const float (&mq)[C], float dpq, float &sw,
-                                                 float (&acc)[C]) {
+template <int C, bool PERCLASS, bool BLEND>
+__device__ __forceinline__ void relax_accumulate(const RelaxArgs &a, int ip, int iq, int gp,
+                                                 int gq, const float (&mq)[C], float dpq,
+                                                 float &sw, float (&acc)[C]) {
     float w = fabsf((float)(ip - iq));
+    if (BLEND)  // wf = alpha |dI| + (1 - alpha)(g_p + g_q) * 0.5f (exp_gradient_weight.cpp:403-405)
+        w = __fadd_rn(__fmul_rn(a.alpha, w),
+                      __fmul_rn(__fsub_rn(1.0f, a.alpha), __fmul_rn((float)(gp + gq), 0.5f)));
     float per_pq;
     if (PERCLASS) {
         per_pq = 0.0f;
@@ -25,6 +28,7 @@ __device__ __forceinline__ void relax_accumulate(const RelaxArgs &a, int ip, int
         w = __fmul_rn(w, __fadd_rn(1.0f, div100_rn(per_pq)));
     else if (ip < iq)
         w = __fmul_rn(w, __fsub_rn(1.0f, div100_rn(per_pq)));
+    if (BLEND && w < 0.0f) w = 0.0f;
     w = __fsub_rn(a.Wmax, w);
     if (w < 0.0f) w = 0.0f;
     w = __fmul_rn(w, w);
@@ -51,9 +55,10 @@ constexpr int RH_X = RT_X + 2, RH_Y = RT_Y + 2, RH_Z = RT_Z + 2;
 constexpr int RH_N = RH_X * RH_Y * RH_Z;
 
 // Tiles holding a voxel with a differently-labelled neighbour get distance 0.
-template <int C, typename T, bool PERCLASS, int ADJ, bool INTERIOR>
+template <int C, typename T, bool PERCLASS, int ADJ, bool INTERIOR, bool BLEND>
 __device__ __forceinline__ void relax_tile_voxels(const RelaxArgs &a, const float *sm,
-                                                  const int *si, float *__restrict__ mout,
+                                                  const int *si, const int *sg,
+                                                  float *__restrict__ mout,
                                                   const uint8_t *__restrict__ seedc, int x,
                                                   int y, int z0, int lx, int ly) {
     const int X = a.X, Y = a.Y, Z = a.Z;
@@ -90,7 +95,8 @@ __device__ __forceinline__ void relax_tile_voxels(const RelaxArgs &a, const floa
 #pragma unroll
             for (int k = 0; k < C; k++) mq[k] = sm[k * RH_N + hq];
             const float dpq = (ADJ == 6) ? 1.0f : a.dpq[i];
-            relax_accumulate<C, PERCLASS>(a, ip, si[hq], mq, dpq, sw, acc);
+            relax_accumulate<C, PERCLASS, BLEND>(a, ip, si[hq], BLEND ? sg[hc] : 0,
+                                                 BLEND ? sg[hq] : 0, mq, dpq, sw, acc);
         }
         const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
         float out[C];
@@ -111,7 +117,7 @@ __device__ __forceinline__ void relax_tile_voxels(const RelaxArgs &a, const floa
     }
 }
 
-template <int C, typename T, bool PERCLASS, int ADJ>
+template <int C, typename T, bool PERCLASS, int ADJ, bool BLEND>
 __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict__ min_,
                                                          float *__restrict__ mout,
                                                          const T *__restrict__ img,
@@ -124,6 +130,7 @@ __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict
     extern __shared__ __align__(16) unsigned char rsm[];
     float *sm = reinterpret_cast<float *>(rsm);          // [C][RH_Z][RH_Y][RH_X]
     int *si = reinterpret_cast<int *>(sm + C * RH_N);    // [RH_Z][RH_Y][RH_X]
+    int *sg = si + RH_N;                                 // gradient halo (BLEND only)
     const int X = a.X, Y = a.Y, Z = a.Z;
     const size_t N = a.N, XY = (size_t)X * Y;
     const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
@@ -137,6 +144,7 @@ __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict
 #pragma unroll
             for (int k = 0; k < C; k++) sm[k * RH_N + i] = __ldg(&min_[(size_t)k * N + g]);
             si[i] = (int)__ldg(&img[g]);
+            if (BLEND) sg[i] = __ldg(&a.gmap[g]);
         }
     }
     __syncthreads();
@@ -147,9 +155,11 @@ __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict
     const bool interior = x0 >= 1 && x0 + RT_X < X && y0 >= 1 && y0 + RT_Y < Y && z0 >= 1 &&
                           z0 + RT_Z < Z;
     if (interior)
-        relax_tile_voxels<C, T, PERCLASS, ADJ, true>(a, sm, si, mout, seedc, x, y, z0, lx, ly);
+        relax_tile_voxels<C, T, PERCLASS, ADJ, true, BLEND>(a, sm, si, sg, mout, seedc, x, y, z0,
+                                                            lx, ly);
     else
-        relax_tile_voxels<C, T, PERCLASS, ADJ, false>(a, sm, si, mout, seedc, x, y, z0, lx, ly);
+        relax_tile_voxels<C, T, PERCLASS, ADJ, false, BLEND>(a, sm, si, sg, mout, seedc, x, y, z0,
+                                                             lx, ly);
 }
 
 // Launches the tile sweep for C classes; one explicit instantiation per translation unit.

@@ -12,14 +12,22 @@ template <int C, typename T, int ADJ>
 static cudaError_t launch_tile_c(const float *in, float *out, const T *img, const uint8_t *seedc,
                                  const uint16_t *tdist, int sweep, const RelaxArgs &a,
                                  bool perclass, int ntiles, int ntx, int nty, cudaStream_t s) {
-    const size_t smem = (size_t)(C + 1) * RH_N * 4;
     dim3 block(32, 8);
+    if (a.blend) {  // gradient blend: 6 / 4 neighbourhood, global polarity
+        if (ADJ != 6 || perclass) return cudaErrorInvalidValue;
+        const size_t smem = (size_t)(C + 2) * RH_N * 4;
+        auto k = relax_tile_kernel<C, T, false, 6, true>;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<ntiles, block, smem, s>>>(in, out, img, seedc, tdist, sweep, a, ntx, nty);
+        return cudaGetLastError();
+    }
+    const size_t smem = (size_t)(C + 1) * RH_N * 4;
     if (perclass) {
-        auto k = relax_tile_kernel<C, T, true, ADJ>;
+        auto k = relax_tile_kernel<C, T, true, ADJ, false>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<ntiles, block, smem, s>>>(in, out, img, seedc, tdist, sweep, a, ntx, nty);
     } else {
-        auto k = relax_tile_kernel<C, T, false, ADJ>;
+        auto k = relax_tile_kernel<C, T, false, ADJ, false>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<ntiles, block, smem, s>>>(in, out, img, seedc, tdist, sweep, a, ntx, nty);
     }

@@ -493,3 +493,59 @@ def test_pyramid_device_int16(roift, adj, mode):
                                     len(c.seeds), out.data_ptr(), 2, 50.0)
     exp = _c2f_expected(img16.astype(np.int32), adj, 0.2, 4, c.seeds, lab0, mode=mode)
     assert np.array_equal(out.cpu().numpy(), exp)
+
+
+# ------------------------------------------------------ gradient-blend weights ----
+BLEND_CASES = [((14, 18, 40), -0.3, 6, 1, 0.6), ((9, 21, 70), 0.4, 6, 2, 0.3),
+               ((1, 45, 67), 0.5, 4, 1, 0.8), ((12, 16, 40), 0.0, 6, 1, 1.0),
+               ((10, 20, 36), 0.2, 6, 1, 0.0)]
+
+
+@pytest.mark.parametrize("shape,pol,adj,nl,alpha", BLEND_CASES)
+def test_blend_oift_and_relax_match_oracle(roift, oracle_lib, shape, pol, adj, nl, alpha):
+    """BLEND_Q: the Sobel map normalised to the image maximum, OIFT with the float blend
+    weights of OIFT_Multi_GradWeight (cost and labels == R2 with those weights), and the
+    blend relaxation of ORelax_1_Multi_GradWeight (membership bit-identical)."""
+    c, img = _case(shape, pol, adj, nl, "grad")
+    X, Y, Z = shape[2], shape[1], shape[0]
+    g = O.sobel_normalized(img.reshape(shape))
+    p = roift.make_params(shape, adjacency=adj, weight_mode="blend_q", blend_a=alpha, pol=pol,
+                          sweeps=0)
+    lab, cost, _, _, _ = roift._ctx().run_host(p, img, c.label_map(), c.seeds, want_cost=True)
+    cost_r2, lab_r2, _ = O.oift_fmax_blend(img.reshape(shape), g, alpha, adj, c.seeds,
+                                           c.seed_labels, pol=pol)
+    assert np.array_equal(cost, cost_r2)
+    assert np.array_equal(lab, lab_r2)
+    K = 6
+    p = roift.make_params(shape, adjacency=adj, weight_mode="blend_q", blend_a=alpha, pol=pol,
+                          sweeps=K)
+    labk, _, memb, _, _ = roift._ctx().run_host(p, img, c.label_map(), c.seeds,
+                                                want_membership=8)
+    exp, m32 = O.relax_blend(img.reshape(shape), g, alpha, adj, c.seeds, lab_r2, K, pol)
+    assert np.array_equal(labk, exp)
+    assert np.array_equal(memb.view(np.uint32), m32.view(np.uint32))
+
+
+BLEND_GOLDEN = [p for p in GOLDEN if "ref_blend_relax_label" in np.load(p).files]
+
+
+@pytest.mark.parametrize("path", BLEND_GOLDEN, ids=[os.path.basename(p)[:-4] for p in BLEND_GOLDEN])
+def test_blend_matches_reference_experiment(roift, oracle_lib, path):
+    """On the reference experiment's inputs (twice-blurred image): the GPU blend OIFT +
+    relaxation equals the reference's OIFT_Multi_GradWeight + ORelax_1_Multi_GradWeight
+    wherever the lexicographic and the Prim-order OIFT agree."""
+    d = np.load(path)
+    f = d["blend_image"]
+    seeds, sl = d["seeds"], d["seed_labels"]
+    pol, K, adj = float(d["pol"]), int(d["sweeps"]), int(d["adjacency"])
+    lab0 = np.full(f.size, -1, np.int32)
+    lab0[seeds] = sl
+    p = roift.make_params(f.shape, adjacency=adj, weight_mode="blend_q", blend_a=0.6, pol=pol,
+                          sweeps=K)
+    got, _, _, _, _ = roift._ctx().run_host(p, f.reshape(-1), lab0.copy(), seeds)
+    g = O.sobel_normalized(f)
+    _, lab_r2, _ = O.oift_fmax_blend(f, g, 0.6, adj, seeds, sl, pol=pol)
+    exp, _ = O.relax_blend(f, g, 0.6, adj, seeds, lab_r2, K, pol)
+    assert np.array_equal(got, exp)
+    if np.array_equal(lab_r2, d["ref_blend_oift_label"]):
+        assert np.array_equal(got, d["ref_blend_relax_label"])
