@@ -72,6 +72,19 @@ __device__ __forceinline__ unsigned long long vload(const volatile unsigned long
     return *p;
 }
 
+// Release / acquire fence at GPU scope: orders this warp's earlier memory operations (and
+// those of the lanes synchronised with it) before its later ones, without the total order
+// of a sequentially consistent fence.
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;\n" ::: "memory"); }
+// Exchange with acquire semantics at GPU scope: the writes released before the value that
+// it takes are visible to this warp's later reads.
+__device__ __forceinline__ unsigned long long exch_acquire_gpu(unsigned long long *p,
+                                                               unsigned long long v) {
+    unsigned long long old;
+    asm volatile("atom.acquire.gpu.exch.b64 %0, [%1], %2;\n" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+
 // Asynchronous global -> shared copies (cp.async): 16 bytes through L2 only, 4 bytes.
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -190,13 +203,13 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         __syncwarp();
         const uint32_t m = *(volatile uint32_t *)rmask;
         if (m == 0u) return;
-        __threadfence();  // every lane's key updates precede the mailbox bits
         __syncwarp();
         if (lane == 0) {
-            atomicAdd(&A.g->outstanding[par], __popc(m));
-            __threadfence();
             *rmask = 0u;
+            atomicAdd(&A.g->outstanding[par], __popc(m));
         }
+        // every lane's key updates and the raised count precede the mailbox bits
+        fence_acq_rel_gpu();
         __syncwarp();
         bool dup = false;
         if (lane < 6 && ((m >> lane) & 1u)) {
@@ -959,13 +972,13 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     {
         const uint32_t m = *(volatile uint32_t *)rmask;
         if (m != 0u) {
-            __threadfence();
             __syncwarp();
             if (lane == 0) {
-                atomicAdd(&A.g->outstanding[par], __popc(m));
-                __threadfence();
                 *rmask = 0u;
+                atomicAdd(&A.g->outstanding[par], __popc(m));
             }
+            // every lane's key updates and the raised count precede the mailbox bits
+            fence_acq_rel_gpu();
             __syncwarp();
             bool dup = false;
             if (lane < 27 && ((m >> lane) & 1u)) {
@@ -1103,7 +1116,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 steps++;
             }
         }
-        __threadfence();
+        fence_acq_rel_gpu();
         __syncwarp();
         if (lane == 0) atomicSub(&g->outstanding[par], 1);
         const long long t_p0 = clock64();
@@ -1117,13 +1130,13 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             int word = -1;
             if (lane < A.mbox_words) {
                 if (*(volatile unsigned long long *)&mybox[lane]) {
-                    bits = atomicExch(&mybox[lane], 0ull);
+                    bits = exch_acquire_gpu(&mybox[lane], 0ull);
                     word = lane;
                 }
             }
             const uint32_t have = __ballot_sync(FULL, bits != 0ull);
             if (have) {
-                __threadfence();
+                __syncwarp();
                 const long long tb = clock64();
                 for (uint32_t hv = have; hv; hv &= hv - 1) {
                     const int src = __ffs(hv) - 1;
@@ -1143,7 +1156,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                             process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey,
                                                  sw, shx, shy, shz, wl, nfm, rmask, cyc_tile);
                         steps++;
-                        __threadfence();
+                        fence_acq_rel_gpu();  // the tile step's writes precede the count
                         __syncwarp();
                         if (lane == 0) atomicSub(&g->outstanding[par], 1);
                     }

@@ -4,42 +4,6 @@
 
 namespace oiftb {
 
-template <int C, bool PERCLASS, bool BLEND>
-__device__ __forceinline__ void relax_accumulate(const RelaxArgs &a, int ip, int iq, int gp,
-                                                 int gq, const float (&mq)[C], float dpq,
-                                                 float &sw, float (&acc)[C]) {
-    float w = fabsf((float)(ip - iq));
-    if (BLEND)  // wf = alpha |dI| + (1 - alpha)(g_p + g_q) * 0.5f (exp_gradient_weight.cpp:403-405)
-        w = __fadd_rn(__fmul_rn(a.alpha, w),
-                      __fmul_rn(__fsub_rn(1.0f, a.alpha), __fmul_rn((float)(gp + gq), 0.5f)));
-    float per_pq;
-    if (PERCLASS) {
-        per_pq = 0.0f;
-#pragma unroll
-        for (int k = 0; k < C; k++) per_pq = __fadd_rn(per_pq, __fmul_rn(a.pcm[k], mq[k]));
-    } else {
-        float pbg = mq[0];
-#pragma unroll
-        for (int k = 1; k < C; k++)
-            if (k == a.bg) pbg = mq[k];
-        per_pq = __fmul_rn(a.per, __fsub_rn(__fmul_rn(2.0f, pbg), 1.0f));
-    }
-    if (ip > iq)
-        w = __fmul_rn(w, __fadd_rn(1.0f, div100_rn(per_pq)));
-    else if (ip < iq)
-        w = __fmul_rn(w, __fsub_rn(1.0f, div100_rn(per_pq)));
-    if (BLEND && w < 0.0f) w = 0.0f;
-    w = __fsub_rn(a.Wmax, w);
-    if (w < 0.0f) w = 0.0f;
-    w = __fmul_rn(w, w);
-    w = __fmul_rn(w, w);
-    w = __fmul_rn(w, w);
-    if (dpq != 1.0f) w = __fdiv_rn(w, dpq);
-    sw = __fadd_rn(sw, w);
-#pragma unroll
-    for (int k = 0; k < C; k++) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, mq[k]));
-}
-
 // ------------------------------------------------------------------------------------
 // Tile relaxation with exact skipping.
 //
@@ -54,10 +18,58 @@ constexpr int RT_X = 32, RT_Y = 8, RT_Z = 4;
 constexpr int RH_X = RT_X + 2, RH_Y = RT_Y + 2, RH_Z = RT_Z + 2;
 constexpr int RH_N = RH_X * RH_Y * RH_Z;
 
+// Polarity factors of the arcs that end at q: (1 + per_pq / 100, 1 - per_pq / 100), with
+// per_pq = per (2 m_bg(q) - 1) (gft_ift.cpp:8804-8811) or sum_k per_k m_k(q) per class
+// (9076-9079).  They depend on q alone, so a tile computes them once per staged voxel.
+template <int C, bool PERCLASS>
+__device__ __forceinline__ float2 relax_polarity_factors(const RelaxArgs &a, const float *sm,
+                                                         int i) {
+    float per_pq;
+    if (PERCLASS) {
+        per_pq = 0.0f;
+#pragma unroll
+        for (int k = 0; k < C; k++) per_pq = __fadd_rn(per_pq, __fmul_rn(a.pcm[k], sm[k * RH_N + i]));
+    } else {
+        float pbg = sm[i];
+#pragma unroll
+        for (int k = 1; k < C; k++)
+            if (k == a.bg) pbg = sm[k * RH_N + i];
+        per_pq = __fmul_rn(a.per, __fsub_rn(__fmul_rn(2.0f, pbg), 1.0f));
+    }
+    const float d = div100_rn(per_pq);
+    return make_float2(__fadd_rn(1.0f, d), __fsub_rn(1.0f, d));
+}
+
+// One arc p <- q of the sweep: w = ((Wmax - w_or)^8) / Dpq, in the C++ operation order.
+template <int C, bool BLEND>
+__device__ __forceinline__ void relax_accumulate(const RelaxArgs &a, int ip, int iq, int gp,
+                                                 int gq, const float (&mq)[C], float2 fq,
+                                                 float dpq, float &sw, float (&acc)[C]) {
+    float w = fabsf((float)(ip - iq));
+    if (BLEND)  // wf = alpha |dI| + (1 - alpha)(g_p + g_q) * 0.5f (exp_gradient_weight.cpp:403-405)
+        w = __fadd_rn(__fmul_rn(a.alpha, w),
+                      __fmul_rn(__fsub_rn(1.0f, a.alpha), __fmul_rn((float)(gp + gq), 0.5f)));
+    if (ip > iq)
+        w = __fmul_rn(w, fq.x);
+    else if (ip < iq)
+        w = __fmul_rn(w, fq.y);
+    if (BLEND && w < 0.0f) w = 0.0f;
+    w = __fsub_rn(a.Wmax, w);
+    if (w < 0.0f) w = 0.0f;
+    w = __fmul_rn(w, w);
+    w = __fmul_rn(w, w);
+    w = __fmul_rn(w, w);
+    if (dpq != 1.0f) w = __fdiv_rn(w, dpq);
+    sw = __fadd_rn(sw, w);
+#pragma unroll
+    for (int k = 0; k < C; k++) acc[k] = __fadd_rn(acc[k], __fmul_rn(w, mq[k]));
+}
+
+
 // Tiles holding a voxel with a differently-labelled neighbour get distance 0.
 template <int C, typename T, bool PERCLASS, int ADJ, bool INTERIOR, bool BLEND>
 __device__ __forceinline__ void relax_tile_voxels(const RelaxArgs &a, const float *sm,
-                                                  const int *si, const int *sg,
+                                                  const int *si, const int *sg, const float2 *sf,
                                                   float *__restrict__ mout,
                                                   const uint8_t *__restrict__ seedc, int x,
                                                   int y, int z0, int lx, int ly) {
@@ -95,8 +107,8 @@ __device__ __forceinline__ void relax_tile_voxels(const RelaxArgs &a, const floa
 #pragma unroll
             for (int k = 0; k < C; k++) mq[k] = sm[k * RH_N + hq];
             const float dpq = (ADJ == 6) ? 1.0f : a.dpq[i];
-            relax_accumulate<C, PERCLASS, BLEND>(a, ip, si[hq], BLEND ? sg[hc] : 0,
-                                                 BLEND ? sg[hq] : 0, mq, dpq, sw, acc);
+            relax_accumulate<C, BLEND>(a, ip, si[hq], BLEND ? sg[hc] : 0, BLEND ? sg[hq] : 0, mq,
+                                       sf[hq], dpq, sw, acc);
         }
         const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
         float out[C];
@@ -131,6 +143,7 @@ __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict
     float *sm = reinterpret_cast<float *>(rsm);          // [C][RH_Z][RH_Y][RH_X]
     int *si = reinterpret_cast<int *>(sm + C * RH_N);    // [RH_Z][RH_Y][RH_X]
     int *sg = si + RH_N;                                 // gradient halo (BLEND only)
+    float2 *sf = reinterpret_cast<float2 *>(si + (BLEND ? 2 : 1) * RH_N);  // polarity factors
     const int X = a.X, Y = a.Y, Z = a.Z;
     const size_t N = a.N, XY = (size_t)X * Y;
     const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
@@ -147,6 +160,13 @@ __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict
             if (BLEND) sg[i] = __ldg(&a.gmap[g]);
         }
     }
+    // each thread reads back only the staged voxels it wrote itself
+    for (int i = tid; i < RH_N; i += 256) {
+        const int hx = i % RH_X, hy = (i / RH_X) % RH_Y, hz = i / (RH_X * RH_Y);
+        const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+        if (gx >= 0 && gx < X && gy >= 0 && gy < Y && gz >= 0 && gz < Z)
+            sf[i] = relax_polarity_factors<C, PERCLASS>(a, sm, i);
+    }
     __syncthreads();
     const int lx = threadIdx.x, ly = threadIdx.y;
     const int x = x0 + lx, y = y0 + ly;
@@ -155,10 +175,10 @@ __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict
     const bool interior = x0 >= 1 && x0 + RT_X < X && y0 >= 1 && y0 + RT_Y < Y && z0 >= 1 &&
                           z0 + RT_Z < Z;
     if (interior)
-        relax_tile_voxels<C, T, PERCLASS, ADJ, true, BLEND>(a, sm, si, sg, mout, seedc, x, y, z0,
+        relax_tile_voxels<C, T, PERCLASS, ADJ, true, BLEND>(a, sm, si, sg, sf, mout, seedc, x, y, z0,
                                                             lx, ly);
     else
-        relax_tile_voxels<C, T, PERCLASS, ADJ, false, BLEND>(a, sm, si, sg, mout, seedc, x, y, z0,
+        relax_tile_voxels<C, T, PERCLASS, ADJ, false, BLEND>(a, sm, si, sg, sf, mout, seedc, x, y, z0,
                                                              lx, ly);
 }
 

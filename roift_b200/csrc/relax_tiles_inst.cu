@@ -15,13 +15,13 @@ static cudaError_t launch_tile_c(const float *in, float *out, const T *img, cons
     dim3 block(32, 8);
     if (a.blend) {  // gradient blend: 6 / 4 neighbourhood, global polarity
         if (ADJ != 6 || perclass) return cudaErrorInvalidValue;
-        const size_t smem = (size_t)(C + 2) * RH_N * 4;
+        const size_t smem = (size_t)(C + 2) * RH_N * 4 + (size_t)RH_N * 8;
         auto k = relax_tile_kernel<C, T, false, 6, true>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<ntiles, block, smem, s>>>(in, out, img, seedc, tdist, sweep, a, ntx, nty);
         return cudaGetLastError();
     }
-    const size_t smem = (size_t)(C + 1) * RH_N * 4;
+    const size_t smem = (size_t)(C + 1) * RH_N * 4 + (size_t)RH_N * 8;
     if (perclass) {
         auto k = relax_tile_kernel<C, T, true, ADJ, false>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
