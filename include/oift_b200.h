@@ -56,9 +56,14 @@ typedef enum {
     OIFT_W_GRAD = 0,    /* |I_p - I_q| exactly (<= 16383, else OIFT_E_RANGE) */
     OIFT_W_GRAD_Q = 1,  /* min(|I_p - I_q|, wq); clamp events counted */
     OIFT_W_RBF_Q = 2,   /* floor(wq*(1 - exp(-d^2/(2 sigma^2))) + 0.5), host LUT */
-    OIFT_W_BLEND_Q = 3  /* float a|dI| + (1-a)(g_p+g_q)/2, g = Sobel map scaled to max I
+    OIFT_W_BLEND_Q = 3, /* float a|dI| + (1-a)(g_p+g_q)/2, g = Sobel map scaled to max I
                            (experiments/exp_gradient_weight.cpp:244-254, 596-608); 6 / 4
                            adjacency, global polarity, image in 0..65535 */
+    OIFT_W_IMAGEGRAPH = 4  /* 2D image graph (gft_imagegraph.cpp:13-47, 981-1016): |dI| + 1
+                              oriented as MAX(ROUND(w (1 +/- per/100)), 1) with per/100 held
+                              in a float; relaxation = ORelax_1(sImageGraph) (gft_ift.cpp:
+                              7683-7847): one membership channel from label / max label,
+                              binary labels.  zsize == 1, adjacency 4 or 8, global polarity */
 } oift_weight_mode;
 
 typedef struct oift_b200_ctx oift_b200_ctx;

@@ -83,6 +83,19 @@ def lib():
         L.or_relax_blend_f32.argtypes = [_i32p, _i32p, C.c_float, C.c_int, C.c_int, C.c_int,
                                          C.c_int, C.c_float, _i32p, C.c_int, _i32p, C.c_int,
                                          C.c_void_p]
+        L.or_oift_fmax_imagegraph.restype = C.c_int
+        L.or_oift_fmax_imagegraph.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _Polarity,
+                                              _i32p, C.c_int, _i32p, _i32p, _i32p, C.c_void_p]
+        L.or_oift_prim_imagegraph.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _Polarity,
+                                              C.c_int, _i32p, C.c_int, _i32p, C.c_void_p,
+                                              C.c_void_p, C.c_void_p]
+        L.or_imagegraph_wmax.restype = C.c_int
+        L.or_imagegraph_wmax.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_float]
+        L.or_energy_imagegraph.restype = C.c_int
+        L.or_energy_imagegraph.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_float, _i32p,
+                                           C.c_int]
+        L.or_relax_imagegraph_f32.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_float,
+                                              _i32p, C.c_int, _i32p, C.c_int, C.c_void_p]
         L.or_adjacency.restype = C.c_int
         L.or_adjacency.argtypes = [C.c_int, _i32p, _i32p, _i32p]
         L.or_conditional_dilation.restype = C.c_longlong
@@ -125,6 +138,12 @@ def ref():
         R.ref_sobel_normalized.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, _i32p]
         R.ref_gradweight.argtypes = [_i32p, _i32p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                      _i32p, C.c_int, _i32p, C.c_int]
+        R.ref_imagegraph.restype = C.c_int
+        R.ref_imagegraph.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_float, _i32p, C.c_int,
+                                     _i32p, C.c_int]
+        R.ref_imagegraph_energy.restype = C.c_int
+        R.ref_imagegraph_energy.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_float, _i32p,
+                                            C.c_int]
         R.ref_coarse_to_fine.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_int, C.c_float, _i32p, C.c_int, _i32p]
         R.ref_oiftrelax_chain.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_double,
@@ -434,6 +453,69 @@ def relax_blend(img, g, alpha, adj, seeds, label, ntimes, pol):
     return lab, mem.reshape(nc, N)
 
 
+def _ig_dims(img):
+    X, Y, Z = _dims(img)
+    assert Z == 1, "the image graph is 2D"
+    return X, Y
+
+
+def imagegraph_wmax(img, adj, pol):
+    """sg->Wmax of Orient2Digraph on ByEuclideanDistance(img, r) (4: r = 1, 8: r = 1.5)."""
+    X, Y = _ig_dims(img)
+    return int(lib().or_imagegraph_wmax(as_i32(img), X, Y, adj, float(np.float32(pol * 100.0))))
+
+
+def oift_fmax_imagegraph(img, adj, seeds, seed_labels, pol, want_pred=False):
+    """R2 with the oriented image-graph weights: (cost, label, levels[, pred])."""
+    X, Y = _ig_dims(img)
+    N = X * Y
+    lab_in = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab_in[seeds] = seed_labels
+    cost = np.empty(N, np.int32)
+    label = np.empty(N, np.int32)
+    pred = np.empty(N, np.int32) if want_pred else None
+    P, keep = polarity(pol)
+    levels = lib().or_oift_fmax_imagegraph(as_i32(img), X, Y, adj, P, seeds, len(seeds), lab_in,
+                                           cost, label,
+                                           pred.ctypes.data if pred is not None else None)
+    return (cost, label, levels, pred) if want_pred else (cost, label, levels)
+
+
+def oift_prim_imagegraph(img, adj, seeds, seed_labels, pol):
+    """R1 on the oriented image graph (OIFT(sImageGraph), seeds queued in the given order):
+    (label, value, pred, fmax)."""
+    X, Y = _ig_dims(img)
+    N = X * Y
+    lab = np.full(N, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    val, pred, fmax = (np.empty(N, np.int32) for _ in range(3))
+    P, keep = polarity(pol)
+    lib().or_oift_prim_imagegraph(as_i32(img), X, Y, adj, P, imagegraph_wmax(img, adj, pol),
+                                  seeds, len(seeds), lab, val.ctypes.data, pred.ctypes.data,
+                                  fmax.ctypes.data)
+    return lab, val, pred, fmax
+
+
+def energy_imagegraph(img, adj, label, pol, lb=1):
+    """GetEnergy_Min(sImageGraph) restated: the cut energy of label lb."""
+    X, Y = _ig_dims(img)
+    return int(lib().or_energy_imagegraph(as_i32(img), X, Y, adj, float(np.float32(pol * 100.0)),
+                                          np.ascontiguousarray(label, np.int32).reshape(-1), lb))
+
+
+def relax_imagegraph(img, adj, seeds, label, ntimes, pol):
+    """ORelax_1(sImageGraph) restated in FP32: (binary labels, memberships [N])."""
+    X, Y = _ig_dims(img)
+    lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    m = np.empty(X * Y, np.float32)
+    lib().or_relax_imagegraph_f32(as_i32(img), X, Y, adj, float(np.float32(pol * 100.0)), seeds,
+                                  len(seeds), lab, int(ntimes), m.ctypes.data)
+    return lab, m
+
+
 def gaussian_blur(img):
     X, Y, Z = _dims(img)
     out = np.empty(X * Y * Z, np.int32)
@@ -569,6 +651,26 @@ def ref_gradweight(img, g, alpha, seeds, seed_labels, pol, ntimes):
     ref().ref_gradweight(as_i32(img), as_i32(g), X, Y, Z, float(np.float32(pol * 100.0)),
                          float(alpha), seeds, len(seeds), lab, int(ntimes))
     return lab
+
+
+def ref_imagegraph(img, adj, seeds, seed_labels, pol, ntimes=0):
+    """The reference 2D pipeline: ByEuclideanDistance + Orient2Digraph, OIFT(sImageGraph)
+    with every labelled pixel as a seed, ORelax_1(sImageGraph) when ntimes > 0:
+    (labels, Wmax)."""
+    X, Y = _ig_dims(img)
+    lab = np.full(X * Y, NIL, np.int32)
+    seeds = np.ascontiguousarray(seeds, np.int32)
+    lab[seeds] = seed_labels
+    wmax = ref().ref_imagegraph(as_i32(img), X, Y, adj, float(np.float32(pol * 100.0)), seeds,
+                                len(seeds), lab, int(ntimes))
+    return lab, int(wmax)
+
+
+def ref_imagegraph_energy(img, adj, label, pol, lb=1):
+    """GetEnergy_Min(sImageGraph) of a label map on the reference's oriented image graph."""
+    X, Y = _ig_dims(img)
+    return int(ref().ref_imagegraph_energy(as_i32(img), X, Y, adj, float(np.float32(pol * 100.0)),
+                                           np.ascontiguousarray(label, np.int32).reshape(-1), lb))
 
 
 def ref_gaussian_blur(img):

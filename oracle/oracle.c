@@ -133,11 +133,34 @@ static inline int blend_weight(const int *img, const int *g, float alpha, size_t
     return w;
 }
 
-/* Where arc weights come from: edge-code planes W, or the blend of image and gradient. */
+/* Arc p -> q of the 2D image graph, oriented from p's side with alpha = per/100 held in a
+ * float: val = |I_p - I_q| + 1 (ImageGraph::ByEuclideanDistance, gft/src/gft_imagegraph.cpp:
+ * 13-47), MAX(ROUND(val * (1.0 + alpha)), 1) if I_p > I_q, MAX(ROUND(val * (1.0 - alpha)), 1)
+ * if I_p < I_q, val otherwise (Orient2Digraph, gft_imagegraph.cpp:981-1016; ROUND is
+ * gft/include/gft_common.h:120). */
+static inline int ig_link(const int *img, size_t p, size_t q, float alpha) {
+    int val = abs(img[p] - img[q]) + 1;
+    double x;
+    if (img[p] > img[q])
+        x = val * (1.0 + alpha);
+    else if (img[p] < img[q])
+        x = val * (1.0 - alpha);
+    else
+        return val;
+    int w = (x < 0) ? (int)(x - 0.5) : (int)(x + 0.5);
+    return w > 1 ? w : 1;
+}
+
+/* Alpha of a polarity given x100, as Orient2Digraph computes it: float alpha = per/100.0. */
+static inline float ig_alpha(float per) { return (float)(per / 100.0); }
+
+/* Where arc weights come from: edge-code planes W, the blend of image and gradient, or (ig)
+ * the oriented image graph. */
 typedef struct {
     const uint16_t *W;
     const int *img, *g;
     float alpha;
+    int ig;
 } wsrc;
 
 /* Arc weight p -> q where q = p + d_i.  For i in the positive half the edge lives in
@@ -162,6 +185,10 @@ static inline int arc_weight_codes(const uint16_t *W, size_t N, int n, int i, si
 
 static inline int arc_weight(const wsrc *ws, size_t N, int n, int i, size_t p, size_t q,
                              float pol) {
+    /* OIFT(sImageGraph) (gft/src/gft_ift.cpp:1358-1439) takes n_link[p] for an object tail
+     * and the transposed arc n_link[q] for a background tail: the arc from p's side with
+     * the tail label's polarity (-per for label 0) */
+    if (ws->ig) return ig_link(ws->img, p, q, ig_alpha(pol));
     if (ws->img) return blend_weight(ws->img, ws->g, ws->alpha, p, q, pol);
     return arc_weight_codes(ws->W, N, n, i, p, q, pol);
 }
@@ -277,6 +304,14 @@ int or_oift_fmax_blend(const int *img, const int *g, float alpha, int X, int Y, 
                        int *cost, int *label) {
     wsrc ws = {NULL, img, g, alpha};
     return fmax_core(&ws, X, Y, Z, adj, pol, seeds, nseeds, label_in, cost, label, NULL);
+}
+
+/* R2 with the weights of the oriented 2D image graph. */
+int or_oift_fmax_imagegraph(const int *img, int X, int Y, int adj, or_polarity pol,
+                            const int *seeds, int nseeds, const int *label_in, int *cost,
+                            int *label, int *pred) {
+    wsrc ws = {NULL, img, NULL, 0.0f, 1};
+    return fmax_core(&ws, X, Y, 1, adj, pol, seeds, nseeds, label_in, cost, label, pred);
 }
 
 /* ------------------------------------------------------- R1: Prim / Dial queue --- */
@@ -429,6 +464,155 @@ void or_oift_prim_blend(const int *img, const int *g, float alpha, int X, int Y,
                         int *label) {
     wsrc ws = {NULL, img, g, alpha};
     prim_core(&ws, X, Y, Z, adj, pol, wmax_buckets, seeds, nseeds, label, NULL, NULL, NULL);
+}
+
+/* R1 on the oriented 2D image graph: OIFT(sImageGraph) (gft/src/gft_ift.cpp:1358-1439),
+ * Dial queue of Wmax + 2 buckets, FIFO ties. */
+void or_oift_prim_imagegraph(const int *img, int X, int Y, int adj, or_polarity pol,
+                             int wmax, const int *seeds, int nseeds, int *label, int *value_out,
+                             int *pred_out, int *fmax_out) {
+    wsrc ws = {NULL, img, NULL, 0.0f, 1};
+    prim_core(&ws, X, Y, 1, adj, pol, wmax, seeds, nseeds, label, value_out, pred_out, fmax_out);
+}
+
+/* sg->Wmax after Orient2Digraph (gft_imagegraph.cpp:981-1016): the largest oriented arc
+ * weight over every in-image arc p -> q, seen from p with the global alpha; 0 without arcs. */
+int or_imagegraph_wmax(const int *img, int X, int Y, int adj, float per) {
+    int dx[26], dy[26], dz[26];
+    int n = or_adjacency(adj, dx, dy, dz);
+    float alpha = ig_alpha(per);
+    int wmax = 0;
+    for (int y = 0; y < Y; y++)
+        for (int x = 0; x < X; x++)
+            for (int i = 0; i < n; i++) {
+                if (dz[i] != 0) continue;
+                int qx = x + dx[i], qy = y + dy[i];
+                if (qx < 0 || qx >= X || qy < 0 || qy >= Y) continue;
+                int w = ig_link(img, (size_t)x + (size_t)y * X, (size_t)qx + (size_t)qy * X, alpha);
+                if (w > wmax) wmax = w;
+            }
+    return wmax;
+}
+
+/* GetEnergy_Min(sImageGraph, label, lb) (gft/src/gft_ift.cpp:287-319): the smallest
+ * oriented weight n_link[p] (global alpha, seen from p) over the arcs p -> q that leave
+ * label lb; INT_MAX without such an arc. */
+int or_energy_imagegraph(const int *img, int X, int Y, int adj, float per, const int *label,
+                         int lb) {
+    int dx[26], dy[26], dz[26];
+    int n = or_adjacency(adj, dx, dy, dz);
+    float alpha = ig_alpha(per);
+    int e = INT_MAX;
+    for (int y = 0; y < Y; y++)
+        for (int x = 0; x < X; x++) {
+            size_t p = (size_t)x + (size_t)y * X;
+            if (label[p] != lb) continue;
+            for (int i = 0; i < n; i++) {
+                if (dz[i] != 0) continue;
+                int qx = x + dx[i], qy = y + dy[i];
+                if (qx < 0 || qx >= X || qy < 0 || qy >= Y) continue;
+                size_t q = (size_t)qx + (size_t)qy * X;
+                if (label[q] == lb) continue;
+                int w = ig_link(img, p, q, alpha);
+                if (w < e) e = w;
+            }
+        }
+    return e;
+}
+
+/* ORelax_1(sImageGraph) (gft/src/gft_ift.cpp:7683-7847) in FP32: one membership value per
+ * pixel, label / Imax at the start and at the seeds after every sweep; the mask starts at
+ * the pixels with a differently-labelled neighbour and grows one ring after every sweep
+ * but the last; a mask pixel takes sum(w m_q) / sum(w) over its neighbours with
+ * w = (Wmax - n_link)^8, where n_link is the arc p -> q when m_q < 0.5 and q -> p
+ * otherwise; the result is 1 where m >= 0.5 (and where it is NaN), else 0.  label is
+ * replaced by that result and m_out receives the final memberships. */
+void or_relax_imagegraph_f32(const int *img, int X, int Y, int adj, float per,
+                             const int *seeds, int nseeds, int *label, int ntimes,
+                             float *m_out) {
+    int dx[26], dy[26], dz[26];
+    int n0 = or_adjacency(adj, dx, dy, dz), n = 0;
+    int ox[8], oy[8];
+    for (int i = 0; i < n0; i++)
+        if (dz[i] == 0) {
+            ox[n] = dx[i];
+            oy[n] = dy[i];
+            n++;
+        }
+    size_t N = (size_t)X * Y;
+    float alpha = ig_alpha(per);
+    int wmax = or_imagegraph_wmax(img, X, Y, adj, per);
+    int imax = label[0];
+    for (size_t p = 1; p < N; p++) imax = label[p] > imax ? label[p] : imax;
+    float *f1 = (float *)malloc(sizeof(float) * N), *f2 = (float *)malloc(sizeof(float) * N);
+    unsigned char *mask = (unsigned char *)calloc(N, 1);
+    int *nodes = (int *)malloc(sizeof(int) * N);
+    size_t nn = 0;
+    for (size_t p = 0; p < N; p++) {
+        f1[p] = (float)label[p] / (float)imax;
+        int px = (int)(p % X), py = (int)(p / X);
+        for (int i = 0; i < n; i++) {
+            int qx = px + ox[i], qy = py + oy[i];
+            if (qx < 0 || qx >= X || qy < 0 || qy >= Y) continue;
+            if (label[p] != label[qx + qy * X]) {
+                mask[p] = 1;
+                nodes[nn++] = (int)p;
+                break;
+            }
+        }
+    }
+    size_t ninic = 0;
+    while (ntimes > 0) {
+        memcpy(f2, f1, sizeof(float) * N);
+        for (size_t j = 0; j < nn; j++) {
+            int p = nodes[j], px = p % X, py = p / X;
+            float acc = 0.0f, sw = 0.0f;
+            for (int i = 0; i < n; i++) {
+                int qx = px + ox[i], qy = py + oy[i];
+                if (qx < 0 || qx >= X || qy < 0 || qy >= Y) continue;
+                int q = qx + qy * X;
+                float w = (f1[q] < 0.5f) ? (float)ig_link(img, (size_t)p, (size_t)q, alpha)
+                                         : (float)ig_link(img, (size_t)q, (size_t)p, alpha);
+                w = (float)wmax - w;
+                w = w * w;
+                w = w * w;
+                w = w * w;
+                sw += w;
+                acc += w * f1[q];
+            }
+            f2[p] = acc / sw;
+        }
+        float *t = f1;
+        f1 = f2;
+        f2 = t;
+        for (int i = 0; i < nseeds; i++) f1[seeds[i]] = (float)label[seeds[i]] / (float)imax;
+        ntimes--;
+        if (ntimes > 0) {
+            size_t last = nn;
+            for (size_t j = ninic; j < nn; j++) {
+                int p = nodes[j], px = p % X, py = p / X;
+                for (int i = 0; i < n; i++) {
+                    int qx = px + ox[i], qy = py + oy[i];
+                    if (qx < 0 || qx >= X || qy < 0 || qy >= Y) continue;
+                    int q = qx + qy * X;
+                    if (!mask[q]) {
+                        mask[q] = 1;
+                        nodes[last++] = q;
+                    }
+                }
+            }
+            ninic = nn;
+            nn = last;
+        }
+    }
+    for (size_t p = 0; p < N; p++) {
+        label[p] = (f1[p] < 0.5f) ? 0 : 1;
+        if (m_out) m_out[p] = f1[p];
+    }
+    free(f1);
+    free(f2);
+    free(mask);
+    free(nodes);
 }
 
 /* R4: gft/src/gft_ift.cpp:287-319 (GetEnergy_Min) in 3D with OIFT_Multi's oriented

@@ -117,6 +117,21 @@ int or_relax_blend_f32(const int *img, const int *g, float alpha, int X, int Y, 
                        float per, const int *seeds, int nseeds, int *label, int ntimes,
                        float *membership);
 
+/* The oriented 2D image graph (gft_imagegraph.cpp:13-47, 981-1016): R2 and R1 with its
+ * arc weights, its Wmax, and ORelax_1(sImageGraph) in FP32 (gft_ift.cpp:7683-7847). */
+int or_oift_fmax_imagegraph(const int *img, int X, int Y, int adj, or_polarity pol,
+                            const int *seeds, int nseeds, const int *label_in, int *cost,
+                            int *label, int *pred);
+void or_oift_prim_imagegraph(const int *img, int X, int Y, int adj, or_polarity pol,
+                             int wmax, const int *seeds, int nseeds, int *label, int *value_out,
+                             int *pred_out, int *fmax_out);
+int or_imagegraph_wmax(const int *img, int X, int Y, int adj, float per);
+int or_energy_imagegraph(const int *img, int X, int Y, int adj, float per, const int *label,
+                         int lb);
+void or_relax_imagegraph_f32(const int *img, int X, int Y, int adj, float per,
+                             const int *seeds, int nseeds, int *label, int ntimes,
+                             float *m_out);
+
 /* oiftrelax.cpp:87-169 conditional dilation (label in/out); returns voxels relabelled. */
 long long or_conditional_dilation(const int *img, int *label, int X, int Y, int Z,
                                   float radius, float percentile);

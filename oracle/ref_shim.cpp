@@ -15,6 +15,12 @@
 //   ref_energy_min_graph      -> gft::ift::GetEnergy_Min(sGraph*) (gft/src/gft_ift.cpp:4xx)
 //   ref_dilation_conditional  -> dilation_conditional             (oiftrelax.cpp:149-165)
 //   ref_inject_boundary_seeds -> inject_boundary_seeds            (oiftrelax.cpp:175-224)
+//   ref_imagegraph            -> ImageGraph::ByEuclideanDistance + Orient2Digraph
+//                                (gft/src/gft_imagegraph.cpp:13-47, 981-1016), then
+//                                ift::OIFT(sImageGraph*) with S = NULL and, for ntimes > 0,
+//                                ift::ORelax_1(sImageGraph*) (gft/src/gft_ift.cpp:1358-1439,
+//                                7683-7847): the 2D pipeline of gft_ift.cpp:9575-9682, 9785-9790
+//   ref_imagegraph_energy     -> ift::GetEnergy_Min(sImageGraph*) (gft/src/gft_ift.cpp:287-319)
 //   ref_oiftrelax_chain       -> the processing chain of the CLI main (oiftrelax.cpp:
 //                                263-268, 368-414): shift, GaussianBlur x2, OIFT_Multi,
 //                                ORelax_1_Multi, conditional dilation when binary
@@ -200,4 +206,49 @@ REF_API void ref_oiftrelax_chain(const int *img, int X, int Y, int Z, double pol
     Scene32::Destroy(&lab);
     Scene32::Destroy(&fscn);
 }
+static sImageGraph *make_imagegraph(const int *img, int X, int Y, int adj, float per,
+                                    sImage32 **im_out) {
+    sImage32 *im = Image32::Create(X, Y);
+    std::memcpy(im->data, img, sizeof(int) * (size_t)X * Y);
+    sImageGraph *sg = ImageGraph::ByEuclideanDistance(im, adj == 8 ? 1.5f : 1.0f);
+    ImageGraph::Orient2Digraph(sg, im, per);
+    *im_out = im;
+    return sg;
+}
+
+// label: in, NIL (-1) except at the seeds; out, the OIFT labels, or the binary relaxed
+// labels when ntimes > 0.  Returns sg->Wmax.
+REF_API int ref_imagegraph(const int *img, int X, int Y, int adj, float per, const int *seeds,
+                           int nseeds, int *label, int ntimes) {
+    sImage32 *im = nullptr;
+    sImageGraph *sg = make_imagegraph(img, X, Y, adj, per, &im);
+    sImage32 *lab = Image32::Create(X, Y);
+    std::memcpy(lab->data, label, sizeof(int) * (size_t)X * Y);
+    ift::OIFT(sg, nullptr, lab);
+    if (ntimes > 0) {
+        int *S = make_S(seeds, nseeds);
+        ift::ORelax_1(sg, S, lab, ntimes);
+        free(S);
+    }
+    std::memcpy(label, lab->data, sizeof(int) * (size_t)X * Y);
+    const int wmax = sg->Wmax;
+    Image32::Destroy(&lab);
+    ImageGraph::Destroy(&sg);
+    Image32::Destroy(&im);
+    return wmax;
+}
+
+REF_API int ref_imagegraph_energy(const int *img, int X, int Y, int adj, float per,
+                                  const int *label, int lb) {
+    sImage32 *im = nullptr;
+    sImageGraph *sg = make_imagegraph(img, X, Y, adj, per, &im);
+    sImage32 *lab = Image32::Create(X, Y);
+    std::memcpy(lab->data, label, sizeof(int) * (size_t)X * Y);
+    const int e = ift::GetEnergy_Min(sg, lab, lb);
+    Image32::Destroy(&lab);
+    ImageGraph::Destroy(&sg);
+    Image32::Destroy(&im);
+    return e;
+}
+
 }  // extern "C"

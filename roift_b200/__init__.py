@@ -28,7 +28,7 @@ STATUS = {0: "OK", -1: "BAD_ARG", -2: "NO_SEEDS", -3: "OOM", -4: "NOT_CONVERGED"
           -5: "QUEUE_OVERFLOW", -6: "CUDA", -7: "RANGE", -8: "UNSUPPORTED", -9: "SEED_RANGE"}
 E_BAD_ARG, E_NO_SEEDS, E_OOM, E_NOT_CONVERGED, E_QUEUE_OVERFLOW = -1, -2, -3, -4, -5
 E_CUDA, E_RANGE, E_UNSUPPORTED, E_SEED_RANGE = -6, -7, -8, -9
-W_MODES = {"grad": 0, "grad_q": 1, "rbf_q": 2, "blend_q": 3}
+W_MODES = {"grad": 0, "grad_q": 1, "rbf_q": 2, "blend_q": 3, "imagegraph": 4}
 
 
 class OiftError(RuntimeError):

@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboift_b200.so")
-SOURCES = ["api.cu", "weights.cu", "oift.cu", "relax.cu", "selftest.cu", "noalloc.cu", "prepost.cu", "adjoint.cu"]
+SOURCES = ["api.cu", "weights.cu", "oift.cu", "relax.cu", "selftest.cu", "noalloc.cu", "prepost.cu", "adjoint.cu", "imagegraph.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]

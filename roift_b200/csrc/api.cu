@@ -47,6 +47,7 @@ struct oift_b200_ctx {
     // adjoint: checkpoints / segment / lambdas / weight sums, mask rings, seed classes, sums
     DevBuf awork, adist, aseedc, asmall, al2c;
     DevBuf gmap;  // normalised Sobel gradient of the gradient-blend weights
+    DevBuf igring, igsmall;  // image-graph relaxation: ring index per pixel, reductions
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -144,7 +145,7 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->dborder, &c->dhist, &c->daux, &c->dlabel, &c->yimg, &c->ylab,
                       &c->yseeds, &c->yslab, &c->yfirst, &c->yup, &c->ymerge, &c->yfseeds,
                       &c->yfslab, &c->yaux, &c->awork, &c->adist, &c->aseedc, &c->asmall,
-                      &c->al2c, &c->gmap};
+                      &c->al2c, &c->gmap, &c->igring, &c->igsmall};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -202,7 +203,7 @@ static int check_params(const oift_b200_params *p) {
     } else if (p->adjacency != 6 && p->adjacency != 26) {
         return OIFT_E_BAD_ARG;
     }
-    if (p->weight_mode < 0 || p->weight_mode > 3) return OIFT_E_BAD_ARG;
+    if (p->weight_mode < 0 || p->weight_mode > OIFT_W_IMAGEGRAPH) return OIFT_E_BAD_ARG;
     if ((p->weight_mode == OIFT_W_GRAD_Q || p->weight_mode == OIFT_W_RBF_Q) &&
         (p->wq <= 0 || p->wq > OIFT_MAX_BASE))
         return OIFT_E_BAD_ARG;
@@ -220,6 +221,13 @@ static int check_params(const oift_b200_params *p) {
         if (p->adjacency != 6 && p->adjacency != 4) return OIFT_E_UNSUPPORTED;
         if (p->per_class) return OIFT_E_UNSUPPORTED;
         if (!(p->blend_a >= 0.0f && p->blend_a <= 1.0f)) return OIFT_E_BAD_ARG;
+    }
+    if (p->weight_mode == OIFT_W_IMAGEGRAPH) {
+        // the 2D image graph of gft_imagegraph.cpp: Circular(1.0) / Circular(1.5), one
+        // global polarity, ring indices of the relaxation in 16 bits
+        if (p->zsize != 1 || (p->adjacency != 4 && p->adjacency != 8)) return OIFT_E_UNSUPPORTED;
+        if (p->per_class) return OIFT_E_UNSUPPORTED;
+        if (p->relax_sweeps >= 0xFFFF) return OIFT_E_BAD_ARG;
     }
     if (p->weight_mode == OIFT_W_RBF_Q && !(p->rbf_sigma > 0.0f)) return OIFT_E_BAD_ARG;
     return OIFT_OK;
@@ -451,6 +459,9 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
     // 26 / 8: the full-neighbourhood OIFT evaluates arc weights from the image itself
     const bool blend = p->weight_mode == OIFT_W_BLEND_Q;
+    const bool ig = p->weight_mode == OIFT_W_IMAGEGRAPH;
+    // exact base weights (|dI|, or |dI| + 1 on the image graph) must fit 14 bits
+    const bool exact = p->weight_mode == OIFT_W_GRAD || ig;
     const bool fulln = p->adjacency == 26 || p->adjacency == 8 || blend;
     OiftPlan plan = fulln ? oift_plan_full(X, Y, Z) : oift_plan(X, Y, Z);
 
@@ -484,7 +495,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     ba.Z = Z;
     ba.planes = planes;
     ba.mode = p->weight_mode;
-    ba.cap = (p->weight_mode == OIFT_W_GRAD) ? OIFT_MAX_BASE : p->wq;
+    ba.cap = exact ? OIFT_MAX_BASE : p->wq;
     for (int k = 0; k < planes; k++) {
         int i = adj.n / 2 + k;
         ba.dx[k] = adj.dx[i];
@@ -516,10 +527,9 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     }
     if (!fulln) {
         CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
-    } else if (p->weight_mode == OIFT_W_GRAD &&
-               (long long)hmm[1] - (long long)hmm[0] > OIFT_MAX_BASE) {
-        // exact gradient weights must fit 14 bits: count the arcs that do not (the planes
-        // are built only for that count)
+    } else if (exact && (long long)hmm[1] - (long long)hmm[0] + (ig ? 1 : 0) > OIFT_MAX_BASE) {
+        // exact base weights must fit 14 bits: count the arcs that do not (the planes are
+        // built only for that count)
         TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
         CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
     }
@@ -566,7 +576,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
                       (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
                       octas, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles,
-                      fulln ? &fn : nullptr);
+                      fulln ? &fn : nullptr, ig);
     if (rc != OIFT_OK) return rc;
     unsigned long long hclamp = 0;
     CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));
@@ -576,14 +586,44 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     const int K = p->relax_sweeps;
     RelaxResult rr;
     bool want_relax = out && (out->label || out->mask || out->membership);
-    if (want_relax) TRY(relax_stage<T>(c, p, d_img, d_seeds, d_slabels, nseeds, d_olab, hmm, out, &rr));
+    int ig_kernels = 0;
+    if (want_relax && ig) {
+        // ORelax_1(sImageGraph): one membership channel, binary labels
+        TRY(grow(c, c->memb, 2 * N * sizeof(float)));
+        TRY(grow(c, c->igring, N * sizeof(uint16_t)));
+        TRY(grow(c, c->seedc, N));
+        TRY(grow(c, c->igsmall, 4 * sizeof(int)));
+        IgRelax R;
+        R.X = X;
+        R.Y = Y;
+        R.adjacency = p->adjacency;
+        R.per = p->per;
+        R.sweeps = K;
+        R.olabel = d_olab;
+        R.seeds = d_seeds;
+        R.nseeds = nseeds;
+        R.m0 = (float *)c->memb.p;
+        R.m1 = R.m0 + N;
+        R.ring = (uint16_t *)c->igring.p;
+        R.seedf = (uint8_t *)c->seedc.p;
+        R.small = (int *)c->igsmall.p;
+        R.label = out->label;
+        R.mask = out->mask;
+        R.membership = out->membership;
+        R.ev_begin = c->ev[6];
+        R.ev_end = c->ev[7];
+        TRY(ig_relax_run<T>(R, d_img, s, c->sms, &ig_kernels));
+        rr.nclasses = 1;
+    } else if (want_relax) {
+        TRY(relax_stage<T>(c, p, d_img, d_seeds, d_slabels, nseeds, d_olab, hmm, out, &rr));
+    }
     const int nclasses = rr.nclasses;
     const long long relax_active = rr.active_voxel_sweeps;
     const int relax_dilations = rr.dilations;
     cudaEventRecord(c->ev[3], s);
     CU(cudaStreamSynchronize(s));
     CU(cudaGetLastError());
-    if (p->weight_mode == OIFT_W_GRAD && hclamp) return OIFT_E_RANGE;
+    if (exact && hclamp) return OIFT_E_RANGE;
     if (st) {
         st->levels = levels;
         st->tile_steps = steps;
@@ -597,7 +637,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         // K sweeps, argmax when relaxing)
         // minmax, build, seeds, persistent OIFT, finalize; relaxing adds presence, 2 inits,
         // seed map, boundary tiles, dilations, histogram, K sweeps, argmax
-        st->kernels = 5 + (want_relax ? 7 + relax_dilations + K : 0);
+        st->kernels = 5 + (want_relax ? (ig ? ig_kernels : 7 + relax_dilations + K) : 0);
         st->relax_active_voxel_sweeps = relax_active;
         cudaEventElapsedTime(&st->ms_oift_kernel, c->ev[4], c->ev[5]);
         st->ms_sweeps = 0.0f;
@@ -701,7 +741,7 @@ int oift_b200_build_weights_i16(oift_b200_ctx *c, const oift_b200_params *p,
     ba.Z = Z;
     ba.planes = oift_b200_weight_planes(p->adjacency);
     ba.mode = p->weight_mode;
-    ba.cap = (p->weight_mode == OIFT_W_GRAD) ? OIFT_MAX_BASE : p->wq;
+    ba.cap = (p->weight_mode == OIFT_W_GRAD || p->weight_mode == OIFT_W_IMAGEGRAPH) ? OIFT_MAX_BASE : p->wq;
     for (int k = 0; k < ba.planes; k++) {
         int i = adj.n / 2 + k;
         ba.dx[k] = adj.dx[i];
@@ -1215,6 +1255,8 @@ int oift_b200_run_cli_host(oift_b200_ctx *c, const oift_b200_params *p, const in
                            float percentile, oift_b200_stats *stats) {
     if (!c || !image || !label || (nseeds > 0 && !seeds) || blur_passes < 0) return OIFT_E_BAD_ARG;
     TRY(check_params(p));
+    // the cascade and the CLI chain run OIFT_Multi / ORelax_1_Multi, not the 2D image graph
+    if (p->weight_mode == OIFT_W_IMAGEGRAPH) return OIFT_E_UNSUPPORTED;
     if (nseeds <= 0) return OIFT_E_NO_SEEDS;
     cudaSetDevice(c->device);
     const int X = p->xsize, Y = p->ysize, Z = p->zsize;
@@ -1368,6 +1410,8 @@ int oift_b200_run_pyramid_host(oift_b200_ctx *c, const oift_b200_params *p, cons
                                float percentile, oift_b200_stats *stats) {
     if (!c || !image || !label || (nseeds > 0 && !seeds) || blur_passes < 0) return OIFT_E_BAD_ARG;
     TRY(check_params(p));
+    // the cascade and the CLI chain run OIFT_Multi / ORelax_1_Multi, not the 2D image graph
+    if (p->weight_mode == OIFT_W_IMAGEGRAPH) return OIFT_E_UNSUPPORTED;
     if (nseeds <= 0) return OIFT_E_NO_SEEDS;
     cudaSetDevice(c->device);
     const int X = p->xsize, Y = p->ysize, Z = p->zsize;
@@ -1405,6 +1449,8 @@ int oift_b200_run_pyramid_device_i16(oift_b200_ctx *c, const oift_b200_params *p
     if (!c || !image || !label_in || !label_out || (nseeds > 0 && !seeds) || blur_passes < 0)
         return OIFT_E_BAD_ARG;
     TRY(check_params(p));
+    // the cascade and the CLI chain run OIFT_Multi / ORelax_1_Multi, not the 2D image graph
+    if (p->weight_mode == OIFT_W_IMAGEGRAPH) return OIFT_E_UNSUPPORTED;
     if (nseeds <= 0) return OIFT_E_NO_SEEDS;
     cudaSetDevice(c->device);
     const int X = p->xsize, Y = p->ysize, Z = p->zsize;
@@ -1477,7 +1523,8 @@ static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_
     if (teams < 1 || teams > c->sms) return OIFT_E_BAD_ARG;
     // the team kernel is the 6 / 4-neighbourhood tile step on prebuilt edge codes
     if (common->adjacency != 6 && common->adjacency != 4) return OIFT_E_UNSUPPORTED;
-    if (common->weight_mode == OIFT_W_BLEND_Q) return OIFT_E_UNSUPPORTED;
+    if (common->weight_mode == OIFT_W_BLEND_Q || common->weight_mode == OIFT_W_IMAGEGRAPH)
+        return OIFT_E_UNSUPPORTED;
     const int ctas_lo = c->sms / teams, ctas_hi = (c->sms + teams - 1) / teams;
 
     // ---- per-job checks; distinct images (pointer + extents) ----

@@ -76,6 +76,37 @@ __host__ __device__ inline int max_base_for_cost(int c, double f) {
     return bi;
 }
 
+// Oriented arc weight of the 2D image graph (Orient2Digraph, gft/src/gft_imagegraph.cpp:
+// 981-1016): base = |dI| + 1 becomes MAX(ROUND(base * f), 1) with ROUND(x) = (int)(x + 0.5)
+// for x >= 0 (gft/include/gft_common.h:120), f = 1.0 +/- alpha and alpha = per/100.0 held in
+// a float; equal intensities keep the base.  The product and the sum are rounded separately,
+// as the C++ evaluates them.
+__host__ __device__ inline int round_weight(uint32_t base, double f) {
+#ifdef __CUDA_ARCH__
+    const int w = (int)__dadd_rn(__dmul_rn((double)base, f), 0.5);
+#else
+    const int w = (int)((double)base * f + 0.5);
+#endif
+    return w > 1 ? w : 1;
+}
+__host__ __device__ inline int oriented_weight_round(uint32_t base, bool tail_gt, bool tail_lt,
+                                                     double fgt, double flt) {
+    if (tail_gt) return round_weight(base, fgt);
+    if (tail_lt) return round_weight(base, flt);
+    return (int)base;
+}
+// Largest base b in [0, OIFT_MAX_BASE] with MAX(ROUND(b f), 1) <= c (monotone in b for
+// f >= 0); -1 when no base qualifies (c < 1).
+__host__ __device__ inline int max_base_for_cost_round(int c, double f) {
+    if (c < 1) return -1;
+    if (f <= 0.0) return OIFT_MAX_BASE;
+    double b = floor(((double)c + 0.5) / f);
+    int bi = b > (double)OIFT_MAX_BASE ? OIFT_MAX_BASE : (b < 0.0 ? 0 : (int)b);
+    while (bi > 0 && round_weight((uint32_t)bi, f) > c) bi--;
+    while (bi < OIFT_MAX_BASE && round_weight((uint32_t)(bi + 1), f) <= c) bi++;
+    return bi;
+}
+
 // x / 100 rounded to nearest-even in FP32, for all finite x (exhaustively checked against
 // the IEEE quotient by oift_b200_selftest_div100): the product with r = RN(1/100) is
 // corrected once by the exact FMA residual e = x - q*100 (Markstein's correction step).

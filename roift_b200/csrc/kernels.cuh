@@ -195,6 +195,28 @@ __global__ void seeds_scatter_kernel(const int32_t *lab, size_t N, size_t chunk,
                                      const unsigned *base_of, int32_t *seeds,
                                      int32_t *seed_labels);
 
+// ---- relaxation of the oriented 2D image graph (imagegraph.cu) ----
+struct IgRelax {
+    int X, Y, adjacency;       // zsize == 1; 4 or 8
+    float per;                 // global polarity x100
+    int sweeps;
+    const int32_t *olabel;     // OIFT labels
+    const int32_t *seeds;
+    int nseeds;
+    float *m0, *m1;            // [N] each
+    uint16_t *ring;            // [N]
+    uint8_t *seedf;            // [N]
+    int *small;                // 2 ints of scratch
+    int32_t *label;            // out: binary labels, may be null
+    uint8_t *mask;             // out, may be null
+    float *membership;         // out: [N], may be null
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;  // around the sweeps
+};
+// sg->Wmax of Orient2Digraph from the largest |dI| over the in-image arcs (-1: none).
+double ig_wmax(int dmax, float per);
+template <typename T>
+int ig_relax_run(const IgRelax &R, const T *img, cudaStream_t s, int sms, int *kernels);
+
 // ---- adjoint of the relaxation (adjoint.cu) ----
 struct AdjointJob {
     int X, Y, Z, adjacency;
@@ -223,7 +245,8 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
              long long *steps_out, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr,
-             unsigned long long *cycles_out = nullptr, const OiftFullN *fn = nullptr);
+             unsigned long long *cycles_out = nullptr, const OiftFullN *fn = nullptr,
+             bool round_orient = false);
 constexpr int OIFT_WARPS_PER_CTA = 16;
 
 }  // namespace oiftb

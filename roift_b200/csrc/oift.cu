@@ -60,6 +60,8 @@ struct OiftArgs {
     // gradient blend (BLEND_Q, 6 / 4 neighbourhoods): normalised Sobel map and mix weight
     const int32_t *gmap;
     float alpha;
+    // image-graph orientation (OIFT_W_IMAGEGRAPH): MAX(ROUND(base f), 1), f from a float alpha
+    int ig;
 };
 
 constexpr int OIFT_WARPS = 16;
@@ -180,8 +182,10 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
     const uint32_t lab_bits = ((uint32_t)l << 1) | 1u;
     auto arc_key = [&](uint32_t code, bool tail_low) -> uint32_t {
         const bool hi = (code >> 15) & 1, lo = (code >> 14) & 1;
-        const int w = oriented_weight(code & OIFT_BASE_MASK, tail_low ? hi : lo,
-                                      tail_low ? lo : hi, fgt, flt);
+        const int w = A.ig ? oriented_weight_round(code & OIFT_BASE_MASK, tail_low ? hi : lo,
+                                                   tail_low ? lo : hi, fgt, flt)
+                           : oriented_weight(code & OIFT_BASE_MASK, tail_low ? hi : lo,
+                                             tail_low ? lo : hi, fgt, flt);
         const int nc = w > c ? w : c;
         return ((uint32_t)nc << 17) | lab_bits;
     };
@@ -714,6 +718,7 @@ __device__ __forceinline__ int gen_base(const OiftArgs &A, int ip, int iq) {
     const int ad = d < 0 ? -d : d;
     int b = ad;
     if (A.wmode == OIFT_W_RBF_Q) b = A.lut[ad < A.lut_len ? ad : A.lut_len - 1];
+    else if (A.wmode == OIFT_W_IMAGEGRAPH) b = ad + 1;
     return b > A.wcap ? A.wcap : b;
 }
 
@@ -766,7 +771,9 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
                                   : (ip < iq ? (int)__fmul_rn(wf, bltf) : (int)wf);
             return w < 0 ? 0 : w;
         }
-        return oriented_weight((uint32_t)gen_base<TI>(A, ip, iq), ip > iq, ip < iq, fgt, flt);
+        const uint32_t b = (uint32_t)gen_base<TI>(A, ip, iq);
+        return A.ig ? oriented_weight_round(b, ip > iq, ip < iq, fgt, flt)
+                    : oriented_weight(b, ip > iq, ip < iq, fgt, flt);
     };
     // arc p -> q with tail p: open at this cost, or the key it offers q
     auto arc_open = [&](int hp, int hq) -> bool {
@@ -1089,8 +1096,20 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         if (leader_cta && threadIdx.x == 0) g->levels = e + 1;
         const int c = key_cost(kk), l = key_label(kk);
         const double per = (double)polarity_of(A, l);
-        const double fgt = 1.0 + per / 100.0, flt = 1.0 - per / 100.0;
-        const int bgt = max_base_for_cost(c, fgt), blt = max_base_for_cost(c, flt);
+        double fgt, flt;
+        int bgt, blt;
+        if (A.ig) {  // Orient2Digraph: float alpha = per / 100.0, val * (1.0 +/- alpha)
+            const float alpha = (float)(per / 100.0);
+            fgt = 1.0 + (double)alpha;
+            flt = 1.0 - (double)alpha;
+            bgt = max_base_for_cost_round(c, fgt);
+            blt = max_base_for_cost_round(c, flt);
+        } else {
+            fgt = 1.0 + per / 100.0;
+            flt = 1.0 - per / 100.0;
+            bgt = max_base_for_cost(c, fgt);
+            blt = max_base_for_cost(c, flt);
+        }
         // ---- S: the owner warp of each tile of this level processes it directly ----
         unsigned long long steps = 0;
         const long long t_s0 = clock64();
@@ -1272,6 +1291,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
             sA.g = g;
             sA.spin_limit = spin_limit;
             sA.max_levels = max_levels;
+            sA.ig = 0;
         }
         // ---- clear the team's state for this volume ----
         for (size_t i = tid; i < N; i += nthr) key[i] = OIFT_KEY_INF;
@@ -1419,7 +1439,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
              long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end,
-             unsigned long long *cycles_out, const OiftFullN *fn) {
+             unsigned long long *cycles_out, const OiftFullN *fn, bool round_orient) {
     size_t N = (size_t)X * Y * Z;
     cudaMemsetAsync(S.key, 0xFF, N * sizeof(uint32_t), st);
     cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
@@ -1471,6 +1491,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.lut_len = fn ? fn->lut_len : 0;
     A.gmap = fn ? fn->gmap : nullptr;
     A.alpha = fn ? fn->alpha : 1.0f;
+    A.ig = round_orient ? 1 : 0;
     size_t smem = oift_smem_bytes();
     void *args[] = {&A};
     cudaError_t err;

@@ -56,6 +56,8 @@ __global__ void __launch_bounds__(256) build_weights_kernel(const T *__restrict_
                                              __fmul_rn(__fsub_rn(1.0f, a.blend_a), gavg));
                         b = (int)wf;
                         if (b < 0) b = 0;
+                    } else if (a.mode == OIFT_W_IMAGEGRAPH) {
+                        b = ad + 1;  // ByEuclideanDistance, gft_imagegraph.cpp:35
                     } else {
                         b = ad;
                     }

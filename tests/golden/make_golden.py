@@ -69,6 +69,16 @@ def make(name, shape, pol, adj, nl, per_class, seed):
         out["ref_blend_oift_label"] = O.ref_gradweight(f, g, 0.6, c.seeds, c.seed_labels, pol, 0)
         out["ref_blend_relax_label"] = O.ref_gradweight(f, g, 0.6, c.seeds, c.seed_labels, pol,
                                                         SWEEPS)
+    # the 2D image-graph pipeline (gft_ift.cpp:9575-9682, 9785-9790): OIFT(sImageGraph) with
+    # every labelled pixel as a seed, then ORelax_1(sImageGraph)
+    if pc is None and adj in (4, 8):
+        img2 = img.reshape(shape[1:])
+        lab_ig, wmax = O.ref_imagegraph(img2, adj, c.seeds, c.seed_labels, pol, 0)
+        out["ref_ig_oift_label"] = lab_ig
+        out["ref_ig_wmax"] = np.int32(wmax)
+        out["ref_ig_energy"] = np.int32(O.ref_imagegraph_energy(img2, adj, lab_ig, pol, 1))
+        out["ref_ig_relax_label"] = O.ref_imagegraph(img2, adj, c.seeds, c.seed_labels, pol,
+                                                     SWEEPS)[0]
     # the coarse-to-fine cascade on the twice-blurred volume (global polarity cases)
     if pc is None and adj in (6, 26):
         f = O.ref_gaussian_blur(O.ref_gaussian_blur(img).reshape(shape)).reshape(shape)

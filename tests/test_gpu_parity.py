@@ -549,3 +549,79 @@ def test_blend_matches_reference_experiment(roift, oracle_lib, path):
     assert np.array_equal(got, exp)
     if np.array_equal(lab_r2, d["ref_blend_oift_label"]):
         assert np.array_equal(got, d["ref_blend_relax_label"])
+
+
+# ------------------------------------------------------------ 2D image graph ----
+IG_CASES = [((1, 40, 48), 0.5, 4, 7, 1), ((1, 45, 67), -0.3, 8, 5, 1), ((1, 64, 33), 0.0, 4, 0, 1),
+            ((1, 31, 90), 1.0, 8, 3, 2), ((1, 50, 50), -1.0, 4, 4, 1), ((1, 37, 70), 0.2, 8, 9, 2)]
+
+
+@pytest.mark.parametrize("shape,pol,adj,K,nl", IG_CASES)
+def test_imagegraph_oift_and_relax_match_oracle(roift, oracle_lib, shape, pol, adj, K, nl):
+    """OIFT_W_IMAGEGRAPH: cost and labels == R2 with the oriented image-graph weights
+    (|dI| + 1, MAX(ROUND(w (1 +/- alpha)), 1)), the cut energy equals R1's (the reference
+    order), and after K sweeps of ORelax_1(sImageGraph) the binary labels, mask and the
+    single membership channel are bit-identical to the FP32 restatement."""
+    c, img = _case(shape, pol, adj, nl, "grad")
+    img2 = img.reshape(shape[1:])
+    ctx = roift._ctx()
+    p = roift.make_params(shape, adjacency=adj, weight_mode="imagegraph", pol=pol, sweeps=0)
+    lab, cost, _, _, st = ctx.run_host(p, img, c.label_map(), c.seeds, want_cost=True)
+    cost_r2, lab_r2, levels = O.oift_fmax_imagegraph(img2, adj, c.seeds, c.seed_labels, pol)
+    assert np.array_equal(cost, cost_r2)
+    assert np.array_equal(lab, lab_r2)
+    assert st.levels >= levels
+    order = np.argsort(c.seeds, kind="stable")
+    r1, _, _, _ = O.oift_prim_imagegraph(img2, adj, c.seeds[order], c.seed_labels[order], pol)
+    for lb in range(1, nl + 1):
+        assert O.energy_imagegraph(img2, adj, lab, pol, lb) == O.energy_imagegraph(img2, adj, r1, pol, lb)
+    p = roift.make_params(shape, adjacency=adj, weight_mode="imagegraph", pol=pol, sweeps=K)
+    labk, _, memb, mask, st = ctx.run_host(p, img, c.label_map(), c.seeds, want_membership=1,
+                                           want_mask=True)
+    exp, m = O.relax_imagegraph(img2, adj, c.seeds, lab_r2, K, pol)
+    assert st.nclasses == 1
+    assert np.array_equal(labk, exp)
+    assert np.array_equal(mask.astype(np.int32), exp)
+    assert np.array_equal(memb.reshape(-1).view(np.uint32), m.view(np.uint32))
+
+
+IG_GOLDEN = [p for p in GOLDEN if "ref_ig_oift_label" in np.load(p).files]
+
+
+@pytest.mark.parametrize("path", IG_GOLDEN, ids=[os.path.basename(p)[:-4] for p in IG_GOLDEN])
+def test_imagegraph_matches_reference_pipeline(roift, oracle_lib, path):
+    """On the fixtures of the reference's own 2D pipeline: the GPU labels have the
+    reference's cut energy; where R2 and the reference's Prim labels agree, the GPU's
+    relaxed labels equal the reference's ORelax_1(sImageGraph) output."""
+    d = np.load(path)
+    shape = d["image"].shape
+    img2 = d["image"].reshape(shape[1:])
+    seeds, sl = d["seeds"], d["seed_labels"]
+    pol, K, adj = float(d["pol"]), int(d["sweeps"]), int(d["adjacency"])
+    lab0 = np.full(img2.size, -1, np.int32)
+    lab0[seeds] = sl
+    ctx = roift._ctx()
+    p = roift.make_params(shape, adjacency=adj, weight_mode="imagegraph", pol=pol, sweeps=0)
+    lab, _, _, _, _ = ctx.run_host(p, img2.reshape(-1), lab0.copy(), seeds)
+    assert O.energy_imagegraph(img2, adj, lab, pol) == int(d["ref_ig_energy"])
+    p = roift.make_params(shape, adjacency=adj, weight_mode="imagegraph", pol=pol, sweeps=K)
+    labk, _, _, _, _ = ctx.run_host(p, img2.reshape(-1), lab0.copy(), seeds)
+    exp, _ = O.relax_imagegraph(img2, adj, seeds, lab, K, pol)
+    assert np.array_equal(labk, exp)
+    if np.array_equal(lab, d["ref_ig_oift_label"]):
+        assert np.array_equal(labk, d["ref_ig_relax_label"])
+
+
+def test_imagegraph_rejections(roift):
+    """The image graph is 2D with one global polarity; the batched driver and the cascade
+    do not take it."""
+    ctx = roift._ctx()
+    img = np.zeros(4 * 5 * 6, np.int32)
+    lab = np.full(img.size, -1, np.int32)
+    lab[0] = 0
+    seeds = np.array([0], np.int32)
+    for shape, adj in (((4, 5, 6), 6), ((1, 20, 6), 6)):
+        p = roift.make_params(shape, adjacency=adj, weight_mode="imagegraph", pol=0.3)
+        with pytest.raises(roift.OiftError) as e:
+            ctx.run_host(p, img[: int(np.prod(shape))], lab[: int(np.prod(shape))].copy(), seeds)
+        assert e.value.status == roift.E_UNSUPPORTED

@@ -238,3 +238,76 @@ def test_blend_weights_match_live_reference(oracle_lib, i, shape, pol, alpha):
     assert np.array_equal(O.oift_prim_blend(f, g, alpha, 6, c.seeds, c.seed_labels, pol=pol), lr)
     out, _ = O.relax_blend(f, g, alpha, 6, c.seeds, lr, 7, pol)
     assert np.array_equal(out, O.ref_gradweight(f, g, alpha, c.seeds, c.seed_labels, pol, 7))
+
+
+# --------------------------------------------------------- the 2D image graph ----
+IG_GOLDEN = [p for p in GOLDEN if "ref_ig_oift_label" in np.load(p).files]
+
+
+def _ig_inputs(d):
+    shape = d["image"].shape
+    return d["image"].reshape(shape[1:]), d["seeds"], d["seed_labels"]
+
+
+@pytest.mark.parametrize("path", IG_GOLDEN, ids=[os.path.basename(p)[:-4] for p in IG_GOLDEN])
+def test_imagegraph_matches_golden(oracle_lib, path):
+    """OIFT(sImageGraph) and ORelax_1(sImageGraph) on ByEuclideanDistance + Orient2Digraph
+    restated against the reference: R1 labels (every labelled pixel queued in address
+    order, as S = NULL does), Wmax, the cut energy of R2's labels, the relaxed labels."""
+    d = np.load(path)
+    img, seeds, sl = _ig_inputs(d)
+    pol, K, adj = float(d["pol"]), int(d["sweeps"]), int(d["adjacency"])
+    order = np.argsort(seeds, kind="stable")
+    assert O.imagegraph_wmax(img, adj, pol) == int(d["ref_ig_wmax"])
+    lab, _, _, _ = O.oift_prim_imagegraph(img, adj, seeds[order], sl[order], pol)
+    assert np.array_equal(lab, d["ref_ig_oift_label"])
+    assert O.energy_imagegraph(img, adj, lab, pol) == int(d["ref_ig_energy"])
+    _, lab_r2, _ = O.oift_fmax_imagegraph(img, adj, seeds, sl, pol)
+    assert O.energy_imagegraph(img, adj, lab_r2, pol) == int(d["ref_ig_energy"])
+    out, m = O.relax_imagegraph(img, adj, seeds, lab, K, pol)
+    assert np.array_equal(out, d["ref_ig_relax_label"])
+    assert np.array_equal(out, (~(m < 0.5)).astype(np.int32))
+
+
+def _ig_random_case(rng, trial):
+    adj = (4, 8)[trial % 2]
+    Y, X = (int(v) for v in rng.integers(8, 40, 2))
+    pol = float(rng.choice([-1.0, -0.5, -0.3, 0.0, 0.2, 0.5, 0.9, 1.0]))
+    img = rng.integers(0, 60, (Y, X)).astype(np.int32)
+    if trial % 3 == 0:  # a noisy disc, as the 2D CLI case
+        yy, xx = np.mgrid[:Y, :X]
+        disc = (yy - Y / 2) ** 2 + (xx - X / 2) ** 2 < (min(X, Y) / 3) ** 2
+        img = np.clip(np.where(disc, 180, 60) + rng.normal(0, 12, (Y, X)), 0, 255).astype(np.int32)
+    border = [p for p in range(X * Y) if p % X in (0, X - 1) or p // X in (0, Y - 1)]
+    c = (Y // 2) * X + X // 2
+    obj = {c, c + 1, c + X}
+    seeds = np.array(sorted(set(border) | obj), np.int32)
+    sl = np.array([1 if s in obj else 0 for s in seeds], np.int32)
+    return img, adj, pol, seeds, sl, int(rng.integers(0, 12))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+def test_imagegraph_matches_live_reference(oracle_lib):
+    """60 random 2D cases, both neighbourhoods, alpha in [-1, 1]: R1 labels, Wmax and the
+    relaxed labels equal the reference's; R2's labels have the reference's cut energy.
+    (The f_max along the reference's Prim forest may differ from R2's cost on these
+    oriented graphs, where a label's competition can block another's path; those pixels
+    are counted, not required to be zero.)"""
+    rng = np.random.default_rng(0)
+    fmax_diff = 0
+    for trial in range(60):
+        img, adj, pol, seeds, sl, K = _ig_random_case(rng, trial)
+        ref_lab, wmax = O.ref_imagegraph(img, adj, seeds, sl, pol, 0)
+        assert wmax == O.imagegraph_wmax(img, adj, pol)
+        r1, _, _, fm = O.oift_prim_imagegraph(img, adj, seeds, sl, pol)
+        assert np.array_equal(r1, ref_lab), trial
+        cost, r2, _ = O.oift_fmax_imagegraph(img, adj, seeds, sl, pol)
+        fmax_diff += int((fm != cost).sum())
+        e = O.ref_imagegraph_energy(img, adj, ref_lab, pol)
+        assert O.energy_imagegraph(img, adj, ref_lab, pol) == e
+        assert O.energy_imagegraph(img, adj, r2, pol) == e
+        out, _ = O.relax_imagegraph(img, adj, seeds, ref_lab, K, pol)
+        exp = O.ref_imagegraph(img, adj, seeds, sl, pol, K)[0] if K else None
+        if K:
+            assert np.array_equal(out, exp), trial
+    print("pixels where the Prim-forest f_max differs from R2:", fmax_diff)
