@@ -216,6 +216,20 @@ OIFT_API int oift_b200_read_seeds(const char *path, int xsize, int ysize, int zs
 /* Per-class polarity file (oiftrelax.cpp:280-300): a count n, then n values in [-1, 1],
  * stored x100 in per_class (may be NULL to count).  Returns n. */
 OIFT_API int oift_b200_read_polarity(const char *path, float *per_class, int cap);
+
+/* Volume files of the CLI (gft::Scene32::Read / Write, gft/src/gft_scene32.cpp:334-420,
+ * 525-580, 600-660, 748-800), host only.  Formats by extension: .scn (8/16/32-bit samples);
+ * NIfTI-1 .nii, .nii.gz, .hdr/.img pairs (either byte order).  Reading widens uint8, int8,
+ * int16, uint16 and int32 samples and scales float32 by 10000 / max with rounding, as
+ * ReadNifti1 does; other sample types and dim[0] outside 3..4 give OIFT_E_UNSUPPORTED.
+ * dims = (xsize, ysize, zsize), spacing = (dx, dy, dz).  With data == NULL only dims and
+ * spacing are filled; a cap below the voxel count gives OIFT_E_RANGE.  Writing follows
+ * Scene32::Write: .scn with the narrowest of 8/16/32 bits that holds the maximum, NIfTI as
+ * int32 samples.  OIFT_E_BAD_ARG when a file cannot be opened, read or written. */
+OIFT_API int oift_b200_read_volume(const char *path, int32_t *data, size_t cap_voxels,
+                                   int dims[3], float spacing[3]);
+OIFT_API int oift_b200_write_volume(const char *path, const int32_t *data, const int dims[3],
+                                    const float spacing[3]);
 /* The CLI's processing chain on host buffers: shift the unshifted int32 `image` to >= 0,
  * `blur_passes` Gaussian blurs (the CLI uses 2), OIFT + relax_sweeps sweeps as run_host,
  * then, if percentile >= 0 and the result is binary, the conditional dilation with

@@ -144,6 +144,9 @@ def ref():
         R.ref_imagegraph_energy.restype = C.c_int
         R.ref_imagegraph_energy.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_float, _i32p,
                                             C.c_int]
+        R.ref_read_volume.restype = C.c_int
+        R.ref_read_volume.argtypes = [C.c_char_p, C.c_void_p, C.c_int, _i32p, _f32p]
+        R.ref_write_volume.argtypes = [C.c_char_p, _i32p, _i32p, _f32p]
         R.ref_coarse_to_fine.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_int, C.c_float, _i32p, C.c_int, _i32p]
         R.ref_oiftrelax_chain.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_double,
@@ -671,6 +674,26 @@ def ref_imagegraph_energy(img, adj, label, pol, lb=1):
     X, Y = _ig_dims(img)
     return int(ref().ref_imagegraph_energy(as_i32(img), X, Y, adj, float(np.float32(pol * 100.0)),
                                            np.ascontiguousarray(label, np.int32).reshape(-1), lb))
+
+
+def ref_read_volume(path):
+    """Scene32::Read: (int32 array (Z, Y, X), spacing (dx, dy, dz))."""
+    dims = np.zeros(3, np.int32)
+    sp = np.zeros(3, np.float32)
+    n = ref().ref_read_volume(os.fsencode(path), None, 0, dims, sp)
+    assert n >= 0
+    out = np.empty(n, np.int32)
+    ref().ref_read_volume(os.fsencode(path), out.ctypes.data, n, dims, sp)
+    X, Y, Z = (int(v) for v in dims)
+    return out.reshape(Z, Y, X), tuple(float(v) for v in sp)
+
+
+def ref_write_volume(path, vol, spacing):
+    """Scene32::Write of an int32 volume (Z, Y, X)."""
+    v = np.ascontiguousarray(vol, np.int32)
+    Z, Y, X = v.shape
+    ref().ref_write_volume(os.fsencode(path), v.reshape(-1), np.array([X, Y, Z], np.int32),
+                           np.array(spacing, np.float32))
 
 
 def ref_gaussian_blur(img):

@@ -21,6 +21,8 @@
 //                                ift::ORelax_1(sImageGraph*) (gft/src/gft_ift.cpp:1358-1439,
 //                                7683-7847): the 2D pipeline of gft_ift.cpp:9575-9682, 9785-9790
 //   ref_imagegraph_energy     -> ift::GetEnergy_Min(sImageGraph*) (gft/src/gft_ift.cpp:287-319)
+//   ref_read_volume           -> gft::Scene32::Read  (gft/src/gft_scene32.cpp:334-420, 525-580)
+//   ref_write_volume          -> gft::Scene32::Write (gft/src/gft_scene32.cpp:600-660, 748-800)
 //   ref_oiftrelax_chain       -> the processing chain of the CLI main (oiftrelax.cpp:
 //                                263-268, 368-414): shift, GaussianBlur x2, OIFT_Multi,
 //                                ORelax_1_Multi, conditional dilation when binary
@@ -249,6 +251,32 @@ REF_API int ref_imagegraph_energy(const int *img, int X, int Y, int adj, float p
     ImageGraph::Destroy(&sg);
     Image32::Destroy(&im);
     return e;
+}
+
+// Reads a volume file; data may be null (dims and spacing only).  Returns the voxel count.
+REF_API int ref_read_volume(const char *path, int *data, int cap, int *dims, float *spacing) {
+    sScene32 *scn = Scene32::Read(const_cast<char *>(path));
+    if (!scn) return -1;
+    dims[0] = scn->xsize;
+    dims[1] = scn->ysize;
+    dims[2] = scn->zsize;
+    spacing[0] = scn->dx;
+    spacing[1] = scn->dy;
+    spacing[2] = scn->dz;
+    const int n = scn->n;
+    if (data && cap >= n) std::memcpy(data, scn->data, sizeof(int) * (size_t)n);
+    Scene32::Destroy(&scn);
+    return n;
+}
+
+REF_API void ref_write_volume(const char *path, const int *data, const int *dims,
+                              const float *spacing) {
+    sScene32 *scn = make_scene(data, dims[0], dims[1], dims[2]);
+    scn->dx = spacing[0];
+    scn->dy = spacing[1];
+    scn->dz = spacing[2];
+    Scene32::Write(scn, const_cast<char *>(path));
+    Scene32::Destroy(&scn);
 }
 
 }  // extern "C"

@@ -99,7 +99,8 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
            "oift_b200_run_pyramid_device_i16", "oift_b200_adjoint",
            "oift_b200_batch_graph_create", "oift_b200_batch_graph_launch",
-           "oift_b200_batch_graph_destroy", "oift_b200_read_seeds", "oift_b200_read_polarity"]
+           "oift_b200_batch_graph_destroy", "oift_b200_read_seeds", "oift_b200_read_polarity",
+           "oift_b200_read_volume", "oift_b200_write_volume"]
 
 _lib = None
 
@@ -133,6 +134,10 @@ def lib():
         L.oift_b200_batch_graph_destroy.argtypes = [vp]
         L.oift_b200_read_seeds.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int]
         L.oift_b200_read_polarity.argtypes = [C.c_char_p, vp, C.c_int]
+        L.oift_b200_read_volume.argtypes = [C.c_char_p, vp, C.c_size_t, C.POINTER(C.c_int),
+                                            C.POINTER(C.c_float)]
+        L.oift_b200_write_volume.argtypes = [C.c_char_p, vp, C.POINTER(C.c_int),
+                                             C.POINTER(C.c_float)]
         L.oift_b200_selftest_div100.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_uint)]
         L.oift_b200_oift_noalloc.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_int, C.c_float, vp, C.c_int, vp, vp, C.c_int,
@@ -430,6 +435,32 @@ def read_polarity(path):
     if n < 0:
         raise OiftError(n, "oift_b200_read_polarity")
     return out
+
+
+def read_volume(path):
+    """Volume file of the CLI (.scn, NIfTI-1 .nii / .nii.gz / .hdr+.img), host only:
+    (int32 array shaped (Z, Y, X), spacing (dx, dy, dz))."""
+    dims, sp = (C.c_int * 3)(), (C.c_float * 3)()
+    st = lib().oift_b200_read_volume(os.fsencode(path), None, 0, dims, sp)
+    if st != 0:
+        raise OiftError(st, "oift_b200_read_volume")
+    X, Y, Z = dims
+    out = np.empty((Z, Y, X), np.int32)
+    st = lib().oift_b200_read_volume(os.fsencode(path), out.ctypes.data, out.size, dims, sp)
+    if st != 0:
+        raise OiftError(st, "oift_b200_read_volume")
+    return out, tuple(float(v) for v in sp)
+
+
+def write_volume(path, vol, spacing=(1.0, 1.0, 1.0)):
+    """Writes an int32 volume shaped (Z, Y, X) (or (Y, X)) as Scene32::Write does."""
+    v = np.ascontiguousarray(vol, np.int32)
+    Z, Y, X = (1,) + v.shape if v.ndim == 2 else v.shape
+    dims = (C.c_int * 3)(X, Y, Z)
+    sp = (C.c_float * 3)(*spacing)
+    st = lib().oift_b200_write_volume(os.fsencode(path), v.ctypes.data, dims, sp)
+    if st != 0:
+        raise OiftError(st, "oift_b200_write_volume")
 
 
 def inject_boundary_seeds(label, shape_zyx, stride):

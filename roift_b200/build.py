@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboift_b200.so")
-SOURCES = ["api.cu", "weights.cu", "oift.cu", "relax.cu", "selftest.cu", "noalloc.cu", "prepost.cu", "adjoint.cu", "imagegraph.cu"]
+SOURCES = ["api.cu", "weights.cu", "oift.cu", "relax.cu", "selftest.cu", "noalloc.cu", "prepost.cu", "adjoint.cu", "imagegraph.cu", "volume_io.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
@@ -46,7 +46,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with ThreadPoolExecutor(workers) as ex:
         objs = list(ex.map(compile_unit, UNITS))
     subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs,
-                    "-o", LIB, "-lcudart"], check=True)
+                    "-o", LIB, "-lcudart", "-lz"], check=True)
     for o in objs:
         os.remove(o)
     return LIB

@@ -115,3 +115,126 @@ def test_cli_text_inputs(roift, tmp_path):
     (tmp_path / "short.txt").write_text("3\n0.1 0.2\n")
     with pytest.raises(roift.OiftError):
         roift.read_polarity(str(tmp_path / "short.txt"))
+
+
+# ------------------------------------------------------------------ volume files ----
+import gzip  # noqa: E402
+import struct  # noqa: E402
+
+import oracle as O  # noqa: E402
+
+_NII_TYPES = {"u1": 2, "i1": 256, "i2": 4, "u2": 512, "i4": 8, "f4": 16, "f8": 64}
+
+
+def _nifti_bytes(vol, spacing, code, bo="<", onefile=True, vox_offset=352.0):
+    """A NIfTI-1 file (or the .hdr of a pair) holding vol (Z, Y, X) with sample type code."""
+    Z, Y, X = vol.shape
+    h = bytearray(348)
+    struct.pack_into(bo + "i", h, 0, 348)
+    struct.pack_into(bo + "8h", h, 40, 3, X, Y, Z, 1, 1, 1, 1)
+    dt = next(k for k, v in _NII_TYPES.items() if v == code)
+    struct.pack_into(bo + "hh", h, 70, code, 8 * np.dtype(dt).itemsize)
+    struct.pack_into(bo + "8f", h, 76, 1.0, *spacing, 0, 0, 0, 0)
+    struct.pack_into(bo + "f", h, 108, vox_offset if onefile else 0.0)
+    h[344:348] = b"n+1\0" if onefile else b"ni1\0"
+    data = np.ascontiguousarray(vol.astype(np.dtype(dt).newbyteorder(bo))).tobytes()
+    if onefile:
+        return bytes(h) + b"\0" * (int(vox_offset) - 348) + data
+    return bytes(h) + b"\0\0\0\0", data
+
+
+def _vol(rng, shape, lo, hi):
+    return rng.integers(lo, hi, shape).astype(np.int64)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("hi", [200, 60000, 400000])
+def test_scn_files_match_reference(roift, oracle_lib, tmp_path, hi):
+    """.scn: the library's reader returns what Scene32::Read returns on the reference's own
+    files, and its writer produces the same bytes as Scene32::Write (8 / 16 / 32-bit
+    samples chosen by the maximum; negative values cast like the reference)."""
+    rng = np.random.default_rng(hi)
+    vol = _vol(rng, (5, 7, 9), -3 if hi < 256 else 0, hi).astype(np.int32)
+    sp = (0.5, 1.25, 2.0)
+    ref_path, our_path = str(tmp_path / "r.scn"), str(tmp_path / "o.scn")
+    O.ref_write_volume(ref_path, vol, sp)
+    roift.write_volume(our_path, vol, sp)
+    assert open(ref_path, "rb").read() == open(our_path, "rb").read()
+    got, gsp = roift.read_volume(ref_path)
+    exp, esp = O.ref_read_volume(ref_path)
+    assert np.array_equal(got, exp) and gsp == esp
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("ext", [".nii", ".hdr", ".img"])
+def test_nifti_write_read_against_reference(roift, oracle_lib, tmp_path, ext):
+    """NIfTI-1: files written by Scene32::Write read back identically through the library,
+    and the library's files (single .nii and .hdr / .img pairs) read back identically
+    through Scene32::Read."""
+    rng = np.random.default_rng(5)
+    vol = _vol(rng, (4, 6, 11), -70000, 70000).astype(np.int32)
+    sp = (0.75, 0.75, 1.5)
+    ref_path = str(tmp_path / ("r" + ext))
+    O.ref_write_volume(ref_path, vol, sp)
+    got, gsp = roift.read_volume(ref_path)
+    assert np.array_equal(got, vol) and gsp == sp
+    our_path = str(tmp_path / ("o" + ext))
+    roift.write_volume(our_path, vol, sp)
+    exp, esp = O.ref_read_volume(our_path)
+    assert np.array_equal(exp, vol) and esp == sp
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("code", [2, 256, 4, 512, 8, 16])
+@pytest.mark.parametrize("bo", ["<", ">"])
+def test_nifti_sample_types_match_reference(roift, oracle_lib, tmp_path, code, bo):
+    """ReadNifti1's conversions, both byte orders, one file and a pair: uint8, int8, int16,
+    uint16 and int32 widened; float32 scaled by 10000 / max and rounded."""
+    rng = np.random.default_rng(code)
+    lo, hi = {2: (0, 256), 256: (-128, 128), 4: (-32768, 32768), 512: (0, 65536),
+              8: (-2**31, 2**31 - 1), 16: (0, 1)}[code]
+    shape = (3, 5, 7)
+    if code == 16:
+        vol = (rng.standard_normal(shape) * 40.0 + 10.0).astype(np.float32)
+    else:
+        vol = _vol(rng, shape, lo, hi)
+    sp = (1.0, 0.5, 3.0)
+    p1 = tmp_path / "a.nii"
+    p1.write_bytes(_nifti_bytes(vol, sp, code, bo, vox_offset=400.0))
+    hdr, img = _nifti_bytes(vol, sp, code, bo, onefile=False)
+    (tmp_path / "b.hdr").write_bytes(hdr)
+    (tmp_path / "b.img").write_bytes(img)
+    for path in (str(p1), str(tmp_path / "b.hdr")):
+        got, gsp = roift.read_volume(path)
+        exp, esp = O.ref_read_volume(path)
+        assert np.array_equal(got, exp) and gsp == esp
+
+
+def test_volume_files_round_trip_and_errors(roift, tmp_path):
+    """Round trips through every writable format (with .nii.gz read back compressed and a
+    gzip copy of a plain file read the same), the dims-only query, and the errors."""
+    rng = np.random.default_rng(9)
+    vol = _vol(rng, (6, 5, 4), -1000, 1000).astype(np.int32)
+    sp = (1.0, 2.0, 3.0)
+    for name in ("v.nii", "v.nii.gz", "v.hdr", "w.img", "v.scn"):
+        p = str(tmp_path / name)
+        roift.write_volume(p, vol if name != "v.scn" else np.abs(vol), sp)
+        got, gsp = roift.read_volume(p)
+        assert np.array_equal(got, vol if name != "v.scn" else np.abs(vol)) and gsp == sp
+    raw = (tmp_path / "v.nii").read_bytes()
+    with gzip.open(tmp_path / "z.nii.gz", "wb") as f:
+        f.write(raw)
+    assert np.array_equal(roift.read_volume(str(tmp_path / "z.nii.gz"))[0], vol)
+    dims, spc = (C.c_int * 3)(), (C.c_float * 3)()
+    assert roift.lib().oift_b200_read_volume(os.fsencode(str(tmp_path / "v.nii")), None, 0,
+                                             dims, spc) == 0
+    assert tuple(dims) == (4, 5, 6)
+    small = np.empty(10, np.int32)
+    assert roift.lib().oift_b200_read_volume(os.fsencode(str(tmp_path / "v.nii")),
+                                             small.ctypes.data, 10, dims, spc) == roift.E_RANGE
+    (tmp_path / "d.nii").write_bytes(_nifti_bytes(vol.astype(np.float64), sp, 64))
+    for bad, code in (("d.nii", roift.E_UNSUPPORTED), ("v.txt", roift.E_UNSUPPORTED),
+                      ("missing.nii", roift.E_BAD_ARG)):
+        with pytest.raises(roift.OiftError) as e:
+            roift.read_volume(str(tmp_path / bad))
+        assert e.value.status == code
