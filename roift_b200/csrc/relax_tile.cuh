@@ -18,6 +18,12 @@ constexpr int RT_X = 32, RT_Y = 8, RT_Z = 4;
 constexpr int RH_X = RT_X + 2, RH_Y = RT_Y + 2, RH_Z = RT_Z + 2;
 constexpr int RH_N = RH_X * RH_Y * RH_Z;
 
+// Asynchronous 4-byte global -> shared copy (cp.async, cached in L1).
+__device__ __forceinline__ void relax_cp_async4(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 // Polarity factors of the arcs that end at q: (1 + per_pq / 100, 1 - per_pq / 100), with
 // per_pq = per (2 m_bg(q) - 1) (gft_ift.cpp:8804-8811) or sum_k per_k m_k(q) per class
 // (9076-9079).  They depend on q alone, so a tile computes them once per staged voxel.
@@ -149,17 +155,31 @@ __global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict
     const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
     const int x0 = tx * RT_X, y0 = ty * RT_Y, z0 = tz * RT_Z;
     const int tid = threadIdx.x + threadIdx.y * 32;
-    for (int i = tid; i < RH_N; i += 256) {
+    // memberships (and the gradient) as asynchronous 4-byte copies, the image through
+    // registers: every load of the halo is in flight before the first wait
+    constexpr int NIT = (RH_N + 255) / 256;
+    int iv[NIT];
+#pragma unroll
+    for (int j = 0; j < NIT; j++) {
+        const int i = tid + 256 * j;
         const int hx = i % RH_X, hy = (i / RH_X) % RH_Y, hz = i / (RH_X * RH_Y);
         const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
-        if (gx >= 0 && gx < X && gy >= 0 && gy < Y && gz >= 0 && gz < Z) {
+        if (i < RH_N && gx >= 0 && gx < X && gy >= 0 && gy < Y && gz >= 0 && gz < Z) {
             const size_t g = (size_t)gx + (size_t)gy * X + (size_t)gz * XY;
 #pragma unroll
-            for (int k = 0; k < C; k++) sm[k * RH_N + i] = __ldg(&min_[(size_t)k * N + g]);
-            si[i] = (int)__ldg(&img[g]);
-            if (BLEND) sg[i] = __ldg(&a.gmap[g]);
+            for (int k = 0; k < C; k++) relax_cp_async4(&sm[k * RH_N + i], &min_[(size_t)k * N + g]);
+            if (BLEND) relax_cp_async4(&sg[i], &a.gmap[g]);
+            iv[j] = (int)__ldg(&img[g]);
         }
     }
+#pragma unroll
+    for (int j = 0; j < NIT; j++) {
+        const int i = tid + 256 * j;
+        const int hx = i % RH_X, hy = (i / RH_X) % RH_Y, hz = i / (RH_X * RH_Y);
+        const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+        if (i < RH_N && gx >= 0 && gx < X && gy >= 0 && gy < Y && gz >= 0 && gz < Z) si[i] = iv[j];
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     // each thread reads back only the staged voxels it wrote itself
     for (int i = tid; i < RH_N; i += 256) {
         const int hx = i % RH_X, hy = (i / RH_X) % RH_Y, hz = i / (RH_X * RH_Y);
