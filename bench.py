@@ -176,6 +176,26 @@ def read_traffic(kernel: str, workload: str):
     return None
 
 
+def replica_seed(rank: int) -> int:
+    """Each rank segments its own volume (replicas, weak scaling): same generator and
+    shape, a different seed per rank."""
+    return 2 + rank
+
+
+def reduce_step_time(ms_local: float, dist, device) -> float:
+    """Max over ranks of a per-rank time (every rank calls it, in the same order)."""
+    import torch
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gvox(world: int, voxels_per_rank: int, ms_step: float) -> float:
+    """Throughput of the whole job: every rank's voxels over the slowest rank's time."""
+    return world * voxels_per_rank / (ms_step * 1e-3) / 1e9
+
+
 def run_batch_workload(args):
     """Many-volume batch: `nvol` int16 volumes (axes from {96..256}), 2-8 seed sets each,
     6-adj uint16 gradient weights, alpha ~ U(-0.5, 0.5), 20 sweeps, a mask per seed set.
@@ -462,7 +482,7 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
     dev = torch.device("cuda", local_rank)
 
-    c = workload_case(size=args.size, seed=2 + rank)
+    c = workload_case(size=args.size, seed=replica_seed(rank))
     N = c.n
     img_t = torch.from_numpy(c.image.copy()).to(dev)
     s_t = torch.from_numpy(c.seeds).to(dev)
@@ -499,11 +519,8 @@ def main():
     if dist:
         dist.barrier()
     tot_ms = sum(s.ms_total for s in stats)
-    t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_step = float(t.item()) / args.steps
-    value = world * N / (ms_step * 1e-3) / 1e9
+    ms_step = reduce_step_time(tot_ms, dist, dev) / args.steps
+    value = whole_job_gvox(world, N, ms_step)
 
     # ---- end to end through the host entry point (pinned buffers) ----
     e2e = None
@@ -523,10 +540,8 @@ def main():
             t0 = time.perf_counter()
             ctx.run_host(prm_h, img_np, lab_np, c.seeds)
             times.append(time.perf_counter() - t0)
-        et = torch.tensor([statistics.mean(times)], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * N / float(et.item()) / 1e9, "unit": UNIT,
+        e2e_s = reduce_step_time(statistics.mean(times), dist, dev)
+        e2e = {"value": whole_job_gvox(world, N, e2e_s * 1e3), "unit": UNIT,
                "h2d_bytes_per_step": 4 * N + 8 * len(c.seeds), "d2h_bytes_per_step": 4 * N}
 
     # ---- roofline of the dominant kernel (CUDA events on the launching stream) ----
