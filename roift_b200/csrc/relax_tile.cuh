@@ -135,8 +135,13 @@ __device__ __forceinline__ void relax_tile_voxels(const RelaxArgs &a, const floa
     }
 }
 
+// Blocks per SM the tile sweep is compiled for: with one or two classes (and no gradient
+// halo) five blocks' shared memory fits an SM, and asking for them caps the kernel at 48
+// registers without spills; larger variants are limited by shared memory first.
+constexpr int relax_min_blocks(int classes, bool blend) { return (!blend && classes <= 2) ? 5 : 1; }
+
 template <int C, typename T, bool PERCLASS, int ADJ, bool BLEND>
-__global__ void __launch_bounds__(256) relax_tile_kernel(const float *__restrict__ min_,
+__global__ void __launch_bounds__(256, relax_min_blocks(C, BLEND)) relax_tile_kernel(const float *__restrict__ min_,
                                                          float *__restrict__ mout,
                                                          const T *__restrict__ img,
                                                          const uint8_t *__restrict__ seedc,

@@ -25,10 +25,14 @@ static cudaError_t launch_tile_c(const float *in, float *out, const T *img, cons
     if (perclass) {
         auto k = relax_tile_kernel<C, T, true, ADJ, false>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (relax_min_blocks(C, false) > 1)  // the shared-memory carve-out that holds them
+            cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         k<<<ntiles, block, smem, s>>>(in, out, img, seedc, tdist, sweep, a, ntx, nty);
     } else {
         auto k = relax_tile_kernel<C, T, false, ADJ, false>;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (relax_min_blocks(C, false) > 1)  // the shared-memory carve-out that holds them
+            cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         k<<<ntiles, block, smem, s>>>(in, out, img, seedc, tdist, sweep, a, ntx, nty);
     }
     return cudaGetLastError();
