@@ -48,6 +48,7 @@ struct oift_b200_ctx {
     DevBuf awork, adist, aseedc, asmall, al2c;
     DevBuf gmap;  // normalised Sobel gradient of the gradient-blend weights
     DevBuf igring, igsmall;  // image-graph relaxation: ring index per pixel, reductions
+    DevBuf Wt;  // tile-major copy of the OIFT code planes
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -145,7 +146,7 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->dborder, &c->dhist, &c->daux, &c->dlabel, &c->yimg, &c->ylab,
                       &c->yseeds, &c->yslab, &c->yfirst, &c->yup, &c->ymerge, &c->yfseeds,
                       &c->yfslab, &c->yaux, &c->awork, &c->adist, &c->aseedc, &c->asmall,
-                      &c->al2c, &c->gmap, &c->igring, &c->igsmall};
+                      &c->al2c, &c->gmap, &c->igring, &c->igsmall, &c->Wt};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -526,6 +527,13 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         ba.lut_len = len;
     }
     if (!fulln) {
+        // tile-major copy of the codes: a tile step stages its 6 KB in one contiguous run
+        TRY(grow(c, c->Wt, (size_t)plan.ntiles * 3 * 1024 * sizeof(uint16_t)));
+        ba.Wt = (uint16_t *)c->Wt.p;
+        ba.tty = plan.TY;
+        ba.ttz = plan.TZ;
+        ba.tntx = plan.ntx;
+        ba.tnty = plan.nty;
         CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
     } else if (exact && (long long)hmm[1] - (long long)hmm[0] + (ig ? 1 : 0) > OIFT_MAX_BASE) {
         // exact base weights must fit 14 bits: count the arcs that do not (the planes are
@@ -576,7 +584,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
                       (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
                       octas, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles,
-                      fulln ? &fn : nullptr, ig);
+                      fulln ? &fn : nullptr, ig, fulln ? nullptr : ba.Wt);
     if (rc != OIFT_OK) return rc;
     unsigned long long hclamp = 0;
     CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));

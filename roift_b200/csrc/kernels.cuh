@@ -14,6 +14,10 @@ struct BuildArgs {
     const int32_t *grad;
     float blend_a;
     unsigned long long *clamped;
+    // optional tile-major copy of the 3 code planes of the 6 / 4 OIFT tiles (32 x tty x ttz):
+    // tile t holds [plane][row][32] as the tile step stages it; null = not written
+    uint16_t *Wt = nullptr;
+    int tty = 0, ttz = 0, tntx = 0, tnty = 0;
 };
 
 struct RelaxArgs {
@@ -246,7 +250,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
              long long *steps_out, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr,
              unsigned long long *cycles_out = nullptr, const OiftFullN *fn = nullptr,
-             bool round_orient = false);
+             bool round_orient = false, const uint16_t *Wt = nullptr);
 constexpr int OIFT_WARPS_PER_CTA = 16;
 
 }  // namespace oiftb

@@ -62,6 +62,8 @@ struct OiftArgs {
     float alpha;
     // image-graph orientation (OIFT_W_IMAGEGRAPH): MAX(ROUND(base f), 1), f from a float alpha
     int ig;
+    // tile-major copy of the code planes ([tile][plane][row][32]), or null
+    const uint16_t *Wt;
 };
 
 constexpr int OIFT_WARPS = 16;
@@ -259,15 +261,27 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             cp_async16(reinterpret_cast<uint4 *>(skey) + j,
                        reinterpret_cast<const uint4 *>(A.key + p0) + col);
         }
+        if (A.Wt) {  // the tile's 6 KB of codes in one contiguous run
+            const uint4 *src = reinterpret_cast<const uint4 *>(A.Wt) + (size_t)t * 384;
 #pragma unroll
-        for (int m = 0; m < 12; m++) {
-            const int j = lane + 32 * m, pl = j >> 7, r = (j >> 2) & 31, col = j & 3;
-            const size_t p0 = (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
-            if (pl < 2 || has_z)
-                cp_async16(reinterpret_cast<uint4 *>(sw) + j,
-                           reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
-            else
-                reinterpret_cast<uint4 *>(sw)[j] = make_uint4(0, 0, 0, 0);
+            for (int m = 0; m < 12; m++) {
+                const int j = lane + 32 * m, pl = j >> 7;
+                if (pl < 2 || has_z)
+                    cp_async16(reinterpret_cast<uint4 *>(sw) + j, src + j);
+                else
+                    reinterpret_cast<uint4 *>(sw)[j] = make_uint4(0, 0, 0, 0);
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < 12; m++) {
+                const int j = lane + 32 * m, pl = j >> 7, r = (j >> 2) & 31, col = j & 3;
+                const size_t p0 = (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
+                if (pl < 2 || has_z)
+                    cp_async16(reinterpret_cast<uint4 *>(sw) + j,
+                               reinterpret_cast<const uint4 *>(A.W + (size_t)pl * N + p0) + col);
+                else
+                    reinterpret_cast<uint4 *>(sw)[j] = make_uint4(0, 0, 0, 0);
+            }
         }
         {
             const int yr = y0 + (lane % TY), zr = z0 + (lane / TY);
@@ -1292,6 +1306,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
             sA.spin_limit = spin_limit;
             sA.max_levels = max_levels;
             sA.ig = 0;
+            sA.Wt = nullptr;
         }
         // ---- clear the team's state for this volume ----
         for (size_t i = tid; i < N; i += nthr) key[i] = OIFT_KEY_INF;
@@ -1439,7 +1454,8 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,
              int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
              long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end,
-             unsigned long long *cycles_out, const OiftFullN *fn, bool round_orient) {
+             unsigned long long *cycles_out, const OiftFullN *fn, bool round_orient,
+             const uint16_t *Wt) {
     size_t N = (size_t)X * Y * Z;
     cudaMemsetAsync(S.key, 0xFF, N * sizeof(uint32_t), st);
     cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
@@ -1492,6 +1508,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.gmap = fn ? fn->gmap : nullptr;
     A.alpha = fn ? fn->alpha : 1.0f;
     A.ig = round_orient ? 1 : 0;
+    A.Wt = fn ? nullptr : Wt;
     size_t smem = oift_smem_bytes();
     void *args[] = {&A};
     cudaError_t err;

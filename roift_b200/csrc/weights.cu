@@ -69,15 +69,21 @@ __global__ void __launch_bounds__(256) build_weights_kernel(const T *__restrict_
                 }
             }
             uint16_t *dst = W + (size_t)k * N + prow + x0;
+            uint4 v;
+            v.x = code[0] | ((uint32_t)code[1] << 16);
+            v.y = code[2] | ((uint32_t)code[3] << 16);
+            v.z = code[4] | ((uint32_t)code[5] << 16);
+            v.w = code[6] | ((uint32_t)code[7] << 16);
             if (x0 + 8 <= X && (((uintptr_t)dst) & 15) == 0) {
-                uint4 v;
-                v.x = code[0] | ((uint32_t)code[1] << 16);
-                v.y = code[2] | ((uint32_t)code[3] << 16);
-                v.z = code[4] | ((uint32_t)code[5] << 16);
-                v.w = code[6] | ((uint32_t)code[7] << 16);
                 *reinterpret_cast<uint4 *>(dst) = v;
             } else {
                 for (int i = 0; i < 8 && x0 + i < X; i++) dst[i] = code[i];
+            }
+            if (a.Wt && k < 3) {  // the same 8 codes in the tile-major copy (16-byte aligned)
+                const size_t t = (size_t)(x0 >> 5) + (size_t)(y / a.tty) * a.tntx +
+                                 (size_t)(z / a.ttz) * a.tntx * a.tnty;
+                const int r = (y % a.tty) + (z % a.ttz) * a.tty;
+                *reinterpret_cast<uint4 *>(a.Wt + (t * 3 + k) * 1024 + r * 32 + (x0 & 31)) = v;
             }
         }
     }
