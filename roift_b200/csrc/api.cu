@@ -466,7 +466,9 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     const bool fulln = p->adjacency == 26 || p->adjacency == 8 || blend;
     OiftPlan plan = fulln ? oift_plan_full(X, Y, Z) : oift_plan(X, Y, Z);
 
-    if (!fulln) TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
+    // with every OIFT tile full, the tile step reads only the tile-major code copy
+    const bool all_full = !fulln && X % 32 == 0 && Y % plan.TY == 0 && Z % plan.TZ == 0;
+    if (!fulln && !all_full) TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
     TRY(grow(c, c->key, N * sizeof(uint32_t)));
     TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
     const int octas = (c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms;
@@ -534,6 +536,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         ba.ttz = plan.TZ;
         ba.tntx = plan.ntx;
         ba.tnty = plan.nty;
+        ba.planes_out = !all_full;
         CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
     } else if (exact && (long long)hmm[1] - (long long)hmm[0] + (ig ? 1 : 0) > OIFT_MAX_BASE) {
         // exact base weights must fit 14 bits: count the arcs that do not (the planes are

@@ -18,6 +18,7 @@ struct BuildArgs {
     // tile t holds [plane][row][32] as the tile step stages it; null = not written
     uint16_t *Wt = nullptr;
     int tty = 0, ttz = 0, tntx = 0, tnty = 0;
+    bool planes_out = true;  // false: only the tile-major copy (every OIFT tile is full)
 };
 
 struct RelaxArgs {

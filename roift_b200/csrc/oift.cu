@@ -283,10 +283,14 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
                     reinterpret_cast<uint4 *>(sw)[j] = make_uint4(0, 0, 0, 0);
             }
         }
+        // halo codes of the -x / -y / -z neighbours: from the tile-major copy (the lower
+        // neighbour tiles of a full tile are full), else from the planes
         {
             const int yr = y0 + (lane % TY), zr = z0 + (lane / TY);
             if (x0 > 0)
-                cp_async4(shx + 2 * lane, A.W + (size_t)(x0 - 2) + (size_t)yr * X + (size_t)zr * XY);
+                cp_async4(shx + 2 * lane,
+                          A.Wt ? A.Wt + ((size_t)(t - 1) * 3) * 1024 + lane * 32 + 30
+                               : A.W + (size_t)(x0 - 2) + (size_t)yr * X + (size_t)zr * XY);
             else
                 shx[2 * lane + 1] = 0;
         }
@@ -294,7 +298,8 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             const int zl = lane >> 2, col = lane & 3;
             if (y0 > 0)
                 cp_async16(shy + zl * 32 + col * 8,
-                           A.W + N + (size_t)(x0 + col * 8) + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY);
+                           A.Wt ? A.Wt + ((size_t)(t - A.ntx) * 3 + 1) * 1024 + ((TY - 1) + zl * TY) * 32 + col * 8
+                                : A.W + N + (size_t)(x0 + col * 8) + (size_t)(y0 - 1) * X + (size_t)(z0 + zl) * XY);
             else
                 *reinterpret_cast<uint4 *>(shy + zl * 32 + col * 8) = make_uint4(0, 0, 0, 0);
         }
@@ -302,7 +307,8 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             const int yl = lane >> 2, col = lane & 3;
             if (z0 > 0)
                 cp_async16(shz + yl * 32 + col * 8,
-                           A.W + 2 * N + (size_t)(x0 + col * 8) + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY);
+                           A.Wt ? A.Wt + ((size_t)(t - A.ntx * A.nty) * 3 + 2) * 1024 + (yl + (TZ - 1) * TY) * 32 + col * 8
+                                : A.W + 2 * N + (size_t)(x0 + col * 8) + (size_t)(y0 + yl) * X + (size_t)(z0 - 1) * XY);
             else
                 *reinterpret_cast<uint4 *>(shz + yl * 32 + col * 8) = make_uint4(0, 0, 0, 0);
         }

@@ -74,7 +74,8 @@ __global__ void __launch_bounds__(256) build_weights_kernel(const T *__restrict_
             v.y = code[2] | ((uint32_t)code[3] << 16);
             v.z = code[4] | ((uint32_t)code[5] << 16);
             v.w = code[6] | ((uint32_t)code[7] << 16);
-            if (x0 + 8 <= X && (((uintptr_t)dst) & 15) == 0) {
+            if (!a.planes_out) {
+            } else if (x0 + 8 <= X && (((uintptr_t)dst) & 15) == 0) {
                 *reinterpret_cast<uint4 *>(dst) = v;
             } else {
                 for (int i = 0; i < 8 && x0 + i < X; i++) dst[i] = code[i];
