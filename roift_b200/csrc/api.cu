@@ -49,6 +49,9 @@ struct oift_b200_ctx {
     DevBuf gmap;  // normalised Sobel gradient of the gradient-blend weights
     DevBuf igring, igsmall;  // image-graph relaxation: ring index per pixel, reductions
     DevBuf Wt;  // tile-major copy of the OIFT code planes
+    // pinned host staging of the seed labels of the host entry
+    int32_t *hslab = nullptr;
+    size_t hslab_n = 0;
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -149,6 +152,7 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->al2c, &c->gmap, &c->igring, &c->igsmall, &c->Wt};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
+    if (c->hslab) cudaFreeHost(c->hslab);
     for (auto &e : c->ev) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -680,7 +684,22 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
     cudaSetDevice(c->device);
     const size_t N = (size_t)p->xsize * p->ysize * p->zsize;
     cudaStream_t s = c->stream;
-    std::vector<int32_t> slab(nseeds);
+    // the seed labels are staged in pinned memory owned by the context, so their copy is
+    // asynchronous; an earlier call's copy from it has ended once the stream is idle
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return OIFT_E_CUDA;
+    if (c->hslab_n < (size_t)nseeds) {
+        if (c->hslab) cudaFreeHost(c->hslab);
+        c->hslab = nullptr;
+        c->hslab_n = 0;
+        if (cudaHostAlloc(&c->hslab, (size_t)nseeds * sizeof(int32_t), cudaHostAllocDefault) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            c->hslab = nullptr;
+            return OIFT_E_OOM;
+        }
+        c->hslab_n = (size_t)nseeds;
+    }
+    int32_t *slab = c->hslab;
     for (int i = 0; i < nseeds; i++) {
         if (seeds[i] < 0 || (size_t)seeds[i] >= N) return OIFT_E_SEED_RANGE;
         int lb = label[seeds[i]];
@@ -695,7 +714,7 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
     if (mask) TRY(grow(c, c->mask8, N));
     CU(cudaMemcpyAsync(c->img32.p, image, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(c->seeds.p, seeds, (size_t)nseeds * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(c->slabels.p, slab.data(), (size_t)nseeds * sizeof(int32_t),
+    CU(cudaMemcpyAsync(c->slabels.p, slab, (size_t)nseeds * sizeof(int32_t),
                        cudaMemcpyHostToDevice, s));
     oift_b200_outputs o{};
     o.cost = cost ? (int32_t *)c->cost.p : nullptr;
