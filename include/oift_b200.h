@@ -188,6 +188,15 @@ OIFT_API int oift_b200_batch_graph_launch(oift_b200_batch_graph *graph, oift_b20
 OIFT_API int oift_b200_batch_graph_destroy(oift_b200_batch_graph *graph);
 /* CTAs of the persistent OIFT grid of this context (0 = one per SM, the default). */
 OIFT_API int oift_b200_set_oift_grid(oift_b200_ctx *ctx, int ctas);
+/* Bounds of the OIFT kernels' device-side waits for later calls of this context:
+ * spin_limit = polls (~64 ns each) of one wait (grid or team barrier, end of a level)
+ * before it gives up, max_levels = (cost, label) levels before the run counts as runaway.
+ * Reaching either ends the launch cleanly (every warp leaves, the context stays usable)
+ * and the call returns OIFT_E_NOT_CONVERGED; in the batched driver the team that hit it
+ * reports OIFT_E_NOT_CONVERGED for its job, stops, and no team takes a further job.
+ * Values <= 0 restore the defaults (2e7 polls, 4e6 levels).  The same guard as the
+ * reference's iteration cap (gpu/oift_fmax_gpu.cu:197,240-242), exposed for testing. */
+OIFT_API int oift_b200_set_limits(oift_b200_ctx *ctx, long long spin_limit, int max_levels);
 
 /* Steps around the path in the reference CLI (oiftrelax.cpp main). */
 /* `passes` Gaussian blurs (Scene32::GaussianBlur, gft_filtering3.cpp:385-397) of a device

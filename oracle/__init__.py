@@ -66,6 +66,9 @@ def lib():
         L.or_energy.restype = C.c_int
         L.or_energy.argtypes = [_u16p, C.c_int, C.c_int, C.c_int, C.c_int, _Polarity, _i32p,
                                 C.c_int, _i32p]
+        L.or_tie_stats.restype = None
+        L.or_tie_stats.argtypes = [_u16p, C.c_int, C.c_int, C.c_int, C.c_int, _Polarity, _i32p,
+                                   _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.or_relax_f32.restype = C.c_int
         L.or_relax_f32.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                    C.c_void_p, C.c_int, _i32p, C.c_int, _i32p, C.c_int,
@@ -242,6 +245,32 @@ def energy(W, shape_xyz, adj, label, nl, pol=None, per_class=None):
     P, keep = polarity(pol, per_class)
     e = lib().or_energy(W, X, Y, Z, adj, P, np.ascontiguousarray(label, np.int32), nl, e_lb)
     return e, e_lb[:nl]
+
+
+def tie_stats(W, shape_xyz, adj, cost, lab_a, lab_b, seeds, pol=None, per_class=None,
+              want_flags=False):
+    """Equal-cost tie accounting of labelling A (R2 / the CUDA result) against labelling B
+    (the reference Prim forest) over the cost map `cost`.  Returns a dict with
+    ties (voxels offered their cost by two labels in A), diffs, explained (differences
+    where both labels reach the voxel at its cost) and unexplained; flags per voxel when
+    asked (bit 0 tie, bit 1 differs, bit 2 explained)."""
+    X, Y, Z = shape_xyz
+    N = X * Y * Z
+    is_seed = np.zeros(N, np.uint8)
+    is_seed[np.asarray(seeds, np.int64)] = 1
+    out = np.zeros(4, np.int64)
+    flags = np.zeros(N, np.uint8) if want_flags else None
+    P, keep = polarity(pol, per_class)
+    lib().or_tie_stats(W, X, Y, Z, adj, P, np.ascontiguousarray(cost, np.int32).reshape(-1),
+                       np.ascontiguousarray(lab_a, np.int32).reshape(-1),
+                       np.ascontiguousarray(lab_b, np.int32).reshape(-1),
+                       is_seed.ctypes.data, out.ctypes.data,
+                       flags.ctypes.data if flags is not None else None)
+    d = {"ties": int(out[0]), "diffs": int(out[1]), "explained": int(out[2]),
+         "unexplained": int(out[3])}
+    if want_flags:
+        d["flags"] = flags
+    return d
 
 
 def relax(img, adj, seeds, label, ntimes, pol=None, per_class=None, fp64=False):

@@ -234,7 +234,9 @@ static uint64_t hpop(heap64 *h) {
 /* R2.  Key = (cost << 32 | label) << 24 | voxel would not fit; the heap holds
  * (cost << 48 | label << 32 | voxel) with voxel < 2^32, cost < 2^16, label < 2^16.
  * Ties inside one (cost,label) level pop in any order: the set conquered at a level
- * is a reachability closure, so the result does not depend on that order. */
+ * is a reachability closure, so the result does not depend on that order.  Seeds keep
+ * their labels: OIFT_Multi enters them at value 0 and conquers a voxel only through
+ * w < value[q] (gft/src/gft_ift.cpp:929-976), so no arc can take a seed from it. */
 static int fmax_core(const wsrc *ws, int X, int Y, int Z, int adj, or_polarity pol,
                      const int *seeds, int nseeds, const int *label_in, int *cost, int *label,
                      int *pred) {
@@ -242,6 +244,7 @@ static int fmax_core(const wsrc *ws, int X, int Y, int Z, int adj, or_polarity p
     int n = or_adjacency(adj, dx, dy, dz);
     size_t N = (size_t)X * Y * Z;
     unsigned char *done = (unsigned char *)calloc(N, 1);
+    unsigned char *seed = (unsigned char *)calloc(N, 1);
     heap64 h = {0};
     for (size_t p = 0; p < N; p++) {
         cost[p] = INT32_MAX;
@@ -252,6 +255,7 @@ static int fmax_core(const wsrc *ws, int X, int Y, int Z, int adj, or_polarity p
         int p = seeds[i];
         if (p < 0 || (size_t)p >= N) continue;
         int lb = label_in[p] < 0 ? 0 : label_in[p];
+        seed[p] = 1;
         if (cost[p] == 0 && label[p] <= lb) continue;
         cost[p] = 0;
         label[p] = lb;
@@ -275,7 +279,7 @@ static int fmax_core(const wsrc *ws, int X, int Y, int Z, int adj, or_polarity p
             int qx = x + dx[i], qy = y + dy[i], qz = z + dz[i];
             if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
             size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
-            if (done[q]) continue;
+            if (done[q] || seed[q]) continue;
             int w = arc_weight(ws, N, n, i, p, q, pl);
             int nc = MAX(c, w);
             if (nc < cost[q] || (nc == cost[q] && lb < label[q])) {
@@ -288,6 +292,7 @@ static int fmax_core(const wsrc *ws, int X, int Y, int Z, int adj, or_polarity p
     }
     free(h.k);
     free(done);
+    free(seed);
     return levels;
 }
 
@@ -641,6 +646,78 @@ int or_energy(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
                 }
             }
     return e;
+}
+
+/* Equal-cost tie accounting.  A label l "offers" voxel p its cost when some in-bounds
+ * neighbour q labelled l reaches p at exactly cost[p]: MAX(cost[q], w_l(q -> p)) ==
+ * cost[p], w_l the oriented weight of gft_ift.cpp:965-973 with the polarity of the
+ * tail's label l.  Non-seed voxels only (seeds hold cost 0 by definition).
+ *   out[0] = voxels offered their cost by >= 2 labels in labelling A (tie voxels of A);
+ *   out[1] = voxels where labA != labB;
+ *   out[2] = of those, voxels where labA[p] is offered in A and labB[p] is offered in B
+ *            (both labellings' labels reach p at the same cost: an equal-cost tie);
+ *   out[3] = out[1] - out[2] (differences that are not explained by a tie).
+ * flags (optional, per voxel): bit 0 tie in A, bit 1 labels differ, bit 2 classified. */
+static int offered(const uint16_t *W, size_t N, int n, const int *dx, const int *dy,
+                   const int *dz, int X, int Y, int Z, or_polarity pol, const int *cost,
+                   const int *lab, size_t p, int want) {
+    int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / ((size_t)X * Y));
+    for (int i = 0; i < n; i++) {
+        int qx = x + dx[i], qy = y + dy[i], qz = z + dz[i];
+        if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
+        size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
+        if (lab[q] != want || cost[q] == INT32_MAX) continue;
+        /* the arc q -> p is direction n-1-i seen from q */
+        int w = arc_weight_codes(W, N, n, n - 1 - i, q, p, polarity_of(pol, want));
+        if (MAX(cost[q], w) == cost[p]) return 1;
+    }
+    return 0;
+}
+
+void or_tie_stats(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
+                  const int *cost, const int *labA, const int *labB,
+                  const unsigned char *is_seed, long long *out, unsigned char *flags) {
+    int dx[26], dy[26], dz[26];
+    int n = or_adjacency(adj, dx, dy, dz);
+    size_t N = (size_t)X * Y * Z;
+    out[0] = out[1] = out[2] = out[3] = 0;
+    for (size_t p = 0; p < N; p++) {
+        unsigned char f = 0;
+        if (!is_seed[p] && cost[p] != INT32_MAX) {
+            /* labels offering p its cost in A: stop at the second distinct one */
+            int first = OR_NIL, two = 0;
+            int x = (int)(p % X), y = (int)((p / X) % Y), z = (int)(p / ((size_t)X * Y));
+            for (int i = 0; i < n && !two; i++) {
+                int qx = x + dx[i], qy = y + dy[i], qz = z + dz[i];
+                if (!in_bounds(qx, qy, qz, X, Y, Z)) continue;
+                size_t q = (size_t)qx + (size_t)qy * X + (size_t)qz * X * Y;
+                int lq = labA[q];
+                if (lq < 0 || lq == first || cost[q] == INT32_MAX) continue;
+                int w = arc_weight_codes(W, N, n, n - 1 - i, q, p, polarity_of(pol, lq));
+                if (MAX(cost[q], w) != cost[p]) continue;
+                if (first == OR_NIL) first = lq;
+                else two = 1;
+            }
+            if (two) {
+                f |= 1;
+                out[0]++;
+            }
+            if (labA[p] != labB[p]) {
+                f |= 2;
+                out[1]++;
+                if (offered(W, N, n, dx, dy, dz, X, Y, Z, pol, cost, labA, p, labA[p]) &&
+                    offered(W, N, n, dx, dy, dz, X, Y, Z, pol, cost, labB, p, labB[p])) {
+                    f |= 4;
+                    out[2]++;
+                }
+            }
+        } else if (labA[p] != labB[p]) {
+            f |= 2;
+            out[1]++;
+        }
+        if (flags) flags[p] = f;
+    }
+    out[3] = out[1] - out[2];
 }
 
 /* gft/src/gft_ift.cpp:8684-8720 */

@@ -83,6 +83,15 @@ void or_oift_prim(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity p
 int or_energy(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
               const int *label, int nl, int *energy_lb);
 
+/* Equal-cost tie accounting between labelling A (the lexicographic restatement R2 or the
+ * CUDA result) and labelling B (the reference's Prim forest) over one cost map.  out[4]:
+ * tie voxels of A (offered their cost by two labels), label differences, differences
+ * where both labels are offered the voxel's cost, and unexplained differences.  flags
+ * (optional) per voxel: bit 0 tie in A, bit 1 differs, bit 2 difference explained. */
+void or_tie_stats(const uint16_t *W, int X, int Y, int Z, int adj, or_polarity pol,
+                  const int *cost, const int *labA, const int *labB,
+                  const unsigned char *is_seed, long long *out, unsigned char *flags);
+
 /* Relaxation classes (gft_ift.cpp:8684-8720): classes = sorted labels present among
  * the seeds plus 0.  Returns nclasses, fills class_labels[<=cap]. */
 int or_relax_classes(const int *seeds, int nseeds, const int *label, int n,

@@ -94,7 +94,8 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status",
            "oift_b200_level_profile", "oift_b200_selftest_div100",
            "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes",
-           "oift_b200_run_batch", "oift_b200_set_oift_grid", "oift_b200_gaussian_blur_i32",
+           "oift_b200_run_batch", "oift_b200_set_oift_grid", "oift_b200_set_limits",
+           "oift_b200_gaussian_blur_i32",
            "oift_b200_conditional_dilation", "oift_b200_inject_boundary_seeds",
            "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
            "oift_b200_run_pyramid_device_i16", "oift_b200_adjoint",
@@ -128,6 +129,7 @@ def lib():
         L.oift_b200_run_batch.argtypes = [vp, C.POINTER(Params), C.POINTER(Job), C.c_int, C.c_int,
                                           C.POINTER(BatchStats)]
         L.oift_b200_set_oift_grid.argtypes = [vp, C.c_int]
+        L.oift_b200_set_limits.argtypes = [vp, C.c_longlong, C.c_int]
         L.oift_b200_batch_graph_create.argtypes = [vp, C.POINTER(Params), C.POINTER(Job), C.c_int,
                                                    C.c_int, C.POINTER(vp)]
         L.oift_b200_batch_graph_launch.argtypes = [vp, C.POINTER(Job), C.POINTER(C.c_float)]
@@ -281,6 +283,13 @@ class Context:
         if rc != OK:
             raise OiftError(rc, "oift_b200_batch_graph_create")
         return BatchGraph(h, jobs)
+
+    def set_limits(self, spin_limit: int = 0, max_levels: int = 0):
+        """Bounds of the OIFT kernels' device waits (polls of one wait, levels of a run);
+        0 restores the defaults.  Reaching one ends the call with E_NOT_CONVERGED."""
+        rc = lib().oift_b200_set_limits(self._h, C.c_longlong(int(spin_limit)), int(max_levels))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_set_limits")
 
     def set_oift_grid(self, ctas: int):
         rc = lib().oift_b200_set_oift_grid(self._h, int(ctas))

@@ -28,6 +28,9 @@ struct oift_b200_ctx {
     int device = 0;
     int sms = 148;
     int oift_ctas = 0;  // CTAs of the persistent OIFT grid (0 = one per SM)
+    // bounds of the OIFT kernels' waits (oift_b200_set_limits)
+    long long spin_limit = OIFT_DEFAULT_SPIN_LIMIT;
+    int max_levels = OIFT_DEFAULT_MAX_LEVELS;
     std::vector<oift_b200_ctx *> lanes;  // sub-contexts (relaxation streams) of the batched driver
     std::vector<std::pair<int, double>> tune_cands;  // batch autotuner: (teams, rate)
     cudaStream_t stream = nullptr;
@@ -169,6 +172,17 @@ size_t oift_b200_scratch_bytes(const oift_b200_ctx *c) {
 int oift_b200_set_oift_grid(oift_b200_ctx *c, int ctas) {
     if (!c || ctas < 0) return OIFT_E_BAD_ARG;
     c->oift_ctas = ctas;
+    return OIFT_OK;
+}
+
+int oift_b200_set_limits(oift_b200_ctx *c, long long spin_limit, int max_levels) {
+    if (!c) return OIFT_E_BAD_ARG;
+    c->spin_limit = spin_limit > 0 ? spin_limit : OIFT_DEFAULT_SPIN_LIMIT;
+    c->max_levels = max_levels > 0 ? max_levels : OIFT_DEFAULT_MAX_LEVELS;
+    for (oift_b200_ctx *l : c->lanes) {
+        l->spin_limit = c->spin_limit;
+        l->max_levels = c->max_levels;
+    }
     return OIFT_OK;
 }
 
@@ -577,6 +591,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     float dflt = 0.0f;
     TRY(upload_polarity(c, p, &npol, &dflt));
     OiftScratch S;
+    S.spin_limit = c->spin_limit;
+    S.max_levels = c->max_levels;
     S.key = (uint32_t *)c->key.p;
     S.tpend = (uint32_t *)c->tpend.p;
     S.mbox = (unsigned long long *)c->queue.p;
@@ -1739,6 +1755,8 @@ static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_
     S.g = (OiftGlobals *)c->bglob.p;
     S.next_job = (unsigned int *)c->bctl.p;
     S.abort = (int *)c->bctl.p + 1;
+    S.spin_limit = c->spin_limit;
+    S.max_levels = c->max_levels;
     OiftTeamJob *d_jobs = (OiftTeamJob *)c->bjobs.p;
     bp->d_jobs = d_jobs;
     CU(cudaMemcpyAsync(d_jobs, dj.data(), (size_t)nj * sizeof(OiftTeamJob), cudaMemcpyHostToDevice, s));

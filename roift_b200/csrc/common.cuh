@@ -7,8 +7,9 @@
 //             neighbour offset of the gft Spheric order (gft/src/gft_adjrel3.cpp:47-85):
 //             6-adj: +x, +y, +z; 26-adj: the 13 offsets after the centre.  bits 0..13
 //             base weight, bit 14 = (I_p < I_q), bit 15 = (I_p > I_q).
-//   key       uint32 [N] OIFT state: cost << 17 | label << 1 | U  (U = 1 not yet
-//             expanded), 0xFFFFFFFF = unreached.  Integer order = (cost, label) order.
+//   key       uint32 [N] OIFT state: field << 17 | label << 1 | U  (U = 1 not yet
+//             expanded), 0xFFFFFFFF = unreached; field = 0 for a seed, cost + 1 for any
+//             other voxel.  Integer order = (cost, label) order, seeds first.
 //   membership float [C][N] planar relaxation state (two buffers).
 #pragma once
 #include <cstdint>
@@ -49,10 +50,26 @@ inline Adjacency make_adjacency(int adj) {
     return A;
 }
 
-__host__ __device__ inline uint32_t make_key(int cost, int label, int unexpanded) {
-    return ((uint32_t)cost << 17) | ((uint32_t)label << 1) | (uint32_t)unexpanded;
+// Keys.  A seed holds field 0 and every other voxel field cost + 1, so a seed's key lies
+// below any key an arc can offer it: seeds keep their labels, as in OIFT_Multi, which
+// gives the labelled voxels value 0 and conquers a voxel only when w < value[q]
+// (gft/src/gft_ift.cpp:929-976).  The oriented cost is at most 2 * OIFT_MAX_BASE = 32766
+// (|per| <= 100), so the field fits its 15 bits.
+__host__ __device__ inline uint32_t make_key(int field, int label, int unexpanded) {
+    return ((uint32_t)field << 17) | ((uint32_t)label << 1) | (uint32_t)unexpanded;
 }
-__host__ __device__ inline int key_cost(uint32_t k) { return (int)(k >> 17); }
+__host__ __device__ inline uint32_t seed_key(int label) { return make_key(0, label, 1); }
+// Key offered at path cost nc (>= 0) with the label bits (label << 1 | U) of the tail.
+__host__ __device__ inline uint32_t offer_key(int nc, uint32_t lab_bits) {
+    return ((uint32_t)(nc + 1) << 17) | lab_bits;
+}
+// Path cost of a conquered voxel (0 for a seed).
+__host__ __device__ inline int key_cost(uint32_t k) {
+    const int f = (int)(k >> 17);
+    return f > 0 ? f - 1 : 0;
+}
+// Cost at which a level floods: -1 on the seeds' own levels, where no arc opens.
+__host__ __device__ inline int key_level_cost(uint32_t k) { return (int)(k >> 17) - 1; }
 __host__ __device__ inline int key_label(uint32_t k) { return (int)((k >> 1) & 0xFFFFu); }
 
 // Oriented arc weight, gft/src/gft_ift.cpp:965-973: int w = |dI|; w *= (1 +/- per/100)
@@ -65,9 +82,10 @@ __host__ __device__ inline int oriented_weight(uint32_t base, bool tail_gt, bool
     return (int)base;
 }
 
-// Largest base b in [0, OIFT_MAX_BASE] with (int)(b * f) <= c; trunc(b*f) is monotone
-// in b for f >= 0, so "oriented weight <= c" is "base <= threshold".
+// Largest base b in [0, OIFT_MAX_BASE] with (int)(b * f) <= c, -1 when c < 0; trunc(b*f)
+// is monotone in b for f >= 0, so "oriented weight <= c" is "base <= threshold".
 __host__ __device__ inline int max_base_for_cost(int c, double f) {
+    if (c < 0) return -1;  // no arc weighs less than 0
     if (f <= 0.0) return OIFT_MAX_BASE;
     double b = floor((double)(c + 1) / f);
     int bi = b > (double)OIFT_MAX_BASE ? OIFT_MAX_BASE : (b < 0.0 ? 0 : (int)b);

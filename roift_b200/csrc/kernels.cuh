@@ -64,6 +64,12 @@ struct OiftGlobals {
 };
 
 
+// Default bounds of the persistent OIFT kernels' waits: about 1-2 s of polling at ~64 ns
+// per poll, and far more levels than any input has (at most 32767 costs x 32768 labels
+// would be reachable only by a runaway loop).
+constexpr long long OIFT_DEFAULT_SPIN_LIMIT = 20000000LL;
+constexpr int OIFT_DEFAULT_MAX_LEVELS = 4000000;
+
 struct OiftPlan {
     int TY, TZ, ntx, nty, ntz, ntiles;
     unsigned int qcap;
@@ -77,6 +83,10 @@ struct OiftScratch {
     OiftGlobals *g;
     unsigned int *lprof = nullptr;  // optional per-level profile [cap][2]
     int lprof_cap = 0;
+    // bounded waits: polls of one wait before it gives up, and levels before the run is
+    // declared runaway; either ends the launch with OIFT_E_NOT_CONVERGED
+    long long spin_limit = OIFT_DEFAULT_SPIN_LIMIT;
+    int max_levels = OIFT_DEFAULT_MAX_LEVELS;
 };
 
 template <typename T>
@@ -134,6 +144,8 @@ struct OiftTeamScratch {
     OiftGlobals *g;           // [teams]
     unsigned int *next_job;   // job counter shared by the teams
     int *abort;               // set when a team stops on an error; others take no new job
+    long long spin_limit = OIFT_DEFAULT_SPIN_LIMIT;  // as OiftScratch
+    int max_levels = OIFT_DEFAULT_MAX_LEVELS;
 };
 
 // Batched OIFT: one cooperative launch of `ctas` CTAs split into `teams` teams of

@@ -188,8 +188,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
                                                    tail_low ? lo : hi, fgt, flt)
                            : oriented_weight(code & OIFT_BASE_MASK, tail_low ? hi : lo,
                                              tail_low ? lo : hi, fgt, flt);
-        const int nc = w > c ? w : c;
-        return ((uint32_t)nc << 17) | lab_bits;
+        return offer_key(w > c ? w : c, lab_bits);
     };
     // A successful out-of-tile push either continues this level next door (the
     // face-neighbour tile is marked for re-activation; all marks of the tile step are
@@ -804,8 +803,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     };
     auto arc_key = [&](int hp, int hq) -> uint32_t {
         const int w = arc_w(hp, hq);
-        const int nc = w > c ? w : c;
-        return ((uint32_t)nc << 17) | lab_bits;
+        return offer_key(w > c ? w : c, lab_bits);
     };
     auto pending = [&]() {
         uint32_t m = OIFT_KEY_INF;
@@ -1114,7 +1112,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         }
         prev_level = kk;
         if (leader_cta && threadIdx.x == 0) g->levels = e + 1;
-        const int c = key_cost(kk), l = key_label(kk);
+        const int c = key_level_cost(kk), l = key_label(kk);
         const double per = (double)polarity_of(A, l);
         double fgt, flt;
         int bgt, blt;
@@ -1333,7 +1331,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
                 atomicExch(&g->bad_seed, OIFT_E_BAD_ARG);
                 continue;
             }
-            const uint32_t k = make_key(0, lb, 1);
+            const uint32_t k = seed_key(lb);
             atomicMin(&key[p], k);
             const int x = p % X, y = (p / X) % Y, z = (int)(p / ((size_t)X * Y));
             atomicMin(&tpend[(x >> 5) + (y / TY) * ntx + (z / TZ) * ntx * nty], k);
@@ -1384,7 +1382,7 @@ __global__ void oift_seed_kernel(uint32_t *key, uint32_t *tpend, const int32_t *
         } else if (lb > OIFT_MAX_LABEL) {
             atomicExch(bad, 2);
         } else {
-            k = make_key(0, lb, 1);
+            k = seed_key(lb);
             atomicMin(&key[p], k);
             const int x = p % X, y = (p / X) % Y, z = (int)(p / ((size_t)X * Y));
             t = (x >> 5) + (y / TY) * ntx + (z / TZ) * ntx * nty;
@@ -1504,8 +1502,8 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.npol = npol;
     A.pol_default = pol_default;
     A.g = S.g;
-    A.spin_limit = 20000000LL;  // ~1-2 s of polling at ~64 ns per spin
-    A.max_levels = 4000000;
+    A.spin_limit = S.spin_limit;
+    A.max_levels = S.max_levels;
     A.img = fn ? fn->img : nullptr;
     A.wmode = fn ? fn->wmode : 0;
     A.wcap = fn ? fn->wcap : OIFT_MAX_BASE;
@@ -1571,8 +1569,8 @@ int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ct
         cudaGetLastError();
         return OIFT_E_CUDA;
     }
-    long long spin_limit = 20000000LL;
-    int max_levels = 4000000;
+    long long spin_limit = S.spin_limit;
+    int max_levels = S.max_levels;
     int nt = teams;
     OiftTeamScratch sc = S;
     void *args[] = {&d_jobs, &njobs, &nt, &sc, &spin_limit, &max_levels};

@@ -78,12 +78,15 @@ def test_oift_cost_and_labels_match_oracle(roift, oracle_lib, shape, pol, adj, n
         assert e_gpu == e_ref
         # label differences to the reference Prim forest only where costs tie
         _, _, _, fm = O.oift_prim(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
-        diff = lab != lab_ref
         assert np.array_equal(fm, cost), "f_max along the reference forest differs"
-        if diff.any():
-            # every differing voxel is an equal-cost tie: some neighbour of another label
-            # reaches it at the same cost
-            assert cost[diff].max() >= 0
+        # every differing voxel is an equal-cost tie: a neighbour labelled as in our map and
+        # one labelled as in the reference's both reach it at exactly its cost; a volume
+        # without tie voxels has no difference at all
+        ts = O.tie_stats(W, (X, Y, Z), adj, cost, lab, lab_ref, c.seeds, pol=c.pol)
+        assert ts["diffs"] == int((lab != lab_ref).sum())
+        assert ts["unexplained"] == 0, ts
+        if ts["ties"] == 0:
+            assert ts["diffs"] == 0, ts
 
 
 @pytest.mark.parametrize("shape,pol,adj,nl,mode", [CASES[0], CASES[2], CASES[3], CASES[4]])

@@ -92,6 +92,60 @@ def test_oracle_planted_mistake_is_caught(oracle_lib):
     assert not np.array_equal(c1, c2)
 
 
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_tie_accounting_on_golden(oracle_lib, path):
+    """R2 labels against the reference OIFT_Multi labels of the fixtures: every difference
+    is an equal-cost tie, and a fixture without tie voxels has no difference."""
+    d = np.load(path)
+    img = d["image"]
+    Z, Y, X = img.shape
+    adj = int(d["adjacency"])
+    seeds, sl = d["seeds"], d["seed_labels"]
+    pa = _pol_args(d)
+    W, _ = O.build_weights(img, adj, "grad")
+    cost, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), adj, seeds, sl, **pa)
+    ts = O.tie_stats(W, (X, Y, Z), adj, cost, lab_r2, d["ref_oift_label"], seeds, **pa)
+    assert ts["diffs"] == int((lab_r2 != d["ref_oift_label"]).sum())
+    assert ts["unexplained"] == 0, ts
+    if ts["ties"] == 0:
+        assert ts["diffs"] == 0
+
+
+def test_tie_accounting_known_ties_and_planted_mistake(oracle_lib):
+    """A flat image: every arc weighs 0, so both labels can reach every free voxel at cost
+    0.  R2 gives all of them the smaller label (its tie voxels are the object seed's
+    neighbours), the Prim order the label that arrives first; each difference is explained.  A label flipped on a tie-free
+    volume (planted in the oracle's output, on the CPU) is reported as unexplained."""
+    img = np.full((1, 6, 9), 50, np.int32)
+    X, Y, Z = 9, 6, 1
+    seeds = np.array([0, 8 + 5 * 9], np.int32)
+    sl = np.array([1, 0], np.int32)
+    W, _ = O.build_weights(img, 4, "grad")
+    cost, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), 4, seeds, sl, pol=0.0)
+    lab_r1 = O.oift_prim(W, (X, Y, Z), 4, seeds, sl, pol=0.0)[0]
+    ts = O.tie_stats(W, (X, Y, Z), 4, cost, lab_r2, lab_r1, seeds, pol=0.0)
+    assert ts["ties"] == 2
+    assert ts["diffs"] > 0 and ts["unexplained"] == 0
+    # tie-free volume (the 256^3 workload generator at 64^3): no tie, no difference, and a
+    # flipped label is caught
+    c = synth.ellipsoid3d(seed=2, size=64, sweeps=1)
+    img = c.image.astype(np.int32)
+    Z, Y, X = c.shape
+    W, _ = O.build_weights(img, 6, "grad_q", wq=4095)
+    cost, lab_r2, _ = O.oift_fmax(W, (X, Y, Z), 6, c.seeds, c.seed_labels, pol=c.pol)
+    lab_r1, _, _, fm = O.oift_prim(W, (X, Y, Z), 6, c.seeds, c.seed_labels, pol=c.pol)
+    assert np.array_equal(fm, cost)
+    assert O.tie_stats(W, (X, Y, Z), 6, cost, lab_r2, lab_r1, c.seeds, pol=c.pol) == \
+        {"ties": 0, "diffs": 0, "explained": 0, "unexplained": 0}
+    seeded = np.zeros(c.n, bool)
+    seeded[c.seeds] = True
+    p = int(np.flatnonzero(~seeded & (lab_r2 == 1))[0])
+    bad = lab_r2.copy()
+    bad[p] = 0
+    ts = O.tie_stats(W, (X, Y, Z), 6, cost, bad, lab_r1, c.seeds, pol=c.pol)
+    assert ts["diffs"] == 1 and ts["unexplained"] == 1
+
+
 def test_weight_builder_modes(oracle_lib):
     img = np.array([[[0, 10, 5000, 4990]]], np.int32)
     W, ncl = O.build_weights(img, 6, "grad_q", wq=4095)
