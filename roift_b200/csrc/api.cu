@@ -489,7 +489,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     if (!fulln && !all_full) TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
     TRY(grow(c, c->key, N * sizeof(uint32_t)));
     TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
-    const int octas = (c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms;
+    const int octas = std::max((c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms,
+                               std::min(c->sms, oift_min_ctas(plan.ntiles)));
     TRY(grow(c, c->queue, oift_mbox_bytes(plan, octas)));
     TRY(grow(c, c->glob, oift_globals_bytes()));
     TRY(grow(c, c->flag, 4 * sizeof(int)));
@@ -1562,6 +1563,20 @@ struct BatchPrep {
     unsigned long long *d_clamp = nullptr;
 };
 
+// Most teams the batch can be split into: every team must hold enough CTAs to own the tiles
+// of the largest job (a CTA's tile sets live in shared memory).
+static int batch_max_teams(const oift_b200_ctx *c, const oift_b200_job *jobs, int first,
+                           int count) {
+    int need = 1;
+    for (int j = first; j < first + count; j++) {
+        const oift_b200_job &jb = jobs[j];
+        if (jb.xsize <= 0 || jb.ysize <= 0 || jb.zsize <= 0) continue;
+        const OiftPlan P = oift_plan(jb.xsize, jb.ysize, jb.zsize);
+        need = std::max(need, oift_min_ctas(P.ntiles));
+    }
+    return std::max(1, c->sms / need);
+}
+
 static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_b200_job *jobs,
                          int first, int count, int teams, BatchPrep *bp) {
     cudaStream_t s = c->stream;
@@ -1791,6 +1806,7 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     const int end = first + count;
 
     BatchPrep bp;
+    teams = std::min(teams, batch_max_teams(c, jobs, first, count));
     TRY(batch_prepare(c, common, jobs, first, count, teams, &bp));
     const int nimg = bp.nimg, nj = bp.nj;
     if (nimg == 0) {
@@ -1920,7 +1936,7 @@ int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_params *com
                 teams = tc.first;
             }
     }
-    teams = std::max(1, std::min(teams, njobs));
+    teams = std::max(1, std::min(std::min(teams, njobs), batch_max_teams(ctx, jobs, 0, njobs)));
     oift_b200_batch_graph *g = new oift_b200_batch_graph();
     g->njobs = njobs;
     g->weight_mode = common->weight_mode;

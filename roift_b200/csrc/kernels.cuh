@@ -68,6 +68,9 @@ struct OiftGlobals {
 // per poll, and far more levels than any input has (at most 32767 costs x 32768 labels
 // would be reachable only by a runaway loop).
 constexpr long long OIFT_DEFAULT_SPIN_LIMIT = 20000000LL;
+// Tiles one CTA of the persistent OIFT kernels can own: its wanted / running sets live in
+// shared memory as 64-bit words (16384 tiles = 16.7 M voxels of 32 x 8 x 4 tiles per CTA).
+constexpr int OIFT_CTA_TILE_WORDS = 256;
 constexpr int OIFT_DEFAULT_MAX_LEVELS = 4000000;
 
 struct OiftPlan {
@@ -117,6 +120,8 @@ OiftPlan oift_plan(int X, int Y, int Z);
 size_t oift_globals_bytes();
 int oift_mbox_words(const OiftPlan &P, int ctas);
 size_t oift_mbox_bytes(const OiftPlan &P, int ctas);
+// Fewest CTAs that can own `ntiles` tiles (each CTA's tile sets live in shared memory).
+int oift_min_ctas(int ntiles);
 // One job (volume + seed set) of the batched OIFT kernel; the device copy is read by
 // the team that draws it and receives the job's status.
 struct OiftTeamJob {

@@ -37,11 +37,12 @@ struct OiftArgs {
     uint32_t *key;
     const uint16_t *W;
     uint32_t *tpend;
-    unsigned long long *mbox;  // [nwarps][mbox_words] re-activation bitmasks
+    unsigned long long *mbox;  // [nctas][mbox_words] re-activation bitmasks
     unsigned int *lprof;       // [lprof_cap][2]: per-level SM cycles and tile steps
     int lprof_cap;
     int mbox_words;
     int nwarps;
+    int nctas;                 // CTAs of the grid (or team); tile t belongs to CTA t % nctas
     int X, Y, Z;
     size_t N;
     int ntx, nty, ntz, ntiles;
@@ -153,10 +154,12 @@ __device__ __forceinline__ bool arc_ok(uint32_t code, bool tail_low, int c, int 
     return (int)base <= thr;
 }
 
-// Re-activating a tile at the current level: tile t is owned by warp t % nwarps; each warp
-// has a bitmask mailbox (bit t / nwarps).  The producer raises the level's outstanding
-// count, then sets the bit; if the bit was already set the tile is already pending and
-// the count is given back.  The owner warp takes all its bits with one exchange.
+// Re-activating a tile at the current level: tile t is owned by CTA t % nctas; each CTA has
+// a bitmask mailbox in global memory (bit t / nctas).  The producer raises the level's
+// outstanding count, then sets the bit; if the bit was already set the tile is already
+// pending and the count is given back.  A warp of the owner CTA takes the bits with one
+// exchange and hands them to the CTA's shared "wanted" set, from which any of its warps
+// claims tiles one at a time.
 
 template <int TY, int TZ>
 __device__ __forceinline__ int tile_of(const OiftArgs &A, int x, int y, int z) {
@@ -222,7 +225,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             const int ny = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
             const int nz = tz + (lane == 4 ? -1 : lane == 5 ? 1 : 0);
             const int tq = nt + ny * A.ntx + nz * A.ntx * A.nty;
-            const int w = tq % A.nwarps, j = tq / A.nwarps;
+            const int w = tq % A.nctas, j = tq / A.nctas;
             const unsigned long long bit = 1ull << (j & 63);
             const unsigned long long old =
                 atomicOr(&A.mbox[(size_t)w * A.mbox_words + (j >> 6)], bit);
@@ -1009,7 +1012,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
             if (lane < 27 && ((m >> lane) & 1u)) {
                 const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
                 const int tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
-                const int w = tq % A.nwarps, j = tq / A.nwarps;
+                const int w = tq % A.nctas, j = tq / A.nctas;
                 const unsigned long long bit = 1ull << (j & 63);
                 const unsigned long long o =
                     atomicOr(&A.mbox[(size_t)w * A.mbox_words + (j >> 6)], bit);
@@ -1027,13 +1030,19 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     cyc[18] += cnt;
 }
 
-// Re-activation bitmask words per warp when `nwarps` warps own `ntiles` tiles round-robin.
-__host__ __device__ __forceinline__ int oift_mbox_words_for(int ntiles, int nwarps) {
-    return ((ntiles + nwarps - 1) / nwarps + 63) / 64;
+// Re-activation bitmask words per CTA when `nctas` CTAs own `ntiles` tiles round-robin.
+__host__ __device__ __forceinline__ int oift_mbox_words_for(int ntiles, int nctas) {
+    return ((ntiles + nctas - 1) / nctas + 63) / 64;
 }
 
 // Shared-memory working set of one CTA of the persistent kernels.
 struct OiftCtaSmem {
+    // tiles of this CTA (bit j = tile team_cta + j * nctas) wanted at the current level, and
+    // those a warp is processing; a tile is processed by one warp at a time
+    unsigned long long want[OIFT_CTA_TILE_WORDS];
+    unsigned long long run[OIFT_CTA_TILE_WORDS];
+    int hits;
+    int err;
     uint32_t blk_min[OIFT_WARPS];
     uint32_t level;
     uint32_t wl[OIFT_WARPS][OIFT_WORKLIST];
@@ -1059,7 +1068,12 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     for (int i = 0; i < 20; i++) cyc_tile[i] = 0;
     uint32_t *rmask = &cs.rmask[warp];
     if (lane == 0) *rmask = 0u;
-    __syncwarp();
+    for (int i = threadIdx.x; i < OIFT_CTA_TILE_WORDS; i += blockDim.x) {
+        cs.want[i] = 0ull;
+        cs.run[i] = 0ull;
+    }
+    if (threadIdx.x == 0) cs.hits = 0;
+    __syncthreads();
     uint32_t *wl = cs.wl[warp];
     uint32_t *nfm = cs.nfm[warp];
     OiftGlobals *g = A.g;
@@ -1089,7 +1103,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             for (int w = 1; w < OIFT_WARPS; w++) bm = blk_min[w] < bm ? blk_min[w] : bm;
             if (bm != OIFT_KEY_INF) atomicMin(&g->nextmin[par], bm);
             if (leader_cta) {
-                g->outstanding[par] = nwarps;
+                g->outstanding[par] = team_ctas;  // one token per CTA for its scan
                 g->nextmin[par ^ 1] = OIFT_KEY_INF;
             }
         }
@@ -1101,10 +1115,15 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         } else if (leader_cta && threadIdx.x == 0 && e == 0) {
             lvl_t0 = clock64();
         }
-        if (threadIdx.x == 0) cs.level = vload(&g->nextmin[par]);
+        // one read of the level and the error flag for the whole CTA: every warp leaves the
+        // loop in the same iteration, so the CTA's barriers stay matched
+        if (threadIdx.x == 0) {
+            cs.level = vload(&g->nextmin[par]);
+            cs.err = vload(&g->error);
+        }
         __syncthreads();
         const uint32_t kk = cs.level;
-        if (kk == OIFT_KEY_INF || vload(&g->error)) break;
+        if (kk == OIFT_KEY_INF || cs.err) break;
         // levels strictly increase; a repeat or a runaway level count is a fault
         if ((e > 0 && kk <= prev_level) || e >= A.max_levels) {
             if (threadIdx.x == 0) atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
@@ -1128,84 +1147,111 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             bgt = max_base_for_cost(c, fgt);
             blt = max_base_for_cost(c, flt);
         }
-        // ---- S: the owner warp of each tile of this level processes it directly ----
+        // ---- S: the tiles of this CTA whose pending key equals the level become wanted ----
         unsigned long long steps = 0;
         const long long t_s0 = clock64();
         cyc_levelsync += t_s0 - t_r0;
-        for (int j0 = 0; gwarp + j0 * nwarps < A.ntiles; j0 += 32) {
-            const int t = gwarp + (j0 + lane) * nwarps;
-            const bool hit = t < A.ntiles && __ldcg(&A.tpend[t]) == kk;
-            uint32_t hits = __ballot_sync(FULL, hit);
-            while (hits) {
-                const int b = __ffs(hits) - 1;
-                hits &= hits - 1;
-                const int th = gwarp + (j0 + b) * nwarps;
-                if (lane == 0) A.tpend[th] = OIFT_KEY_INF;
-                __syncwarp();
-                if constexpr (FULLN)
-                    process_tile_full<TY, TZ, TI, BLEND>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey,
-                                                  reinterpret_cast<int32_t *>(sw),
-                                                  reinterpret_cast<uint16_t *>(wl), nfm, rmask,
-                                                  cyc_tile);
-                else
-                    process_tile<TY, TZ>(A, th, par, kk, c, l, fgt, flt, bgt, blt, skey, sw,
-                                         shx, shy, shz, wl, nfm, rmask, cyc_tile);
-                steps++;
+        {
+            int h = 0;
+            for (int j = threadIdx.x; team_cta + j * team_ctas < A.ntiles; j += blockDim.x) {
+                const int t = team_cta + j * team_ctas;
+                if (__ldcg(&A.tpend[t]) == kk) {
+                    A.tpend[t] = OIFT_KEY_INF;
+                    atomicOr(&cs.want[j >> 6], 1ull << (j & 63));
+                    h++;
+                }
             }
+            for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(FULL, h, o);
+            if (lane == 0 && h) atomicAdd(&cs.hits, h);
         }
-        fence_acq_rel_gpu();
-        __syncwarp();
-        if (lane == 0) atomicSub(&g->outstanding[par], 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // the CTA's token of the level becomes one count per wanted tile
+            const int h = cs.hits;
+            cs.hits = 0;
+            if (h != 1) atomicAdd(&g->outstanding[par], h - 1);
+        }
         const long long t_p0 = clock64();
         cyc_owner += t_p0 - t_s0;
-        // ---- P: take this warp's re-activated tiles until the level is complete ----
-        unsigned long long *mybox = A.mbox + (size_t)gwarp * A.mbox_words;
+        // ---- P: the CTA's warps claim its wanted tiles, one warp per tile, and fetch the
+        // CTA's mailbox into the wanted set, until the level's outstanding count is zero ----
+        unsigned long long *ctabox = A.mbox + (size_t)team_cta * A.mbox_words;
+        const int words = A.mbox_words;
         long long spins = 0;
         int idle = 0;
         for (;;) {
-            unsigned long long bits = 0;
-            int word = -1;
-            if (lane < A.mbox_words) {
-                if (*(volatile unsigned long long *)&mybox[lane]) {
-                    bits = exch_acquire_gpu(&mybox[lane], 0ull);
-                    word = lane;
+            // claim: the first lane that sees a wanted tile no warp is processing takes it
+            // with an atomic OR on the running set; a lost race looks again
+            int j = -1;
+            for (int w0 = 0; w0 < words && j < 0;) {
+                const int w = w0 + lane;
+                const unsigned long long avail =
+                    w < words ? (vload(&cs.want[w]) & ~vload(&cs.run[w])) : 0ull;
+                const uint32_t have = __ballot_sync(FULL, avail != 0ull);
+                if (!have) {
+                    w0 += 32;
+                    continue;
                 }
-            }
-            const uint32_t have = __ballot_sync(FULL, bits != 0ull);
-            if (have) {
-                __syncwarp();
-                const long long tb = clock64();
-                for (uint32_t hv = have; hv; hv &= hv - 1) {
-                    const int src = __ffs(hv) - 1;
-                    unsigned long long b = __shfl_sync(FULL, bits, src);
-                    const int wd = __shfl_sync(FULL, word, src);
-                    while (b) {
-                        const int j = wd * 64 + __ffsll((long long)b) - 1;
-                        b &= b - 1;
-                        const int t = gwarp + j * nwarps;
-                        if constexpr (FULLN)
-                            process_tile_full<TY, TZ, TI, BLEND>(A, t, par, kk, c, l, fgt, flt, bgt,
-                                                          blt, skey,
-                                                          reinterpret_cast<int32_t *>(sw),
-                                                          reinterpret_cast<uint16_t *>(wl), nfm,
-                                                          rmask, cyc_tile);
-                        else
-                            process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey,
-                                                 sw, shx, shy, shz, wl, nfm, rmask, cyc_tile);
-                        steps++;
-                        fence_acq_rel_gpu();  // the tile step's writes precede the count
-                        __syncwarp();
-                        if (lane == 0) atomicSub(&g->outstanding[par], 1);
+                const int src = __ffs(have) - 1;
+                int got = -1;
+                if (lane == src) {
+                    const int b = __ffsll((long long)avail) - 1;
+                    const unsigned long long bit = 1ull << b;
+                    if (!(atomicOr(&cs.run[w], bit) & bit)) {
+                        atomicAnd(&cs.want[w], ~bit);
+                        got = w * 64 + b;
                     }
+                }
+                j = __shfl_sync(FULL, got, src);
+            }
+            if (j >= 0) {
+                // the activations merged into this claim precede the staging of the tile
+                __threadfence_block();
+                const long long tb = clock64();
+                const int t = team_cta + j * team_ctas;
+                if constexpr (FULLN)
+                    process_tile_full<TY, TZ, TI, BLEND>(A, t, par, kk, c, l, fgt, flt, bgt, blt,
+                                                         skey, reinterpret_cast<int32_t *>(sw),
+                                                         reinterpret_cast<uint16_t *>(wl), nfm,
+                                                         rmask, cyc_tile);
+                else
+                    process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey, sw, shx,
+                                         shy, shz, wl, nfm, rmask, cyc_tile);
+                steps++;
+                fence_acq_rel_gpu();  // the tile step's writes precede the release and count
+                __syncwarp();
+                if (lane == 0) {
+                    atomicAnd(&cs.run[j >> 6], ~(1ull << (j & 63)));
+                    atomicSub(&g->outstanding[par], 1);
                 }
                 cyc_busy += clock64() - tb;
                 spins = 0;
                 idle = 0;
                 continue;
             }
+            // fetch: the CTA's mailbox bits join the wanted set; bits already wanted merge
+            // into the pending activation and give their count back
+            bool fetched = false;
+            for (int w0 = 0; w0 < words; w0 += 32) {
+                const int w = w0 + lane;
+                unsigned long long b = 0ull;
+                if (w < words && vload(&ctabox[w])) b = exch_acquire_gpu(&ctabox[w], 0ull);
+                if (b) {
+                    __threadfence_block();
+                    const unsigned long long old = atomicOr(&cs.want[w], b);
+                    const int dups = __popcll(old & b);
+                    if (dups) atomicSub(&g->outstanding[par], dups);
+                }
+                fetched |= __any_sync(FULL, b != 0ull);
+            }
+            if (fetched) {
+                spins = 0;
+                idle = 0;
+                continue;
+            }
             int done = 0;
             if (lane == 0) {
-                // the global counter is polled sparsely; the CTA queue every time
+                // the global counter is polled sparsely; the CTA's sets every time
                 if ((idle & 3) == 0)
                     done = vload(&g->outstanding[par]) == 0 || vload(&g->error) != 0;
                 if (!done && ++spins > A.spin_limit) {
@@ -1284,7 +1330,11 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
         OiftTeamJob *J = jobs + j;
         const int X = J->X, Y = J->Y, Z = J->Z, ntx = J->ntx, nty = J->nty;
         const int ntiles = J->ntiles;
-        const int mbox_words = oift_mbox_words_for(ntiles, team_ctas * OIFT_WARPS);
+        const int mbox_words = oift_mbox_words_for(ntiles, team_ctas);
+        if (mbox_words > OIFT_CTA_TILE_WORDS) {  // the job needs a team of more CTAs
+            if (leader) J->status = OIFT_E_UNSUPPORTED;
+            continue;
+        }
         const size_t N = (size_t)X * Y * Z;
         if (threadIdx.x == 0) {
             sA.key = key;
@@ -1295,6 +1345,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
             sA.lprof_cap = 0;
             sA.mbox_words = mbox_words;
             sA.nwarps = team_ctas * OIFT_WARPS;
+            sA.nctas = team_ctas;
             sA.X = X;
             sA.Y = Y;
             sA.Z = Z;
@@ -1315,7 +1366,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
         // ---- clear the team's state for this volume ----
         for (size_t i = tid; i < N; i += nthr) key[i] = OIFT_KEY_INF;
         for (size_t i = tid; i < (size_t)ntiles; i += nthr) tpend[i] = OIFT_KEY_INF;
-        const size_t nmb = (size_t)team_ctas * OIFT_WARPS * mbox_words;
+        const size_t nmb = (size_t)team_ctas * mbox_words;
         for (size_t i = tid; i < nmb; i += nthr) mbox[i] = 0ull;
         if (!team_barrier(g, spin_limit, team_ctas)) break;
         // ---- seeds (as oift_seed_kernel) ----
@@ -1446,10 +1497,14 @@ size_t oift_smem_bytes() { return (size_t)OIFT_WARPS * (4096 + 6144 + 896); }
 
 size_t oift_globals_bytes() { return sizeof(OiftGlobals); }
 int oift_mbox_words(const OiftPlan &P, int ctas) {
-    return oift_mbox_words_for(P.ntiles, ctas * OIFT_WARPS);
+    return oift_mbox_words_for(P.ntiles, ctas);
 }
 size_t oift_mbox_bytes(const OiftPlan &P, int ctas) {
-    return (size_t)ctas * OIFT_WARPS * oift_mbox_words(P, ctas) * sizeof(unsigned long long);
+    return (size_t)ctas * oift_mbox_words(P, ctas) * sizeof(unsigned long long);
+}
+int oift_min_ctas(int ntiles) {
+    const int per = OIFT_CTA_TILE_WORDS * 64;
+    return (ntiles + per - 1) / per;
 }
 
 // Runs the seeds kernel, the persistent kernel and (optionally) the finalize kernel.
@@ -1489,7 +1544,9 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.lprof_cap = S.lprof_cap;
     if (S.lprof) cudaMemsetAsync(S.lprof, 0, (size_t)S.lprof_cap * 2 * sizeof(unsigned int), st);
     A.nwarps = sms * OIFT_WARPS;
+    A.nctas = sms;
     A.mbox_words = oift_mbox_words(P, sms);
+    if (A.mbox_words > OIFT_CTA_TILE_WORDS) return OIFT_E_UNSUPPORTED;
     A.X = X;
     A.Y = Y;
     A.Z = Z;
