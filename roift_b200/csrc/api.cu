@@ -35,7 +35,9 @@ struct oift_b200_ctx {
     std::vector<std::pair<int, double>> tune_cands;  // batch autotuner: (teams, rate)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    cudaEvent_t ev[10];
+    // ev[10]: the early readback of one pipeline call has landed; ev[11]: the host entry's
+    // copy of the pinned seed labels has ended
+    cudaEvent_t ev[12];
     // scratch (grow-only)
     DevBuf img32, img16, W, key, tpend, inq, queue, glob, flag, minmax, seeds, slabels, cost,
         olabel, flabel, memb, seedc, l2c, classes, pol, presence, lut, mask8, ctaq, lprof, rtdist;
@@ -55,6 +57,22 @@ struct oift_b200_ctx {
     // pinned host staging of the seed labels of the host entry
     int32_t *hslab = nullptr;
     size_t hslab_n = 0;
+    // pinned host copies of the small device results a call reads at its end (a copy into
+    // pageable memory would wait for the stream)
+    struct HostMirror {
+        OiftGlobals g;
+        int flag[4];
+        int mm[2];
+        int mm_init[2];
+        unsigned long long clamp;
+        uint32_t presence[1024];
+    } *hm = nullptr;
+    unsigned *hhist = nullptr;  // per-sweep tile histogram of the relaxation
+    size_t hhist_n = 0;
+    // Gaussian-RBF table on the device, built for (lut_sigma, lut_wq); lut_len 0 = none
+    float lut_sigma = -1.0f;
+    int lut_wq = -1, lut_len = 0;
+    DevBuf hmemb;  // membership of the host entry
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -134,6 +152,12 @@ int oift_b200_create(oift_b200_ctx **out, int device) {
     }
     c->own_stream = true;
     for (auto &e : c->ev) cudaEventCreate(&e);
+    if (cudaHostAlloc((void **)&c->hm, sizeof(oift_b200_ctx::HostMirror), cudaHostAllocDefault) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        oift_b200_destroy(c);
+        return OIFT_E_OOM;
+    }
     *out = c;
     return OIFT_OK;
 }
@@ -152,10 +176,12 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->dborder, &c->dhist, &c->daux, &c->dlabel, &c->yimg, &c->ylab,
                       &c->yseeds, &c->yslab, &c->yfirst, &c->yup, &c->ymerge, &c->yfseeds,
                       &c->yfslab, &c->yaux, &c->awork, &c->adist, &c->aseedc, &c->asmall,
-                      &c->al2c, &c->gmap, &c->igring, &c->igsmall, &c->Wt};
+                      &c->al2c, &c->gmap, &c->igring, &c->igsmall, &c->Wt, &c->hmemb};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     if (c->hslab) cudaFreeHost(c->hslab);
+    if (c->hm) cudaFreeHost(c->hm);
+    if (c->hhist) cudaFreeHost(c->hhist);
     for (auto &e : c->ev) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -285,21 +311,36 @@ struct RelaxPlan {
     RelaxArgs ra{};
 };
 
-static int relax_plan(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *d_slabels,
-                      int nseeds, const int hmm[2], RelaxPlan *pl) {
+// Queues the scan of the labels present among the seeds and its copy to the context's
+// pinned mirror (hm->presence); relax_plan_finish reads it once the copy has completed.
+static int relax_classes_launch(oift_b200_ctx *c, const int32_t *d_slabels, int nseeds) {
     cudaStream_t s = c->stream;
-    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
-    const size_t N = (size_t)X * Y * Z;
-    Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
     TRY(grow(c, c->presence, 1024 * sizeof(uint32_t)));
     CU(cudaMemsetAsync(c->presence.p, 0, 1024 * sizeof(uint32_t), s));
     if (nseeds > 0)
         seed_presence_kernel<<<std::min((nseeds + 255) / 256, c->sms * 4), 256, 0, s>>>(
             d_slabels, nseeds, (uint32_t *)c->presence.p);
-    std::vector<uint32_t> bits(1024);
-    CU(cudaMemcpyAsync(bits.data(), c->presence.p, 1024 * sizeof(uint32_t),
+    CU(cudaMemcpyAsync(c->hm->presence, c->presence.p, 1024 * sizeof(uint32_t),
                        cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
+    return OIFT_OK;
+}
+
+static int relax_plan_finish(oift_b200_ctx *c, const oift_b200_params *p, const int hmm[2],
+                             RelaxPlan *pl);
+
+static int relax_plan(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *d_slabels,
+                      int nseeds, const int hmm[2], RelaxPlan *pl) {
+    TRY(relax_classes_launch(c, d_slabels, nseeds));
+    CU(cudaStreamSynchronize(c->stream));
+    return relax_plan_finish(c, p, hmm, pl);
+}
+
+static int relax_plan_finish(oift_b200_ctx *c, const oift_b200_params *p, const int hmm[2],
+                             RelaxPlan *pl) {
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    const size_t N = (size_t)X * Y * Z;
+    Adjacency adj = make_adjacency(p->adjacency == 4 ? 6 : (p->adjacency == 8 ? 26 : p->adjacency));
+    std::vector<uint32_t> bits(c->hm->presence, c->hm->presence + 1024);
     bits[0] |= 1u;
     pl->classes.clear();
     for (int l = 0; l <= OIFT_MAX_LABEL; l++)
@@ -372,13 +413,14 @@ static int relax_reserve(oift_b200_ctx *c, size_t N, int C, int maxl, int X, int
 
 // The sweeps of one planned relaxation: kernel launches and device-side memsets only (the
 // context's scratch must already be reserved), so the sequence can also be captured in a
-// CUDA graph.  With `active` non-null the sweep histogram is read back (a host sync) to
-// count the voxel-sweeps computed, and the sweep loop is bracketed by the context's events.
+// CUDA graph.  With `active` true the sweep histogram is copied to the context's pinned
+// c->hhist (count it with relax_active_sweeps once the stream has reached that copy), and
+// the sweep loop is bracketed by the context's events.
 template <typename T>
 static int relax_launch(oift_b200_ctx *c, const oift_b200_params *p, const T *d_img,
                         const int32_t *d_seeds, int nseeds, const int32_t *d_olab,
                         const RelaxPlan &pl, const int *d_l2c, const int *d_classes,
-                        const oift_b200_outputs *out, long long *active) {
+                        const oift_b200_outputs *out, bool active) {
     cudaStream_t s = c->stream;
     const int X = p->xsize, Y = p->ysize, Z = p->zsize;
     const size_t N = (size_t)X * Y * Z;
@@ -422,15 +464,14 @@ static int relax_launch(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         std::swap(cur, nxt);
     }
     if (K > 0 && active) {
-        std::vector<unsigned> h(K);
-        CU(cudaMemcpyAsync(h.data(), hist, K * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        CU(cudaStreamSynchronize(s));
-        long long run = 0, active_vs = 0;
-        for (int t = 1; t <= K; t++) {  // tiles with distance <= t-1 run at sweep t
-            run += h[t - 1];
-            active_vs += run * 1024;
+        if (c->hhist_n < (size_t)K) {
+            if (c->hhist) cudaFreeHost(c->hhist);
+            c->hhist = nullptr;
+            c->hhist_n = 0;
+            CU(cudaHostAlloc((void **)&c->hhist, (size_t)K * sizeof(unsigned), cudaHostAllocDefault));
+            c->hhist_n = (size_t)K;
         }
-        *active = active_vs;
+        CU(cudaMemcpyAsync(c->hhist, hist, K * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     }
     if (active) cudaEventRecord(c->ev[7], s);
     relax_argmax_kernel<<<(int)std::min<size_t>((N + 255) / 256, (size_t)c->sms * 16), 256, 0, s>>>(
@@ -439,6 +480,17 @@ static int relax_launch(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         CU(cudaMemcpyAsync(out->membership, cur, (size_t)nclasses * N * sizeof(float),
                            cudaMemcpyDeviceToDevice, s));
     return OIFT_OK;
+}
+
+// Voxel-sweeps computed by the last relax_launch with `active` (its histogram copy must have
+// completed): tiles at block distance <= t-1 from the label boundary run at sweep t.
+static long long relax_active_sweeps(const oift_b200_ctx *c, int K) {
+    long long run = 0, active_vs = 0;
+    for (int t = 1; t <= K && (size_t)t <= c->hhist_n; t++) {
+        run += c->hhist[t - 1];
+        active_vs += run * 1024;
+    }
+    return active_vs;
 }
 
 // Relaxation of one job on the context's stream: classes from the seed labels, one-hot
@@ -458,12 +510,58 @@ static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_i
                        cudaMemcpyHostToDevice, c->stream));
     CU(cudaMemcpyAsync(c->classes.p, pl.classes.data(), pl.nclasses * sizeof(int),
                        cudaMemcpyHostToDevice, c->stream));
-    long long act = 0;
     TRY(relax_launch<T>(c, p, d_img, d_seeds, nseeds, d_olab, pl, (const int *)c->l2c.p,
-                        (const int *)c->classes.p, out, &act));
+                        (const int *)c->classes.p, out, true));
+    CU(cudaStreamSynchronize(c->stream));
     rr->nclasses = pl.nclasses;
-    rr->active_voxel_sweeps = act;
+    rr->active_voxel_sweeps = relax_active_sweeps(c, p->relax_sweeps);
     rr->dilations = 3;
+    return OIFT_OK;
+}
+
+// Gaussian-RBF base weights over |dI| = d: lut[d] = floor(wq (1 - exp(-d^2 / (2 sigma^2))) +
+// 0.5), clamped to [0, wq].  The values rise to wq and stay there, so the table ends at its
+// first wq entry (a larger |dI| reads the last entry) and does not depend on the image's
+// range; it is built once per (sigma, wq) and kept on the device.  A sigma so wide that the
+// table has not reached wq by 2^20 entries takes one entry per value of the image's range
+// (`need_range` waits for the range readback).
+template <typename F>
+static int rbf_table(oift_b200_ctx *c, const oift_b200_params *p, F &&need_range,
+                     const uint16_t **lut_out, int *len_out) {
+    if (c->lut_len > 0 && c->lut_sigma == p->rbf_sigma && c->lut_wq == p->wq) {
+        *lut_out = (const uint16_t *)c->lut.p;
+        *len_out = c->lut_len;
+        return OIFT_OK;
+    }
+    const double sg = p->rbf_sigma;
+    auto value = [&](long long d) -> uint16_t {
+        double a = std::exp(-((double)d * (double)d) / (2.0 * sg * sg));
+        double v = std::floor((double)p->wq * (1.0 - a) + 0.5);
+        if (v < 0) v = 0;
+        if (v > p->wq) v = p->wq;
+        return (uint16_t)v;
+    };
+    std::vector<uint16_t> lut;
+    bool saturated = false;
+    for (long long d = 0; d < (1 << 20) && !saturated; d++) {
+        lut.push_back(value(d));
+        saturated = lut.back() == p->wq;
+    }
+    if (!saturated) {
+        TRY(need_range());
+        const long long len = (long long)c->hm->mm[1] - (long long)c->hm->mm[0] + 1;
+        if (len > (1ll << 24)) return OIFT_E_RANGE;
+        for (long long d = (long long)lut.size(); d < len; d++) lut.push_back(value(d));
+    }
+    const int len = (int)lut.size();
+    TRY(grow(c, c->lut, len * sizeof(uint16_t)));
+    CU(cudaMemcpyAsync(c->lut.p, lut.data(), len * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                       c->stream));
+    c->lut_len = saturated ? len : 0;  // a range-sized table is rebuilt for the next image
+    c->lut_sigma = p->rbf_sigma;
+    c->lut_wq = p->wq;
+    *lut_out = (const uint16_t *)c->lut.p;
+    *len_out = len;
     return OIFT_OK;
 }
 
@@ -498,17 +596,30 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     TRY(grow(c, c->olabel, N * sizeof(int32_t)));
     TRY(grow(c, c->presence, 1024 * sizeof(uint32_t)));
 
+    bool want_relax = out && (out->label || out->mask || out->membership);
+    const bool tile_relax = want_relax && !ig;
     cudaEventRecord(c->ev[0], s);
-    // ---- intensity range (Wmax of the relaxation, RBF table length) ----
-    int mm_init[2] = {0x7fffffff, (int)0x80000000};
+    // ---- intensity range (Wmax of the relaxation) and the labels among the seeds (the
+    // relaxation's classes): read back while the weights and the OIFT run, so the host
+    // waits for them only when it queues the relaxation ----
     int *d_mm = (int *)c->minmax.p;
     unsigned long long *d_clamp = (unsigned long long *)((char *)c->minmax.p + 2 * sizeof(int) + 8);
-    CU(cudaMemcpyAsync(d_mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, s));
+    // the previous call ended with the stream idle, so the pinned mirror is free to reuse
+    c->hm->mm_init[0] = 0x7fffffff;
+    c->hm->mm_init[1] = (int)0x80000000;
+    CU(cudaMemcpyAsync(d_mm, c->hm->mm_init, 2 * sizeof(int), cudaMemcpyHostToDevice, s));
     CU(cudaMemsetAsync(d_clamp, 0, sizeof(unsigned long long), s));
     CU(launch_minmax<T>(d_img, N, d_mm, c->sms, s));
-    int hmm[2];
-    CU(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
+    CU(cudaMemcpyAsync(c->hm->mm, d_mm, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (tile_relax) TRY(relax_classes_launch(c, d_slabels, nseeds));
+    cudaEventRecord(c->ev[10], s);
+    const int *hmm = c->hm->mm;
+    bool have_range = false;
+    auto need_range = [&]() -> int {
+        if (!have_range && cudaEventSynchronize(c->ev[10]) != cudaSuccess) return OIFT_E_CUDA;
+        have_range = true;
+        return OIFT_OK;
+    };
 
     // ---- arc weights ----
     BuildArgs ba;
@@ -529,24 +640,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     ba.grad = nullptr;
     ba.blend_a = p->blend_a;
     ba.clamped = d_clamp;
-    if (p->weight_mode == OIFT_W_RBF_Q) {
-        long long range = (long long)hmm[1] - (long long)hmm[0];
-        int len = (int)(range + 1);
-        std::vector<uint16_t> lut(len);
-        double sg = p->rbf_sigma;
-        for (int d = 0; d < len; d++) {
-            double a = std::exp(-((double)d * (double)d) / (2.0 * sg * sg));
-            double v = std::floor((double)p->wq * (1.0 - a) + 0.5);
-            if (v < 0) v = 0;
-            if (v > p->wq) v = p->wq;
-            lut[d] = (uint16_t)v;
-        }
-        TRY(grow(c, c->lut, len * sizeof(uint16_t)));
-        CU(cudaMemcpyAsync(c->lut.p, lut.data(), len * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
-        CU(cudaStreamSynchronize(s));
-        ba.lut = (const uint16_t *)c->lut.p;
-        ba.lut_len = len;
-    }
+    if (p->weight_mode == OIFT_W_RBF_Q) TRY(rbf_table(c, p, need_range, &ba.lut, &ba.lut_len));
     if (!fulln) {
         // tile-major copy of the codes: a tile step stages its 6 KB in one contiguous run
         TRY(grow(c, c->Wt, (size_t)plan.ntiles * 3 * 1024 * sizeof(uint16_t)));
@@ -557,11 +651,14 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         ba.tnty = plan.nty;
         ba.planes_out = !all_full;
         CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
-    } else if (exact && (long long)hmm[1] - (long long)hmm[0] + (ig ? 1 : 0) > OIFT_MAX_BASE) {
-        // exact base weights must fit 14 bits: count the arcs that do not (the planes are
-        // built only for that count)
-        TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
-        CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
+    } else if (exact) {
+        // exact base weights must fit 14 bits: with a range wider than that, count the arcs
+        // that do not (the planes are built only for that count)
+        TRY(need_range());
+        if ((long long)hmm[1] - (long long)hmm[0] + (ig ? 1 : 0) > OIFT_MAX_BASE) {
+            TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
+            CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
+        }
     }
     OiftFullN fn{};
     fn.img = d_img;
@@ -575,6 +672,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         // gradient normalised to the image maximum (596-608).  The tile stages both as 16-bit
         // values, and an oriented weight must fit the 15-bit cost: wf <= max(I), so
         // max(I) (1 + |per| / 100) must stay below 32767.
+        TRY(need_range());
         if (hmm[0] < 0 || hmm[1] > 65535 ||
             (double)hmm[1] * (1.0 + std::fabs((double)p->per) / 100.0) >= 32767.0)
             return OIFT_E_RANGE;
@@ -587,7 +685,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     }
     cudaEventRecord(c->ev[1], s);
 
-    // ---- OIFT ----
+    // ---- OIFT (queued; its outcome is read at the end) ----
     int npol = 0;
     float dflt = 0.0f;
     TRY(upload_polarity(c, p, &npol, &dflt));
@@ -603,21 +701,18 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     S.lprof_cap = 8192;
     int32_t *d_cost = out ? out->cost : nullptr;
     int32_t *d_olab = (out && out->oift_label) ? out->oift_label : (int32_t *)c->olabel.p;
-    int levels = 0;
-    long long steps = 0;
-    int rc = oift_run(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
-                      (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
-                      octas, s, &levels, &steps, c->ev[4], c->ev[5], c->oift_cycles,
-                      fulln ? &fn : nullptr, ig, fulln ? nullptr : ba.Wt);
-    if (rc != OIFT_OK) return rc;
-    unsigned long long hclamp = 0;
-    CU(cudaMemcpyAsync(&hclamp, d_clamp, sizeof(hclamp), cudaMemcpyDeviceToHost, s));
+    TRY(oift_enqueue(plan, S, (const uint16_t *)c->W.p, X, Y, Z, d_seeds, d_slabels, nseeds,
+                     (const float *)c->pol.p, npol, dflt, d_cost, d_olab, (int *)c->flag.p,
+                     octas, s, c->ev[4], c->ev[5], fulln ? &fn : nullptr, ig,
+                     fulln ? nullptr : ba.Wt));
+    CU(cudaMemcpyAsync(&c->hm->g, S.g, sizeof(OiftGlobals), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(c->hm->flag, c->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&c->hm->clamp, d_clamp, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     cudaEventRecord(c->ev[2], s);
 
     // ---- relaxation ----
     const int K = p->relax_sweeps;
     RelaxResult rr;
-    bool want_relax = out && (out->label || out->mask || out->membership);
     int ig_kernels = 0;
     if (want_relax && ig) {
         // ORelax_1(sImageGraph): one membership channel, binary labels
@@ -646,16 +741,33 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         R.ev_end = c->ev[7];
         TRY(ig_relax_run<T>(R, d_img, s, c->sms, &ig_kernels));
         rr.nclasses = 1;
-    } else if (want_relax) {
-        TRY(relax_stage<T>(c, p, d_img, d_seeds, d_slabels, nseeds, d_olab, hmm, out, &rr));
+    } else if (tile_relax) {
+        // the early readback landed long ago: the OIFT is still running when the sweeps
+        // are queued behind it
+        TRY(need_range());
+        RelaxPlan pl;
+        TRY(relax_plan_finish(c, p, hmm, &pl));
+        TRY(relax_reserve(c, N, pl.nclasses, pl.maxl, X, Y, Z, K));
+        CU(cudaMemcpyAsync(c->l2c.p, pl.l2c.data(), (pl.maxl + 1) * sizeof(int),
+                           cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(c->classes.p, pl.classes.data(), pl.nclasses * sizeof(int),
+                           cudaMemcpyHostToDevice, s));
+        TRY(relax_launch<T>(c, p, d_img, d_seeds, nseeds, d_olab, pl, (const int *)c->l2c.p,
+                            (const int *)c->classes.p, out, true));
+        rr.nclasses = pl.nclasses;
+        rr.dilations = 3;
     }
-    const int nclasses = rr.nclasses;
-    const long long relax_active = rr.active_voxel_sweeps;
     const int relax_dilations = rr.dilations;
     cudaEventRecord(c->ev[3], s);
     CU(cudaStreamSynchronize(s));
     CU(cudaGetLastError());
+    int levels = 0;
+    long long steps = 0;
+    TRY(oift_result(c->hm->g, c->hm->flag[0], &levels, &steps, c->oift_cycles));
+    const unsigned long long hclamp = c->hm->clamp;
     if (exact && hclamp) return OIFT_E_RANGE;
+    const int nclasses = rr.nclasses;
+    const long long relax_active = tile_relax ? relax_active_sweeps(c, K) : 0;
     if (st) {
         st->levels = levels;
         st->tile_steps = steps;
@@ -702,8 +814,8 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
     const size_t N = (size_t)p->xsize * p->ysize * p->zsize;
     cudaStream_t s = c->stream;
     // the seed labels are staged in pinned memory owned by the context, so their copy is
-    // asynchronous; an earlier call's copy from it has ended once the stream is idle
-    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return OIFT_E_CUDA;
+    // asynchronous; wait for an earlier call's copy from it (and nothing else on the stream)
+    if (cudaEventSynchronize(c->ev[11]) != cudaSuccess) return OIFT_E_CUDA;
     if (c->hslab_n < (size_t)nseeds) {
         if (c->hslab) cudaFreeHost(c->hslab);
         c->hslab = nullptr;
@@ -733,6 +845,7 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
     CU(cudaMemcpyAsync(c->seeds.p, seeds, (size_t)nseeds * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(c->slabels.p, slab, (size_t)nseeds * sizeof(int32_t),
                        cudaMemcpyHostToDevice, s));
+    CU(cudaEventRecord(c->ev[11], s));
     oift_b200_outputs o{};
     o.cost = cost ? (int32_t *)c->cost.p : nullptr;
     const bool relax = p->relax_sweeps > 0 || membership || mask;
@@ -742,20 +855,22 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
     else
         o.oift_label = (int32_t *)c->flabel.p;
     o.mask = mask ? (uint8_t *)c->mask8.p : nullptr;
-    DevBuf tmpm;
     oift_b200_stats lst{};
     oift_b200_stats *sp = stats ? stats : &lst;
     int rc;
     if (membership) {
-        if (cudaMalloc(&tmpm.p, (size_t)membership_cap_classes * N * sizeof(float)) != cudaSuccess) {
-            cudaGetLastError();
-            return OIFT_E_OOM;
-        }
-        o.membership = (float *)tmpm.p;
+        // the relaxation's classes are 0 and the labels among the seeds (gft_ift.cpp:
+        // 8684-8712): the membership holds one plane per class, checked against the cap first
+        std::vector<int32_t> present(slab, slab + nseeds);
+        present.push_back(0);
+        std::sort(present.begin(), present.end());
+        const long long nclasses = std::unique(present.begin(), present.end()) - present.begin();
+        if (nclasses > membership_cap_classes) return OIFT_E_BAD_ARG;
+        TRY(grow(c, c->hmemb, (size_t)nclasses * N * sizeof(float)));
+        o.membership = (float *)c->hmemb.p;
     }
     rc = run_pipeline<int32_t>(c, p, (const int32_t *)c->img32.p, (const int32_t *)c->seeds.p,
                                (const int32_t *)c->slabels.p, nseeds, &o, sp);
-    if (rc == OIFT_OK && membership && sp->nclasses > membership_cap_classes) rc = OIFT_E_BAD_ARG;
     if (rc == OIFT_OK) {
         cudaMemcpyAsync(label, c->flabel.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
         if (cost) cudaMemcpyAsync(cost, o.cost, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
@@ -765,7 +880,6 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
                             cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) rc = OIFT_E_CUDA;
     }
-    if (tmpm.p) cudaFree(tmpm.p);
     return rc;
 }
 
@@ -817,6 +931,7 @@ int oift_b200_build_weights_i16(oift_b200_ctx *c, const oift_b200_params *p,
             lut[d] = (uint16_t)(v < 0 ? 0 : (v > p->wq ? p->wq : v));
         }
         TRY(grow(c, c->lut, len * sizeof(uint16_t)));
+        c->lut_len = 0;  // the cached pipeline table is overwritten
         CU(cudaMemcpyAsync(c->lut.p, lut.data(), len * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
         ba.lut = (const uint16_t *)c->lut.p;
         ba.lut_len = len;
@@ -1665,6 +1780,7 @@ static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_
             t[d] = (uint16_t)(v < 0 ? 0 : (v > common->wq ? common->wq : v));
         }
         TRY(grow(c, c->lut, lut_len * sizeof(uint16_t)));
+        c->lut_len = 0;  // the cached pipeline table is overwritten
         CU(cudaMemcpyAsync(c->lut.p, t.data(), lut_len * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
         lut = (const uint16_t *)c->lut.p;
     }
@@ -2012,7 +2128,7 @@ int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_params *com
         o.mask = jb.mask;
         const int *d_l2c = (const int *)g->plans + off[i];
         rc = relax_launch<int16_t>(c, &prm[i], jb.image, jb.seeds, jb.nseeds, bp.olab[i], plans[i],
-                                   d_l2c, d_l2c + plans[i].l2c.size(), &o, nullptr);
+                                   d_l2c, d_l2c + plans[i].l2c.size(), &o, false);
     }
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(s, &graph);

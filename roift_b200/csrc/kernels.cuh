@@ -262,6 +262,16 @@ size_t adjoint_work_floats(size_t N, int C, int K, int c);
 int adjoint_run(const AdjointJob &J, cudaStream_t s, int sms, float *work, size_t work_floats,
                 void *small, double *loss_out, double *grad_out);
 
+// Queues one OIFT (seeds, persistent kernel, optional finalize) without host
+// synchronisation; copy S.g and d_flag to the host after it and pass them to oift_result.
+int oift_enqueue(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y,
+                 int Z, const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
+                 const float *d_pol_table, int npol, float pol_default, int32_t *cost,
+                 int32_t *label, int *d_flag, int sms, cudaStream_t st, cudaEvent_t ev_begin,
+                 cudaEvent_t ev_end, const OiftFullN *fn, bool round_orient,
+                 const uint16_t *Wt);
+int oift_result(const OiftGlobals &g, int seed_flag, int *levels_out, long long *steps_out,
+                unsigned long long *cycles_out);
 int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
              const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
              const float *d_pol_table, int npol, float pol_default, int32_t *cost,

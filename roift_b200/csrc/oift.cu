@@ -65,6 +65,8 @@ struct OiftArgs {
     int ig;
     // tile-major copy of the code planes ([tile][plane][row][32]), or null
     const uint16_t *Wt;
+    // set by the seeds kernel when a seed is out of range or has a bad label (or null)
+    const int *seed_flag;
 };
 
 constexpr int OIFT_WARPS = 16;
@@ -1282,6 +1284,12 @@ template <int TY, int TZ, bool FULLN = false, typename TI = int16_t, bool BLEND 
 __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(OiftArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ OiftCtaSmem cs;
+    __shared__ int s_bad;
+    // a bad seed (flagged by the seeds kernel queued before) ends the launch at once; the
+    // host reads the flag with the launch's outcome
+    if (threadIdx.x == 0) s_bad = A.seed_flag ? *(volatile const int *)A.seed_flag : 0;
+    __syncthreads();
+    if (s_bad) return;
     oift_solve<TY, TZ, FULLN, TI, BLEND>(A, blockIdx.x, gridDim.x, cs, smem_raw);
 }
 
@@ -1507,33 +1515,28 @@ int oift_min_ctas(int ntiles) {
     return (ntiles + per - 1) / per;
 }
 
-// Runs the seeds kernel, the persistent kernel and (optionally) the finalize kernel.
-int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
-             const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
-             const float *d_pol_table, int npol, float pol_default, int32_t *cost,
-             int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
-             long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end,
-             unsigned long long *cycles_out, const OiftFullN *fn, bool round_orient,
-             const uint16_t *Wt) {
+// Queues the seeds kernel, the persistent kernel and (optionally) the finalize kernel with
+// no host synchronisation: a bad seed stops the persistent kernel at its start.  The
+// outcome is in the globals S.g and the seed flag d_flag, which oift_result interprets
+// once they are on the host.
+int oift_enqueue(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y,
+                 int Z, const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
+                 const float *d_pol_table, int npol, float pol_default, int32_t *cost,
+                 int32_t *label, int *d_flag, int sms, cudaStream_t st, cudaEvent_t ev_begin,
+                 cudaEvent_t ev_end, const OiftFullN *fn, bool round_orient,
+                 const uint16_t *Wt) {
     size_t N = (size_t)X * Y * Z;
     cudaMemsetAsync(S.key, 0xFF, N * sizeof(uint32_t), st);
     cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
     cudaMemsetAsync(S.mbox, 0, oift_mbox_bytes(P, sms), st);
     cudaMemsetAsync(S.g, 0, sizeof(OiftGlobals), st);
-    OiftGlobals init{};
-    init.nextmin[0] = init.nextmin[1] = OIFT_KEY_INF;
-    cudaMemcpyAsync(S.g, &init, sizeof(OiftGlobals), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(S.g->nextmin, 0xFF, sizeof(S.g->nextmin), st);
     cudaMemsetAsync(d_flag, 0, sizeof(int), st);
     if (nseeds > 0)
         oift_seed_kernel<<<(nseeds + 255) / 256, 256, 0, st>>>(S.key, S.tpend, d_seeds,
                                                                d_seed_labels, nseeds, X, Y,
                                                                Z, P.ntx, P.nty, P.TY, P.TZ,
                                                                d_flag);
-    int hflag = 0;
-    cudaMemcpyAsync(&hflag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return OIFT_E_CUDA;
-    if (hflag == 1) return OIFT_E_SEED_RANGE;
-    if (hflag == 2) return OIFT_E_BAD_ARG;
 
     OiftArgs A;
     A.key = S.key;
@@ -1570,6 +1573,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     A.alpha = fn ? fn->alpha : 1.0f;
     A.ig = round_orient ? 1 : 0;
     A.Wt = fn ? nullptr : Wt;
+    A.seed_flag = d_flag;
     size_t smem = oift_smem_bytes();
     void *args[] = {&A};
     cudaError_t err;
@@ -1604,9 +1608,13 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
         if (blocks > sms * 16) blocks = sms * 16;
         oift_finalize_kernel<<<blocks, 256, 0, st>>>(S.key, N, cost, label);
     }
-    OiftGlobals hg;
-    cudaMemcpyAsync(&hg, S.g, sizeof(OiftGlobals), cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return OIFT_E_CUDA;
+    return cudaGetLastError() == cudaSuccess ? OIFT_OK : OIFT_E_CUDA;
+}
+
+int oift_result(const OiftGlobals &hg, int seed_flag, int *levels_out, long long *steps_out,
+                unsigned long long *cycles_out) {
+    if (seed_flag == 1) return OIFT_E_SEED_RANGE;
+    if (seed_flag == 2) return OIFT_E_BAD_ARG;
     if (levels_out) *levels_out = hg.levels;
     if (steps_out) *steps_out = (long long)hg.tile_steps;
     if (cycles_out)
@@ -1614,6 +1622,26 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
     if (hg.error == OIFT_DEV_TIMEOUT) return OIFT_E_NOT_CONVERGED;
     if (hg.error == OIFT_DEV_QUEUE) return OIFT_E_QUEUE_OVERFLOW;
     return OIFT_OK;
+}
+
+// oift_enqueue, then a synchronous read of the outcome.
+int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, int Y, int Z,
+             const int32_t *d_seeds, const int32_t *d_seed_labels, int nseeds,
+             const float *d_pol_table, int npol, float pol_default, int32_t *cost,
+             int32_t *label, int *d_flag, int sms, cudaStream_t st, int *levels_out,
+             long long *steps_out, cudaEvent_t ev_begin, cudaEvent_t ev_end,
+             unsigned long long *cycles_out, const OiftFullN *fn, bool round_orient,
+             const uint16_t *Wt) {
+    const int rc = oift_enqueue(P, S, W, X, Y, Z, d_seeds, d_seed_labels, nseeds, d_pol_table,
+                                npol, pol_default, cost, label, d_flag, sms, st, ev_begin, ev_end,
+                                fn, round_orient, Wt);
+    if (rc != OIFT_OK) return rc;
+    OiftGlobals hg;
+    int hflag = 0;
+    cudaMemcpyAsync(&hg, S.g, sizeof(OiftGlobals), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&hflag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return OIFT_E_CUDA;
+    return oift_result(hg, hflag, levels_out, steps_out, cycles_out);
 }
 
 int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ctas,
