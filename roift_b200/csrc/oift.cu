@@ -472,50 +472,55 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
                 const int r = (int)(li >> 5), xl = (int)(li & 31);
                 const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
                 const size_t p = (size_t)xg + (size_t)y * X + (size_t)z * XY;
-                const uint32_t cxp = sw[r * 32 + xl];
-                const uint32_t cxm = xl > 0 ? sw[r * 32 + xl - 1] : 0u;
-                const uint32_t cyp = sw[1024 + r * 32 + xl];
-                const uint32_t cym = (r % TY) > 0 ? sw[1024 + (r - 1) * 32 + xl] : 0u;
-                const uint32_t czp = sw[2048 + r * 32 + xl];
-                const uint32_t czm = r >= TY ? sw[2048 + (r - TY) * 32 + xl] : 0u;
+                // the six arcs: in-tile head, its slot, the edge code and which side stores
+                // it; every head key is read before any update (keys only decrease, so an
+                // early read costs at most a redundant push)
+                bool in[6];
+                int lq[6];
+                uint32_t code[6], sk[6];
+                const bool tail_low[6] = {false, false, false, true, true, true};
+                in[0] = r >= TY;                              // -z
+                lq[0] = li - 32 * TY;
+                in[1] = (r % TY) > 0;                         // -y
+                lq[1] = li - 32;
+                in[2] = xl > 0;                               // -x
+                lq[2] = li - 1;
+                in[3] = xl < 31 && xg + 1 < X;                // +x
+                lq[3] = li + 1;
+                in[4] = (r % TY) < TY - 1 && y + 1 < Y;       // +y
+                lq[4] = li + 32;
+                in[5] = r + TY < 32 && has_z && z + 1 < Z;    // +z
+                lq[5] = li + 32 * TY;
+                code[0] = in[0] ? sw[2048 + lq[0]] : 0u;
+                code[1] = in[1] ? sw[1024 + lq[1]] : 0u;
+                code[2] = in[2] ? sw[lq[2]] : 0u;
+                code[3] = sw[li];
+                code[4] = sw[1024 + li];
+                code[5] = sw[2048 + li];
+#pragma unroll
+                for (int d = 0; d < 6; d++) sk[d] = in[d] ? skey[lq[d]] : 0u;
                 A.key[p] = kexp;
                 skey[li] = kexp;
+                uint32_t same_row = 0u;  // open x-neighbours, marked with one update
 #pragma unroll
                 for (int d = 0; d < 6; d++) {
-                    int rq = r, xq = xl;
-                    uint32_t code;
-                    bool tail_low, in_tile;
-                    if (d == 0) {  // -z
-                        rq = r - TY; in_tile = r >= TY; code = czm; tail_low = false;
-                    } else if (d == 1) {  // -y
-                        rq = r - 1; in_tile = (r % TY) > 0; code = cym; tail_low = false;
-                    } else if (d == 2) {  // -x
-                        xq = xl - 1; in_tile = xl > 0; code = cxm; tail_low = false;
-                    } else if (d == 3) {  // +x
-                        xq = xl + 1; in_tile = xl < 31 && xg + 1 < X; code = cxp; tail_low = true;
-                    } else if (d == 4) {  // +y
-                        rq = r + 1; in_tile = (r % TY) < TY - 1 && y + 1 < Y; code = cyp;
-                        tail_low = true;
-                    } else {  // +z
-                        rq = r + TY; in_tile = r + TY < 32 && has_z && z + 1 < Z; code = czp;
-                        tail_low = true;
-                    }
-                    if (!in_tile) continue;  // across a face: push_out
-                    const int lq = rq * 32 + xq;
-                    // keys only decrease, so a stale read costs at most a redundant push
-                    const uint32_t sk = skey[lq];
-                    if (sk <= kk) continue;  // at this level or expanded
-                    if (arc_ok(code, tail_low, c, bgt, blt)) {
-                        atomicOr(&nfm[rq], 1u << xq);
+                    if (!in[d] || sk[d] <= kk) continue;  // across a face, at this level, or expanded
+                    const int rq = lq[d] >> 5, xq = lq[d] & 31;
+                    if (arc_ok(code[d], tail_low[d], c, bgt, blt)) {
+                        if (rq == r)
+                            same_row |= 1u << xq;
+                        else
+                            atomicOr(&nfm[rq], 1u << xq);
                     } else {
-                        const uint32_t nk = arc_key(code, tail_low);
-                        if (nk < sk) {
-                            atomicMin(&skey[lq], nk);
+                        const uint32_t nk = arc_key(code[d], tail_low[d]);
+                        if (nk < sk[d]) {
+                            atomicMin(&skey[lq[d]], nk);
                             atomicMin(&A.key[(size_t)(x0 + xq) + (size_t)(y0 + rq % TY) * X +
                                              (size_t)(z0 + rq / TY) * XY], nk);
                         }
                     }
                 }
+                if (same_row) atomicOr(&nfm[r], same_row);
             }
             done = (done + 32 < cnt) ? done + 32 : cnt;
             rounds++;
