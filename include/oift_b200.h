@@ -138,6 +138,18 @@ OIFT_API int oift_b200_run_host(oift_b200_ctx *ctx, const oift_b200_params *prm,
                        int32_t *cost, float *membership, int membership_cap_classes,
                        uint8_t *mask, oift_b200_stats *stats);
 
+/* The relaxation alone on HOST pointers, as gft::ift::ORelax_1_Multi /
+ * ORelax_1_Multi_PerClass (gft/include/gft_ift.h:451-465, gft/src/gft_ift.cpp:8655-9187)
+ * relaxes the labels it is given: label in = the labels to relax (e.g. the OIFT's), out =
+ * the relaxed labels; classes = 0 and the labels found at the seeds; prm->relax_sweeps
+ * sweeps of the prm->adjacency neighbourhood with prm->per / per_class.  membership
+ * ([nclasses][N], may be NULL, at most membership_cap_classes planes) and mask (may be
+ * NULL) as in oift_b200_run_host. */
+OIFT_API int oift_b200_relax_host(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                                  const int32_t *image, int32_t *label, const int32_t *seeds,
+                                  int nseeds, float *membership, int membership_cap_classes,
+                                  uint8_t *mask);
+
 /* One job of the batched driver: a volume and one seed set (device pointers). */
 typedef struct {
     const int16_t *image;

@@ -16,7 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgft_ref.so")
 REF_GPU_SO = os.path.join(HERE, "_ref", "liboift_fmax_ref.so")
-REF_SRC = "/root/reference"
+# the reference source tree (jung0221/roift), where a build of the checker libraries may read
+# it; unset where only the prebuilt libraries in oracle/_ref are present
+REF_SRC = os.environ.get("ROIFT_REFERENCE")
 
 NIL = -1
 W_MODES = {"grad": 0, "grad_q": 1, "rbf_q": 2, "blend_q": 3}
@@ -27,15 +29,31 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
+def ref_tree_present() -> bool:
+    return bool(REF_SRC) and os.path.isdir(REF_SRC)
+
+
 def build(with_ref: bool | None = None) -> None:
-    """Compile liboracle.so, and libgft_ref.so when the reference tree is present."""
+    """Compile liboracle.so and, when the reference tree is present (ROIFT_REFERENCE),
+    libgft_ref.so, the reference's plain-GPU library and the drop-in CLI programs."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if with_ref is None:
-        with_ref = os.path.isdir(REF_SRC)
-    if with_ref:
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+        with_ref = ref_tree_present()
+    if with_ref and ref_tree_present():
+        ref = [f"REF={REF_SRC}"]
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", *ref], check=True)
         if os.path.exists("/usr/local/cuda/bin/nvcc"):
-            subprocess.run(["make", "-s", "-C", HERE, "refgpu"], check=True)
+            subprocess.run(["make", "-s", "-C", HERE, "refgpu", *ref], check=True)
+        pkg = os.path.join(HERE, "..", "roift_b200")
+        if os.path.exists(os.path.join(pkg, "libgft_oift_b200.so")):
+            subprocess.run(["make", "-s", "-j8", "-C", HERE, "dropin", *ref], check=True)
+
+
+def dropin_programs():
+    """The reference's CLIs built against the product (oracle/Makefile `dropin`), or None."""
+    a = os.path.join(HERE, "_ref", "oiftrelax_gft_dropin")
+    b = os.path.join(HERE, "_ref", "oiftrelax_fmax_gpu_dropin")
+    return (a, b) if os.path.exists(a) and os.path.exists(b) else None
 
 
 class _Polarity(C.Structure):

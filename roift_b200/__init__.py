@@ -90,7 +90,8 @@ class BatchStats(C.Structure):
 
 EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_set_stream", "oift_b200_status_string", "oift_b200_run_device_i16",
-           "oift_b200_run_host", "oift_b200_build_weights_i16", "oift_b200_weight_planes",
+           "oift_b200_run_host", "oift_b200_relax_host", "oift_b200_build_weights_i16",
+           "oift_b200_weight_planes",
            "oift_fmax_gpu_run", "oift_gpu_run", "oift_b200_last_status",
            "oift_b200_level_profile", "oift_b200_selftest_div100",
            "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes",
@@ -130,6 +131,8 @@ def lib():
                                           C.POINTER(BatchStats)]
         L.oift_b200_set_oift_grid.argtypes = [vp, C.c_int]
         L.oift_b200_set_limits.argtypes = [vp, C.c_longlong, C.c_int]
+        L.oift_b200_relax_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
+                                           vp, C.c_int, vp]
         L.oift_b200_batch_graph_create.argtypes = [vp, C.POINTER(Params), C.POINTER(Job), C.c_int,
                                                    C.c_int, C.POINTER(vp)]
         L.oift_b200_batch_graph_launch.argtypes = [vp, C.POINTER(Job), C.POINTER(C.c_float)]
@@ -263,6 +266,23 @@ class Context:
         if memb is not None:
             memb = memb[: st.nclasses * N].reshape(st.nclasses, N)
         return lab, cost, memb, mask, st
+
+    def relax_host(self, params, image, label, seeds, want_membership=0, want_mask=False):
+        """The relaxation alone (ORelax_1_Multi): relaxes the labels `label` (e.g. an OIFT's)
+        with params.relax_sweeps sweeps; returns (labels, membership or None, mask or None)."""
+        img = np.ascontiguousarray(np.asarray(image).reshape(-1), np.int32)
+        lab = np.ascontiguousarray(label, np.int32).reshape(-1).copy()
+        sd = np.ascontiguousarray(seeds, np.int32)
+        N = img.size
+        memb = np.empty(want_membership * N, np.float32) if want_membership else None
+        mask = np.empty(N, np.uint8) if want_mask else None
+        rc = lib().oift_b200_relax_host(self._h, C.byref(params), img, lab, sd, len(sd),
+                                        memb.ctypes.data if memb is not None else None,
+                                        int(want_membership),
+                                        mask.ctypes.data if mask is not None else None)
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_relax_host")
+        return lab, memb, mask
 
     def run_batch(self, params, jobs, teams=0) -> BatchStats:
         """Batched driver: `jobs` is a ctypes array of Job (device pointers); teams = 0

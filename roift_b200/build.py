@@ -8,6 +8,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboift_b200.so")
+# gft::ift drop-ins (OIFT_Multi, ORelax_1_Multi and their per-class forms) over the C ABI
+SHIM = os.path.join(HERE, "libgft_oift_b200.so")
+SHIM_SRC = os.path.join(CSRC, "gft_shims.cpp")
 SOURCES = ["api.cu", "weights.cu", "oift.cu", "relax.cu", "selftest.cu", "noalloc.cu", "prepost.cu", "adjoint.cu", "imagegraph.cu", "volume_io.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
@@ -15,7 +18,7 @@ FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-li
 
 
 def _stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(SHIM):
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
@@ -49,6 +52,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
                     "-o", LIB, "-lcudart", "-lz"], check=True)
     for o in objs:
         os.remove(o)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", SHIM_SRC, "-o", SHIM,
+                    "-L" + HERE, "-loift_b200", "-Wl,-rpath,$ORIGIN"], check=True)
     return LIB
 
 

@@ -883,6 +883,82 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
     return rc;
 }
 
+int oift_b200_relax_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_t *image,
+                         int32_t *label, const int32_t *seeds, int nseeds, float *membership,
+                         int membership_cap_classes, uint8_t *mask) {
+    if (!c || !image || !label || (nseeds > 0 && !seeds)) return OIFT_E_BAD_ARG;
+    TRY(check_params(p));
+    if (p->weight_mode == OIFT_W_IMAGEGRAPH) return OIFT_E_UNSUPPORTED;
+    if (nseeds <= 0) return OIFT_E_NO_SEEDS;
+    cudaSetDevice(c->device);
+    const int X = p->xsize, Y = p->ysize, Z = p->zsize;
+    const size_t N = (size_t)X * Y * Z;
+    cudaStream_t s = c->stream;
+    if (cudaEventSynchronize(c->ev[11]) != cudaSuccess) return OIFT_E_CUDA;
+    if (c->hslab_n < (size_t)nseeds) {
+        if (c->hslab) cudaFreeHost(c->hslab);
+        c->hslab = nullptr;
+        c->hslab_n = 0;
+        if (cudaHostAlloc(&c->hslab, (size_t)nseeds * sizeof(int32_t), cudaHostAllocDefault) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            c->hslab = nullptr;
+            return OIFT_E_OOM;
+        }
+        c->hslab_n = (size_t)nseeds;
+    }
+    int32_t *slab = c->hslab;
+    for (int i = 0; i < nseeds; i++) {
+        if (seeds[i] < 0 || (size_t)seeds[i] >= N) return OIFT_E_SEED_RANGE;
+        const int lb = label[seeds[i]];
+        slab[i] = lb < 0 ? 0 : lb;
+        if (slab[i] > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
+    }
+    TRY(grow(c, c->img32, N * sizeof(int32_t)));
+    TRY(grow(c, c->seeds, (size_t)nseeds * sizeof(int32_t)));
+    TRY(grow(c, c->slabels, (size_t)nseeds * sizeof(int32_t)));
+    TRY(grow(c, c->flabel, N * sizeof(int32_t)));
+    TRY(grow(c, c->minmax, 2 * sizeof(unsigned long long) + 2 * sizeof(int)));
+    if (mask) TRY(grow(c, c->mask8, N));
+    CU(cudaMemcpyAsync(c->img32.p, image, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->flabel.p, label, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->seeds.p, seeds, (size_t)nseeds * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->slabels.p, slab, (size_t)nseeds * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, s));
+    CU(cudaEventRecord(c->ev[11], s));
+    // intensity range (Wmax, gft_ift.cpp:8733-8734) and the classes among the seeds
+    int *d_mm = (int *)c->minmax.p;
+    c->hm->mm_init[0] = 0x7fffffff;
+    c->hm->mm_init[1] = (int)0x80000000;
+    CU(cudaMemcpyAsync(d_mm, c->hm->mm_init, 2 * sizeof(int), cudaMemcpyHostToDevice, s));
+    CU(launch_minmax<int32_t>((const int32_t *)c->img32.p, N, d_mm, c->sms, s));
+    CU(cudaMemcpyAsync(c->hm->mm, d_mm, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    RelaxPlan pl;
+    TRY(relax_plan(c, p, (const int32_t *)c->slabels.p, nseeds, c->hm->mm, &pl));
+    if (membership && pl.nclasses > membership_cap_classes) return OIFT_E_BAD_ARG;
+    if (membership) TRY(grow(c, c->hmemb, (size_t)pl.nclasses * N * sizeof(float)));
+    TRY(relax_reserve(c, N, pl.nclasses, pl.maxl, X, Y, Z, p->relax_sweeps));
+    CU(cudaMemcpyAsync(c->l2c.p, pl.l2c.data(), (pl.maxl + 1) * sizeof(int),
+                       cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c->classes.p, pl.classes.data(), pl.nclasses * sizeof(int),
+                       cudaMemcpyHostToDevice, s));
+    oift_b200_outputs o{};
+    o.label = (int32_t *)c->flabel.p;  // the one-hot start is read before the argmax writes
+    o.mask = mask ? (uint8_t *)c->mask8.p : nullptr;
+    o.membership = membership ? (float *)c->hmemb.p : nullptr;
+    TRY(relax_launch<int32_t>(c, p, (const int32_t *)c->img32.p, (const int32_t *)c->seeds.p,
+                              nseeds, (const int32_t *)c->flabel.p, pl, (const int *)c->l2c.p,
+                              (const int *)c->classes.p, &o, false));
+    CU(cudaMemcpyAsync(label, c->flabel.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    if (mask) CU(cudaMemcpyAsync(mask, c->mask8.p, N, cudaMemcpyDeviceToHost, s));
+    if (membership)
+        CU(cudaMemcpyAsync(membership, c->hmemb.p, (size_t)pl.nclasses * N * sizeof(float),
+                           cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    CU(cudaGetLastError());
+    return OIFT_OK;
+}
+
 int oift_b200_build_weights_i16(oift_b200_ctx *c, const oift_b200_params *p,
                                 const int16_t *image, uint16_t *weights, long long *clamped) {
     if (!c || !image || !weights) return OIFT_E_BAD_ARG;

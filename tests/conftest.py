@@ -23,7 +23,7 @@ def gpu_available() -> bool:
 @pytest.fixture(scope="session")
 def oracle_lib():
     import oracle
-    oracle.build(with_ref=os.path.isdir(oracle.REF_SRC) and not oracle.ref_available())
+    oracle.build(with_ref=oracle.ref_tree_present() and not oracle.ref_available())
     return oracle
 
 
