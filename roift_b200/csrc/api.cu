@@ -860,11 +860,13 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
     int rc;
     if (membership) {
         // the relaxation's classes are 0 and the labels among the seeds (gft_ift.cpp:
-        // 8684-8712): the membership holds one plane per class, checked against the cap first
+        // 8684-8712): the membership holds one plane per class, checked against the cap
+        // first; the image-graph relaxation keeps a single channel (gft_ift.cpp:7683-7847)
         std::vector<int32_t> present(slab, slab + nseeds);
         present.push_back(0);
         std::sort(present.begin(), present.end());
-        const long long nclasses = std::unique(present.begin(), present.end()) - present.begin();
+        const long long nclasses = p->weight_mode == OIFT_W_IMAGEGRAPH
+            ? 1 : std::unique(present.begin(), present.end()) - present.begin();
         if (nclasses > membership_cap_classes) return OIFT_E_BAD_ARG;
         TRY(grow(c, c->hmemb, (size_t)nclasses * N * sizeof(float)));
         o.membership = (float *)c->hmemb.p;
