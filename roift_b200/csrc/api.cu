@@ -73,6 +73,7 @@ struct oift_b200_ctx {
     float lut_sigma = -1.0f;
     int lut_wq = -1, lut_len = 0;
     DevBuf hmemb;  // membership of the host entry
+    bool relax_tma = false;  // the last relax_launch staged its tiles with TMA
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
 };
@@ -420,7 +421,7 @@ template <typename T>
 static int relax_launch(oift_b200_ctx *c, const oift_b200_params *p, const T *d_img,
                         const int32_t *d_seeds, int nseeds, const int32_t *d_olab,
                         const RelaxPlan &pl, const int *d_l2c, const int *d_classes,
-                        const oift_b200_outputs *out, bool active) {
+                        const oift_b200_outputs *out, bool active, bool use_tma = true) {
     cudaStream_t s = c->stream;
     const int X = p->xsize, Y = p->ysize, Z = p->zsize;
     const size_t N = (size_t)X * Y * Z;
@@ -457,12 +458,25 @@ static int relax_launch(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         relax_tile_hist_kernel<<<(rnt + 255) / 256, 256, 0, s>>>(td0, rnt, K, hist);
     }
     float *cur = m0, *nxt = m1;
+    // TMA boxes for the tiles' halos when the extents allow them; a tile whose loads do not
+    // land sets flag[1], read back with the sweeps (relax_tma_status)
+    RelaxTma tma;
+    if (use_tma) TRY(grow(c, c->flag, 4 * sizeof(int)));
+    c->relax_tma = use_tma && relax_tma_encode(&tma, m0, m1, d_img, sizeof(T) == 4, X, Y, Z,
+                                               nclasses);
+    if (c->relax_tma) {
+        tma.err = (int *)c->flag.p + 1;
+        CU(cudaMemsetAsync(tma.err, 0, sizeof(int), s));
+    }
     if (active) cudaEventRecord(c->ev[6], s);
     for (int it = 0; it < K; it++) {
         CU(launch_relax_tiles<T>(nclasses, cur, nxt, d_img, (const uint8_t *)c->seedc.p, td0,
-                                 it + 1, ra, p->per_class != nullptr, rnt, rtx, rty, s));
+                                 it + 1, ra, p->per_class != nullptr, rnt, rtx, rty, s,
+                                 c->relax_tma ? &tma : nullptr));
         std::swap(cur, nxt);
     }
+    if (c->relax_tma)
+        CU(cudaMemcpyAsync(&c->hm->flag[1], tma.err, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (K > 0 && active) {
         if (c->hhist_n < (size_t)K) {
             if (c->hhist) cudaFreeHost(c->hhist);
@@ -480,6 +494,11 @@ static int relax_launch(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         CU(cudaMemcpyAsync(out->membership, cur, (size_t)nclasses * N * sizeof(float),
                            cudaMemcpyDeviceToDevice, s));
     return OIFT_OK;
+}
+
+// Outcome of the TMA loads of the last relax_launch, once the stream has passed it.
+static int relax_tma_status(const oift_b200_ctx *c) {
+    return (c->relax_tma && c->hm->flag[1]) ? OIFT_E_CUDA : OIFT_OK;
 }
 
 // Voxel-sweeps computed by the last relax_launch with `active` (its histogram copy must have
@@ -513,6 +532,7 @@ static int relax_stage(oift_b200_ctx *c, const oift_b200_params *p, const T *d_i
     TRY(relax_launch<T>(c, p, d_img, d_seeds, nseeds, d_olab, pl, (const int *)c->l2c.p,
                         (const int *)c->classes.p, out, true));
     CU(cudaStreamSynchronize(c->stream));
+    TRY(relax_tma_status(c));
     rr->nclasses = pl.nclasses;
     rr->active_voxel_sweeps = relax_active_sweeps(c, p->relax_sweeps);
     rr->dilations = 3;
@@ -764,6 +784,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     int levels = 0;
     long long steps = 0;
     TRY(oift_result(c->hm->g, c->hm->flag[0], &levels, &steps, c->oift_cycles));
+    if (tile_relax) TRY(relax_tma_status(c));
     const unsigned long long hclamp = c->hm->clamp;
     if (exact && hclamp) return OIFT_E_RANGE;
     const int nclasses = rr.nclasses;
@@ -958,7 +979,7 @@ int oift_b200_relax_host(oift_b200_ctx *c, const oift_b200_params *p, const int3
                            cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     CU(cudaGetLastError());
-    return OIFT_OK;
+    return relax_tma_status(c);
 }
 
 int oift_b200_build_weights_i16(oift_b200_ctx *c, const oift_b200_params *p,
@@ -2206,7 +2227,7 @@ int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_params *com
         o.mask = jb.mask;
         const int *d_l2c = (const int *)g->plans + off[i];
         rc = relax_launch<int16_t>(c, &prm[i], jb.image, jb.seeds, jb.nseeds, bp.olab[i], plans[i],
-                                   d_l2c, d_l2c + plans[i].l2c.size(), &o, false);
+                                   d_l2c, d_l2c + plans[i].l2c.size(), &o, false, false);
     }
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(s, &graph);

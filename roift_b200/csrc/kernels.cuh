@@ -1,5 +1,7 @@
 // kernels.cuh -- host-visible launch interfaces of the kernel translation units.
 #pragma once
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace oiftb {
@@ -98,11 +100,26 @@ cudaError_t launch_build_weights(const T *img, uint16_t *W, const BuildArgs &a, 
 template <typename T>
 cudaError_t launch_minmax(const T *img, size_t n, int *mm, int sms, cudaStream_t s);
 
+// Tensor maps of one relaxation's TMA-staged sweeps: the two ping-pong membership buffers
+// as [C][Z][Y][X] floats and the image as [Z][Y][X], encoded on the host over this GPU's
+// own buffers; err is a device flag a tile sets when its loads do not land.
+struct RelaxTma {
+    CUtensorMap memb[2];
+    CUtensorMap img;
+    const float *base[2];
+    int *err;
+};
+// Encodes the maps; false when the extents do not allow TMA boxes (rows of the planes must
+// start 16-byte aligned: X % 4 == 0 for int32 images, X % 8 == 0 for int16) or the driver
+// entry point is missing -- the sweeps then stage with per-element copies.
+bool relax_tma_encode(RelaxTma *t, const float *m0, const float *m1, const void *img,
+                      bool img32, int X, int Y, int Z, int C);
+
 template <typename T>
 cudaError_t launch_relax_tiles(int C, const float *in, float *out, const T *img,
                                const uint8_t *seedc, const uint16_t *tdist, int sweep,
                                const RelaxArgs &a, bool perclass, int ntiles, int ntx, int nty,
-                               cudaStream_t s);
+                               cudaStream_t s, const RelaxTma *tma = nullptr);
 __global__ void relax_boundary_tiles_kernel(const int32_t *label, int X, int Y, int Z, int nadj,
                                             RelaxArgs a, uint16_t *tdist, int ntx, int nty);
 __global__ void relax_tile_gap_pass_kernel(const uint16_t *din, uint16_t *dout, int ntx, int nty,

@@ -19,6 +19,8 @@
 // identical bits, provided sum(w) is finite (Wmax^8 * degree < FLT_MAX; the host
 // rejects larger Wmax with OIFT_E_RANGE, where the reference itself would produce
 // inf/inf = NaN).  So the sweep is a plain dense stencil with no mask state.
+#include <cudaTypedefs.h>
+
 #include "relax_tile.cuh"
 
 namespace oiftb {
@@ -139,16 +141,74 @@ __global__ void relax_tile_hist_kernel(const uint16_t *__restrict__ tdist, int n
     if (d < K) atomicAdd(&hist[d], 1u);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+bool relax_tma_encode(RelaxTma *t, const float *m0, const float *m1, const void *img,
+                      bool img32, int X, int Y, int Z, int C) {
+    if (X % (img32 ? 4 : 8) != 0 || C < 1 || C > 8) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t row = (cuuint64_t)X * 4, plane = row * (cuuint64_t)Y;
+    const cuuint64_t vol = plane * (cuuint64_t)Z;
+    const cuuint64_t mdim[4] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z, (cuuint64_t)C};
+    const cuuint64_t mstride[3] = {row, plane, vol};
+    const cuuint32_t mbox[4] = {(cuuint32_t)RB_X, (cuuint32_t)RB_Y, (cuuint32_t)RB_Z,
+                                (cuuint32_t)C};
+    const cuuint32_t ones[4] = {1, 1, 1, 1};
+    const float *bases[2] = {m0, m1};
+    for (int i = 0; i < 2; i++) {
+        if (enc(&t->memb[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)bases[i], mdim, mstride,
+                mbox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+        t->base[i] = bases[i];
+    }
+    const cuuint64_t esz = img32 ? 4 : 2;
+    const cuuint64_t idim[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
+    const cuuint64_t istride[2] = {(cuuint64_t)X * esz, (cuuint64_t)X * esz * (cuuint64_t)Y};
+    const cuuint32_t ibox[3] = {(cuuint32_t)(img32 ? RelaxImgBox<int32_t>::X : RelaxImgBox<int16_t>::X),
+                                (cuuint32_t)RB_Y, (cuuint32_t)RB_Z};
+    if (enc(&t->img, img32 ? CU_TENSOR_MAP_DATA_TYPE_INT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 3,
+            (void *)img, idim, istride, ibox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    return true;
+}
+
 template <typename T>
 cudaError_t launch_relax_tiles(int C, const float *in, float *out, const T *img,
                                const uint8_t *seedc, const uint16_t *tdist, int sweep,
                                const RelaxArgs &a, bool perclass, int ntiles, int ntx, int nty,
-                               cudaStream_t s) {
+                               cudaStream_t s, const RelaxTma *tma) {
     const bool img32 = sizeof(T) == 4;
+    // the TMA-staged sweep reads `in` through its tensor map (not with gradient blending)
+    const CUtensorMap *mmap = nullptr;
+    if (tma && !a.blend) mmap = tma->base[0] == in ? &tma->memb[0] : tma->base[1] == in ? &tma->memb[1] : nullptr;
 #define RELAX_TILE_CASE(CC)                                                                  \
     case CC:                                                                                 \
-        return launch_relax_tiles_c<CC>(in, out, img, img32, seedc, tdist, sweep, a, perclass, \
-                                        ntiles, ntx, nty, s);
+        return mmap ? launch_relax_tiles_tma_c<CC>(*mmap, tma->img, out, img32, seedc, tdist,  \
+                                                   sweep, a, perclass, ntiles, ntx, nty, s,   \
+                                                   tma->err)                                  \
+                    : launch_relax_tiles_c<CC>(in, out, img, img32, seedc, tdist, sweep, a,   \
+                                               perclass, ntiles, ntx, nty, s);
     switch (C) {
         RELAX_TILE_CASE(1)
         RELAX_TILE_CASE(2)
@@ -166,10 +226,10 @@ cudaError_t launch_relax_tiles(int C, const float *in, float *out, const T *img,
 template cudaError_t launch_relax_tiles<int16_t>(int, const float *, float *, const int16_t *,
                                                  const uint8_t *, const uint16_t *, int,
                                                  const RelaxArgs &, bool, int, int, int,
-                                                 cudaStream_t);
+                                                 cudaStream_t, const RelaxTma *);
 template cudaError_t launch_relax_tiles<int32_t>(int, const float *, float *, const int32_t *,
                                                  const uint8_t *, const uint16_t *, int,
                                                  const RelaxArgs &, bool, int, int, int,
-                                                 cudaStream_t);
+                                                 cudaStream_t, const RelaxTma *);
 
 }  // namespace oiftb

@@ -38,6 +38,42 @@ static cudaError_t launch_tile_c(const float *in, float *out, const T *img, cons
     return cudaGetLastError();
 }
 
+template <int C, typename T, int ADJ>
+static cudaError_t launch_tile_tma_c(const CUtensorMap &mmap, const CUtensorMap &imap, float *out,
+                                     const uint8_t *seedc, const uint16_t *tdist, int sweep,
+                                     const RelaxArgs &a, bool perclass, int ntiles, int ntx,
+                                     int nty, cudaStream_t s, int *err) {
+    dim3 block(32, 8);
+    const size_t smem = relax_tma_smem_bytes<C, T>();
+    auto launch = [&](auto k) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (relax_min_blocks(C, false) > 1)  // the shared-memory carve-out that holds them
+            cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        k<<<ntiles, block, smem, s>>>(mmap, imap, out, seedc, tdist, sweep, a, ntx, nty, err);
+        return cudaGetLastError();
+    };
+    return perclass ? launch(relax_tile_tma_kernel<C, T, true, ADJ>)
+                    : launch(relax_tile_tma_kernel<C, T, false, ADJ>);
+}
+
+template <>
+cudaError_t launch_relax_tiles_tma_c<RELAX_TILE_C>(const CUtensorMap &mmap, const CUtensorMap &imap,
+                                                   float *out, bool img32, const uint8_t *seedc,
+                                                   const uint16_t *tdist, int sweep,
+                                                   const RelaxArgs &a, bool perclass, int ntiles,
+                                                   int ntx, int nty, cudaStream_t s, int *err) {
+    const bool six = (a.nadj == 6);
+    if (img32)
+        return six ? launch_tile_tma_c<RELAX_TILE_C, int32_t, 6>(mmap, imap, out, seedc, tdist, sweep,
+                                                                 a, perclass, ntiles, ntx, nty, s, err)
+                   : launch_tile_tma_c<RELAX_TILE_C, int32_t, 26>(mmap, imap, out, seedc, tdist, sweep,
+                                                                  a, perclass, ntiles, ntx, nty, s, err);
+    return six ? launch_tile_tma_c<RELAX_TILE_C, int16_t, 6>(mmap, imap, out, seedc, tdist, sweep, a,
+                                                             perclass, ntiles, ntx, nty, s, err)
+               : launch_tile_tma_c<RELAX_TILE_C, int16_t, 26>(mmap, imap, out, seedc, tdist, sweep, a,
+                                                              perclass, ntiles, ntx, nty, s, err);
+}
+
 template <>
 cudaError_t launch_relax_tiles_c<RELAX_TILE_C>(const float *in, float *out, const void *img,
                                                bool img32, const uint8_t *seedc,

@@ -30,7 +30,7 @@ needs_progs = pytest.mark.skipif(PROGS is None, reason="drop-in programs not bui
 
 def _write_inputs(tmp_path, c):
     Z, Y, X = c.shape
-    vol = os.path.join(tmp_path, "vol.scn")
+    vol = os.path.join(tmp_path, "vol.nii")   # signed samples (a .scn file holds unsigned ones)
     rb.write_volume(vol, c.image.astype(np.int32), (1.0, 1.0, 1.0))
     seeds = os.path.join(tmp_path, "seeds.txt")
     with open(seeds, "w") as f:
