@@ -1050,6 +1050,8 @@ struct OiftCtaSmem {
     unsigned long long run[OIFT_CTA_TILE_WORDS];
     int hits;
     int err;
+    int fetcher;     // 1 while a warp watches the CTA's mailbox and the level's count
+    int level_done;  // e + 1 once level e has ended
     uint32_t blk_min[OIFT_WARPS];
     uint32_t level;
     uint32_t wl[OIFT_WARPS][OIFT_WORKLIST];
@@ -1079,7 +1081,11 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         cs.want[i] = 0ull;
         cs.run[i] = 0ull;
     }
-    if (threadIdx.x == 0) cs.hits = 0;
+    if (threadIdx.x == 0) {
+        cs.hits = 0;
+        cs.fetcher = 0;
+        cs.level_done = 0;
+    }
     __syncthreads();
     uint32_t *wl = cs.wl[warp];
     uint32_t *nfm = cs.nfm[warp];
@@ -1170,6 +1176,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             }
             for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(FULL, h, o);
             if (lane == 0 && h) atomicAdd(&cs.hits, h);
+            if (threadIdx.x == 0) cs.fetcher = 0;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1186,6 +1193,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         const int words = A.mbox_words;
         long long spins = 0;
         int idle = 0;
+        bool fetcher = false;
         for (;;) {
             // claim: the first lane that sees a wanted tile no warp is processing takes it
             // with an atomic OR on the running set; a lost race looks again
@@ -1212,6 +1220,10 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 j = __shfl_sync(FULL, got, src);
             }
             if (j >= 0) {
+                if (fetcher) {  // another idle warp takes over the watch while this one works
+                    if (lane == 0) atomicExch(&cs.fetcher, 0);
+                    fetcher = false;
+                }
                 // the activations merged into this claim precede the staging of the tile
                 __threadfence_block();
                 const long long tb = clock64();
@@ -1236,35 +1248,55 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 idle = 0;
                 continue;
             }
-            // fetch: the CTA's mailbox bits join the wanted set; bits already wanted merge
-            // into the pending activation and give their count back
-            bool fetched = false;
-            for (int w0 = 0; w0 < words; w0 += 32) {
-                const int w = w0 + lane;
-                unsigned long long b = 0ull;
-                if (w < words && vload(&ctabox[w])) b = exch_acquire_gpu(&ctabox[w], 0ull);
-                if (b) {
-                    __threadfence_block();
-                    const unsigned long long old = atomicOr(&cs.want[w], b);
-                    const int dups = __popcll(old & b);
-                    if (dups) atomicSub(&g->outstanding[par], dups);
-                }
-                fetched |= __any_sync(FULL, b != 0ull);
-            }
-            if (fetched) {
-                spins = 0;
-                idle = 0;
-                continue;
-            }
+            // no wanted tile is free.  One warp of the CTA at a time (the fetcher) watches the
+            // CTA's mailbox and the level's outstanding count and publishes the level's end
+            // in shared memory; the others watch only the CTA's shared state.
             int done = 0;
-            if (lane == 0) {
-                // the global counter is polled sparsely; the CTA's sets every time
-                if ((idle & 3) == 0)
-                    done = vload(&g->outstanding[par]) == 0 || vload(&g->error) != 0;
-                if (!done && ++spins > A.spin_limit) {
-                    atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
-                    done = 1;
+            if (lane == 0) done = vload(&cs.level_done) == e + 1;
+            done = __shfl_sync(FULL, done, 0);
+            if (done) break;
+            if (!fetcher) {
+                int got = 0;
+                if (lane == 0) got = atomicCAS(&cs.fetcher, 0, 1) == 0;
+                fetcher = __shfl_sync(FULL, got, 0) != 0;
+            }
+            if (fetcher) {
+                // fetch: the CTA's mailbox bits join the wanted set; bits already wanted merge
+                // into the pending activation and give their count back
+                bool fetched = false;
+                for (int w0 = 0; w0 < words; w0 += 32) {
+                    const int w = w0 + lane;
+                    unsigned long long b = 0ull;
+                    if (w < words && vload(&ctabox[w])) b = exch_acquire_gpu(&ctabox[w], 0ull);
+                    if (b) {
+                        __threadfence_block();
+                        const unsigned long long old = atomicOr(&cs.want[w], b);
+                        const int dups = __popcll(old & b);
+                        if (dups) atomicSub(&g->outstanding[par], dups);
+                    }
+                    fetched |= __any_sync(FULL, b != 0ull);
                 }
+                if (fetched) {
+                    spins = 0;
+                    idle = 0;
+                    continue;
+                }
+                if (lane == 0) {
+                    // the global counter is polled sparsely, the mailbox every time
+                    if ((idle & 3) == 0)
+                        done = vload(&g->outstanding[par]) == 0 || vload(&g->error) != 0;
+                    if (!done && ++spins > A.spin_limit) {
+                        atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
+                        done = 1;
+                    }
+                    if (done) {
+                        *(volatile int *)&cs.level_done = e + 1;
+                        atomicExch(&cs.fetcher, 0);
+                    }
+                }
+            } else if (lane == 0 && ++spins > A.spin_limit) {
+                atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
+                done = 1;
             }
             idle++;
             done = __shfl_sync(FULL, done, 0);
