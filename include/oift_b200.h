@@ -333,7 +333,9 @@ OIFT_API int oift_b200_selftest_div100(unsigned long long *mismatches, unsigned 
  * (either may be NULL).  per / per_class / max_label as in oift_b200_params.
  * Limits: at most OIFT_NOALLOC_MAX_VOXELS voxels and 65536 warp tiles; larger volumes
  * return OIFT_E_RANGE before any device work.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) -- make it before any stream capture.
+ * array's device address (cudaGetSymbolAddress) -- make it before any stream capture.  The
+ * address is kept for the process: do not call this entry on a device after a
+ * cudaDeviceReset of it (the reset reloads the library's device code elsewhere).
  * All calls share the array: calls that overlap on the GPU race and corrupt each other.
  * Runs on `stream` (cudaStream_t as void*) and synchronises it before returning. */
 #define OIFT_NOALLOC_MAX_VOXELS (1u << 20)

@@ -22,12 +22,13 @@ def _device_case(c):
     return img, seeds, labels
 
 
-def _regular(c, img, seeds, labels, mode):
+def _regular(c, img, seeds, labels, mode, per_class=None):
     import torch
     N = c.n
     cost = torch.empty(N, dtype=torch.int32, device=img.device)
     lab = torch.empty(N, dtype=torch.int32, device=img.device)
-    p = rb.make_params(c.shape, adjacency=c.adjacency, weight_mode=mode, wq=4095, pol=c.pol,
+    p = rb.make_params(c.shape, adjacency=c.adjacency, weight_mode=mode, wq=4095,
+                       pol=None if per_class is not None else c.pol, per_class=per_class,
                        sweeps=0)
     rb._ctx().run_device(p, img.data_ptr(), seeds.data_ptr(), labels.data_ptr(), len(c.seeds),
                          cost=cost.data_ptr(), oift_label=lab.data_ptr())
@@ -36,21 +37,33 @@ def _regular(c, img, seeds, labels, mode):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["ellipsoid64", "disc2d"])
+@pytest.mark.parametrize("kind", ["ellipsoid64", "disc2d", "odd37", "perclass", "disc1024"])
 def test_noalloc_matches_regular_entry_twice(roift, kind):
+    """Full tiles (64^3, 256^2), partial tiles on every axis (37 x 41 x 29), a per-class
+    polarity table with two object labels, and a 1024 x 1024 plane at the voxel limit."""
     import torch
+    per_class = None
     if kind == "ellipsoid64":
         c, mode = synth.ellipsoid3d(seed=8, size=64, sweeps=0), "grad_q"
-    else:
+    elif kind == "disc2d":
         c, mode = synth.disc2d(seed=9), "grad"
+    elif kind == "odd37":
+        c, mode = synth.small_case(seed=12, shape=(29, 41, 37), pol=-0.4, nlabels=1), "grad_q"
+    elif kind == "perclass":
+        c, mode = synth.small_case(seed=13, shape=(20, 33, 47), pol=0.0, nlabels=2), "grad"
+        per_class = np.array([-30.0, 25.0, -45.0], np.float32)
+    else:
+        c, mode = synth.disc2d(seed=10, size=1024), "grad"
+    assert c.n <= 1 << 20
     img, seeds, labels = _device_case(c)
-    cost_ref, lab_ref = _regular(c, img, seeds, labels, mode)
+    cost_ref, lab_ref = _regular(c, img, seeds, labels, mode, per_class)
     for _ in range(2):  # two calls in a row share (and must reset) the static scratch
         cost = torch.full((c.n,), -7, dtype=torch.int32, device=img.device)
         lab = torch.full((c.n,), -7, dtype=torch.int32, device=img.device)
         rb.oift_noalloc(img.data_ptr(), c.shape, seeds.data_ptr(), labels.data_ptr(),
                         len(c.seeds), cost_ptr=cost.data_ptr(), label_ptr=lab.data_ptr(),
-                        adjacency=c.adjacency, weight_mode=mode, wq=4095, pol=c.pol)
+                        adjacency=c.adjacency, weight_mode=mode, wq=4095,
+                        pol=None if per_class is not None else c.pol, per_class=per_class)
         torch.cuda.synchronize()
         assert np.array_equal(cost.cpu().numpy(), cost_ref)
         assert np.array_equal(lab.cpu().numpy(), lab_ref)
