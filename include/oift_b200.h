@@ -306,6 +306,31 @@ OIFT_API int oift_b200_adjoint(oift_b200_ctx *ctx, const oift_b200_adjoint_param
                                const int32_t *seed_labels, int nseeds, const uint8_t *truth,
                                float *membership_out, double *loss, double *grad);
 
+/* Arc-weight-map part of the adjoint, on the forest of an integer OIFT result held fixed.
+ * oift_b200_bottleneck_arcs reads the forest from that result (DEVICE int16 image, cost
+ * and label maps [N] as the OIFT returned them for `prm`, GRAD or GRAD_Q weights, global
+ * polarity, and its seeds) and writes, per voxel, the arc that carries its f_max cost:
+ * arcs[p] = tail * 32 + d (the arc tail -> tail + offset d of the gft Spheric order,
+ * gft/src/gft_adjrel3.cpp:47-85), -2 at seeds, -3 at unreached voxels.  In each (cost, label)
+ * level the entry voxels take the arc of weight exactly `cost` from a voxel of their label
+ * conquered earlier; the others inherit, round by round, from a same-level neighbour that
+ * reaches them through an open arc (gft/src/gft_ift.cpp:965-981 with f_max).  Call it once
+ * per OIFT result.  oift_b200_cost_adjoint evaluates, for the weight parameters of `ap`
+ * (sigma, alpha, beta, eps), the continuous RBF cost of every voxel's bottleneck arc
+ * w = 1 - exp(-c^2 / (2 sigma^2)), c = (beta |dI| + (1 - beta)(g_t + g_h) / 2) (1 + s alpha_l)
+ * with alpha_l = -alpha for a background tail, the object confidence u = 1 - w/2 (object
+ * label) or w/2 (background, 0 / 1 at seeds), the soft-Dice loss of u against `truth`, and
+ * (grad may be NULL) its gradient with respect to (sigma, alpha, beta): the f_max
+ * bottleneck-arc subgradient through the fixed forest.  grad_map may be NULL (g = 0). */
+OIFT_API int oift_b200_bottleneck_arcs(oift_b200_ctx *ctx, const oift_b200_params *prm,
+                                       const int16_t *image, const int32_t *cost,
+                                       const int32_t *label, const int32_t *seeds, int nseeds,
+                                       int64_t *arcs);
+OIFT_API int oift_b200_cost_adjoint(oift_b200_ctx *ctx, const oift_b200_adjoint_params *ap,
+                                    const int16_t *image, const float *grad_map,
+                                    const int32_t *label, const int64_t *arcs,
+                                    const uint8_t *truth, double *loss, double *grad);
+
 /* Stage entry points on device pointers (used by the batched driver and tests). */
 OIFT_API int oift_b200_build_weights_i16(oift_b200_ctx *ctx, const oift_b200_params *prm,
                                 const int16_t *image, uint16_t *weights /* [planes][N] */,

@@ -214,3 +214,121 @@ class Problem:
             new[:, self.seed] = 0.0
             lam = new
         return loss, g
+
+
+# ------------------------------------------------------- arc-weight-map term -------
+# The cost map of a fixed OIFT forest as a function of (sigma, alpha, beta): each voxel's
+# f_max cost is carried by one arc of its path (its bottleneck), read from the integer OIFT
+# result; the continuous RBF weight of that arc gives a soft cost, the soft cost an object
+# confidence, and the confidence a soft-Dice loss whose gradient is the bottleneck-arc
+# subgradient of f_max (gft/src/gft_ift.cpp:965-981 with f_max; weights of
+# experiments/exp_gaussian_rbf_relax.cpp:343-345 and exp_gradient_weight.cpp:244-247).
+
+def _oriented_int(base, gt, lt, fgt, flt):
+    """int(base * f) in double, truncated (gft_ift.cpp:965-973); base >= 0."""
+    out = base.astype(np.int64).copy()
+    out = np.where(gt, np.floor(base.astype(np.float64) * fgt).astype(np.int64), out)
+    out = np.where(lt, np.floor(base.astype(np.float64) * flt).astype(np.int64), out)
+    return out
+
+
+def bottleneck_arcs(img, cost, label, seeds, adj, pol, mode="grad_q", wq=4095):
+    """Restatement of oift_b200_bottleneck_arcs: int64 [N], tail * 32 + direction (Spheric
+    order, tail -> tail + d), -2 at seeds, -3 unreached, -1 never assigned."""
+    img = np.asarray(img, np.int64)
+    Z, Y, X = img.shape
+    N = X * Y * Z
+    I = img.reshape(-1)
+    cost = np.asarray(cost, np.int64).reshape(-1)
+    label = np.asarray(label, np.int64).reshape(-1)
+    seed = np.zeros(N, bool)
+    seed[np.asarray(seeds, np.int64)] = True
+    per = float(np.float32(pol * 100.0))
+    fac = {0: (1.0 + (-per) / 100.0, 1.0 - (-per) / 100.0), 1: (1.0 + per / 100.0, 1.0 - per / 100.0)}
+    offs = offsets(adj)
+    n = len(offs)
+    z, y, x = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    z, y, x = z.reshape(-1), y.reshape(-1), x.reshape(-1)
+    arcs = np.full(N, -1, np.int64)
+    arcs[(cost == np.iinfo(np.int32).max) | (label < 0)] = -3
+    arcs[seed] = -2
+
+    def neighbour(i):
+        dx, dy, dz = offs[i]
+        qx, qy, qz = x + dx, y + dy, z + dz
+        ok = (qx >= 0) & (qx < X) & (qy >= 0) & (qy < Y) & (qz >= 0) & (qz < Z)
+        q = np.where(ok, qx + qy * X + qz * X * Y, 0)
+        return q, ok
+
+    def weight_to_p(q, lp):
+        """Integer weight of the arc q -> p with the tail label lp (both labels equal)."""
+        d = I[q] - I
+        base = np.abs(d)
+        if mode == "grad_q":
+            base = np.minimum(base, wq)
+        f0, f1 = fac[0], fac[1]
+        fgt = np.where(lp == 0, f0[0], f1[0])
+        flt = np.where(lp == 0, f0[1], f1[1])
+        return _oriented_int(base, d > 0, d < 0, fgt, flt)
+
+    unset = arcs == -1
+    for i in range(n):
+        q, ok = neighbour(i)
+        cond = unset & (arcs == -1) & ok & (label[q] == label) & (seed[q] | (cost[q] < cost))
+        cond &= weight_to_p(q, label) == cost
+        arcs[cond] = q[cond] * 32 + (n - 1 - i)
+    while True:
+        old = arcs
+        new = arcs.copy()
+        done = np.zeros(N, bool)
+        unset = old == -1
+        for i in range(n):
+            q, ok = neighbour(i)
+            cond = unset & ~done & ok & (old[q] >= 0) & ~seed[q] & (label[q] == label)
+            cond &= (cost[q] == cost) & (weight_to_p(q, label) <= cost)
+            new[cond] = old[q][cond]
+            done |= cond
+        arcs = new
+        if not done.any():
+            break
+    return arcs
+
+
+def cost_loss(img, label, arcs, truth, sigma, alpha, beta, eps=1.0, adj=6, g=None):
+    """FP64 soft-Dice loss of the cost-map confidence and its gradient (sigma, alpha, beta)."""
+    img = np.asarray(img, np.float64)
+    Z, Y, X = img.shape
+    I = img.reshape(-1)
+    G = None if g is None else np.asarray(g, np.float64).reshape(-1)
+    label = np.asarray(label, np.int64).reshape(-1)
+    arcs = np.asarray(arcs, np.int64).reshape(-1)
+    t = (np.asarray(truth).reshape(-1) != 0).astype(np.float64)
+    offs = np.array(offsets(adj), np.int64)
+    has = arcs >= 0
+    tail = np.where(has, arcs >> 5, 0)
+    dirs = np.where(has, arcs & 31, 0)
+    tx, ty, tz = tail % X, (tail // X) % Y, tail // (X * Y)
+    head = (tx + offs[dirs, 0]) + (ty + offs[dirs, 1]) * X + (tz + offs[dirs, 2]) * X * Y
+    head = np.where(has, head, 0)
+    diff = I[tail] - I[head]
+    s = np.sign(diff)
+    dabs = np.abs(diff)
+    gavg = 0.5 * (G[tail] + G[head]) if G is not None else np.zeros_like(diff)
+    d = beta * dabs + (1.0 - beta) * gavg
+    sl = np.where(label[tail] == 0, -1.0, 1.0)
+    fac = 1.0 + s * sl * alpha
+    c = d * fac
+    e = np.exp(-0.5 * c * c / (sigma * sigma))
+    w = 1.0 - e
+    dw_dc = e * c / (sigma * sigma)
+    dw = np.stack([-e * c * c / sigma ** 3, dw_dc * d * s * sl, dw_dc * (dabs - gavg) * fac])
+    obj = label != 0
+    u = np.where(has, np.where(obj, 1.0 - 0.5 * w, 0.5 * w),
+                 np.where((arcs == -2) & obj, 1.0, 0.0))
+    du = np.where(has, np.where(obj, -0.5, 0.5), 0.0)
+    Isum, P, T = float((u * t).sum()), float(u.sum()), float(t.sum())
+    den = P + T + eps
+    loss = 1.0 - (2.0 * Isum + eps) / den
+    dL_du = -2.0 * t / den + (2.0 * Isum + eps) / den ** 2
+    grad = (dw * (dL_du * du)[None, :]).sum(axis=1)
+    return loss, grad

@@ -100,6 +100,7 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_conditional_dilation", "oift_b200_inject_boundary_seeds",
            "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
            "oift_b200_run_pyramid_device_i16", "oift_b200_adjoint",
+           "oift_b200_bottleneck_arcs", "oift_b200_cost_adjoint",
            "oift_b200_batch_graph_create", "oift_b200_batch_graph_launch",
            "oift_b200_batch_graph_destroy", "oift_b200_read_seeds", "oift_b200_read_polarity",
            "oift_b200_read_volume", "oift_b200_write_volume"]
@@ -166,6 +167,10 @@ def lib():
         L.oift_b200_run_pyramid_host.argtypes = L.oift_b200_run_cli_host.argtypes
         L.oift_b200_adjoint.argtypes = [vp, C.POINTER(AdjointParams), vp, vp, vp, vp, vp, C.c_int,
                                         vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.oift_b200_bottleneck_arcs.argtypes = [vp, C.POINTER(Params), vp, vp, vp, vp, C.c_int,
+                                                vp]
+        L.oift_b200_cost_adjoint.argtypes = [vp, C.POINTER(AdjointParams), vp, vp, vp, vp, vp,
+                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.oift_b200_run_pyramid_device_i16.argtypes = [vp, C.POINTER(Params), vp, vp, vp, C.c_int,
                                                        C.c_int, C.c_float, vp,
                                                        C.POINTER(Stats)]
@@ -394,6 +399,36 @@ class Context:
                                      C.byref(loss), g if want_grad else None)
         if rc != OK:
             raise OiftError(rc, "oift_b200_adjoint")
+        return loss.value, np.array(list(g))
+
+    def bottleneck_arcs(self, params, image_ptr, cost_ptr, label_ptr, seeds_ptr, nseeds,
+                        arcs_ptr):
+        """Per-voxel bottleneck arc of the fixed OIFT forest (int64 [N] device output:
+        tail * 32 + direction, -2 at seeds, -3 unreached) from an integer OIFT result."""
+        rc = lib().oift_b200_bottleneck_arcs(self._h, C.byref(params), C.c_void_p(image_ptr),
+                                             C.c_void_p(cost_ptr), C.c_void_p(label_ptr),
+                                             C.c_void_p(seeds_ptr), int(nseeds),
+                                             C.c_void_p(arcs_ptr))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_bottleneck_arcs")
+
+    def cost_adjoint(self, shape_zyx, image_ptr, label_ptr, arcs_ptr, truth_ptr, sigma=150.0,
+                     alpha=0.0, beta=1.0, eps=1.0, adjacency=6, grad_map_ptr=None,
+                     want_grad=True):
+        """Soft-Dice loss of the object confidence of the cost map (continuous RBF weights
+        of the bottleneck arcs) and its gradient w.r.t. (sigma, alpha, beta)."""
+        Z, Y, X = shape_zyx
+        ap = AdjointParams(X, Y, Z, adjacency, 1, 0, ADJ_KERNELS["rbf"], float(sigma),
+                           float(alpha), float(beta), float(eps))
+        loss = C.c_double(0.0)
+        g = (C.c_double * 3)()
+        rc = lib().oift_b200_cost_adjoint(self._h, C.byref(ap), C.c_void_p(image_ptr),
+                                          C.c_void_p(grad_map_ptr) if grad_map_ptr else None,
+                                          C.c_void_p(label_ptr), C.c_void_p(arcs_ptr),
+                                          C.c_void_p(truth_ptr), C.byref(loss),
+                                          g if want_grad else None)
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_cost_adjoint")
         return loss.value, np.array(list(g))
 
     def level_profile(self, cap=8192):

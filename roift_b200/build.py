@@ -11,7 +11,7 @@ LIB = os.path.join(HERE, "liboift_b200.so")
 # gft::ift drop-ins (OIFT_Multi, ORelax_1_Multi and their per-class forms) over the C ABI
 SHIM = os.path.join(HERE, "libgft_oift_b200.so")
 SHIM_SRC = os.path.join(CSRC, "gft_shims.cpp")
-SOURCES = ["api.cu", "weights.cu", "oift.cu", "relax.cu", "selftest.cu", "noalloc.cu", "prepost.cu", "adjoint.cu", "imagegraph.cu", "volume_io.cu"]
+SOURCES = ["api.cu", "weights.cu", "oift.cu", "relax.cu", "selftest.cu", "noalloc.cu", "prepost.cu", "adjoint.cu", "imagegraph.cu", "volume_io.cu", "costgrad.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]

@@ -73,6 +73,7 @@ struct oift_b200_ctx {
     float lut_sigma = -1.0f;
     int lut_wq = -1, lut_len = 0;
     DevBuf hmemb;  // membership of the host entry
+    DevBuf bseed, barcs, csums;  // arc-weight-map adjoint: seed flags, arcs, block sums
     bool relax_tma = false;  // the last relax_launch staged its tiles with TMA
     size_t total = 0;
     unsigned long long oift_cycles[24] = {0};
@@ -177,7 +178,8 @@ int oift_b200_destroy(oift_b200_ctx *c) {
                       &c->dborder, &c->dhist, &c->daux, &c->dlabel, &c->yimg, &c->ylab,
                       &c->yseeds, &c->yslab, &c->yfirst, &c->yup, &c->ymerge, &c->yfseeds,
                       &c->yfslab, &c->yaux, &c->awork, &c->adist, &c->aseedc, &c->asmall,
-                      &c->al2c, &c->gmap, &c->igring, &c->igsmall, &c->Wt, &c->hmemb};
+                      &c->al2c, &c->gmap, &c->igring, &c->igsmall, &c->Wt, &c->hmemb,
+                      &c->bseed, &c->barcs, &c->csums};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     if (c->hslab) cudaFreeHost(c->hslab);
@@ -980,6 +982,73 @@ int oift_b200_relax_host(oift_b200_ctx *c, const oift_b200_params *p, const int3
     CU(cudaStreamSynchronize(s));
     CU(cudaGetLastError());
     return relax_tma_status(c);
+}
+
+int oift_b200_bottleneck_arcs(oift_b200_ctx *c, const oift_b200_params *p, const int16_t *image,
+                              const int32_t *cost, const int32_t *label, const int32_t *seeds,
+                              int nseeds, int64_t *arcs) {
+    if (!c || !image || !cost || !label || !arcs || (nseeds > 0 && !seeds)) return OIFT_E_BAD_ARG;
+    TRY(check_params(p));
+    if (p->weight_mode != OIFT_W_GRAD && p->weight_mode != OIFT_W_GRAD_Q) return OIFT_E_UNSUPPORTED;
+    if (p->per_class) return OIFT_E_UNSUPPORTED;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    const size_t N = (size_t)p->xsize * p->ysize * p->zsize;
+    TRY(grow(c, c->bseed, N));
+    TRY(grow(c, c->barcs, N * sizeof(long long)));
+    TRY(grow(c, c->flag, 4 * sizeof(int)));
+    CU(cudaMemsetAsync(c->bseed.p, 0, N, s));
+    if (nseeds > 0)
+        seed_flag_kernel<<<(nseeds + 255) / 256, 256, 0, s>>>(seeds, nseeds, N,
+                                                              (uint8_t *)c->bseed.p);
+    BottleneckSetup S{};
+    S.X = p->xsize;
+    S.Y = p->ysize;
+    S.Z = p->zsize;
+    S.adjacency = p->adjacency;
+    S.img = image;
+    S.cost = cost;
+    S.label = label;
+    S.seed = (const uint8_t *)c->bseed.p;
+    S.wmode = p->weight_mode;
+    S.wq = p->wq;
+    S.per = p->per;
+    return bottleneck_run(S, s, c->sms, (long long *)arcs, (long long *)c->barcs.p,
+                          (int *)c->flag.p + 2, &c->hm->flag[2], nullptr);
+}
+
+int oift_b200_cost_adjoint(oift_b200_ctx *c, const oift_b200_adjoint_params *ap,
+                           const int16_t *image, const float *grad_map, const int32_t *label,
+                           const int64_t *arcs, const uint8_t *truth, double *loss,
+                           double *grad) {
+    if (!c || !ap || !image || !label || !arcs || !truth || !loss) return OIFT_E_BAD_ARG;
+    if (ap->xsize <= 0 || ap->ysize <= 0 || ap->zsize <= 0 || !(ap->sigma > 0.0f) ||
+        !(std::fabs(ap->alpha) <= 1.0f) || !(ap->beta >= 0.0f && ap->beta <= 1.0f) ||
+        !(ap->eps >= 0.0f))
+        return OIFT_E_BAD_ARG;
+    if (ap->adjacency == 4 || ap->adjacency == 8) {
+        if (ap->zsize != 1) return OIFT_E_BAD_ARG;
+    } else if (ap->adjacency != 6 && ap->adjacency != 26) {
+        return OIFT_E_BAD_ARG;
+    }
+    cudaSetDevice(c->device);
+    const int max_blocks = c->sms * 8;
+    TRY(grow(c, c->csums, (size_t)max_blocks * 9 * sizeof(double)));
+    CostLossSetup S{};
+    S.X = ap->xsize;
+    S.Y = ap->ysize;
+    S.Z = ap->zsize;
+    S.adjacency = ap->adjacency;
+    S.img = image;
+    S.g = grad_map;
+    S.label = label;
+    S.arcs = (const long long *)arcs;
+    S.truth = truth;
+    S.sigma = ap->sigma;
+    S.alpha = ap->alpha;
+    S.beta = ap->beta;
+    S.eps = ap->eps;
+    return cost_loss_run(S, c->stream, c->sms, (double *)c->csums.p, max_blocks, loss, grad);
 }
 
 int oift_b200_build_weights_i16(oift_b200_ctx *c, const oift_b200_params *p,

@@ -276,6 +276,34 @@ struct AdjointJob {
     float *membership_out;    // [C][N] final membership, may be null
 };
 size_t adjoint_work_floats(size_t N, int C, int K, int c);
+
+// ---- arc-weight-map adjoint (costgrad.cu) ----
+// Bottleneck arcs of the fixed OIFT forest read from an integer OIFT result; arcs[p] =
+// tail * 32 + direction (gft Spheric order, tail -> tail + d), -2 at seeds, -3 unreached.
+struct BottleneckSetup {
+    int X, Y, Z, adjacency;
+    const int16_t *img;
+    const int32_t *cost, *label;
+    const uint8_t *seed;
+    int wmode, wq;
+    float per;  // global polarity x100 of the OIFT
+};
+__global__ void seed_flag_kernel(const int32_t *seeds, int nseeds, size_t N, uint8_t *flag);
+int bottleneck_run(const BottleneckSetup &S, cudaStream_t s, int sms, long long *arcs,
+                   long long *tmp, int *d_changed, int *h_changed, int *rounds_out);
+// Soft-Dice loss of the cost-derived object confidence and its gradient w.r.t. (sigma,
+// alpha, beta); d_sums holds max_blocks * 9 doubles.
+struct CostLossSetup {
+    int X, Y, Z, adjacency;
+    const int16_t *img;
+    const float *g;
+    const int32_t *label;
+    const long long *arcs;
+    const uint8_t *truth;
+    double sigma, alpha, beta, eps;
+};
+int cost_loss_run(const CostLossSetup &S, cudaStream_t s, int sms, double *d_sums,
+                  int max_blocks, double *loss, double *grad);
 int adjoint_run(const AdjointJob &J, cudaStream_t s, int sms, float *work, size_t work_floats,
                 void *small, double *loss_out, double *grad_out);
 

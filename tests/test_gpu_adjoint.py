@@ -110,3 +110,61 @@ def test_adjoint_autograd_function_trains(roift, oracle_lib):
             theta[2].clamp_(0.0, 1.0)
         first = first if first is not None else float(loss)
     assert float(RelaxDice.apply(theta)) < first
+
+
+# ---------------------------------------------------------- arc-weight-map term ----
+@pytest.mark.parametrize("adj,shape,mode", [(6, (20, 24, 28), "grad_q"), (4, (1, 48, 56), "grad"),
+                                            (26, (12, 16, 20), "grad_q")])
+def test_cost_adjoint_matches_fp64_and_central_differences(roift, oracle_lib, adj, shape, mode):
+    """Bottleneck arcs of the fixed OIFT forest (from the GPU's own integer OIFT result)
+    equal the restatement's; the cost-map loss and its gradient equal the FP64
+    restatement's; and the C-ABI gradient is within 1e-4 relative of central differences
+    (h = 1e-3) of the GPU forward."""
+    import torch
+    c, img, lab, truth, g = _problem(adj, shape)
+    dev = torch.device("cuda:0")
+    N = c.n
+    t_img = torch.from_numpy(img.astype(np.int16).reshape(-1).copy()).to(dev)
+    t_sd = torch.from_numpy(c.seeds).to(dev)
+    t_sl = torch.from_numpy(c.seed_labels).to(dev)
+    cost = torch.empty(N, dtype=torch.int32, device=dev)
+    olab = torch.empty(N, dtype=torch.int32, device=dev)
+    arcs = torch.empty(N, dtype=torch.int64, device=dev)
+    ctx = roift.Context(0)
+    p = roift.make_params(c.shape, adjacency=adj, weight_mode=mode, wq=4095, pol=c.pol, sweeps=0)
+    ctx.run_device(p, t_img.data_ptr(), t_sd.data_ptr(), t_sl.data_ptr(), len(c.seeds),
+                   cost=cost.data_ptr(), oift_label=olab.data_ptr())
+    ctx.bottleneck_arcs(p, t_img.data_ptr(), cost.data_ptr(), olab.data_ptr(), t_sd.data_ptr(),
+                        len(c.seeds), arcs.data_ptr())
+    torch.cuda.synchronize()
+    cost_h, lab_h, arcs_h = cost.cpu().numpy(), olab.cpu().numpy(), arcs.cpu().numpy()
+    arcs64 = A.bottleneck_arcs(img.reshape(c.shape), cost_h, lab_h, c.seeds, adj, c.pol, mode=mode)
+    assert np.array_equal(arcs_h, arcs64)
+    assert not (arcs_h == -1).any()
+    t_lab = torch.from_numpy(lab_h).to(dev)
+    t_tr = torch.from_numpy(truth).to(dev)
+    t_g = torch.from_numpy(g.reshape(-1).copy()).to(dev)
+    th = np.array([140.0, -0.25, 0.7])
+
+    def gpu(theta, want_grad=True):
+        return ctx.cost_adjoint(c.shape, t_img.data_ptr(), t_lab.data_ptr(), arcs.data_ptr(),
+                                t_tr.data_ptr(), sigma=theta[0], alpha=theta[1], beta=theta[2],
+                                adjacency=adj, grad_map_ptr=t_g.data_ptr(), want_grad=want_grad)
+
+    loss, grad = gpu(th)
+    # the C ABI takes float parameters: compare with FP64 at the same float values
+    thf = np.array([np.float32(v) for v in th], np.float64)
+    loss64, grad64 = A.cost_loss(img.reshape(c.shape), lab_h, arcs_h, truth, *thf, adj=adj,
+                                 g=g.reshape(c.shape))
+    assert abs(loss - loss64) <= 1e-9 * max(abs(loss64), 1e-12)
+    assert np.allclose(grad, grad64, rtol=1e-8, atol=1e-12 * np.abs(grad64).max())
+    h = 1e-3
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = h
+        # float parameters: difference the exact float points the GPU sees
+        hi = np.array([np.float32(v) for v in th + e], np.float64)
+        lo = np.array([np.float32(v) for v in th - e], np.float64)
+        fd = (gpu(hi, False)[0] - gpu(lo, False)[0]) / (hi[k] - lo[k])
+        assert abs(grad[k] - fd) <= 1e-4 * abs(grad[k]) + 1e-6 * np.abs(grad).max(), (k, grad, fd)
+    ctx.close()

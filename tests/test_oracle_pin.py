@@ -365,3 +365,41 @@ def test_imagegraph_matches_live_reference(oracle_lib):
         if K:
             assert np.array_equal(out, exp), trial
     print("pixels where the Prim-forest f_max differs from R2:", fmax_diff)
+
+
+@pytest.mark.parametrize("adj,shape", [(6, (16, 20, 24)), (4, (1, 40, 52)), (26, (10, 14, 18))])
+def test_bottleneck_arcs_carry_the_cost_and_gradient_is_exact(oracle_lib, adj, shape):
+    """Restated bottleneck arcs: every reached non-seed voxel gets one; the arc's tail has the
+    voxel's label and its integer oriented weight equals the voxel's f_max cost; the FP64
+    cost-map loss has the gradient of its central differences."""
+    from oracle import adjoint as AD
+    c = synth.small_case(seed=44, shape=shape, pol=-0.3, adjacency=adj, nlabels=1, noise=120,
+                         contrast=400)
+    img = c.image.astype(np.int32)
+    Z, Y, X = c.shape
+    W, _ = O.build_weights(img, adj, "grad_q", wq=4095)
+    cost, lab, _ = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=c.pol)
+    arcs = AD.bottleneck_arcs(img.reshape(c.shape), cost, lab, c.seeds, adj, c.pol)
+    assert not (arcs == -1).any()
+    has = arcs >= 0
+    offs = np.array(AD.offsets(adj))
+    tail, d = arcs[has] >> 5, arcs[has] & 31
+    head = (tail % X + offs[d, 0]) + ((tail // X) % Y + offs[d, 1]) * X + (tail // (X * Y) + offs[d, 2]) * X * Y
+    assert np.array_equal(lab[tail], lab[has])
+    I = img.reshape(-1).astype(np.int64)
+    base = np.minimum(np.abs(I[tail] - I[head]), 4095)
+    per = float(np.float32(c.pol * 100.0))
+    pl = np.where(lab[tail] == 0, -per, per)
+    f = np.where(I[tail] > I[head], 1.0 + pl / 100.0, np.where(I[tail] < I[head], 1.0 - pl / 100.0, 1.0))
+    assert np.array_equal(np.floor(base * f).astype(np.int64), cost[has].astype(np.int64))
+    truth = (img.reshape(-1) > 850).astype(np.uint8)
+    th = np.array([160.0, 0.2, 0.9])
+    g = np.abs(np.gradient(img.astype(np.float64), axis=-1))
+    loss, grad = AD.cost_loss(img.reshape(c.shape), lab, arcs, truth, *th, adj=adj, g=g)
+    h = 1e-3
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = h
+        fd = (AD.cost_loss(img.reshape(c.shape), lab, arcs, truth, *(th + e), adj=adj, g=g)[0] -
+              AD.cost_loss(img.reshape(c.shape), lab, arcs, truth, *(th - e), adj=adj, g=g)[0]) / (2 * h)
+        assert abs(grad[k] - fd) <= 1e-6 * abs(grad[k]) + 1e-9
