@@ -236,6 +236,8 @@ def run_batch_workload(args):
         torch.cuda.synchronize()
         return time.perf_counter() - t0, r
 
+    sampler = ClockSampler(0)
+    sampler.start()
     scan, parts = {}, {}
     for teams in [int(t) for t in args.team_scan.split(",")]:
         scan[teams], st = timed(lambda: ctx.run_batch(common, jobs, teams=teams))
@@ -259,7 +261,37 @@ def run_batch_workload(args):
                               mask=mask.data_ptr())
     per_volume()                                     # warm-up (scratch growth)
     per_volume_s, _ = timed(per_volume)
+    clocks = sampler.stop()
     best_s = min(batched_s, graph_s)
+    # the reference's own plain-GPU OIFT (gpu/oift_fmax_gpu.cu, built from its source for
+    # sm_100a), one job after the other through its entry point with host buffers, beside our
+    # batched OIFT (weights + team launch, device time) and our drop-in of the same entry
+    plain = None
+    if not args.no_plain_gpu:
+        import oracle as O
+        if O.ref_gpu_available():
+            ref_s = ours_s = 0.0
+            for case, img, st, lt, mask, ns in jobs_py:
+                img32 = case.image.astype(np.int32).reshape(-1)
+                img32 -= min(0, int(img32.min()))
+                sd, sl = st.cpu().numpy(), lt.cpu().numpy()
+                per = float(np.float32(case.pol * 100.0))
+                pc = np.array([-per, per], np.float32)
+                t0 = time.perf_counter()
+                O.ref_oift_fmax_gpu_run(img32, sd, sl, pc)
+                ref_s += time.perf_counter() - t0
+                lab = np.full(case.n, -1, np.int32)
+                lab[sd] = sl
+                Z, Y, X = case.shape
+                t0 = time.perf_counter()
+                rb.oift_fmax_gpu_run(img32, lab, X, Y, Z, pc, sd)
+                ours_s += time.perf_counter() - t0
+            ours_batched_s = min(p["oift_ms"] for p in parts.values()) / 1e3
+            plain = {"scope": "OIFT only, every seed set of the mix one after the other",
+                     "reference_oift_fmax_gpu_run_s": ref_s,
+                     "ours_oift_fmax_gpu_run_s": ours_s,
+                     "ours_batched_oift_s": ours_batched_s,
+                     "batched_vs_reference_per_volume": ref_s / ours_batched_s}
     out = {"metric": "batched vol/s (64-volume mix, OIFT + 20 sweeps per seed set)",
            "value": args.nvol / best_s, "unit": "vol/s", "n_gpus": 1,
            "higher_is_better": True, "data": "synthetic", "dtype": "int32/fp32",
@@ -275,7 +307,8 @@ def run_batch_workload(args):
                        "gvox_s": vox / batched_s / 1e9},
            "graph_replay": {"s": graph_s, "device_ms": graph_dev_ms,
                             "vol_s": args.nvol / graph_s, "gvox_s": vox / graph_s / 1e9},
-           "speedup_vs_per_volume": per_volume_s / best_s}
+           "speedup_vs_per_volume": per_volume_s / best_s,
+           "plain_gpu_reference": plain, "clocks": clocks}
     print(json.dumps(out))
     single.close()
     ctx.close()
@@ -359,9 +392,11 @@ def run_threeobj_workload(args):
 
 def run_diff_workload(args):
     """Sixteen 192^3 ellipsoid volumes with ground-truth masks: one training step computes,
-    for every volume, the soft-Dice loss after 40 RBF relaxation sweeps and its gradient
-    with respect to (sigma, alpha, beta) through the adjoint (checkpoint every 7 sweeps), and
-    applies one Adam update.  OIFT labels are computed once (fixed forest)."""
+    for every volume, the loss = soft-Dice of the membership after 40 RBF relaxation sweeps
+    + soft-Dice of the cost-map confidence, and its gradient with respect to (sigma, alpha,
+    beta): through the relaxation adjoint (checkpoint every 7 sweeps) and through the
+    bottleneck arcs of the fixed OIFT forest; then one Adam update.  The OIFT (labels, cost)
+    and its bottleneck arcs are computed once per volume (fixed forest)."""
     import torch
     import roift_b200 as rb
     from roift_b200 import synth
@@ -375,24 +410,31 @@ def run_diff_workload(args):
         sd = torch.from_numpy(c.seeds).to(dev)
         sl = torch.from_numpy(c.seed_labels).to(dev)
         lab = torch.empty(c.n, dtype=torch.int32, device=dev)
+        cost = torch.empty(c.n, dtype=torch.int32, device=dev)
+        arcs = torch.empty(c.n, dtype=torch.int64, device=dev)
         prm = rb.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095, pol=c.pol,
                              sweeps=0)
         ctx.run_device(prm, img.data_ptr(), sd.data_ptr(), sl.data_ptr(), len(c.seeds),
-                       oift_label=lab.data_ptr())
+                       oift_label=lab.data_ptr(), cost=cost.data_ptr())
+        ctx.bottleneck_arcs(prm, img.data_ptr(), cost.data_ptr(), lab.data_ptr(), sd.data_ptr(),
+                            len(c.seeds), arcs.data_ptr())
         tr = torch.from_numpy(c.truth.reshape(-1).astype(np.uint8)).to(dev)
-        data.append((c, img, sd, sl, lab, tr))
+        data.append((c, img, sd, sl, lab, tr, arcs))
     theta = np.array([150.0, -0.3, 1.0])
     mom, vel, b1, b2, lr = np.zeros(3), np.zeros(3), 0.9, 0.999, np.array([5.0, 0.02, 0.02])
 
     def step(it):
         nonlocal mom, vel, theta
         total, grad = 0.0, np.zeros(3)
-        for c, img, sd, sl, lab, tr in data:
+        for c, img, sd, sl, lab, tr, arcs in data:
             l, g = ctx.adjoint(c.shape, img.data_ptr(), lab.data_ptr(), sd.data_ptr(),
                                sl.data_ptr(), len(c.seeds), tr.data_ptr(), sigma=theta[0],
                                alpha=theta[1], beta=theta[2], sweeps=40, checkpoint=7)
-            total += l
-            grad += g
+            lc, gc = ctx.cost_adjoint(c.shape, img.data_ptr(), lab.data_ptr(), arcs.data_ptr(),
+                                      tr.data_ptr(), sigma=theta[0], alpha=theta[1],
+                                      beta=theta[2])
+            total += l + lc
+            grad += g + gc
         mom = b1 * mom + (1 - b1) * grad
         vel = b2 * vel + (1 - b2) * grad * grad
         mh, vh = mom / (1 - b1 ** (it + 1)), vel / (1 - b2 ** (it + 1))
@@ -413,14 +455,16 @@ def run_diff_workload(args):
     clocks = sampler.stop()
     vox = sum(d[0].n for d in data)
     print(json.dumps({
-        "metric": "adjoint training steps/s (16 x 192^3, 40 RBF sweeps, checkpoint 7, Adam)",
+        "metric": "adjoint training steps/s (16 x 192^3, 40 RBF sweeps, checkpoint 7, cost-map term, Adam)",
         "value": 1.0 / dt, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (fp64 gradient sums)",
         "data": "synthetic",
         "config": {"workload": f"{len(data)} ellipsoid volumes {args.size_diff}^3 int16 with "
-                               "ground truth, OIFT labels fixed, soft-Dice, 40 sweeps, "
-                               "checkpoint every 7, Adam on (sigma, alpha, beta)",
+                               "ground truth, OIFT forest fixed, soft-Dice of the membership "
+                               "after 40 sweeps (checkpoint every 7) + soft-Dice of the "
+                               "cost-map confidence (bottleneck arcs), Adam on "
+                               "(sigma, alpha, beta)",
                    "voxels": vox},
         "gvox_per_s_forward_backward": vox / dt / 1e9,
         "loss_first_last": [losses[0], losses[-1]], "theta": theta.tolist(),
