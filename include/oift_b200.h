@@ -170,6 +170,7 @@ typedef struct {
     float ms_wall;      /* host wall time of the jobs after tuning */
     float ms_oift;      /* device time of weights + batched OIFT */
     float ms_relax;     /* host wall time of the relaxation phase */
+    int tile_ty;        /* 3D warp tile of the OIFT teams: 8 = 32x8x4, 4 = 32x4x8 */
 } oift_b200_batch_stats;
 
 /* Batched driver for many volumes of uneven sizes with several seed sets per volume.  Runs
@@ -198,6 +199,9 @@ OIFT_API int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_pa
 OIFT_API int oift_b200_batch_graph_launch(oift_b200_batch_graph *graph, oift_b200_job *jobs,
                                           float *ms);
 OIFT_API int oift_b200_batch_graph_destroy(oift_b200_batch_graph *graph);
+/* 3D warp tile of the batched OIFT for explicit team counts (teams > 0): 8 = 32x8x4 (the
+ * default) or 4 = 32x4x8.  With teams = 0 the autotuner chooses the tile with the team count. */
+OIFT_API int oift_b200_set_batch_tile(oift_b200_ctx *ctx, int tile_ty);
 /* CTAs of the persistent OIFT grid of this context (0 = one per SM, the default). */
 OIFT_API int oift_b200_set_oift_grid(oift_b200_ctx *ctx, int ctas);
 /* Bounds of the OIFT kernels' device-side waits for later calls of this context:

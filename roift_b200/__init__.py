@@ -85,7 +85,8 @@ ADJ_KERNELS = {"rbf": 0, "pow8": 1}
 
 class BatchStats(C.Structure):
     _fields_ = [("teams", C.c_int), ("jobs", C.c_int), ("tuning", C.c_int),
-                ("ms_wall", C.c_float), ("ms_oift", C.c_float), ("ms_relax", C.c_float)]
+                ("ms_wall", C.c_float), ("ms_oift", C.c_float), ("ms_relax", C.c_float),
+                ("tile_ty", C.c_int)]
 
 
 EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
@@ -96,6 +97,7 @@ EXPORTS = ["oift_b200_create", "oift_b200_destroy", "oift_b200_scratch_bytes",
            "oift_b200_level_profile", "oift_b200_selftest_div100",
            "oift_b200_oift_noalloc", "oift_b200_noalloc_scratch_bytes",
            "oift_b200_run_batch", "oift_b200_set_oift_grid", "oift_b200_set_limits",
+           "oift_b200_set_batch_tile",
            "oift_b200_gaussian_blur_i32",
            "oift_b200_conditional_dilation", "oift_b200_inject_boundary_seeds",
            "oift_b200_run_cli_host", "oift_b200_run_pyramid_host",
@@ -132,6 +134,7 @@ def lib():
                                           C.POINTER(BatchStats)]
         L.oift_b200_set_oift_grid.argtypes = [vp, C.c_int]
         L.oift_b200_set_limits.argtypes = [vp, C.c_longlong, C.c_int]
+        L.oift_b200_set_batch_tile.argtypes = [vp, C.c_int]
         L.oift_b200_relax_host.argtypes = [vp, C.POINTER(Params), i32p, i32p, i32p, C.c_int,
                                            vp, C.c_int, vp]
         L.oift_b200_batch_graph_create.argtypes = [vp, C.POINTER(Params), C.POINTER(Job), C.c_int,
@@ -315,6 +318,12 @@ class Context:
         rc = lib().oift_b200_set_limits(self._h, C.c_longlong(int(spin_limit)), int(max_levels))
         if rc != OK:
             raise OiftError(rc, "oift_b200_set_limits")
+
+    def set_batch_tile(self, tile_ty: int):
+        """Warp tile of the batched OIFT for explicit team counts: 8 (32x8x4) or 4 (32x4x8)."""
+        rc = lib().oift_b200_set_batch_tile(self._h, int(tile_ty))
+        if rc != OK:
+            raise OiftError(rc, "oift_b200_set_batch_tile")
 
     def set_oift_grid(self, ctas: int):
         rc = lib().oift_b200_set_oift_grid(self._h, int(ctas))

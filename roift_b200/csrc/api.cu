@@ -32,7 +32,13 @@ struct oift_b200_ctx {
     long long spin_limit = OIFT_DEFAULT_SPIN_LIMIT;
     int max_levels = OIFT_DEFAULT_MAX_LEVELS;
     std::vector<oift_b200_ctx *> lanes;  // sub-contexts (relaxation streams) of the batched driver
-    std::vector<std::pair<int, double>> tune_cands;  // batch autotuner: (teams, rate)
+    // batch autotuner: candidate (teams, warp-tile shape) with its measured rate (< 0 untried)
+    struct TuneCand {
+        int teams, tile_ty;
+        double rate;
+    };
+    std::vector<TuneCand> tune_cands;
+    int batch_tile_ty = 8;  // warp tile of explicit team counts: 8 (32x8x4) or 4 (32x4x8)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     // ev[10]: the early readback of one pipeline call has landed; ev[11]: the host entry's
@@ -196,6 +202,12 @@ size_t oift_b200_scratch_bytes(const oift_b200_ctx *c) {
     size_t t = c->total;
     for (const oift_b200_ctx *l : c->lanes) t += l->total;
     return t;
+}
+
+int oift_b200_set_batch_tile(oift_b200_ctx *c, int tile_ty) {
+    if (!c || (tile_ty != 8 && tile_ty != 4)) return OIFT_E_BAD_ARG;
+    c->batch_tile_ty = tile_ty;
+    return OIFT_OK;
 }
 
 int oift_b200_set_oift_grid(oift_b200_ctx *c, int ctas) {
@@ -1844,25 +1856,27 @@ struct BatchPrep {
     OiftTeamScratch S;
     OiftTeamJob *d_jobs = nullptr;
     unsigned long long *d_clamp = nullptr;
+    int tile_ty = 8;  // 3D warp tile of the team kernel (oift_plan)
 };
 
 // Most teams the batch can be split into: every team must hold enough CTAs to own the tiles
 // of the largest job (a CTA's tile sets live in shared memory).
 static int batch_max_teams(const oift_b200_ctx *c, const oift_b200_job *jobs, int first,
-                           int count) {
+                           int count, int tile_ty) {
     int need = 1;
     for (int j = first; j < first + count; j++) {
         const oift_b200_job &jb = jobs[j];
         if (jb.xsize <= 0 || jb.ysize <= 0 || jb.zsize <= 0) continue;
-        const OiftPlan P = oift_plan(jb.xsize, jb.ysize, jb.zsize);
+        const OiftPlan P = oift_plan(jb.xsize, jb.ysize, jb.zsize, tile_ty);
         need = std::max(need, oift_min_ctas(P.ntiles));
     }
     return std::max(1, c->sms / need);
 }
 
 static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_b200_job *jobs,
-                         int first, int count, int teams, BatchPrep *bp) {
+                         int first, int count, int teams, int tile_ty, BatchPrep *bp) {
     cudaStream_t s = c->stream;
+    bp->tile_ty = tile_ty == 4 ? 4 : 8;
     const int end = first + count;
     if (teams < 1 || teams > c->sms) return OIFT_E_BAD_ARG;
     // the team kernel is the 6 / 4-neighbourhood tile step on prebuilt edge codes
@@ -2008,7 +2022,7 @@ static int batch_prepare(oift_b200_ctx *c, const oift_b200_params *common, oift_
     int n3d = 0;
     for (int i = 0; i < nj; i++) {
         const oift_b200_job &jb = jobs[order[i]];
-        const OiftPlan P = oift_plan(jb.xsize, jb.ysize, jb.zsize);
+        const OiftPlan P = oift_plan(jb.xsize, jb.ysize, jb.zsize, bp->tile_ty);
         const size_t n = (size_t)jb.xsize * jb.ysize * jb.zsize;
         OiftTeamJob &d = dj[i];
         d.W = (const uint16_t *)c->W.p + imgs[job_img[order[i] - first]].woff;
@@ -2075,14 +2089,14 @@ static int batch_enqueue_oift(oift_b200_ctx *c, const BatchPrep &bp, int teams,
     if (d_pristine)
         CU(cudaMemcpyAsync(bp.d_jobs, d_pristine, (size_t)bp.nj * sizeof(OiftTeamJob),
                            cudaMemcpyDeviceToDevice, s));
-    if (bp.n3d > 0) TRY(oift_team_run(bp.d_jobs, bp.n3d, false, teams, c->sms, bp.S, s));
+    if (bp.n3d > 0) TRY(oift_team_run(bp.d_jobs, bp.n3d, false, teams, c->sms, bp.S, s, bp.tile_ty));
     if (bp.nj - bp.n3d > 0)
         TRY(oift_team_run(bp.d_jobs + bp.n3d, bp.nj - bp.n3d, true, teams, c->sms, bp.S, s));
     return OIFT_OK;
 }
 
 static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
-                           oift_b200_job *jobs, int first, int count, int teams,
+                           oift_b200_job *jobs, int first, int count, int teams, int tile_ty,
                            BatchTimes *bt) {
     using clk = std::chrono::steady_clock;
     const auto t0 = clk::now();
@@ -2090,8 +2104,8 @@ static int run_batch_teams(oift_b200_ctx *c, const oift_b200_params *common,
     const int end = first + count;
 
     BatchPrep bp;
-    teams = std::min(teams, batch_max_teams(c, jobs, first, count));
-    TRY(batch_prepare(c, common, jobs, first, count, teams, &bp));
+    teams = std::min(teams, batch_max_teams(c, jobs, first, count, tile_ty));
+    TRY(batch_prepare(c, common, jobs, first, count, teams, tile_ty, &bp));
     const int nimg = bp.nimg, nj = bp.nj;
     if (nimg == 0) {
         for (int j = first; j < end; j++)
@@ -2210,17 +2224,19 @@ int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_params *com
         return OIFT_E_BAD_ARG;
     *out = nullptr;
     cudaSetDevice(ctx->device);
+    int tile_ty = ctx->batch_tile_ty;
     if (teams == 0) {
         // the context's autotuned choice when it has one, else half the SMs
         double best = -1.0;
         teams = ctx->sms / 2;
         for (auto &tc : ctx->tune_cands)
-            if (tc.second > best) {
-                best = tc.second;
-                teams = tc.first;
+            if (tc.rate > best) {
+                best = tc.rate;
+                teams = tc.teams;
+                tile_ty = tc.tile_ty;
             }
     }
-    teams = std::max(1, std::min(std::min(teams, njobs), batch_max_teams(ctx, jobs, 0, njobs)));
+    teams = std::max(1, std::min(std::min(teams, njobs), batch_max_teams(ctx, jobs, 0, njobs, tile_ty)));
     oift_b200_batch_graph *g = new oift_b200_batch_graph();
     g->njobs = njobs;
     g->weight_mode = common->weight_mode;
@@ -2233,7 +2249,7 @@ int oift_b200_batch_graph_create(oift_b200_ctx *ctx, const oift_b200_params *com
     oift_b200_ctx *c = g->c;
     cudaStream_t s = c->stream;
     BatchPrep &bp = g->bp;
-    rc = batch_prepare(c, common, jobs, 0, njobs, teams, &bp);
+    rc = batch_prepare(c, common, jobs, 0, njobs, teams, tile_ty, &bp);
     for (int j = 0; rc == OIFT_OK && j < njobs; j++)
         if (jobs[j].status != OIFT_OK) rc = jobs[j].status;
     if (rc == OIFT_OK && bp.nj == 0) rc = OIFT_E_BAD_ARG;
@@ -2356,37 +2372,44 @@ int oift_b200_run_batch(oift_b200_ctx *c, const oift_b200_params *common, oift_b
     // untried candidate and records its rate (voxels per wall millisecond of the call);
     // once every candidate has a rate, calls use the fastest.
     int cand = -1;
+    int tile_ty = c->batch_tile_ty;
     if (teams == 0) {
+        // candidates: team counts x the two 3D warp tiles of 32 rows that keep the OIFT's
+        // chains short (32 x 8 x 4 and 32 x 4 x 8; flatter tiles need more tile crossings)
         if (c->tune_cands.empty()) {
             const int G = c->sms;
-            for (int t : {G / 2, G / 4, G, G / 8})
-                if (t >= 1) c->tune_cands.push_back({t, -1.0});
+            for (int ty : {8, 4})
+                for (int t : {G / 2, G / 4, G, G / 8})
+                    if (t >= 1) c->tune_cands.push_back({t, ty, -1.0});
         }
         for (size_t i = 0; i < c->tune_cands.size(); i++)
-            if (c->tune_cands[i].second < 0) {
+            if (c->tune_cands[i].rate < 0) {
                 cand = (int)i;
                 break;
             }
         if (cand >= 0) {
-            teams = c->tune_cands[cand].first;
+            teams = c->tune_cands[cand].teams;
+            tile_ty = c->tune_cands[cand].tile_ty;
         } else {
             double best = -1.0;
             for (auto &tc : c->tune_cands)
-                if (tc.second > best) {
-                    best = tc.second;
-                    teams = tc.first;
+                if (tc.rate > best) {
+                    best = tc.rate;
+                    teams = tc.teams;
+                    tile_ty = tc.tile_ty;
                 }
         }
     }
     const int used = std::min(teams, njobs);  // more teams than jobs would idle
     BatchTimes bt;
-    const int rc = run_batch_teams(c, common, jobs, 0, njobs, used, &bt);
+    const int rc = run_batch_teams(c, common, jobs, 0, njobs, used, tile_ty, &bt);
     if (cand >= 0 && rc == OIFT_OK) {
         double vox = 0;
         for (int j = 0; j < njobs; j++) vox += (double)jobs[j].xsize * jobs[j].ysize * jobs[j].zsize;
-        c->tune_cands[cand].second = vox / std::max(bt.wall_ms, 1e-3);
+        c->tune_cands[cand].rate = vox / std::max(bt.wall_ms, 1e-3);
     }
     if (stats) {
+        stats->tile_ty = tile_ty;
         stats->teams = used;
         stats->jobs = njobs;
         stats->tuning = cand >= 0 ? 1 : 0;

@@ -133,7 +133,9 @@ __global__ void seed_presence_kernel(const int32_t *seed_labels, int nseeds, uin
 __global__ void relax_argmax_kernel(const float *m, size_t N, int C, const int *classes,
                                     int32_t *label, uint8_t *mask);
 
-OiftPlan oift_plan(int X, int Y, int Z);
+// Warp tiling of the 6 / 4 OIFT: 32 x 32 in 2D; 32 x 8 x 4 in 3D, or 32 x 4 x 8 with tile_ty 4
+// (the batched driver's second tile shape).
+OiftPlan oift_plan(int X, int Y, int Z, int tile_ty = 8);
 size_t oift_globals_bytes();
 int oift_mbox_words(const OiftPlan &P, int ctas);
 size_t oift_mbox_bytes(const OiftPlan &P, int ctas);
@@ -176,8 +178,9 @@ struct OiftTeamScratch {
 // writes cost / label.  All jobs of one call must be 2D (Z == 1) when planar, else 3D.
 // The mailbox stride must hold oift_mbox_bytes for both team sizes.  Returns OIFT_OK once
 // the launch is queued; per-job results are in d_jobs[].status.
+// tile_ty selects the 3D warp tile: 8 (32 x 8 x 4, the default) or 4 (32 x 4 x 8).
 int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ctas,
-                  const OiftTeamScratch &S, cudaStream_t st);
+                  const OiftTeamScratch &S, cudaStream_t st, int tile_ty = 8);
 
 // ---- steps around the path (prepost.cu) ----
 template <typename T>

@@ -307,7 +307,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             else
                 *reinterpret_cast<uint4 *>(shy + zl * 32 + col * 8) = make_uint4(0, 0, 0, 0);
         }
-        if (TZ > 1) {
+        if (TZ > 1 && (lane >> 2) < TY) {  // TY rows of four 16-byte chunks
             const int yl = lane >> 2, col = lane & 3;
             if (z0 > 0)
                 cp_async16(shz + yl * 32 + col * 8,
@@ -1070,7 +1070,9 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     uint16_t *sw = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * 4096) + warp * 3072;
     uint16_t *shx = reinterpret_cast<uint16_t *>(smem_raw + OIFT_WARPS * (4096 + 6144)) + warp * 448;
     uint16_t *shy = shx + 64;
-    uint16_t *shz = shx + 64 + 4 * 32;
+    uint16_t *shz = shx + 64 + TZ * 32;  // 64 + 32 (TY + TZ) <= 448 halo codes per warp
+    static_assert(FULLN || (TY * TZ == 32 && (TZ == 1 || TY + TZ <= 12)),
+                  "the halo codes of a warp tile must fit their 448-entry region");
     uint32_t *blk_min = cs.blk_min;
     long long cyc_tile[20];
 #pragma unroll
@@ -1520,11 +1522,14 @@ OiftPlan oift_plan_full(int X, int Y, int Z) {
     return P;
 }
 
-OiftPlan oift_plan(int X, int Y, int Z) {
+OiftPlan oift_plan(int X, int Y, int Z, int tile_ty) {
     OiftPlan P;
     if (Z == 1) {
         P.TY = 32;
         P.TZ = 1;
+    } else if (tile_ty == 4) {
+        P.TY = 4;
+        P.TZ = 8;
     } else {
         P.TY = 8;
         P.TZ = 4;
@@ -1682,7 +1687,7 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
 }
 
 int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ctas,
-                  const OiftTeamScratch &S, cudaStream_t st) {
+                  const OiftTeamScratch &S, cudaStream_t st, int tile_ty) {
     if (njobs <= 0) return OIFT_OK;
     if (teams <= 0 || ctas < teams) return OIFT_E_BAD_ARG;
     if (cudaMemsetAsync(S.g, 0, (size_t)teams * sizeof(OiftGlobals), st) != cudaSuccess ||
@@ -1714,7 +1719,8 @@ int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ct
         return cudaLaunchKernelExC(&cfg, kfn, args);
     };
     cudaError_t err = planar ? launch((const void *)oift_team_kernel<32, 1>)
-                             : launch((const void *)oift_team_kernel<8, 4>);
+                      : tile_ty == 4 ? launch((const void *)oift_team_kernel<4, 8>)
+                                     : launch((const void *)oift_team_kernel<8, 4>);
     if (err != cudaSuccess) {
         cudaGetLastError();
         return OIFT_E_CUDA;

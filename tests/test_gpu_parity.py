@@ -247,10 +247,11 @@ def _batch_cases():
     return cases
 
 
-@pytest.mark.parametrize("teams", [1, 3, 16, 0])
-def test_batch_matches_single_runs(roift, teams):
-    """The team-batched OIFT (and the autotuner, teams=0) gives, per job, the labels, mask
-    and costs of one-at-a-time runs, for every mix of requested outputs."""
+@pytest.mark.parametrize("teams,tile", [(1, 8), (3, 8), (16, 8), (0, 8), (3, 4), (16, 4)])
+def test_batch_matches_single_runs(roift, teams, tile):
+    """The team-batched OIFT (and the autotuner, teams=0) with either 3D warp tile (32x8x4,
+    32x4x8) gives, per job, the labels, mask and costs of one-at-a-time runs, for every mix
+    of requested outputs."""
     import torch
     dev = torch.device("cuda:0")
     cases = _batch_cases()
@@ -259,9 +260,12 @@ def test_batch_matches_single_runs(roift, teams):
     p = roift.make_params((1, 1, 1), adjacency=6, weight_mode="grad_q", wq=4095, sweeps=6)
     jobs, bufs = _batch_jobs(roift, cases, torch, dev, outs)
     ctx = roift.Context(0)
+    ctx.set_batch_tile(tile)
     st = ctx.run_batch(p, jobs, teams=teams)
     torch.cuda.synchronize()
     assert st.jobs == len(cases) and st.teams >= 1
+    if teams:
+        assert st.tile_ty == tile
     for c, (img, sd, sl, lab, mask, cost), job, want in zip(cases, bufs, jobs, outs):
         assert job.status == 0
         single = roift.make_params(c.shape, adjacency=6, weight_mode="grad_q", wq=4095,
