@@ -620,13 +620,11 @@ def main():
               "relax_active_fraction": active_per_sweep / N,
               "oift_levels": stats[0].levels, "oift_tile_steps": stats[0].tile_steps,
               "oift_warp_cycles": list(stats[-1].oift_cycles),
-              "oift_tiles_stale_sparse_dense": list(stats[-1].oift_cycles)[7:10],
-              "oift_cycles_stage_sparse_dense": list(stats[-1].oift_cycles)[4:7],
-              "oift_dense_cycles_masks_flood_iters_expand_faces_pending":
+              "oift_cycles_levelwait_owner_busy_drain": list(stats[-1].oift_cycles)[0:4],
+              "oift_tiles_stale_sparse_bit": list(stats[-1].oift_cycles)[7:10],
+              "oift_cycles_stage_sparse_bit": list(stats[-1].oift_cycles)[4:7],
+              "oift_bit_cycles_closure_layers_maskrows_expand_voxels_tail":
                   list(stats[-1].oift_cycles)[10:16],
-              "oift_sparse_cycles_worklist_rounds_push_publish_pending":
-                  list(stats[-1].oift_cycles)[16:21],
-              "oift_sparse_rounds_voxels_publications": list(stats[-1].oift_cycles)[21:24],
               "oift_gbs": oift_bytes / (ms_oiftk * 1e-3) / 1e9,
               "relax_sweep_gbs": relax_bytes / (ms_sweep * 1e-3) / 1e9}
 

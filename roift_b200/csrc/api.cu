@@ -622,7 +622,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     TRY(grow(c, c->key, N * sizeof(uint32_t)));
     TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
     const int octas = std::max((c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms,
-                               std::min(c->sms, oift_min_ctas(plan.ntiles)));
+                               std::min(c->sms, oift_min_ctas(plan)));
     TRY(grow(c, c->queue, oift_mbox_bytes(plan, octas)));
     TRY(grow(c, c->glob, oift_globals_bytes()));
     TRY(grow(c, c->flag, 4 * sizeof(int)));
@@ -1868,7 +1868,7 @@ static int batch_max_teams(const oift_b200_ctx *c, const oift_b200_job *jobs, in
         const oift_b200_job &jb = jobs[j];
         if (jb.xsize <= 0 || jb.ysize <= 0 || jb.zsize <= 0) continue;
         const OiftPlan P = oift_plan(jb.xsize, jb.ysize, jb.zsize, tile_ty);
-        need = std::max(need, oift_min_ctas(P.ntiles));
+        need = std::max(need, oift_min_ctas(P));
     }
     return std::max(1, c->sms / need);
 }

@@ -42,10 +42,11 @@ struct RelaxArgs {
 // Hot scheduling counters of the persistent OIFT kernel, one 128-byte line each so
 // that polling one does not serialise atomics on another.
 struct OiftGlobals {
-    unsigned int nextmin[2];
-    unsigned int pad0[30];
-    int outstanding[2];
-    unsigned int pad1[30];
+    unsigned int first;          // smallest pending key before the first level
+    unsigned int runmin[3];      // level e: smallest key left pending above it (slot e % 3)
+    unsigned int pad0[28];
+    int outstanding[3];          // level e: tiles wanted, running or announced (slot e % 3)
+    unsigned int pad1[29];
     unsigned int bar_count;
     unsigned int pad2[31];
     unsigned int bar_gen;
@@ -84,7 +85,7 @@ struct OiftPlan {
 struct OiftScratch {
     uint32_t *key;                // [N]
     uint32_t *tpend;              // [ntiles]
-    unsigned long long *mbox;     // [warps][words] re-activation bitmasks
+    unsigned long long *mbox;     // [3][ctas][words] re-activation bitmasks, per level slot
     OiftGlobals *g;
     unsigned int *lprof = nullptr;  // optional per-level profile [cap][2]
     int lprof_cap = 0;
@@ -140,7 +141,7 @@ size_t oift_globals_bytes();
 int oift_mbox_words(const OiftPlan &P, int ctas);
 size_t oift_mbox_bytes(const OiftPlan &P, int ctas);
 // Fewest CTAs that can own `ntiles` tiles (each CTA's tile sets live in shared memory).
-int oift_min_ctas(int ntiles);
+int oift_min_ctas(const OiftPlan &P);
 // One job (volume + seed set) of the batched OIFT kernel; the device copy is read by
 // the team that draws it and receives the job's status.
 struct OiftTeamJob {

@@ -37,7 +37,7 @@ struct OiftArgs {
     uint32_t *key;
     const uint16_t *W;
     uint32_t *tpend;
-    unsigned long long *mbox;  // [nctas][mbox_words] re-activation bitmasks
+    unsigned long long *mbox;  // [3][nctas][mbox_words] re-activation bitmasks, per level slot
     unsigned int *lprof;       // [lprof_cap][2]: per-level SM cycles and tile steps
     int lprof_cap;
     int mbox_words;
@@ -69,8 +69,19 @@ struct OiftArgs {
     const int *seed_flag;
 };
 
+#ifndef OIFT_WARPS_OVERRIDE
 constexpr int OIFT_WARPS = 16;
+#else
+constexpr int OIFT_WARPS = OIFT_WARPS_OVERRIDE;
+#endif
 constexpr int OIFT_SPARSE_MAX = 64;   // level voxels in a tile up to which it runs sparse
+// Worklist rounds of a tile step before a flood that still runs finishes in bit mode.  With
+// 0 (the default) every tile step floods in bit mode: the critical path of a level is its
+// chain of flood layers, and a bit-mode layer costs a few row-mask operations where a
+// worklist round costs a round of shared-memory traffic (256^3 ellipsoid: 45.8 -> 38.7 ms).
+#ifndef OIFT_BIT_AFTER
+#define OIFT_BIT_AFTER 0
+#endif
 constexpr int OIFT_WORKLIST = 256;    // per-warp voxel worklist of the sparse mode
 
 __device__ __forceinline__ unsigned int vload(const volatile unsigned int *p) { return *p; }
@@ -79,6 +90,21 @@ __device__ __forceinline__ unsigned long long vload(const volatile unsigned long
     return *p;
 }
 
+#ifndef OIFT_PROBE
+#define OIFT_PROBE 0
+#endif
+#if OIFT_PROBE
+// latency probes (globaltimer ns): [0,1] publish -> claim, [2,3] claim -> first publish,
+// [4,5] claim -> end of step
+__device__ unsigned long long g_probe[8];
+__device__ unsigned long long g_hist[3][32];  // log2(ns) histograms of the three latencies
+__device__ unsigned long long g_tpub[1 << 20];
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+#endif
 // Release / acquire fence at GPU scope: orders this warp's earlier memory operations (and
 // those of the lanes synchronised with it) before its later ones, without the total order
 // of a sequentially consistent fence.
@@ -168,6 +194,33 @@ __device__ __forceinline__ int tile_of(const OiftArgs &A, int x, int y, int z) {
     return (x >> 5) + (y / TY) * A.ntx + (z / TZ) * A.ntx * A.nty;
 }
 
+// Publishes the re-activations of a tile step; lane i names the tile it re-activates in
+// tq (-1: none).  Tile tq belongs to CTA tq % nctas, bit tq / nctas of its mailbox for the
+// level's slot `par` (a CTA still finishing the level before reads only that one's).  The
+// level's outstanding count is raised first and the warp's key updates are released
+// before the mailbox bits; a tile already marked gives its count back.
+__device__ __forceinline__ void publish_reactivations(const OiftArgs &A, int par, int tq) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint32_t act = __ballot_sync(FULL, tq >= 0);
+#if OIFT_PROBE
+    if (tq >= 0) g_tpub[tq] = gtimer();
+#endif
+    if (lane == 0) atomicAdd(&A.g->outstanding[par], __popc(act));
+    // every lane's key updates and the raised count precede the mailbox bits
+    fence_acq_rel_gpu();
+    __syncwarp();
+    bool dup = false;
+    if (tq >= 0) {
+        const int w = tq % A.nctas, j = tq / A.nctas;
+        const unsigned long long bit = 1ull << (j & 63);
+        dup = (atomicOr(&A.mbox[((size_t)par * A.nctas + w) * A.mbox_words + (j >> 6)], bit) &
+               bit) != 0ull;
+    }
+    const uint32_t dups = __ballot_sync(FULL, dup);
+    if (lane == 0 && dups) atomicSub(&A.g->outstanding[par], __popc(dups));
+}
+
 // Process one tile at level kk (cost c, label l).  All 32 lanes of the warp call it.
 template <int TY, int TZ>
 __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
@@ -183,8 +236,19 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
     const int x0 = tx * 32, y0 = ty * TY, z0 = tz * TZ;
     const int x = x0 + lane;
     const bool has_z = (Z > 1);
+#if OIFT_PROBE
+    const unsigned long long probe_t0 = gtimer();
+    bool probe_pub = false;
+    if (lane == 0) {
+        const unsigned long long tp = atomicExch(&g_tpub[t], 0ull);
+        if (tp && probe_t0 > tp) {
+            atomicAdd(&g_probe[0], probe_t0 - tp);
+            atomicAdd(&g_probe[1], 1ull);
+            atomicAdd(&g_hist[0][63 - __clzll(probe_t0 - tp)], 1ull);
+        }
+    }
+#endif
 
-    uint32_t myF = 0, myOpen = 0, cpx = 0, cmx = 0, cpy = 0, cmy = 0, cpz = 0, cmz = 0;
     const uint32_t kexp = kk - 1u;
     const uint32_t lab_bits = ((uint32_t)l << 1) | 1u;
     auto arc_key = [&](uint32_t code, bool tail_low) -> uint32_t {
@@ -206,6 +270,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
                 atomicOr(rmask, 1u << face);
             } else {
                 atomicMin(&A.tpend[tile_of<TY, TZ>(A, qx, qy, qz)], nk);
+                atomicMin(&A.g->runmin[par], nk);
             }
         }
     };
@@ -214,27 +279,26 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         const uint32_t m = *(volatile uint32_t *)rmask;
         if (m == 0u) return;
         __syncwarp();
-        if (lane == 0) {
-            *rmask = 0u;
-            atomicAdd(&A.g->outstanding[par], __popc(m));
-        }
-        // every lane's key updates and the raised count precede the mailbox bits
-        fence_acq_rel_gpu();
-        __syncwarp();
-        bool dup = false;
+        if (lane == 0) *rmask = 0u;
+        int tq = -1;
         if (lane < 6 && ((m >> lane) & 1u)) {
             const int nt = tx + (lane == 0 ? -1 : lane == 1 ? 1 : 0);
             const int ny = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
             const int nz = tz + (lane == 4 ? -1 : lane == 5 ? 1 : 0);
-            const int tq = nt + ny * A.ntx + nz * A.ntx * A.nty;
-            const int w = tq % A.nctas, j = tq / A.nctas;
-            const unsigned long long bit = 1ull << (j & 63);
-            const unsigned long long old =
-                atomicOr(&A.mbox[(size_t)w * A.mbox_words + (j >> 6)], bit);
-            dup = (old & bit) != 0ull;
+            tq = nt + ny * A.ntx + nz * A.ntx * A.nty;
         }
-        const uint32_t dups = __ballot_sync(FULL, dup);
-        if (lane == 0 && dups) atomicSub(&A.g->outstanding[par], __popc(dups));
+        publish_reactivations(A, par, tq);
+#if OIFT_PROBE
+        {
+            const unsigned long long now = gtimer();
+            if (lane == 0 && !probe_pub) {
+                atomicAdd(&g_probe[2], now - probe_t0);
+                atomicAdd(&g_probe[3], 1ull);
+                atomicAdd(&g_hist[1][63 - __clzll(now - probe_t0 + 1)], 1ull);
+            }
+            probe_pub = true;
+        }
+#endif
     };
     auto pending = [&]() {
         uint32_t m = OIFT_KEY_INF;
@@ -250,7 +314,10 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             uint32_t v = __shfl_xor_sync(FULL, m, o);
             m = v < m ? v : m;
         }
-        if (lane == 0 && m != OIFT_KEY_INF) atomicMin(&A.tpend[t], m);
+        if (lane == 0 && m != OIFT_KEY_INF) {
+            atomicMin(&A.tpend[t], m);
+            atomicMin(&A.g->runmin[par], m);
+        }
     };
     // ---- stage keys, edge codes and the -x/-y/-z halo codes in shared memory ----
     // shx holds the -x halo as 32-bit pairs (codes of x0-2, x0-1): entry 2r+1 is row r's.
@@ -376,13 +443,95 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         cyc[3] += 1;
         return;
     }
-    bool dense = nf0 > OIFT_SPARSE_MAX;
-    if (!dense) {
+    // Sparse rounds first: a voxel worklist expands up to 32 voxels per round.  A flood
+    // that is still running after OIFT_BIT_AFTER rounds (or that starts with more than
+    // OIFT_SPARSE_MAX level voxels) finishes in bit mode: the closure of the level inside
+    // the tile advances one layer per step of row-mask operations, then every voxel it
+    // reached is expanded from a compacted worklist.
+    // Pushes across the tile faces from the expanded voxels wl[0, n), all lanes at once:
+    // the global atomics of a batch share one round trip.
+    auto push_out = [&](int n) {
+        for (int base = 0; base < n; base += 32) {
+            const int idx = base + lane;
+            // one slot per axis: a voxel leaves the tile at most once along each axis
+            uint32_t nk[3] = {OIFT_KEY_INF, OIFT_KEY_INF, OIFT_KEY_INF}, old[3] = {0, 0, 0};
+            int qx[3] = {0, 0, 0}, qy[3] = {0, 0, 0}, qz[3] = {0, 0, 0};
+            if (idx < n) {
+                const uint32_t li = wl[idx];
+                const int r = (int)(li >> 5), xl = (int)(li & 31);
+                const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
+                if (xl == 0 && xg > 0) {
+                    nk[0] = arc_key(shx[2 * r + 1], false);
+                    qx[0] = xg - 1; qy[0] = y; qz[0] = z;
+                } else if (xl == 31 && xg + 1 < X) {
+                    nk[0] = arc_key(sw[r * 32 + xl], true);
+                    qx[0] = xg + 1; qy[0] = y; qz[0] = z;
+                }
+                if ((r % TY) == 0 && y > 0) {
+                    nk[1] = arc_key(shy[(r / TY) * 32 + xl], false);
+                    qx[1] = xg; qy[1] = y - 1; qz[1] = z;
+                } else if ((r % TY) == TY - 1 && y + 1 < Y) {
+                    nk[1] = arc_key(sw[1024 + r * 32 + xl], true);
+                    qx[1] = xg; qy[1] = y + 1; qz[1] = z;
+                }
+                if (has_z) {
+                    if (r < TY && z > 0) {
+                        nk[2] = arc_key(TZ > 1 ? shz[(r % TY) * 32 + xl] : 0u, false);
+                        qx[2] = xg; qy[2] = y; qz[2] = z - 1;
+                    } else if (r + TY >= 32 && z + 1 < Z) {
+                        nk[2] = arc_key(sw[2048 + r * 32 + xl], true);
+                        qx[2] = xg; qy[2] = y; qz[2] = z + 1;
+                    }
+                }
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+                    if (nk[a] != OIFT_KEY_INF)
+                        old[a] = atomicMin(&A.key[(size_t)qx[a] + (size_t)qy[a] * X +
+                                                  (size_t)qz[a] * XY], nk[a]);
+            }
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+                if (nk[a] != OIFT_KEY_INF) settle(nk[a], old[a], qx[a], qy[a], qz[a]);
+        }
+    };
+    // The six arcs of worklist voxel li: in-tile head, its slot, the edge code and whether
+    // the tail is the voxel that stores the edge.
+    struct Arcs {
+        bool in[6];
+        int lq[6];
+        uint32_t code[6];
+    };
+    auto arcs_of = [&](uint32_t li, Arcs &a) {
+        const int r = (int)(li >> 5), xl = (int)(li & 31);
+        const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
+        a.in[0] = r >= TY;                              // -z
+        a.lq[0] = li - 32 * TY;
+        a.in[1] = (r % TY) > 0;                         // -y
+        a.lq[1] = li - 32;
+        a.in[2] = xl > 0;                               // -x
+        a.lq[2] = li - 1;
+        a.in[3] = xl < 31 && xg + 1 < X;                // +x
+        a.lq[3] = li + 1;
+        a.in[4] = (r % TY) < TY - 1 && y + 1 < Y;       // +y
+        a.lq[4] = li + 32;
+        a.in[5] = r + TY < 32 && has_z && z + 1 < Z;    // +z
+        a.lq[5] = li + 32 * TY;
+        a.code[0] = a.in[0] ? sw[2048 + a.lq[0]] : 0u;
+        a.code[1] = a.in[1] ? sw[1024 + a.lq[1]] : 0u;
+        a.code[2] = a.in[2] ? sw[a.lq[2]] : 0u;
+        a.code[3] = sw[li];
+        a.code[4] = sw[1024 + li];
+        a.code[5] = sw[2048 + li];
+    };
+    const bool tail_low[6] = {false, false, false, true, true, true};
+    int done = 0, cnt = 0, rounds = 0;
+    bool bitmode = OIFT_BIT_AFTER == 0 || nf0 > OIFT_SPARSE_MAX;
+    if (!bitmode) {
         // ---- sparse mode: flood and expand from a voxel worklist ----
         // append_rows(m, base): the voxels of row `lane` in m join the worklist after `base`
         // entries (a warp prefix sum places them) and are marked at this level; returns the
-        // new count.  Entries past OIFT_WORKLIST are not stored: the caller switches to the
-        // dense path, which finds them through their key.
+        // new count.  Entries past OIFT_WORKLIST are not stored: bit mode then finds them
+        // through their key.
         auto append_rows = [&](uint32_t m, int base) -> int {
             const int n = __popc(m);
             int incl = n;
@@ -405,116 +554,47 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         };
         const long long ts0 = clock64();
         nfm[lane] = 0u;
-        int cnt = append_rows(rowF, 0);
+        cnt = append_rows(rowF, 0);
         __syncwarp();
-        // Pushes across the tile faces from the expanded voxels wl[0, n), all lanes at once:
-        // the flood rounds stay in shared memory and the global atomics of the tile step
-        // share one round trip.
-        auto push_out = [&](int n) {
-            for (int base = 0; base < n; base += 32) {
-                const int idx = base + lane;
-                // one slot per axis: a voxel leaves the tile at most once along each axis
-                uint32_t nk[3] = {OIFT_KEY_INF, OIFT_KEY_INF, OIFT_KEY_INF}, old[3] = {0, 0, 0};
-                int qx[3] = {0, 0, 0}, qy[3] = {0, 0, 0}, qz[3] = {0, 0, 0};
-                if (idx < n) {
-                    const uint32_t li = wl[idx];
-                    const int r = (int)(li >> 5), xl = (int)(li & 31);
-                    const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
-                    if (xl == 0 && xg > 0) {
-                        nk[0] = arc_key(shx[2 * r + 1], false);
-                        qx[0] = xg - 1; qy[0] = y; qz[0] = z;
-                    } else if (xl == 31 && xg + 1 < X) {
-                        nk[0] = arc_key(sw[r * 32 + xl], true);
-                        qx[0] = xg + 1; qy[0] = y; qz[0] = z;
-                    }
-                    if ((r % TY) == 0 && y > 0) {
-                        nk[1] = arc_key(shy[(r / TY) * 32 + xl], false);
-                        qx[1] = xg; qy[1] = y - 1; qz[1] = z;
-                    } else if ((r % TY) == TY - 1 && y + 1 < Y) {
-                        nk[1] = arc_key(sw[1024 + r * 32 + xl], true);
-                        qx[1] = xg; qy[1] = y + 1; qz[1] = z;
-                    }
-                    if (has_z) {
-                        if (r < TY && z > 0) {
-                            nk[2] = arc_key(TZ > 1 ? shz[(r % TY) * 32 + xl] : 0u, false);
-                            qx[2] = xg; qy[2] = y; qz[2] = z - 1;
-                        } else if (r + TY >= 32 && z + 1 < Z) {
-                            nk[2] = arc_key(sw[2048 + r * 32 + xl], true);
-                            qx[2] = xg; qy[2] = y; qz[2] = z + 1;
-                        }
-                    }
-#pragma unroll
-                    for (int a = 0; a < 3; a++)
-                        if (nk[a] != OIFT_KEY_INF)
-                            old[a] = atomicMin(&A.key[(size_t)qx[a] + (size_t)qy[a] * X +
-                                                      (size_t)qz[a] * XY], nk[a]);
-                }
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-                    if (nk[a] != OIFT_KEY_INF) settle(nk[a], old[a], qx[a], qy[a], qz[a]);
-            }
-        };
-        int done = 0, rounds = 0;
         const long long ts1 = clock64();
         cyc[12] += ts1 - ts0;
         for (;;) {
-            if (cnt > OIFT_WORKLIST) {  // overflow: the dense path finishes the level
-                push_out(done);
-                dense = true;
+            if (done >= cnt) break;
+            if (cnt > OIFT_WORKLIST || rounds >= OIFT_BIT_AFTER) {
+                bitmode = true;
                 break;
             }
-            if (done >= cnt) break;
             // ---- one flood round: expand up to 32 worklist voxels, one per lane; open arcs
             // mark their in-tile heads in nfm, other arcs lower the heads' keys ----
             const int idx = done + lane;
             if (idx < cnt) {
                 const uint32_t li = wl[idx];
                 const int r = (int)(li >> 5), xl = (int)(li & 31);
-                const int xg = x0 + xl, y = y0 + (r % TY), z = z0 + (r / TY);
-                const size_t p = (size_t)xg + (size_t)y * X + (size_t)z * XY;
-                // the six arcs: in-tile head, its slot, the edge code and which side stores
-                // it; every head key is read before any update (keys only decrease, so an
-                // early read costs at most a redundant push)
-                bool in[6];
-                int lq[6];
-                uint32_t code[6], sk[6];
-                const bool tail_low[6] = {false, false, false, true, true, true};
-                in[0] = r >= TY;                              // -z
-                lq[0] = li - 32 * TY;
-                in[1] = (r % TY) > 0;                         // -y
-                lq[1] = li - 32;
-                in[2] = xl > 0;                               // -x
-                lq[2] = li - 1;
-                in[3] = xl < 31 && xg + 1 < X;                // +x
-                lq[3] = li + 1;
-                in[4] = (r % TY) < TY - 1 && y + 1 < Y;       // +y
-                lq[4] = li + 32;
-                in[5] = r + TY < 32 && has_z && z + 1 < Z;    // +z
-                lq[5] = li + 32 * TY;
-                code[0] = in[0] ? sw[2048 + lq[0]] : 0u;
-                code[1] = in[1] ? sw[1024 + lq[1]] : 0u;
-                code[2] = in[2] ? sw[lq[2]] : 0u;
-                code[3] = sw[li];
-                code[4] = sw[1024 + li];
-                code[5] = sw[2048 + li];
+                const size_t p = (size_t)(x0 + xl) + (size_t)(y0 + (r % TY)) * X +
+                                 (size_t)(z0 + (r / TY)) * XY;
+                // every head key is read before any update (keys only decrease, so an early
+                // read costs at most a redundant push)
+                Arcs a;
+                arcs_of(li, a);
+                uint32_t sk[6];
 #pragma unroll
-                for (int d = 0; d < 6; d++) sk[d] = in[d] ? skey[lq[d]] : 0u;
+                for (int d = 0; d < 6; d++) sk[d] = a.in[d] ? skey[a.lq[d]] : 0u;
                 A.key[p] = kexp;
                 skey[li] = kexp;
                 uint32_t same_row = 0u;  // open x-neighbours, marked with one update
 #pragma unroll
                 for (int d = 0; d < 6; d++) {
-                    if (!in[d] || sk[d] <= kk) continue;  // across a face, at this level, or expanded
-                    const int rq = lq[d] >> 5, xq = lq[d] & 31;
-                    if (arc_ok(code[d], tail_low[d], c, bgt, blt)) {
+                    if (!a.in[d] || sk[d] <= kk) continue;  // across a face, at this level, or expanded
+                    const int rq = a.lq[d] >> 5, xq = a.lq[d] & 31;
+                    if (arc_ok(a.code[d], tail_low[d], c, bgt, blt)) {
                         if (rq == r)
                             same_row |= 1u << xq;
                         else
                             atomicOr(&nfm[rq], 1u << xq);
                     } else {
-                        const uint32_t nk = arc_key(code[d], tail_low[d]);
+                        const uint32_t nk = arc_key(a.code[d], tail_low[d]);
                         if (nk < sk[d]) {
-                            atomicMin(&skey[lq[d]], nk);
+                            atomicMin(&skey[a.lq[d]], nk);
                             atomicMin(&A.key[(size_t)(x0 + xq) + (size_t)(y0 + rq % TY) * X +
                                              (size_t)(z0 + rq / TY) * XY], nk);
                         }
@@ -533,201 +613,244 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             __syncwarp();
         }
         __syncwarp();
-        if (!dense) {
-            const long long ts2 = clock64();
-            push_out(done);
-            __syncwarp();
-            const long long ts3 = clock64();
+        const long long ts2 = clock64();
+        push_out(done < OIFT_WORKLIST ? done : OIFT_WORKLIST);
+        __syncwarp();
+        const long long ts3 = clock64();
+        cyc[13] += ts2 - ts1;
+        cyc[14] += ts3 - ts2;
+        cyc[17] += rounds;
+        cyc[18] += done;
+        if (!bitmode) {
             cyc[19] += (*(volatile uint32_t *)rmask != 0u);
             flush_reactivations();
             const long long ts4 = clock64();
             pending();
             const long long ts5 = clock64();
-            cyc[13] += ts2 - ts1;
-            cyc[14] += ts3 - ts2;
             cyc[15] += ts4 - ts3;
             cyc[16] += ts5 - ts4;
-            cyc[17] += rounds;
-            cyc[18] += done;
             cyc[1] += ts5 - tcount;
             cyc[4] += 1;
             return;
         }
     }
-    long long td0 = clock64();
-    // ---- level masks (one ballot per row and arc family) ----
-#pragma unroll 4
-    for (int r = 0; r < 32; r++) {
-        const int y = y0 + (r % TY), z = z0 + (r / TY);
-        const bool valid = (x < X) && (y < Y) && (z < Z);
-        const uint32_t k = skey[r * 32 + lane];
-        const uint32_t cx = sw[r * 32 + lane];
-        const uint32_t cy = sw[1024 + r * 32 + lane];
-        const uint32_t cz = sw[2048 + r * 32 + lane];
-        const uint32_t bF = __ballot_sync(FULL, valid && k == kk);
-        const uint32_t bO = __ballot_sync(FULL, valid && k > kk);
-        const uint32_t cxm1 = __shfl_up_sync(FULL, cx, 1);
-        const uint32_t bPX = __ballot_sync(FULL, lane > 0 && arc_ok(cxm1, true, c, bgt, blt));
-        const uint32_t bMX = __ballot_sync(FULL, lane < 31 && arc_ok(cx, false, c, bgt, blt));
-        const uint32_t bFY = __ballot_sync(FULL, arc_ok(cy, true, c, bgt, blt));
-        const uint32_t bBY = __ballot_sync(FULL, arc_ok(cy, false, c, bgt, blt));
-        const uint32_t bFZ = __ballot_sync(FULL, arc_ok(cz, true, c, bgt, blt));
-        const uint32_t bBZ = __ballot_sync(FULL, arc_ok(cz, false, c, bgt, blt));
-        if (lane == r) {
-            myF = bF;
-            myOpen = bO;
-            cpx = bPX;
-            cmx = bMX;
-            cmy = ((r % TY) < TY - 1) ? bBY : 0u;
-            cmz = (r + TY < 32) ? bBZ : 0u;
-        }
-        if (lane == r + 1 && ((r % TY) < TY - 1)) cpy = bFY;
-        if (TZ > 1 && lane == r + TY) cpz = bFZ;
-    }
-    long long td1 = clock64();
-    cyc[6] += td1 - td0;
-    // ---- flood of the level inside the tile ----
-    const bool ylo = (lane % TY) != 0, yhi = (lane % TY) != TY - 1;
-    const bool zlo = lane >= TY, zhi = lane + TY < 32;
-    uint32_t F = myF;
-    int flood_it = 0;
-    for (int it = 0; it < 2048; it++) {
-        flood_it++;
-        uint32_t fym = __shfl_up_sync(FULL, F, 1);
-        uint32_t fyp = __shfl_down_sync(FULL, F, 1);
-        uint32_t fzm = __shfl_up_sync(FULL, F, TY);
-        uint32_t fzp = __shfl_down_sync(FULL, F, TY);
-        uint32_t grow = ((F << 1) & cpx) | ((F >> 1) & cmx) | (ylo ? (fym & cpy) : 0u) |
-                        (yhi ? (fyp & cmy) : 0u) | (zlo ? (fzm & cpz) : 0u) |
-                        (zhi ? (fzp & cmz) : 0u);
-        uint32_t nF = F | (grow & myOpen);
-        if (!__any_sync(FULL, nF != F)) break;
-        F = nF;
-    }
-    __syncwarp();
-    long long td2 = clock64();
-    cyc[7] += td2 - td1;
-    cyc[8] += flood_it;
-    // ---- pass 2a: mark the voxels conquered at this level as expanded and give every open
-    // in-tile voxel outside the flood the best key offered by its flooded neighbours
-    // ("pull": one lane per target, one global update per improved target) ----
-    const uint32_t targets = myOpen & ~F;
-    for (int r = 0; r < 32; r++) {
-        const uint32_t fr = __shfl_sync(FULL, F, r);
-        const uint32_t tr = __shfl_sync(FULL, targets, r);
-        if ((fr | tr) == 0u) continue;
-        const int y = y0 + (r % TY), z = z0 + (r / TY);
-        const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
-        if ((fr >> lane) & 1u) {
-            A.key[p] = kexp;
-            skey[r * 32 + lane] = kexp;
-        }
-        if (tr == 0u) continue;
-        const bool hasm_z = r >= TY, hasp_z = r + TY < 32;
-        const bool hasm_y = (r % TY) > 0, hasp_y = (r % TY) < TY - 1;
-        const uint32_t f_mz = __shfl_sync(FULL, F, hasm_z ? r - TY : r);
-        const uint32_t f_pz = __shfl_sync(FULL, F, hasp_z ? r + TY : r);
-        const uint32_t f_my = __shfl_sync(FULL, F, hasm_y ? r - 1 : r);
-        const uint32_t f_py = __shfl_sync(FULL, F, hasp_y ? r + 1 : r);
-        if ((tr >> lane) & 1u) {
-            uint32_t best = OIFT_KEY_INF;
-            if (hasm_z && ((f_mz >> lane) & 1u))
-                best = min(best, arc_key(sw[2048 + (r - TY) * 32 + lane], true));
-            if (hasm_y && ((f_my >> lane) & 1u))
-                best = min(best, arc_key(sw[1024 + (r - 1) * 32 + lane], true));
-            if (lane > 0 && ((fr >> (lane - 1)) & 1u))
-                best = min(best, arc_key(sw[r * 32 + lane - 1], true));
-            if (lane < 31 && ((fr >> (lane + 1)) & 1u))
-                best = min(best, arc_key(sw[r * 32 + lane], false));
-            if (hasp_y && ((f_py >> lane) & 1u))
-                best = min(best, arc_key(sw[1024 + r * 32 + lane], false));
-            if (hasp_z && ((f_pz >> lane) & 1u))
-                best = min(best, arc_key(sw[2048 + r * 32 + lane], false));
-            if (best < skey[r * 32 + lane]) {
-                skey[r * 32 + lane] = best;
-                atomicMin(&A.key[p], best);
+    // ---- bit mode ----
+    const long long tb0 = clock64();
+    // lane r: row r's flooded voxels not yet expanded (P) and its open voxels (Om: key above
+    // the level, neither final nor flooded at this level).  Straight from the level rows
+    // when no sparse round ran; rebuilt from the keys otherwise.
+    uint32_t P, Om;
+    if (done == 0 && cnt <= OIFT_WORKLIST) {
+        P = rowF;
+        Om = ~rowV;  // positions outside the volume were staged as key 0 (at or below)
+    } else {
+        P = 0u;
+        Om = 0u;
+#pragma unroll 8
+        for (int r = 0; r < 32; r++) {
+            const uint32_t k = skey[r * 32 + lane];
+            const uint32_t bP = __ballot_sync(FULL, k == kk);
+            const uint32_t bO = __ballot_sync(FULL, k > kk);
+            if (lane == r) {
+                P = bP;
+                Om = bO;
             }
         }
     }
-    long long td3 = clock64();
-    cyc[9] += td3 - td2;
-    // ---- pass 2b: out-of-tile targets, face by face; the atomics of a face are all
-    // issued before their results are examined ----
-    {   // -x / +x faces: lane = row
-        const int y = y0 + (lane % TY), z = z0 + (lane / TY);
-        const size_t prow = (size_t)y * X + (size_t)z * XY;
-        const bool mx = (F & 1u) && x0 > 0;
-        const bool px = ((F >> 31) & 1u) && x0 + 32 < X;
-        uint32_t nkm = OIFT_KEY_INF, nkp = OIFT_KEY_INF, om = 0, op = 0;
-        if (mx) {
-            nkm = arc_key(shx[2 * lane + 1], false);
-            om = atomicMin(&A.key[prow + x0 - 1], nkm);
-        }
-        if (px) {
-            nkp = arc_key(sw[lane * 32 + 31], true);
-            op = atomicMin(&A.key[prow + x0 + 32], nkp);
-        }
-        if (mx) settle(nkm, om, x0 - 1, y, z);
-        if (px) settle(nkp, op, x0 + 32, y, z);
-    }
-    {   // -y / +y faces: rows r % TY == 0 and TY - 1, lane = x
-        uint32_t nk[2 * TZ], old[2 * TZ];
-#pragma unroll
-        for (int i = 0; i < 2 * TZ; i++) {
-            const int zl = i >> 1, up = i & 1;
-            const int r = zl * TY + (up ? TY - 1 : 0);
-            const int y = y0 + (up ? TY - 1 : 0), z = z0 + zl;
-            const bool on = ((__shfl_sync(FULL, F, r) >> lane) & 1u) &&
-                            (up ? (y + 1 < Y) : (y0 > 0));
-            nk[i] = OIFT_KEY_INF;
-            old[i] = 0;
-            if (on) {
-                const size_t q = (size_t)x + (size_t)(up ? y + 1 : y - 1) * X + (size_t)z * XY;
-                nk[i] = up ? arc_key(sw[1024 + r * 32 + lane], true)
-                           : arc_key(shy[zl * 32 + lane], false);
-                old[i] = atomicMin(&A.key[q], nk[i]);
+    // rows that have a y neighbour row inside the tile below / above them
+    constexpr uint32_t ROWS_YM = []() constexpr {
+        uint32_t m = 0;
+        for (int r = 0; r < 32; r++) if (r % TY != 0) m |= 1u << r;
+        return m;
+    }();
+    constexpr uint32_t ROWS_YP = []() constexpr {
+        uint32_t m = 0;
+        for (int r = 0; r < 32; r++) if (r % TY != TY - 1) m |= 1u << r;
+        return m;
+    }();
+    // Closure of the level inside the tile.  Lane r keeps the pull masks of row r: bit x of
+    // Mpx is "the arc (x-1 -> x) is open at this level", Mmx (x+1 -> x), Mym / Myp from the
+    // rows y-1 / y+1, Mzm / Mzp from z-1 / z+1.  A family of masks of a row is computed the
+    // first time the frontier reaches the row's neighbour on that side while the row still
+    // has open voxels: one ballot with lane = x.
+    uint32_t Fm = P, fr = P;
+    uint32_t Mpx = 0u, Mmx = 0u, Mym = 0u, Myp = 0u, Mzm = 0u, Mzp = 0u;
+    uint32_t rx = 0u, rym = 0u, ryp = 0u, rzm = 0u, rzp = 0u;  // families computed, per row
+    int biters = 0, mrows = 0;
+    for (;;) {
+        const uint32_t frows = __ballot_sync(FULL, fr != 0u);
+        const uint32_t orows = __ballot_sync(FULL, (Om & ~Fm) != 0u);
+        uint32_t need = frows & orows & ~rx;
+        rx |= need;
+        while (need) {
+            const int q = __ffs(need) - 1;
+            need &= need - 1;
+            mrows++;
+            const uint32_t c0 = sw[q * 32 + lane];
+            const uint32_t c0m = __shfl_up_sync(FULL, c0, 1);
+            const uint32_t bPX = __ballot_sync(FULL, lane > 0 && arc_ok(c0m, true, c, bgt, blt));
+            const uint32_t bMX = __ballot_sync(FULL, lane < 31 && arc_ok(c0, false, c, bgt, blt));
+            if (lane == q) {
+                Mpx = bPX;
+                Mmx = bMX;
             }
         }
-#pragma unroll
-        for (int i = 0; i < 2 * TZ; i++) {
-            const int zl = i >> 1, up = i & 1;
-            if (nk[i] != OIFT_KEY_INF)
-                settle(nk[i], old[i], x, up ? y0 + TY : y0 - 1, z0 + zl);
+        need = (frows << 1) & ROWS_YM & orows & ~rym;
+        rym |= need;
+        while (need) {
+            const int q = __ffs(need) - 1;
+            need &= need - 1;
+            mrows++;
+            const uint32_t b = __ballot_sync(FULL, arc_ok(sw[1024 + (q - 1) * 32 + lane], true, c, bgt, blt));
+            if (lane == q) Mym = b;
         }
-    }
-    if (TZ > 1 && has_z) {   // -z / +z faces: rows r < TY and r >= 32 - TY, lane = x
-        uint32_t nk[2 * TY], old[2 * TY];
-#pragma unroll
-        for (int i = 0; i < 2 * TY; i++) {
-            const int yl = i >> 1, up = i & 1;
-            const int r = up ? (32 - TY + yl) : yl;
-            const int y = y0 + yl, z = up ? z0 + TZ - 1 : z0;
-            const bool on = ((__shfl_sync(FULL, F, r) >> lane) & 1u) &&
-                            (up ? (z + 1 < Z) : (z0 > 0));
-            nk[i] = OIFT_KEY_INF;
-            old[i] = 0;
-            if (on) {
-                const size_t q = (size_t)x + (size_t)y * X + (size_t)(up ? z + 1 : z - 1) * XY;
-                nk[i] = up ? arc_key(sw[2048 + r * 32 + lane], true)
-                           : arc_key(shz[yl * 32 + lane], false);
-                old[i] = atomicMin(&A.key[q], nk[i]);
+        need = (frows >> 1) & ROWS_YP & orows & ~ryp;
+        ryp |= need;
+        while (need) {
+            const int q = __ffs(need) - 1;
+            need &= need - 1;
+            mrows++;
+            const uint32_t b = __ballot_sync(FULL, arc_ok(sw[1024 + q * 32 + lane], false, c, bgt, blt));
+            if (lane == q) Myp = b;
+        }
+        if constexpr (TZ > 1) {
+            need = (frows << TY) & orows & ~rzm;
+            rzm |= need;
+            while (need) {
+                const int q = __ffs(need) - 1;
+                need &= need - 1;
+                mrows++;
+                const uint32_t b = __ballot_sync(FULL, arc_ok(sw[2048 + (q - TY) * 32 + lane], true, c, bgt, blt));
+                if (lane == q) Mzm = b;
+            }
+            need = (frows >> TY) & orows & ~rzp;
+            rzp |= need;
+            while (need) {
+                const int q = __ffs(need) - 1;
+                need &= need - 1;
+                mrows++;
+                const uint32_t b = __ballot_sync(FULL, arc_ok(sw[2048 + q * 32 + lane], false, c, bgt, blt));
+                if (lane == q) Mzp = b;
             }
         }
-#pragma unroll
-        for (int i = 0; i < 2 * TY; i++) {
-            const int yl = i >> 1, up = i & 1;
-            if (nk[i] != OIFT_KEY_INF)
-                settle(nk[i], old[i], x, y0 + yl, up ? z0 + TZ : z0 - 1);
-        }
+        // one layer: the open, unflooded voxels next to the frontier through an open arc
+        uint32_t g = ((fr << 1) & Mpx) | ((fr >> 1) & Mmx) |
+                     (__shfl_up_sync(FULL, fr, 1) & Mym) | (__shfl_down_sync(FULL, fr, 1) & Myp);
+        if constexpr (TZ > 1)
+            g |= (__shfl_up_sync(FULL, fr, TY) & Mzm) | (__shfl_down_sync(FULL, fr, TY) & Mzp);
+        g &= Om & ~Fm;
+        biters++;
+        if (!__any_sync(FULL, g != 0u)) break;
+        Fm |= g;
+        fr = g;
     }
-    __syncwarp();
-    long long td4 = clock64();
-    cyc[10] += td4 - td3;
-    // ---- pass 3: publish re-activations, pending key of this tile ----
-    flush_reactivations();
+    const long long tb1 = clock64();
+    // ---- expansion of the closure.  The voxels on the tile's faces go first: they are
+    // expanded in global memory, their arcs across the faces are pushed and the tile's
+    // same-level crossings are published, so that the flood continues next door while this
+    // tile gives its in-tile heads that the closure did not reach the arc's key (the arc is
+    // closed there).  Voxels join the worklist OIFT_WORKLIST at a time ----
+    nfm[lane] = Fm;
+    // compact(m): the voxels of row `lane` in m join the worklist (up to OIFT_WORKLIST in all)
+    // and leave m; returns how many joined
+    auto compact = [&](uint32_t &m) -> int {
+        const int n = __popc(m);
+        int incl = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        int pos = incl - n;
+        while (m && pos < OIFT_WORKLIST) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            wl[pos++] = (uint32_t)(lane << 5 | b);
+        }
+        __syncwarp();
+        return total < OIFT_WORKLIST ? total : OIFT_WORKLIST;
+    };
+    constexpr uint32_t ROWS_FACE = []() constexpr {
+        uint32_t m = 0;
+        for (int r = 0; r < 32; r++)
+            if (r % TY == 0 || r % TY == TY - 1 || (TZ > 1 && (r < TY || r >= 32 - TY))) m |= 1u << r;
+        return m;
+    }();
+    int nexp = 0;
+    {
+        uint32_t frem = Fm & (((ROWS_FACE >> lane) & 1u) ? FULL : 0x80000001u);
+        while (__any_sync(FULL, frem != 0u)) {
+            const int nb = compact(frem);
+            for (int base = 0; base < nb; base += 32) {
+                const int idx = base + lane;
+                if (idx < nb) {
+                    const uint32_t li = wl[idx];
+                    const int r = (int)(li >> 5), xl = (int)(li & 31);
+                    A.key[(size_t)(x0 + xl) + (size_t)(y0 + (r % TY)) * X + (size_t)(z0 + (r / TY)) * XY] = kexp;
+                }
+            }
+            push_out(nb);
+            __syncwarp();
+        }
+        flush_reactivations();
+    }
+    uint32_t rem = Fm;
+    while (__any_sync(FULL, rem != 0u)) {
+        const int nb = compact(rem);
+        nexp += nb;
+        for (int base = 0; base < nb; base += 32) {
+            const int idx = base + lane;
+            if (idx < nb) {
+                const uint32_t li = wl[idx];
+                const int r = (int)(li >> 5), xl = (int)(li & 31);
+                const size_t p = (size_t)(x0 + xl) + (size_t)(y0 + (r % TY)) * X +
+                                 (size_t)(z0 + (r / TY)) * XY;
+                Arcs a;
+                arcs_of(li, a);
+                uint32_t sk[6];
+                bool tgt[6];
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    tgt[d] = a.in[d] && !((nfm[a.lq[d] >> 5] >> (a.lq[d] & 31)) & 1u);
+                    sk[d] = tgt[d] ? skey[a.lq[d]] : 0u;
+                }
+                A.key[p] = kexp;
+                skey[li] = kexp;
+#pragma unroll
+                for (int d = 0; d < 6; d++) {
+                    if (!tgt[d] || sk[d] <= kk) continue;
+                    const uint32_t nk = arc_key(a.code[d], tail_low[d]);
+                    if (nk < sk[d]) {
+                        const int rq = a.lq[d] >> 5, xq = a.lq[d] & 31;
+                        atomicMin(&skey[a.lq[d]], nk);
+                        atomicMin(&A.key[(size_t)(x0 + xq) + (size_t)(y0 + rq % TY) * X +
+                                         (size_t)(z0 + rq / TY) * XY], nk);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    const long long tb2 = clock64();
+    // ---- pending key of this tile ----
     pending();
-    cyc[11] += clock64() - td4;
-    cyc[2] += clock64() - tcount;
+    const long long tb3 = clock64();
+#if OIFT_PROBE
+    if (lane == 0) {
+        const unsigned long long dt = gtimer() - probe_t0;
+        atomicAdd(&g_probe[4], dt);
+        atomicAdd(&g_probe[5], 1ull);
+        atomicAdd(&g_hist[2][63 - __clzll(dt + 1)], 1ull);
+    }
+#endif
+    cyc[6] += tb1 - tb0;
+    cyc[7] += biters;
+    cyc[8] += mrows;
+    cyc[9] += tb2 - tb1;
+    cyc[10] += nexp;
+    cyc[11] += tb3 - tb2;
+    cyc[2] += tb3 - tcount;
     cyc[5] += 1;
 }
 
@@ -829,7 +952,10 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
             uint32_t v = __shfl_xor_sync(FULL, m, o);
             m = v < m ? v : m;
         }
-        if (lane == 0 && m != OIFT_KEY_INF) atomicMin(&A.tpend[t], m);
+        if (lane == 0 && m != OIFT_KEY_INF) {
+            atomicMin(&A.tpend[t], m);
+            atomicMin(&A.g->runmin[par], m);
+        }
     };
     // ---- stage keys and the intensities with a one-voxel halo ----
     const bool full = (x0 + 32 <= X) && (y0 + TY <= Y) && (z0 + TZ <= Z) && ((X & 7) == 0);
@@ -998,6 +1124,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
                 } else {
                     const int tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
                     atomicMin(&A.tpend[tq], nk[j]);
+                    atomicMin(&A.g->runmin[par], nk[j]);
                 }
             }
         }
@@ -1008,25 +1135,13 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
         const uint32_t m = *(volatile uint32_t *)rmask;
         if (m != 0u) {
             __syncwarp();
-            if (lane == 0) {
-                *rmask = 0u;
-                atomicAdd(&A.g->outstanding[par], __popc(m));
-            }
-            // every lane's key updates and the raised count precede the mailbox bits
-            fence_acq_rel_gpu();
-            __syncwarp();
-            bool dup = false;
+            if (lane == 0) *rmask = 0u;
+            int tq = -1;
             if (lane < 27 && ((m >> lane) & 1u)) {
                 const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
-                const int tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
-                const int w = tq % A.nctas, j = tq / A.nctas;
-                const unsigned long long bit = 1ull << (j & 63);
-                const unsigned long long o =
-                    atomicOr(&A.mbox[(size_t)w * A.mbox_words + (j >> 6)], bit);
-                dup = (o & bit) != 0ull;
+                tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
             }
-            const uint32_t dups = __ballot_sync(FULL, dup);
-            if (lane == 0 && dups) atomicSub(&A.g->outstanding[par], __popc(dups));
+            publish_reactivations(A, par, tq);
         }
     }
     __syncwarp();
@@ -1036,6 +1151,8 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     cyc[17] += rounds;
     cyc[18] += cnt;
 }
+
+
 
 // Re-activation bitmask words per CTA when `nctas` CTAs own `ntiles` tiles round-robin.
 __host__ __device__ __forceinline__ int oift_mbox_words_for(int ntiles, int nctas) {
@@ -1092,23 +1209,24 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     uint32_t *wl = cs.wl[warp];
     uint32_t *nfm = cs.nfm[warp];
     OiftGlobals *g = A.g;
-    const int gwarp = team_cta * OIFT_WARPS + warp;
-    const int nwarps = team_ctas * OIFT_WARPS;
     const bool leader_cta = team_cta == 0;
     uint32_t prev_level = 0;
     long long lvl_t0 = 0;
     long long cyc_levelsync = 0, cyc_owner = 0, cyc_busy = 0, cyc_drain = 0;
-    for (int e = 0;; e++) {
-        const int par = e & 1;
-        const long long t_r0 = clock64();
-        // ---- R: global minimum of the pending keys ----
+    // ---- the first level: global minimum of the pending keys, one barrier.  Level e then
+    // counts its outstanding work in g->outstanding[e % 3] and collects every pending key
+    // above it in g->runmin[e % 3], whose value once the count is zero is level e + 1:
+    // each CTA moves on as soon as it sees its level end, with no barrier between levels
+    // (three slots, so a slot is reset only after every CTA has left the level that used
+    // it before) ----
+    {
         uint32_t m = OIFT_KEY_INF;
-        for (int t = gwarp * 32 + lane; t < A.ntiles; t += nwarps * 32) {
-            uint32_t v = __ldcg(&A.tpend[t]);
+        for (int j = threadIdx.x; team_cta + j * team_ctas < A.ntiles; j += blockDim.x) {
+            const uint32_t v = __ldcg(&A.tpend[team_cta + j * team_ctas]);
             m = v < m ? v : m;
         }
         for (int o = 16; o > 0; o >>= 1) {
-            uint32_t v = __shfl_xor_sync(FULL, m, o);
+            const uint32_t v = __shfl_xor_sync(FULL, m, o);
             m = v < m ? v : m;
         }
         if (lane == 0) blk_min[warp] = m;
@@ -1116,13 +1234,22 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         if (threadIdx.x == 0) {
             uint32_t bm = blk_min[0];
             for (int w = 1; w < OIFT_WARPS; w++) bm = blk_min[w] < bm ? blk_min[w] : bm;
-            if (bm != OIFT_KEY_INF) atomicMin(&g->nextmin[par], bm);
+            if (bm != OIFT_KEY_INF) atomicMin(&g->first, bm);
             if (leader_cta) {
-                g->outstanding[par] = team_ctas;  // one token per CTA for its scan
-                g->nextmin[par ^ 1] = OIFT_KEY_INF;
+                g->outstanding[0] = team_ctas;  // one token per CTA for its scan
+                g->runmin[0] = OIFT_KEY_INF;
             }
         }
         team_barrier(g, A.spin_limit, team_ctas);
+        if (threadIdx.x == 0) {
+            cs.level = vload(&g->first);
+            cs.err = vload(&g->error);
+        }
+        __syncthreads();
+    }
+    for (int e = 0;; e++) {
+        const int par = e % 3;
+        const long long t_r0 = clock64();
         if (leader_cta && threadIdx.x == 0 && A.lprof && e > 0 && e - 1 < A.lprof_cap) {
             const long long now = clock64();
             A.lprof[2 * (e - 1)] = (unsigned int)min(now - lvl_t0, 0xffffffffll);
@@ -1130,13 +1257,8 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         } else if (leader_cta && threadIdx.x == 0 && e == 0) {
             lvl_t0 = clock64();
         }
-        // one read of the level and the error flag for the whole CTA: every warp leaves the
-        // loop in the same iteration, so the CTA's barriers stay matched
-        if (threadIdx.x == 0) {
-            cs.level = vload(&g->nextmin[par]);
-            cs.err = vload(&g->error);
-        }
-        __syncthreads();
+        // the level and the error flag were read once for the whole CTA: every warp leaves
+        // the loop in the same iteration, so the CTA's barriers stay matched
         const uint32_t kk = cs.level;
         if (kk == OIFT_KEY_INF || cs.err) break;
         // levels strictly increase; a repeat or a runaway level count is a fault
@@ -1162,36 +1284,59 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             bgt = max_base_for_cost(c, fgt);
             blt = max_base_for_cost(c, flt);
         }
-        // ---- S: the tiles of this CTA whose pending key equals the level become wanted ----
+        // ---- S: the tiles of this CTA whose pending key equals the level become wanted; the
+        // smallest pending key of its other tiles joins the level's running minimum ----
         unsigned long long steps = 0;
         const long long t_s0 = clock64();
         cyc_levelsync += t_s0 - t_r0;
         {
             int h = 0;
+            uint32_t m = OIFT_KEY_INF;
             for (int j = threadIdx.x; team_cta + j * team_ctas < A.ntiles; j += blockDim.x) {
                 const int t = team_cta + j * team_ctas;
-                if (__ldcg(&A.tpend[t]) == kk) {
+                const uint32_t v = __ldcg(&A.tpend[t]);
+                if (v == kk) {
                     A.tpend[t] = OIFT_KEY_INF;
                     atomicOr(&cs.want[j >> 6], 1ull << (j & 63));
                     h++;
+                } else if (v < m) {
+                    m = v;
                 }
             }
-            for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(FULL, h, o);
-            if (lane == 0 && h) atomicAdd(&cs.hits, h);
+            for (int o = 16; o > 0; o >>= 1) {
+                h += __shfl_xor_sync(FULL, h, o);
+                const uint32_t v = __shfl_xor_sync(FULL, m, o);
+                m = v < m ? v : m;
+            }
+            if (lane == 0) {
+                if (h) atomicAdd(&cs.hits, h);
+                blk_min[warp] = m;
+            }
             if (threadIdx.x == 0) cs.fetcher = 0;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            // the CTA's token of the level becomes one count per wanted tile
+            if (leader_cta) {  // the slot of the next level, free since every CTA left e - 2
+                g->outstanding[(e + 1) % 3] = team_ctas;
+                g->runmin[(e + 1) % 3] = OIFT_KEY_INF;
+            }
+            uint32_t bm = blk_min[0];
+            for (int w = 1; w < OIFT_WARPS; w++) bm = blk_min[w] < bm ? blk_min[w] : bm;
+            if (bm != OIFT_KEY_INF) atomicMin(&g->runmin[par], bm);
+            // the resets and the running minimum precede any count of this CTA given back
+            __threadfence();
+            // the CTA's token of the level becomes one count per wanted tile, before any of
+            // them can be claimed and counted off
             const int h = cs.hits;
             cs.hits = 0;
             if (h != 1) atomicAdd(&g->outstanding[par], h - 1);
         }
+        __syncthreads();
         const long long t_p0 = clock64();
         cyc_owner += t_p0 - t_s0;
         // ---- P: the CTA's warps claim its wanted tiles, one warp per tile, and fetch the
         // CTA's mailbox into the wanted set, until the level's outstanding count is zero ----
-        unsigned long long *ctabox = A.mbox + (size_t)team_cta * A.mbox_words;
+        unsigned long long *ctabox = A.mbox + ((size_t)par * team_ctas + team_cta) * A.mbox_words;
         const int words = A.mbox_words;
         long long spins = 0;
         int idle = 0;
@@ -1264,12 +1409,18 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             }
             if (fetcher) {
                 // fetch: the CTA's mailbox bits join the wanted set; bits already wanted merge
-                // into the pending activation and give their count back
+                // into the pending activation and give their count back.  The level's
+                // outstanding count and the error flag are read in the same round trip.
+                int outst = 1, errf = 0;
+                if (lane == 0) {
+                    outst = vload(&g->outstanding[par]);
+                    errf = vload(&g->error);
+                }
                 bool fetched = false;
                 for (int w0 = 0; w0 < words; w0 += 32) {
                     const int w = w0 + lane;
                     unsigned long long b = 0ull;
-                    if (w < words && vload(&ctabox[w])) b = exch_acquire_gpu(&ctabox[w], 0ull);
+                    if (w < words) b = exch_acquire_gpu(&ctabox[w], 0ull);
                     if (b) {
                         __threadfence_block();
                         const unsigned long long old = atomicOr(&cs.want[w], b);
@@ -1284,14 +1435,18 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                     continue;
                 }
                 if (lane == 0) {
-                    // the global counter is polled sparsely, the mailbox every time
-                    if ((idle & 3) == 0)
-                        done = vload(&g->outstanding[par]) == 0 || vload(&g->error) != 0;
+                    done = outst == 0 || errf != 0;
                     if (!done && ++spins > A.spin_limit) {
                         atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
                         done = 1;
                     }
                     if (done) {
+                        // every key the level's tile steps left pending reached the running
+                        // minimum before their counts were given back: it is the next level
+                        fence_acq_rel_gpu();
+                        cs.level = vload(&g->runmin[par]);
+                        cs.err = vload(&g->error);
+                        __threadfence_block();
                         *(volatile int *)&cs.level_done = e + 1;
                         atomicExch(&cs.fetcher, 0);
                     }
@@ -1303,12 +1458,15 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             idle++;
             done = __shfl_sync(FULL, done, 0);
             if (done) break;
-            __nanosleep(64);
+            if (!fetcher) __nanosleep(64);
         }
         if (lane == 0 && steps) atomicAdd(&g->tile_steps, steps);
         if (lane == 0 && steps && A.lprof && e < A.lprof_cap)
             atomicAdd(&A.lprof[2 * e + 1], (unsigned int)steps);
         cyc_drain += clock64() - t_p0;
+        // every warp has left the level; a warp whose own wait ran out has set the error
+        // flag, which the watching warp reads before it ends the level
+        __syncthreads();
     }
     if (lane == 0) {
         atomicAdd(&g->cycles[0], (unsigned long long)cyc_levelsync);
@@ -1364,7 +1522,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
         // ---- the leader draws a job and clears the per-job globals ----
         if (leader) {
             g->job = vload(S.abort) ? njobs : (int)atomicAdd(S.next_job, 1u);
-            g->nextmin[0] = g->nextmin[1] = OIFT_KEY_INF;
+            g->first = OIFT_KEY_INF;
             g->levels = 0;
             g->tile_steps = 0;
             g->bad_seed = 0;
@@ -1413,7 +1571,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
         // ---- clear the team's state for this volume ----
         for (size_t i = tid; i < N; i += nthr) key[i] = OIFT_KEY_INF;
         for (size_t i = tid; i < (size_t)ntiles; i += nthr) tpend[i] = OIFT_KEY_INF;
-        const size_t nmb = (size_t)team_ctas * mbox_words;
+        const size_t nmb = (size_t)3 * team_ctas * mbox_words;
         for (size_t i = tid; i < nmb; i += nthr) mbox[i] = 0ull;
         if (!team_barrier(g, spin_limit, team_ctas)) break;
         // ---- seeds (as oift_seed_kernel) ----
@@ -1549,12 +1707,15 @@ size_t oift_globals_bytes() { return sizeof(OiftGlobals); }
 int oift_mbox_words(const OiftPlan &P, int ctas) {
     return oift_mbox_words_for(P.ntiles, ctas);
 }
+// one mailbox per CTA for each of the three level slots
 size_t oift_mbox_bytes(const OiftPlan &P, int ctas) {
-    return (size_t)ctas * oift_mbox_words(P, ctas) * sizeof(unsigned long long);
+    return (size_t)3 * ctas * oift_mbox_words(P, ctas) * sizeof(unsigned long long);
 }
-int oift_min_ctas(int ntiles) {
+int oift_min_ctas(const OiftPlan &P) {
     const int per = OIFT_CTA_TILE_WORDS * 64;
-    return (ntiles + per - 1) / per;
+    int n = (P.ntiles + per - 1) / per;
+    while (oift_mbox_words(P, n) > OIFT_CTA_TILE_WORDS) n++;
+    return n;
 }
 
 // Queues the seeds kernel, the persistent kernel and (optionally) the finalize kernel with
@@ -1572,7 +1733,7 @@ int oift_enqueue(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int
     cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
     cudaMemsetAsync(S.mbox, 0, oift_mbox_bytes(P, sms), st);
     cudaMemsetAsync(S.g, 0, sizeof(OiftGlobals), st);
-    cudaMemsetAsync(S.g->nextmin, 0xFF, sizeof(S.g->nextmin), st);
+    cudaMemsetAsync(&S.g->first, 0xFF, sizeof(S.g->first), st);
     cudaMemsetAsync(d_flag, 0, sizeof(int), st);
     if (nseeds > 0)
         oift_seed_kernel<<<(nseeds + 255) / 256, 256, 0, st>>>(S.key, S.tpend, d_seeds,
@@ -1729,3 +1890,13 @@ int oift_team_run(OiftTeamJob *d_jobs, int njobs, bool planar, int teams, int ct
 }
 
 }  // namespace oiftb
+
+#if OIFT_PROBE
+extern "C" __attribute__((visibility("default"))) int oift_b200_probe_read(unsigned long long *out) {
+    cudaMemcpyFromSymbol(out, oiftb::g_probe, sizeof(oiftb::g_probe));
+    cudaMemcpyFromSymbol(out + 8, oiftb::g_hist, sizeof(oiftb::g_hist));
+    static unsigned long long z[8 + 96];
+    cudaMemcpyToSymbol(oiftb::g_hist, z, sizeof(oiftb::g_hist));
+    return (int)cudaMemcpyToSymbol(oiftb::g_probe, z, sizeof(oiftb::g_probe));
+}
+#endif
