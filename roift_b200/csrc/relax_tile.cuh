@@ -57,10 +57,16 @@ __device__ __forceinline__ void relax_accumulate(const RelaxArgs &a, int ip, int
     if (BLEND)  // wf = alpha |dI| + (1 - alpha)(g_p + g_q) * 0.5f (exp_gradient_weight.cpp:403-405)
         w = __fadd_rn(__fmul_rn(a.alpha, w),
                       __fmul_rn(__fsub_rn(1.0f, a.alpha), __fmul_rn((float)(gp + gq), 0.5f)));
-    if (ip > iq)
-        w = __fmul_rn(w, fq.x);
-    else if (ip < iq)
-        w = __fmul_rn(w, fq.y);
+    if (BLEND) {
+        if (ip > iq)
+            w = __fmul_rn(w, fq.x);
+        else if (ip < iq)
+            w = __fmul_rn(w, fq.y);
+    } else {
+        // with equal intensities w is 0 and stays 0 (or -0) whatever the factor, and
+        // Wmax - w below is then Wmax either way: one select instead of two tests
+        w = __fmul_rn(w, ip > iq ? fq.x : fq.y);
+    }
     if (BLEND && w < 0.0f) w = 0.0f;
     w = __fsub_rn(a.Wmax, w);
     if (w < 0.0f) w = 0.0f;
@@ -252,6 +258,139 @@ __device__ __forceinline__ bool relax_mbar_wait_bounded(unsigned long long *bar,
     return false;
 }
 
+// The polarity factors (1 + d, 1 - d), d = per_pq / 100, of a voxel with memberships mk
+// (gft_ift.cpp:8800-8806; per-class form 9076-9079).
+template <int C, bool PERCLASS>
+__device__ __forceinline__ float2 relax_factor(const RelaxArgs &a, const float (&mk)[C]) {
+    float per_pq;
+    if (PERCLASS) {
+        per_pq = 0.0f;
+#pragma unroll
+        for (int k = 0; k < C; k++) per_pq = __fadd_rn(per_pq, __fmul_rn(a.pcm[k], mk[k]));
+    } else {
+        float pbg = mk[0];
+#pragma unroll
+        for (int k = 1; k < C; k++)
+            if (k == a.bg) pbg = mk[k];
+        per_pq = __fmul_rn(a.per, __fsub_rn(__fmul_rn(2.0f, pbg), 1.0f));
+    }
+    const float d = div100_rn(per_pq);
+    return make_float2(__fadd_rn(1.0f, d), __fsub_rn(1.0f, d));
+}
+
+// 6-neighbourhood sweep of one tile column (x, y, z0 .. z0+3) by its own thread, with the
+// staged boxes already in shared memory.  The thread keeps the memberships, intensities
+// and polarity factors of its column (z0-1 .. z0+4) in registers: it computes the factors of
+// those six voxels itself, and the column supplies the -z / +z neighbours of each voxel, so
+// only the four x / y neighbours come from shared memory.  The threads of the block also
+// compute the factors of the x / y face halo; the caller synchronises the block between the
+// two phases.  Neighbours are summed in the Spheric order (-z, -y, -x, +x, +y, +z).
+template <int C, typename T, bool PERCLASS>
+struct RelaxColumn6 {
+    float cm[RB_Z][C];
+    float2 cf[RB_Z];
+    int ci[RB_Z];
+
+    __device__ __forceinline__ void stage(const RelaxArgs &a, const float *sm, const T *si,
+                                          float2 *sf, int x0, int y0, int z0, int lx, int ly,
+                                          int tid) {
+        using IB = RelaxImgBox<T>;
+        const int X = a.X, Y = a.Y, Z = a.Z;
+        const bool col_ok = x0 + lx < X && y0 + ly < Y;
+#pragma unroll
+        for (int bz = 0; bz < RB_Z; bz++) {
+            const int gz = z0 - 1 + bz;
+            const int j = (lx + RB_OFF) + (ly + 1) * RB_X + bz * RB_X * RB_Y;
+#pragma unroll
+            for (int k = 0; k < C; k++) cm[bz][k] = sm[k * RB_N + j];
+            ci[bz] = (int)si[(lx + IB::OFF) + (ly + 1) * IB::X + bz * IB::X * RB_Y];
+            cf[bz] = make_float2(0.0f, 0.0f);
+            if (col_ok && gz >= 0 && gz < Z) {
+                cf[bz] = relax_factor<C, PERCLASS>(a, cm[bz]);
+                sf[j] = cf[bz];
+            }
+        }
+        // the x faces (2 x RT_Y x RT_Z voxels) and y faces (2 x RT_X x RT_Z) of the halo
+        for (int e = tid; e < 2 * RT_Y * RT_Z + 2 * RT_X * RT_Z; e += RT_X * RT_Y) {
+            int bx, by, bz;
+            if (e < 2 * RT_Y * RT_Z) {
+                bx = (e & 1) ? RB_OFF + RT_X : RB_OFF - 1;
+                by = 1 + ((e >> 1) % RT_Y);
+                bz = 1 + (e >> 1) / RT_Y;
+            } else {
+                const int f = e - 2 * RT_Y * RT_Z;
+                bx = RB_OFF + f % RT_X;
+                by = ((f / RT_X) & 1) ? RT_Y + 1 : 0;
+                bz = 1 + f / (2 * RT_X);
+            }
+            const int gx = x0 - RB_OFF + bx, gy = y0 - 1 + by, gz = z0 - 1 + bz;
+            if (gx >= 0 && gx < X && gy >= 0 && gy < Y && gz < Z) {
+                const int j = bx + by * RB_X + bz * RB_X * RB_Y;
+                float mk[C];
+#pragma unroll
+                for (int k = 0; k < C; k++) mk[k] = sm[k * RB_N + j];
+                sf[j] = relax_factor<C, PERCLASS>(a, mk);
+            }
+        }
+    }
+
+    template <bool INTERIOR>
+    __device__ __forceinline__ void sweep(const RelaxArgs &a, const float *sm, const T *si,
+                                          const float2 *sf, float *__restrict__ mout,
+                                          const uint8_t *__restrict__ seedc, int x, int y,
+                                          int z0, int lx, int ly) const {
+        using IB = RelaxImgBox<T>;
+        const int X = a.X, Y = a.Y, Z = a.Z;
+        const size_t N = a.N, XY = (size_t)X * Y;
+#pragma unroll
+        for (int lz = 0; lz < RT_Z; lz++) {
+            const int z = z0 + lz;
+            if (z >= Z) break;
+            const int bz = lz + 1;
+            const int hc = (lx + RB_OFF) + (ly + 1) * RB_X + bz * RB_X * RB_Y;
+            const int ic = (lx + IB::OFF) + (ly + 1) * IB::X + bz * IB::X * RB_Y;
+            const int ip = ci[bz];
+            float acc[C];
+#pragma unroll
+            for (int k = 0; k < C; k++) acc[k] = 0.0f;
+            float sw = 0.0f;
+            auto from_smem = [&](int dh, int di) {
+                float mq[C];
+#pragma unroll
+                for (int k = 0; k < C; k++) mq[k] = sm[k * RB_N + hc + dh];
+                relax_accumulate<C, false>(a, ip, (int)si[ic + di], 0, 0, mq, sf[hc + dh], 1.0f,
+                                           sw, acc);
+            };
+            if (INTERIOR || z > 0)
+                relax_accumulate<C, false>(a, ip, ci[bz - 1], 0, 0, cm[bz - 1], cf[bz - 1], 1.0f,
+                                           sw, acc);
+            if (INTERIOR || y > 0) from_smem(-RB_X, -IB::X);
+            if (INTERIOR || x > 0) from_smem(-1, -1);
+            if (INTERIOR || x + 1 < X) from_smem(1, 1);
+            if (INTERIOR || y + 1 < Y) from_smem(RB_X, IB::X);
+            if (INTERIOR || z + 1 < Z)
+                relax_accumulate<C, false>(a, ip, ci[bz + 1], 0, 0, cm[bz + 1], cf[bz + 1], 1.0f,
+                                           sw, acc);
+            const size_t p = (size_t)x + (size_t)y * X + (size_t)z * XY;
+            float out[C];
+            if (sw > 0.0f) {
+#pragma unroll
+                for (int k = 0; k < C; k++) out[k] = __fdiv_rn(acc[k], sw);
+            } else {
+#pragma unroll
+                for (int k = 0; k < C; k++) out[k] = cm[bz][k];
+            }
+            const uint8_t sc = __ldg(&seedc[p]);
+            if (sc != 0xFF) {
+#pragma unroll
+                for (int k = 0; k < C; k++) out[k] = (k == sc) ? 1.0f : 0.0f;
+            }
+#pragma unroll
+            for (int k = 0; k < C; k++) mout[(size_t)k * N + p] = out[k];
+        }
+    }
+};
+
 template <int C, typename T, bool PERCLASS, int ADJ, bool INTERIOR>
 __device__ __forceinline__ void relax_tile_voxels_tma(const RelaxArgs &a, const float *sm,
                                                       const T *si, const float2 *sf,
@@ -368,6 +507,21 @@ __global__ void __launch_bounds__(256, relax_min_blocks(C, false))
         relax_mbar_wait_bounded(&mbar, 0, RELAX_TMA_SPIN_LIMIT);
         return;
     }
+    if constexpr (ADJ == 6) {
+        RelaxColumn6<C, T, PERCLASS> col;
+        col.stage(a, sm, si, sf, x0, y0, z0, threadIdx.x, threadIdx.y, tid);
+        __syncthreads();
+        const int x = x0 + (int)threadIdx.x, y = y0 + (int)threadIdx.y;
+        if (x >= X || y >= Y) return;
+        const bool interior = x0 >= 1 && x0 + RT_X < X && y0 >= 1 && y0 + RT_Y < Y &&
+                              z0 >= 1 && z0 + RT_Z < Z;
+        if (interior)
+            col.template sweep<true>(a, sm, si, sf, mout, seedc, x, y, z0, threadIdx.x,
+                                     threadIdx.y);
+        else
+            col.template sweep<false>(a, sm, si, sf, mout, seedc, x, y, z0, threadIdx.x,
+                                      threadIdx.y);
+    } else {
     // polarity factors of the staged voxels that neighbour the tile (box columns 3 .. 36)
     for (int j = tid; j < RB_N; j += 256) {
         const int bx = j % RB_X, row = j / RB_X;
@@ -405,6 +559,7 @@ __global__ void __launch_bounds__(256, relax_min_blocks(C, false))
     else
         relax_tile_voxels_tma<C, T, PERCLASS, ADJ, false>(a, sm, si, sf, mout, seedc, x, y, z0,
                                                           lx, ly);
+    }
 }
 
 template <int C, typename T>
