@@ -278,7 +278,7 @@ def run_batch_workload(args):
                 per = float(np.float32(case.pol * 100.0))
                 pc = np.array([-per, per], np.float32)
                 t0 = time.perf_counter()
-                O.ref_oift_fmax_gpu_run(img32, sd, sl, pc)
+                O.ref_oift_fmax_gpu_run(img32.reshape(case.shape), sd, sl, pc)
                 ref_s += time.perf_counter() - t0
                 lab = np.full(case.n, -1, np.int32)
                 lab[sd] = sl

@@ -328,6 +328,5 @@ int oift_run(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int X, 
              long long *steps_out, cudaEvent_t ev_begin = nullptr, cudaEvent_t ev_end = nullptr,
              unsigned long long *cycles_out = nullptr, const OiftFullN *fn = nullptr,
              bool round_orient = false, const uint16_t *Wt = nullptr);
-constexpr int OIFT_WARPS_PER_CTA = 16;
 
 }  // namespace oiftb

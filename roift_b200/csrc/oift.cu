@@ -69,8 +69,10 @@ struct OiftArgs {
     const int *seed_flag;
 };
 
+// Warps per CTA of the persistent kernels: 12 leaves each busy warp more issue slots than 16
+// (32.3 against 33.3 ms on the 256^3 ellipsoid; 8 warps: 34.5 ms)
 #ifndef OIFT_WARPS_OVERRIDE
-constexpr int OIFT_WARPS = 16;
+constexpr int OIFT_WARPS = 12;
 #else
 constexpr int OIFT_WARPS = OIFT_WARPS_OVERRIDE;
 #endif
@@ -81,6 +83,13 @@ constexpr int OIFT_SPARSE_MAX = 64;   // level voxels in a tile up to which it r
 // worklist round costs a round of shared-memory traffic (256^3 ellipsoid: 45.8 -> 38.7 ms).
 #ifndef OIFT_BIT_AFTER
 #define OIFT_BIT_AFTER 0
+#endif
+// 1 (the default): a row's six families of arc masks are computed together the first time
+// the frontier comes next to the row; 0: each family the first time the frontier reaches
+// that side (32.8 against 36.3 ms on the 256^3 ellipsoid); 2: every row with open voxels at
+// the first layer (39.7 ms)
+#ifndef OIFT_MASK_ROWS
+#define OIFT_MASK_ROWS 1
 #endif
 constexpr int OIFT_WORKLIST = 256;    // per-warp voxel worklist of the sparse mode
 
@@ -198,8 +207,12 @@ __device__ __forceinline__ int tile_of(const OiftArgs &A, int x, int y, int z) {
 // tq (-1: none).  Tile tq belongs to CTA tq % nctas, bit tq / nctas of its mailbox for the
 // level's slot `par` (a CTA still finishing the level before reads only that one's).  The
 // level's outstanding count is raised first and the warp's key updates are released
-// before the mailbox bits; a tile already marked gives its count back.
-__device__ __forceinline__ void publish_reactivations(const OiftArgs &A, int par, int tq) {
+// before the mailbox bits.  A tile that was marked already gives its count back in
+// give_back_duplicates, which the tile step calls once it has nothing else to do, so that
+// waiting for the mailbox update's reply does not delay the rest of the step.
+__device__ __forceinline__ void publish_reactivations(const OiftArgs &A, int par, int tq,
+                                                      unsigned long long &old,
+                                                      unsigned long long &bit) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const uint32_t act = __ballot_sync(FULL, tq >= 0);
@@ -210,15 +223,17 @@ __device__ __forceinline__ void publish_reactivations(const OiftArgs &A, int par
     // every lane's key updates and the raised count precede the mailbox bits
     fence_acq_rel_gpu();
     __syncwarp();
-    bool dup = false;
     if (tq >= 0) {
         const int w = tq % A.nctas, j = tq / A.nctas;
-        const unsigned long long bit = 1ull << (j & 63);
-        dup = (atomicOr(&A.mbox[((size_t)par * A.nctas + w) * A.mbox_words + (j >> 6)], bit) &
-               bit) != 0ull;
+        const unsigned long long b = 1ull << (j & 63);
+        old |= atomicOr(&A.mbox[((size_t)par * A.nctas + w) * A.mbox_words + (j >> 6)], b) & b;
+        bit |= b;
     }
-    const uint32_t dups = __ballot_sync(FULL, dup);
-    if (lane == 0 && dups) atomicSub(&A.g->outstanding[par], __popc(dups));
+}
+__device__ __forceinline__ void give_back_duplicates(const OiftArgs &A, int par,
+                                                     unsigned long long old) {
+    const uint32_t dups = __ballot_sync(0xffffffffu, old != 0ull);
+    if ((threadIdx.x & 31) == 0 && dups) atomicSub(&A.g->outstanding[par], __popc(dups));
 }
 
 // Process one tile at level kk (cost c, label l).  All 32 lanes of the warp call it.
@@ -236,6 +251,8 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
     const int x0 = tx * 32, y0 = ty * TY, z0 = tz * TZ;
     const int x = x0 + lane;
     const bool has_z = (Z > 1);
+    // per lane: a re-activation published by this step found its mailbox bit set already
+    unsigned long long pub_old = 0ull, pub_bit = 0ull;
 #if OIFT_PROBE
     const unsigned long long probe_t0 = gtimer();
     bool probe_pub = false;
@@ -287,7 +304,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             const int nz = tz + (lane == 4 ? -1 : lane == 5 ? 1 : 0);
             tq = nt + ny * A.ntx + nz * A.ntx * A.nty;
         }
-        publish_reactivations(A, par, tq);
+        publish_reactivations(A, par, tq, pub_old, pub_bit);
 #if OIFT_PROBE
         {
             const unsigned long long now = gtimer();
@@ -624,6 +641,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         if (!bitmode) {
             cyc[19] += (*(volatile uint32_t *)rmask != 0u);
             flush_reactivations();
+            give_back_duplicates(A, par, pub_old);
             const long long ts4 = clock64();
             pending();
             const long long ts5 = clock64();
@@ -675,11 +693,48 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
     // has open voxels: one ballot with lane = x.
     uint32_t Fm = P, fr = P;
     uint32_t Mpx = 0u, Mmx = 0u, Mym = 0u, Myp = 0u, Mzm = 0u, Mzp = 0u;
-    uint32_t rx = 0u, rym = 0u, ryp = 0u, rzm = 0u, rzp = 0u;  // families computed, per row
+    uint32_t rx = 0u;  // rows (families x) whose masks are computed
+#if !OIFT_MASK_ROWS
+    uint32_t rym = 0u, ryp = 0u, rzm = 0u, rzp = 0u;  // the other families, per row
+#endif
     int biters = 0, mrows = 0;
     for (;;) {
         const uint32_t frows = __ballot_sync(FULL, fr != 0u);
         const uint32_t orows = __ballot_sync(FULL, (Om & ~Fm) != 0u);
+#if OIFT_MASK_ROWS
+        // every family of masks of a row the frontier reaches, computed together (2: of
+        // every row with open voxels, at the first layer)
+        uint32_t trows = frows | ((frows << 1) & ROWS_YM) | ((frows >> 1) & ROWS_YP);
+        if constexpr (TZ > 1) trows |= (frows << TY) | (frows >> TY);
+        if (OIFT_MASK_ROWS == 2) trows = FULL;
+        uint32_t need = trows & orows & ~rx;
+        rx |= need;
+        while (need) {
+            const int q = __ffs(need) - 1;
+            need &= need - 1;
+            mrows++;
+            const uint32_t c0 = sw[q * 32 + lane];
+            const uint32_t cym = (q % TY != 0) ? sw[1024 + (q - 1) * 32 + lane] : 0u;
+            const uint32_t cyp = sw[1024 + q * 32 + lane];
+            const uint32_t czm = (TZ > 1 && q >= TY) ? sw[2048 + (q - TY) * 32 + lane] : 0u;
+            const uint32_t czp = sw[2048 + q * 32 + lane];
+            const uint32_t c0m = __shfl_up_sync(FULL, c0, 1);
+            const uint32_t bPX = __ballot_sync(FULL, lane > 0 && arc_ok(c0m, true, c, bgt, blt));
+            const uint32_t bMX = __ballot_sync(FULL, lane < 31 && arc_ok(c0, false, c, bgt, blt));
+            const uint32_t bYM = __ballot_sync(FULL, arc_ok(cym, true, c, bgt, blt));
+            const uint32_t bYP = __ballot_sync(FULL, arc_ok(cyp, false, c, bgt, blt));
+            const uint32_t bZM = __ballot_sync(FULL, arc_ok(czm, true, c, bgt, blt));
+            const uint32_t bZP = __ballot_sync(FULL, arc_ok(czp, false, c, bgt, blt));
+            if (lane == q) {
+                Mpx = bPX;
+                Mmx = bMX;
+                Mym = (q % TY != 0) ? bYM : 0u;
+                Myp = (q % TY != TY - 1) ? bYP : 0u;
+                Mzm = (TZ > 1 && q >= TY) ? bZM : 0u;
+                Mzp = (TZ > 1 && q + TY < 32) ? bZP : 0u;
+            }
+        }
+#else
         uint32_t need = frows & orows & ~rx;
         rx |= need;
         while (need) {
@@ -733,6 +788,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
                 if (lane == q) Mzp = b;
             }
         }
+#endif
         // one layer: the open, unflooded voxels next to the frontier through an open arc
         uint32_t g = ((fr << 1) & Mpx) | ((fr >> 1) & Mmx) |
                      (__shfl_up_sync(FULL, fr, 1) & Mym) | (__shfl_down_sync(FULL, fr, 1) & Myp);
@@ -793,8 +849,13 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             push_out(nb);
             __syncwarp();
         }
+        const long long tf1 = clock64();
         flush_reactivations();
+        const long long tf2 = clock64();
+        cyc[16] += tf1 - tb1;
+        cyc[17] += tf2 - tf1;
     }
+    const long long tf3 = clock64();
     uint32_t rem = Fm;
     while (__any_sync(FULL, rem != 0u)) {
         const int nb = compact(rem);
@@ -833,8 +894,10 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         __syncwarp();
     }
     const long long tb2 = clock64();
-    // ---- pending key of this tile ----
+    cyc[18] += tb2 - tf3;
+    // ---- pending key of this tile; published activations that merged give their counts back
     pending();
+    give_back_duplicates(A, par, pub_old);
     const long long tb3 = clock64();
 #if OIFT_PROBE
     if (lane == 0) {
@@ -1141,7 +1204,9 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
                 const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
                 tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
             }
-            publish_reactivations(A, par, tq);
+            unsigned long long o = 0ull, b = 0ull;
+            publish_reactivations(A, par, tq, o, b);
+            give_back_duplicates(A, par, o);
         }
     }
     __syncwarp();
