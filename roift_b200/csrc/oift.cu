@@ -11,20 +11,20 @@
 // bit-exact against the oracle, unlike the arrival-order-dependent Bellman-Ford of the
 // reference GPU path (gpu/oift_fmax_gpu.cu:33-107, 202-238).
 //
-// Execution: ONE persistent cooperative launch, 16 warps per SM.  The volume is cut into
-// warp tiles of 32 (x) x TY (y) x TZ (z) voxels, TY*TZ = 32 rows: a lane owns one row as
-// a 32-bit mask.  Per level:
-//   R  every warp reduces its share of the per-tile pending minima -> global level key;
-//      one grid barrier;
-//   S  tiles whose pending key equals the level are queued (device work queue);
-//   P  warps pop tiles: load keys + edge codes of the tile (coalesced rows), build the
-//      "arc may be used at this level" masks with a per-level base-weight threshold,
-//      flood the level inside the tile with bit operations and warp shuffles, then
-//      expand the newly conquered voxels: in-tile neighbours get tentative keys, out-of-
-//      tile neighbours are lowered with a 32-bit atomicMin; a same-level crossing
-//      re-queues the neighbour tile, a higher one lowers its pending key.
-// The level ends when no tile is pending or in flight (the level's outstanding counter).
-// Every wait (grid barrier, queue slot, level end) is bounded; on expiry the kernel sets
+// Execution: ONE persistent cooperative launch, OIFT_WARPS warps per SM.  The volume is cut
+// into warp tiles of 32 (x) x TY (y) x TZ (z) voxels, TY*TZ = 32 rows: a lane owns one row
+// as a 32-bit mask.  Tile t belongs to CTA t % #CTAs.  Per level (cost, label):
+//   S  each CTA marks its tiles whose pending key equals the level as wanted and adds the
+//      smallest pending key of its other tiles to the level's running minimum;
+//   P  its warps claim wanted tiles one at a time: stage keys + edge codes of the tile,
+//      flood the level inside the tile with row-mask operations (arc masks per row from a
+//      per-level base-weight threshold), push across the tile faces and publish same-level
+//      crossings to the owner CTAs' mailboxes, then give the in-tile heads the flood did
+//      not reach their tentative keys; every pending-key update also lowers the running
+//      minimum.
+// The level ends when no tile is pending or in flight (the level's outstanding count); the
+// running minimum is then the next level, so no grid barrier separates levels.
+// Every wait (first-level barrier, level end, claims) is bounded; on expiry the kernel sets
 // an error flag, every warp leaves, and the host reports OIFT_E_NOT_CONVERGED.
 #include <cooperative_groups.h>
 
