@@ -684,6 +684,9 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         ba.tntx = plan.ntx;
         ba.tnty = plan.nty;
         ba.planes_out = !all_full;
+        // the TMA-staged builder reports an image box that did not land in flag[3]
+        ba.tma_err = (int *)c->flag.p + 3;
+        CU(cudaMemsetAsync(ba.tma_err, 0, sizeof(int), s));
         CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
     } else if (exact) {
         // exact base weights must fit 14 bits: with a range wider than that, count the arcs
@@ -740,7 +743,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
                      octas, s, c->ev[4], c->ev[5], fulln ? &fn : nullptr, ig,
                      fulln ? nullptr : ba.Wt));
     CU(cudaMemcpyAsync(&c->hm->g, S.g, sizeof(OiftGlobals), cudaMemcpyDeviceToHost, s));
-    CU(cudaMemcpyAsync(c->hm->flag, c->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(c->hm->flag, c->flag.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(&c->hm->clamp, d_clamp, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     cudaEventRecord(c->ev[2], s);
 
@@ -798,6 +801,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     int levels = 0;
     long long steps = 0;
     TRY(oift_result(c->hm->g, c->hm->flag[0], &levels, &steps, c->oift_cycles));
+    if (!fulln && c->hm->flag[3]) return OIFT_E_CUDA;  // a builder tile whose image box did not land
     if (tile_relax) TRY(relax_tma_status(c));
     const unsigned long long hclamp = c->hm->clamp;
     if (exact && hclamp) return OIFT_E_RANGE;

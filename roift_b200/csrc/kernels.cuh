@@ -21,6 +21,9 @@ struct BuildArgs {
     uint16_t *Wt = nullptr;
     int tty = 0, ttz = 0, tntx = 0, tnty = 0;
     bool planes_out = true;  // false: only the tile-major copy (every OIFT tile is full)
+    // set by the TMA-staged builder when a tile's image box did not land (null: that builder
+    // is not used)
+    int *tma_err = nullptr;
 };
 
 struct RelaxArgs {
@@ -115,6 +118,10 @@ struct RelaxTma {
 // entry point is missing -- the sweeps then stage with per-element copies.
 bool relax_tma_encode(RelaxTma *t, const float *m0, const float *m1, const void *img,
                       bool img32, int X, int Y, int Z, int C);
+// A 3D tensor map over an int16 / int32 image [Z][Y][X] with the given box (innermost
+// first); false when the driver cannot encode it.
+bool image_tma_encode(CUtensorMap *m, const void *img, bool img32, int X, int Y, int Z, int bx,
+                      int by, int bz);
 
 template <typename T>
 cudaError_t launch_relax_tiles(int C, const float *in, float *out, const T *img,

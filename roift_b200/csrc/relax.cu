@@ -159,6 +159,22 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
+bool image_tma_encode(CUtensorMap *m, const void *img, bool img32, int X, int Y, int Z, int bx,
+                      int by, int bz) {
+    if (X % (img32 ? 4 : 8) != 0) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t esz = img32 ? 4 : 2;
+    const cuuint64_t dim[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
+    const cuuint64_t stride[2] = {(cuuint64_t)X * esz, (cuuint64_t)X * esz * (cuuint64_t)Y};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+    const cuuint32_t ones[3] = {1, 1, 1};
+    return enc(m, img32 ? CU_TENSOR_MAP_DATA_TYPE_INT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 3,
+               const_cast<void *>(img), dim, stride, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool relax_tma_encode(RelaxTma *t, const float *m0, const float *m1, const void *img,
                       bool img32, int X, int Y, int Z, int C) {
     if (X % (img32 ? 4 : 8) != 0 || C < 1 || C > 8) return false;
