@@ -867,20 +867,44 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
         }
         c->hslab_n = (size_t)nseeds;
     }
-    int32_t *slab = c->hslab;
-    for (int i = 0; i < nseeds; i++) {
-        if (seeds[i] < 0 || (size_t)seeds[i] >= N) return OIFT_E_SEED_RANGE;
-        int lb = label[seeds[i]];
-        slab[i] = lb < 0 ? 0 : lb;
-        if (slab[i] > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
-    }
     TRY(grow(c, c->img32, N * sizeof(int32_t)));
     TRY(grow(c, c->seeds, (size_t)nseeds * sizeof(int32_t)));
     TRY(grow(c, c->slabels, (size_t)nseeds * sizeof(int32_t)));
     TRY(grow(c, c->flabel, N * sizeof(int32_t)));
     if (cost) TRY(grow(c, c->cost, N * sizeof(int32_t)));
     if (mask) TRY(grow(c, c->mask8, N));
+    // the image copy is queued first: from pinned memory it runs while the host gathers the
+    // seed labels (a bad seed then returns with the copy still queued into a context buffer)
     CU(cudaMemcpyAsync(c->img32.p, image, N * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    // the seed labels, gathered from the label map (a read scattered over the whole map, so
+    // large seed lists are split over a few host threads); the first bad seed in list order
+    // decides the error, as a single pass would
+    int32_t *slab = c->hslab;
+    auto gather = [&](int i0, int i1) -> int {
+        for (int i = i0; i < i1; i++) {
+            if (seeds[i] < 0 || (size_t)seeds[i] >= N) return OIFT_E_SEED_RANGE;
+            const int lb = label[seeds[i]];
+            slab[i] = lb < 0 ? 0 : lb;
+            if (slab[i] > OIFT_MAX_LABEL) return OIFT_E_BAD_ARG;
+        }
+        return OIFT_OK;
+    };
+    const int nthreads = nseeds < (1 << 16) ? 1
+        : (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    if (nthreads == 1) {
+        TRY(gather(0, nseeds));
+    } else {
+        std::vector<int> rcs(nthreads, OIFT_OK);
+        std::vector<std::thread> pool;
+        const int chunk = (nseeds + nthreads - 1) / nthreads;
+        for (int k = 1; k < nthreads; k++)
+            pool.emplace_back([&, k]() {
+                rcs[k] = gather(std::min(nseeds, k * chunk), std::min(nseeds, (k + 1) * chunk));
+            });
+        rcs[0] = gather(0, std::min(nseeds, chunk));
+        for (auto &th : pool) th.join();
+        for (int k = 0; k < nthreads; k++) TRY(rcs[k]);
+    }
     CU(cudaMemcpyAsync(c->seeds.p, seeds, (size_t)nseeds * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(c->slabels.p, slab, (size_t)nseeds * sizeof(int32_t),
                        cudaMemcpyHostToDevice, s));
