@@ -53,7 +53,8 @@ typedef enum {
 
 /* Arc-weight builders (row a1-a3): base weight of the undirected edge {p,q}. */
 typedef enum {
-    OIFT_W_GRAD = 0,    /* |I_p - I_q| exactly (<= 16383, else OIFT_E_RANGE) */
+    OIFT_W_GRAD = 0,    /* |I_p - I_q| exactly: up to 16383 on 32-bit keys, up to 2^30 - 1 on
+                           64-bit keys (single-volume entries), else OIFT_E_RANGE */
     OIFT_W_GRAD_Q = 1,  /* min(|I_p - I_q|, wq); clamp events counted */
     OIFT_W_RBF_Q = 2,   /* floor(wq*(1 - exp(-d^2/(2 sigma^2))) + 0.5), host LUT */
     OIFT_W_BLEND_Q = 3, /* float a|dI| + (1-a)(g_p+g_q)/2, g = Sobel map scaled to max I

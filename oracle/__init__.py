@@ -238,6 +238,101 @@ def oift_fmax(W, shape_xyz, adj, seeds, seed_labels, pol=None, per_class=None, w
     return (cost, label, levels, pred) if want_pred else (cost, label, levels)
 
 
+def _offsets(adj):
+    """Neighbour offsets of Spheric(1.0) (4 / 6) or Spheric(1.75) (8 / 26) without the
+    centre (gft_adjrel3.cpp:47-85); z offsets only in 3D."""
+    r2 = 3 if adj in (8, 26) else 1
+    out = []
+    for dz in ((0,) if adj in (4, 8) else (-1, 0, 1)):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                if (dx, dy, dz) != (0, 0, 0) and dx * dx + dy * dy + dz * dz <= r2:
+                    out.append((dx, dy, dz))
+    return out
+
+
+def oift_fmax_wide(img, adj, seeds, seed_labels, pol=None, per_class=None):
+    """R2 for exact weights of any width: the lexicographic (cost, label) Dijkstra of the
+    f_max path cost in which a seed keeps its label (its key lies below every offer) and
+    the arc p -> q weighs |I_p - I_q| oriented by the tail's label,
+    (int)(w * (1 +/- per/100.0)) in double as gft/src/gft_ift.cpp:965-973 evaluates it, with
+    no 14-bit edge code in between.  A pure-Python heap loop: small volumes only.
+    Returns (cost, label) with cost 0 at the seeds."""
+    import heapq
+    X, Y, Z = _dims(img)
+    I = [int(v) for v in as_i32(img)]
+    N = X * Y * Z
+    if per_class is None:
+        per = float(np.float32(pol * 100.0))
+        table, dflt = [-per], per
+    else:
+        table, dflt = [float(v) for v in np.asarray(per_class, np.float32)], 0.0
+    pol_of = lambda l: table[l] if l < len(table) else dflt
+    offs = _offsets(adj)
+    INF = (1 << 62, 1 << 62)
+    key = [INF] * N
+    for s, l in zip(np.asarray(seeds).tolist(), np.asarray(seed_labels).tolist()):
+        k = (0, max(int(l), 0))
+        if k < key[s]:
+            key[s] = k
+    heap = [(key[p][0], key[p][1], p) for p in set(np.asarray(seeds).tolist())]
+    heapq.heapify(heap)
+    done = [False] * N
+    while heap:
+        f, l, p = heapq.heappop(heap)
+        if done[p] or (f, l) != key[p]:
+            continue
+        done[p] = True
+        c = f - 1 if f > 0 else 0
+        fgt, flt = 1.0 + pol_of(l) / 100.0, 1.0 - pol_of(l) / 100.0
+        x, y, z = p % X, (p // X) % Y, p // (X * Y)
+        for dx, dy, dz in offs:
+            qx, qy, qz = x + dx, y + dy, z + dz
+            if not (0 <= qx < X and 0 <= qy < Y and 0 <= qz < Z):
+                continue
+            q = qx + qy * X + qz * X * Y
+            if done[q]:
+                continue
+            d = I[p] - I[q]
+            b = abs(d)
+            w = int(b * fgt) if d > 0 else (int(b * flt) if d < 0 else b)
+            k = (max(c, w) + 1, l)
+            if k < key[q]:
+                key[q] = k
+                heapq.heappush(heap, (k[0], k[1], q))
+    cost = np.array([k[0] - 1 if 0 < k[0] < (1 << 62) else 0 for k in key], np.int64)
+    label = np.array([k[1] if k[0] < (1 << 62) else NIL for k in key], np.int32)
+    return cost, label
+
+
+def energy_wide(img, adj, label, pol=None, per_class=None):
+    """Oriented cut energy (gft_ift.cpp:287-319, as or_energy): the smallest weight of an
+    arc p -> q with label[q] != label[p], oriented by the polarity of label[p], with exact
+    weights of any width."""
+    X, Y, Z = _dims(img)
+    I = as_i32(img).astype(np.int64).reshape(Z, Y, X)
+    lab = np.asarray(label).reshape(Z, Y, X)
+    if per_class is None:
+        per = float(np.float32(pol * 100.0))
+        table, dflt = np.array([-per]), per
+    else:
+        table, dflt = np.asarray(per_class, np.float64), 0.0
+    pl = np.where((lab >= 0) & (lab < len(table)), table[np.clip(lab, 0, len(table) - 1)], dflt)
+    e = None
+    for dx, dy, dz in _offsets(adj):
+        sl_p = tuple(slice(max(0, -o), n - max(0, o)) for o, n in ((dz, Z), (dy, Y), (dx, X)))
+        sl_q = tuple(slice(max(0, o), n - max(0, -o)) for o, n in ((dz, Z), (dy, Y), (dx, X)))
+        d = I[sl_p] - I[sl_q]
+        b = np.abs(d).astype(np.float64)
+        f = pl[sl_p] / 100.0
+        w = np.where(d > 0, np.trunc(b * (1.0 + f)), np.where(d < 0, np.trunc(b * (1.0 - f)), b))
+        m = lab[sl_p] != lab[sl_q]
+        if m.any():
+            v = int(w[m].min())
+            e = v if e is None else min(e, v)
+    return e
+
+
 def oift_prim(W, shape_xyz, adj, seeds, seed_labels, pol=None, per_class=None):
     """R1 (restated OIFT_Multi).  Returns (label, value, pred, fmax)."""
     X, Y, Z = shape_xyz

@@ -613,7 +613,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     const bool ig = p->weight_mode == OIFT_W_IMAGEGRAPH;
     // exact base weights (|dI|, or |dI| + 1 on the image graph) must fit 14 bits
     const bool exact = p->weight_mode == OIFT_W_GRAD || ig;
-    const bool fulln = p->adjacency == 26 || p->adjacency == 8 || blend;
+    bool fulln = p->adjacency == 26 || p->adjacency == 8 || blend;
     OiftPlan plan = fulln ? oift_plan_full(X, Y, Z) : oift_plan(X, Y, Z);
 
     // with every OIFT tile full, the tile step reads only the tile-major code copy
@@ -621,8 +621,11 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     if (!fulln && !all_full) TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
     TRY(grow(c, c->key, N * sizeof(uint32_t)));
     TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(uint32_t)));
-    const int octas = std::max((c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms,
-                               std::min(c->sms, oift_min_ctas(plan)));
+    auto oift_ctas_for = [&](const OiftPlan &pl) {
+        return std::max((c->oift_ctas > 0 && c->oift_ctas < c->sms) ? c->oift_ctas : c->sms,
+                        std::min(c->sms, oift_min_ctas(pl)));
+    };
+    int octas = oift_ctas_for(plan);
     TRY(grow(c, c->queue, oift_mbox_bytes(plan, octas)));
     TRY(grow(c, c->glob, oift_globals_bytes()));
     TRY(grow(c, c->flag, 4 * sizeof(int)));
@@ -655,6 +658,26 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         return OIFT_OK;
     };
 
+    // ---- exact base weights wider than 14 bits (|dI| above 16383, or |dI| + 1 on the image
+    // graph): the OIFT runs with 64-bit keys and evaluates each arc from the image, as the
+    // full-neighbourhood tile step does (on the face neighbours for 6 / 4), instead of
+    // returning OIFT_E_RANGE; ranges above 2^30 - 1 still do ----
+    bool wide = false;
+    if (exact && !blend) {
+        TRY(need_range());
+        const long long span = (long long)hmm[1] - (long long)hmm[0] + (ig ? 1 : 0);
+        if (span > OIFT_MAX_BASE) {
+            if (span > OIFT_WIDE_MAX_BASE) return OIFT_E_RANGE;
+            wide = true;
+            fulln = true;
+            plan = oift_plan_full(X, Y, Z);
+            octas = oift_ctas_for(plan);
+            TRY(grow(c, c->key, N * sizeof(unsigned long long)));
+            TRY(grow(c, c->tpend, (size_t)plan.ntiles * sizeof(unsigned long long)));
+            TRY(grow(c, c->queue, oift_mbox_bytes(plan, octas)));
+        }
+    }
+
     // ---- arc weights ----
     BuildArgs ba;
     ba.X = X;
@@ -662,7 +685,7 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     ba.Z = Z;
     ba.planes = planes;
     ba.mode = p->weight_mode;
-    ba.cap = exact ? OIFT_MAX_BASE : p->wq;
+    ba.cap = wide ? OIFT_WIDE_MAX_BASE : (exact ? OIFT_MAX_BASE : p->wq);
     for (int k = 0; k < planes; k++) {
         int i = adj.n / 2 + k;
         ba.dx[k] = adj.dx[i];
@@ -688,14 +711,6 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
         ba.tma_err = (int *)c->flag.p + 3;
         CU(cudaMemsetAsync(ba.tma_err, 0, sizeof(int), s));
         CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
-    } else if (exact) {
-        // exact base weights must fit 14 bits: with a range wider than that, count the arcs
-        // that do not (the planes are built only for that count)
-        TRY(need_range());
-        if ((long long)hmm[1] - (long long)hmm[0] + (ig ? 1 : 0) > OIFT_MAX_BASE) {
-            TRY(grow(c, c->W, (size_t)planes * N * sizeof(uint16_t)));
-            CU(launch_build_weights<T>(d_img, (uint16_t *)c->W.p, ba, c->sms, s));
-        }
     }
     OiftFullN fn{};
     fn.img = d_img;
@@ -704,6 +719,8 @@ static int run_pipeline(oift_b200_ctx *c, const oift_b200_params *p, const T *d_
     fn.wcap = ba.cap;
     fn.lut = ba.lut;
     fn.lut_len = ba.lut_len;
+    fn.wide = wide;
+    fn.faces = wide && (p->adjacency == 6 || p->adjacency == 4);
     if (blend) {
         // blend weights (exp_gradient_weight.cpp:244-254) from the image and its Sobel
         // gradient normalised to the image maximum (596-608).  The tile stages both as 16-bit

@@ -72,6 +72,30 @@ __host__ __device__ inline int key_cost(uint32_t k) {
 __host__ __device__ inline int key_level_cost(uint32_t k) { return (int)(k >> 17) - 1; }
 __host__ __device__ inline int key_label(uint32_t k) { return (int)((k >> 1) & 0xFFFFu); }
 
+// The same keys in either width: uint32_t (costs up to OIFT_MAX_COST) or, for exact
+// weights wider than 14 bits, unsigned long long with the same layout and a 32-bit field
+// (costs up to 2^31 - 2).
+template <typename K> __host__ __device__ constexpr K key_inf_t() { return ~(K)0; }
+template <typename K> __host__ __device__ inline K seed_key_t(int label) {
+    return ((K)(unsigned)label << 1) | (K)1;
+}
+template <typename K> __host__ __device__ inline K offer_key_t(int nc, K lab_bits) {
+    return ((K)(unsigned)(nc + 1) << 17) | lab_bits;
+}
+template <typename K> __host__ __device__ inline int key_cost_t(K k) {
+    const long long f = (long long)(k >> 17);
+    return f > 0 ? (int)(f - 1) : 0;
+}
+template <typename K> __host__ __device__ inline int key_level_cost_t(K k) {
+    return (int)((long long)(k >> 17) - 1);
+}
+template <typename K> __host__ __device__ inline int key_label_t(K k) {
+    return (int)((k >> 1) & (K)0xFFFFu);
+}
+// Wide keys: exact base weights up to 2^30 - 1, so an oriented weight (|per| <= 100)
+// stays below 2^31 - 1.
+#define OIFT_WIDE_MAX_BASE 1073741823
+
 // Oriented arc weight, gft/src/gft_ift.cpp:965-973: int w = |dI|; w *= (1 +/- per/100)
 // evaluated in double and truncated.  fgt = 1.0 + per/100.0, flt = 1.0 - per/100.0 are
 // computed once per label with the same double expression as the reference.
@@ -84,13 +108,14 @@ __host__ __device__ inline int oriented_weight(uint32_t base, bool tail_gt, bool
 
 // Largest base b in [0, OIFT_MAX_BASE] with (int)(b * f) <= c, -1 when c < 0; trunc(b*f)
 // is monotone in b for f >= 0, so "oriented weight <= c" is "base <= threshold".
-__host__ __device__ inline int max_base_for_cost(int c, double f) {
+// maxb is the largest base weight of the run (OIFT_MAX_BASE, or OIFT_WIDE_MAX_BASE).
+__host__ __device__ inline int max_base_for_cost(int c, double f, int maxb = OIFT_MAX_BASE) {
     if (c < 0) return -1;  // no arc weighs less than 0
-    if (f <= 0.0) return OIFT_MAX_BASE;
-    double b = floor((double)(c + 1) / f);
-    int bi = b > (double)OIFT_MAX_BASE ? OIFT_MAX_BASE : (b < 0.0 ? 0 : (int)b);
+    if (f <= 0.0) return maxb;
+    double b = floor(((double)c + 1.0) / f);
+    int bi = b > (double)maxb ? maxb : (b < 0.0 ? 0 : (int)b);
     while (bi > 0 && (int)((double)bi * f) > c) bi--;
-    while (bi < OIFT_MAX_BASE && (int)((double)(bi + 1) * f) <= c) bi++;
+    while (bi < maxb && (int)((double)(bi + 1) * f) <= c) bi++;
     return bi;
 }
 
@@ -115,13 +140,13 @@ __host__ __device__ inline int oriented_weight_round(uint32_t base, bool tail_gt
 }
 // Largest base b in [0, OIFT_MAX_BASE] with MAX(ROUND(b f), 1) <= c (monotone in b for
 // f >= 0); -1 when no base qualifies (c < 1).
-__host__ __device__ inline int max_base_for_cost_round(int c, double f) {
+__host__ __device__ inline int max_base_for_cost_round(int c, double f, int maxb = OIFT_MAX_BASE) {
     if (c < 1) return -1;
-    if (f <= 0.0) return OIFT_MAX_BASE;
+    if (f <= 0.0) return maxb;
     double b = floor(((double)c + 0.5) / f);
-    int bi = b > (double)OIFT_MAX_BASE ? OIFT_MAX_BASE : (b < 0.0 ? 0 : (int)b);
+    int bi = b > (double)maxb ? maxb : (b < 0.0 ? 0 : (int)b);
     while (bi > 0 && round_weight((uint32_t)bi, f) > c) bi--;
-    while (bi < OIFT_MAX_BASE && round_weight((uint32_t)(bi + 1), f) <= c) bi++;
+    while (bi < maxb && round_weight((uint32_t)(bi + 1), f) <= c) bi++;
     return bi;
 }
 

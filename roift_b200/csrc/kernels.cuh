@@ -47,7 +47,9 @@ struct RelaxArgs {
 struct OiftGlobals {
     unsigned int first;          // smallest pending key before the first level
     unsigned int runmin[3];      // level e: smallest key left pending above it (slot e % 3)
-    unsigned int pad0[28];
+    unsigned long long first64;      // the same two for the 64-bit keys of a wide-range run
+    unsigned long long runmin64[3];
+    unsigned int pad0[20];
     int outstanding[3];          // level e: tiles wanted, running or announced (slot e % 3)
     unsigned int pad1[29];
     unsigned int bar_count;
@@ -86,8 +88,8 @@ struct OiftPlan {
 
 // Scratch layout for one OIFT run (device pointers supplied by the caller).
 struct OiftScratch {
-    uint32_t *key;                // [N]
-    uint32_t *tpend;              // [ntiles]
+    uint32_t *key;                // [N] (a wide-range run: [N] 64-bit keys at this address)
+    uint32_t *tpend;              // [ntiles] (a wide-range run: 64-bit)
     unsigned long long *mbox;     // [3][ctas][words] re-activation bitmasks, per level slot
     OiftGlobals *g;
     unsigned int *lprof = nullptr;  // optional per-level profile [cap][2]
@@ -224,6 +226,11 @@ struct OiftFullN {
     bool blend;
     const int32_t *gmap;
     float alpha;
+    // exact weights wider than 14 bits: 64-bit keys (the scratch keys and pending keys are
+    // twice as wide), base weights up to OIFT_WIDE_MAX_BASE; faces: only the 6 / 4 face
+    // neighbours of the 3x3(x3) neighbourhood are arcs
+    bool wide = false;
+    bool faces = false;
 };
 // Tiling of the full-neighbourhood kernel: 32 x 4 x 4 (3D) or 32 x 16 (2D).
 OiftPlan oift_plan_full(int X, int Y, int Z);

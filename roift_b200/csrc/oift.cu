@@ -37,6 +37,9 @@ struct OiftArgs {
     uint32_t *key;
     const uint16_t *W;
     uint32_t *tpend;
+    // a wide-range run's 64-bit keys and pending keys (the full-neighbourhood kernel only)
+    unsigned long long *key64;
+    unsigned long long *tpend64;
     unsigned long long *mbox;  // [3][nctas][mbox_words] re-activation bitmasks, per level slot
     unsigned int *lprof;       // [lprof_cap][2]: per-level SM cycles and tile steps
     int lprof_cap;
@@ -191,6 +194,28 @@ __device__ bool team_barrier(OiftGlobals *g, long long limit, unsigned int nctas
     }
     __syncthreads();
     return s_ok != 0;
+}
+
+// Keys, pending keys and the level minima of a run, by key width.
+template <typename K> __device__ __forceinline__ K *keys_of(const OiftArgs &A);
+template <> __device__ __forceinline__ uint32_t *keys_of<uint32_t>(const OiftArgs &A) { return A.key; }
+template <> __device__ __forceinline__ unsigned long long *keys_of<unsigned long long>(const OiftArgs &A) {
+    return A.key64;
+}
+template <typename K> __device__ __forceinline__ K *tpend_of(const OiftArgs &A);
+template <> __device__ __forceinline__ uint32_t *tpend_of<uint32_t>(const OiftArgs &A) { return A.tpend; }
+template <> __device__ __forceinline__ unsigned long long *tpend_of<unsigned long long>(const OiftArgs &A) {
+    return A.tpend64;
+}
+template <typename K> __device__ __forceinline__ K *runmin_of(OiftGlobals *g);
+template <> __device__ __forceinline__ uint32_t *runmin_of<uint32_t>(OiftGlobals *g) { return g->runmin; }
+template <> __device__ __forceinline__ unsigned long long *runmin_of<unsigned long long>(OiftGlobals *g) {
+    return g->runmin64;
+}
+template <typename K> __device__ __forceinline__ K *first_of(OiftGlobals *g);
+template <> __device__ __forceinline__ uint32_t *first_of<uint32_t>(OiftGlobals *g) { return &g->first; }
+template <> __device__ __forceinline__ unsigned long long *first_of<unsigned long long>(OiftGlobals *g) {
+    return &g->first64;
 }
 
 __device__ __forceinline__ float polarity_of(const OiftArgs &A, int l) {
@@ -954,9 +979,9 @@ __device__ __forceinline__ int gen_base(const OiftArgs &A, int ip, int iq) {
     return b > A.wcap ? A.wcap : b;
 }
 
-template <int TY, int TZ, typename TI, bool BLEND>
-__device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int par, uint32_t kk, int c, int l,
-                                  double fgt, double flt, int bgt, int blt, uint32_t *skey,
+template <int TY, int TZ, typename TI, bool BLEND, typename K = uint32_t, bool FACES = BLEND>
+__device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int par, K kk, int c, int l,
+                                  double fgt, double flt, int bgt, int blt, K *skey,
                                   int32_t *simg, uint16_t *wl, uint32_t *nfm, uint32_t *rmask,
                                   long long *cyc) {
     constexpr int NR = TY * TZ;           // rows of 32 voxels
@@ -972,8 +997,12 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     const int tx = t % A.ntx, ty = (t / A.ntx) % A.nty, tz = t / (A.ntx * A.nty);
     const int x0 = tx * 32, y0 = ty * TY, z0 = tz * TZ;
     const int x = x0 + lane;
-    const uint32_t kexp = kk - 1u;
-    const uint32_t lab_bits = ((uint32_t)l << 1) | 1u;
+    const K kexp = kk - (K)1;
+    const K lab_bits = ((K)(unsigned)l << 1) | (K)1;
+    K *const keys = keys_of<K>(A);
+    K *const tpend = tpend_of<K>(A);
+    K *const runmin = runmin_of<K>(A.g);
+    constexpr K KINF = key_inf_t<K>();
     const TI *img = static_cast<const TI *>(A.img);
     // staged halo: int32 intensities, or (BLEND) 16-bit intensities followed by 16-bit
     // gradients; both index by halo position
@@ -1014,38 +1043,49 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
         const int b = gen_base<TI>(A, ip, iq);
         return ip > iq ? b <= bgt : (ip < iq ? b <= blt : b <= c);
     };
-    auto arc_key = [&](int hp, int hq) -> uint32_t {
+    auto arc_key = [&](int hp, int hq) -> K {
         const int w = arc_w(hp, hq);
-        return offer_key(w > c ? w : c, lab_bits);
+        return offer_key_t<K>(w > c ? w : c, lab_bits);
     };
     auto pending = [&]() {
-        uint32_t m = OIFT_KEY_INF;
+        K m = KINF;
+        if constexpr (sizeof(K) == 4) {
 #pragma unroll
-        for (int i = 0; i < NR / 4; i++) {
-            const uint4 v = reinterpret_cast<const uint4 *>(skey)[lane + 32 * i];
-            if (v.x > kk && v.x < m) m = v.x;
-            if (v.y > kk && v.y < m) m = v.y;
-            if (v.z > kk && v.z < m) m = v.z;
-            if (v.w > kk && v.w < m) m = v.w;
+            for (int i = 0; i < NR / 4; i++) {
+                const uint4 v = reinterpret_cast<const uint4 *>(skey)[lane + 32 * i];
+                if (v.x > kk && v.x < m) m = v.x;
+                if (v.y > kk && v.y < m) m = v.y;
+                if (v.z > kk && v.z < m) m = v.z;
+                if (v.w > kk && v.w < m) m = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < NR / 2; i++) {
+                const ulonglong2 v = reinterpret_cast<const ulonglong2 *>(skey)[lane + 32 * i];
+                if (v.x > kk && v.x < m) m = v.x;
+                if (v.y > kk && v.y < m) m = v.y;
+            }
         }
         for (int o = 16; o > 0; o >>= 1) {
-            uint32_t v = __shfl_xor_sync(FULL, m, o);
+            const K v = __shfl_xor_sync(FULL, m, o);
             m = v < m ? v : m;
         }
-        if (lane == 0 && m != OIFT_KEY_INF) {
-            atomicMin(&A.tpend[t], m);
-            atomicMin(&A.g->runmin[par], m);
+        if (lane == 0 && m != KINF) {
+            atomicMin(&tpend[t], m);
+            atomicMin(&runmin[par], m);
         }
     };
     // ---- stage keys and the intensities with a one-voxel halo ----
     const bool full = (x0 + 32 <= X) && (y0 + TY <= Y) && (z0 + TZ <= Z) && ((X & 7) == 0);
     if (full) {
+        // 16-byte chunks: CPR per row of 32 keys, NR * CPR / 32 per lane
+        constexpr int CPR = 32 * (int)sizeof(K) / 16;
 #pragma unroll
-        for (int m = 0; m < NR / 4; m++) {
-            const int j = lane + 32 * m, r = j >> 3, col = j & 7;
+        for (int m = 0; m < NR * CPR / 32; m++) {
+            const int j = lane + 32 * m, r = j / CPR, col = j % CPR;
             const size_t p0 = (size_t)x0 + (size_t)(y0 + r % TY) * X + (size_t)(z0 + r / TY) * XY;
             cp_async16(reinterpret_cast<uint4 *>(skey) + j,
-                       reinterpret_cast<const uint4 *>(A.key + p0) + col);
+                       reinterpret_cast<const uint4 *>(keys + p0) + col);
         }
     } else {
 #pragma unroll 4
@@ -1053,7 +1093,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
             const int y = y0 + (r % TY), z = z0 + (r / TY);
             const bool valid = (x < X) && (y < Y) && (z < Z);
             skey[r * 32 + lane] =
-                valid ? __ldcg(&A.key[(size_t)x + (size_t)y * X + (size_t)z * XY]) : 0u;
+                valid ? __ldcg(&keys[(size_t)x + (size_t)y * X + (size_t)z * XY]) : (K)0;
         }
     }
     for (int i = lane; i < HN; i += 32) {
@@ -1074,7 +1114,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     uint32_t rowF = 0, rowV = 0;
 #pragma unroll
     for (int r = 0; r < NR; r++) {
-        const uint32_t k = skey[r * 32 + lane];
+        const K k = skey[r * 32 + lane];
         const uint32_t bF = __ballot_sync(FULL, k == kk);
         const uint32_t bV = __ballot_sync(FULL, k <= kk);
         if (lane == r) {
@@ -1121,7 +1161,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
             const int li = wl[idx];
             const int r = li >> 5, xl = li & 31, yl = r % TY, zl = r / TY;
             const int xg = x0 + xl, y = y0 + yl, z = z0 + zl;
-            A.key[(size_t)xg + (size_t)y * X + (size_t)z * XY] = kexp;
+            keys[(size_t)xg + (size_t)y * X + (size_t)z * XY] = kexp;
             skey[li] = kexp;
             const int hp = hidx(xl, yl, zl);
 #pragma unroll
@@ -1131,24 +1171,24 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
 #pragma unroll
                     for (int dx = -1; dx <= 1; dx++) {
                         if (dx == 0 && dy == 0 && dz == 0) continue;
-                        // the blend weights come with the 6 / 4 face neighbourhood
-                        if (BLEND && (dx != 0) + (dy != 0) + (dz != 0) != 1) continue;
+                        // the blend weights and a wide-range 6 / 4 run: the face neighbours
+                        if (FACES && (dx != 0) + (dy != 0) + (dz != 0) != 1) continue;
                         const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
                         if (qxl < 0 || qxl >= 32 || qyl < 0 || qyl >= TY || qzl < 0 || qzl >= TZ)
                             continue;  // across the tile boundary: after the flood
                         if (xg + dx >= X || y + dy >= Y || z + dz >= Z) continue;
                         const int lq = (qyl + TY * qzl) * 32 + qxl;
-                        const uint32_t sk = skey[lq];
+                        const K sk = skey[lq];
                         if (sk <= kk) continue;
                         const int hq = hidx(qxl, qyl, qzl);
                         if (arc_open(hp, hq)) {
                             atomicOr(&nfm[qyl + TY * qzl], 1u << qxl);
                         } else {
-                            const uint32_t nk = arc_key(hp, hq);
+                            const K nk = arc_key(hp, hq);
                             if (nk < sk) {
                                 atomicMin(&skey[lq], nk);
-                                atomicMin(&A.key[(size_t)(xg + dx) + (size_t)(y + dy) * X +
-                                                 (size_t)(z + dz) * XY], nk);
+                                atomicMin(&keys[(size_t)(xg + dx) + (size_t)(y + dy) * X +
+                                                (size_t)(z + dz) * XY], nk);
                             }
                         }
                     }
@@ -1178,22 +1218,22 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
         const int hp = hidx(xl, yl, zl);
 #pragma unroll
         for (int dz = (TZ > 1 ? -1 : 0); dz <= (TZ > 1 ? 1 : 0); dz++) {
-            uint32_t nk[9], old[9];
+            K nk[9], old[9];
 #pragma unroll
             for (int j = 0; j < 9; j++) {
                 const int dy = j / 3 - 1, dx = j % 3 - 1;
-                nk[j] = OIFT_KEY_INF;
-                if (BLEND && (dx != 0) + (dy != 0) + (dz != 0) != 1) continue;
+                nk[j] = KINF;
+                if (FACES && (dx != 0) + (dy != 0) + (dz != 0) != 1) continue;
                 const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
                 const bool out = qxl < 0 || qxl >= 32 || qyl < 0 || qyl >= TY || qzl < 0 || qzl >= TZ;
                 const int qx = xg + dx, qy = y + dy, qz = z + dz;
                 if (!out || qx < 0 || qy < 0 || qz < 0 || qx >= X || qy >= Y || qz >= Z) continue;
                 nk[j] = arc_key(hp, hidx(qxl, qyl, qzl));
-                old[j] = atomicMin(&A.key[(size_t)qx + (size_t)qy * X + (size_t)qz * XY], nk[j]);
+                old[j] = atomicMin(&keys[(size_t)qx + (size_t)qy * X + (size_t)qz * XY], nk[j]);
             }
 #pragma unroll
             for (int j = 0; j < 9; j++) {
-                if (nk[j] == OIFT_KEY_INF || !(nk[j] < old[j])) continue;
+                if (nk[j] == KINF || !(nk[j] < old[j])) continue;
                 const int dy = j / 3 - 1, dx = j % 3 - 1;
                 const int qxl = xl + dx, qyl = yl + dy, qzl = zl + dz;
                 const int ox = qxl < 0 ? -1 : (qxl >= 32 ? 1 : 0);
@@ -1203,8 +1243,8 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
                     atomicOr(rmask, 1u << ((oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)));
                 } else {
                     const int tq = (tx + ox) + (ty + oy) * A.ntx + (tz + oz) * A.ntx * A.nty;
-                    atomicMin(&A.tpend[tq], nk[j]);
-                    atomicMin(&A.g->runmin[par], nk[j]);
+                    atomicMin(&tpend[tq], nk[j]);
+                    atomicMin(&runmin[par], nk[j]);
                 }
             }
         }
@@ -1254,8 +1294,8 @@ struct OiftCtaSmem {
     int err;
     int fetcher;     // warps that watch the CTA's mailbox and the level's count
     int level_done;  // e + 1 once level e has ended
-    uint32_t blk_min[OIFT_WARPS];
-    uint32_t level;
+    unsigned long long blk_min[OIFT_WARPS];  // keys of either width
+    unsigned long long level;
     uint32_t wl[OIFT_WARPS][OIFT_WORKLIST];
     uint32_t nfm[OIFT_WARPS][32];  // per row: voxels reached by open arcs in a flood round
     uint32_t rmask[OIFT_WARPS];
@@ -1263,7 +1303,8 @@ struct OiftCtaSmem {
 
 // The level loop of one OIFT job, run by the `team_ctas` CTAs starting at team CTA index
 // `team_cta` (0 .. team_ctas-1).  A.nwarps must equal team_ctas * OIFT_WARPS.
-template <int TY, int TZ, bool FULLN = false, typename TI = int16_t, bool BLEND = false>
+template <int TY, int TZ, bool FULLN = false, typename TI = int16_t, bool BLEND = false,
+          typename K = uint32_t, bool FACES = BLEND>
 __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftCtaSmem &cs,
                            unsigned char *smem_raw) {
     const unsigned FULL = 0xffffffffu;
@@ -1275,7 +1316,10 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     uint16_t *shz = shx + 64 + TZ * 32;  // 64 + 32 (TY + TZ) <= 448 halo codes per warp
     static_assert(FULLN || (TY * TZ == 32 && (TZ == 1 || TY + TZ <= 12)),
                   "the halo codes of a warp tile must fit their 448-entry region");
-    uint32_t *blk_min = cs.blk_min;
+    static_assert(FULLN || sizeof(K) == 4, "64-bit keys run the full-neighbourhood tile step");
+    constexpr K KINF = key_inf_t<K>();
+    K *const tpend = tpend_of<K>(A);
+    unsigned long long *blk_min = cs.blk_min;
     long long cyc_tile[20];
 #pragma unroll
     for (int i = 0; i < 20; i++) cyc_tile[i] = 0;
@@ -1298,7 +1342,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     uint32_t *nfm = cs.nfm[warp];
     OiftGlobals *g = A.g;
     const bool leader_cta = team_cta == 0;
-    uint32_t prev_level = 0;
+    K prev_level = 0;
     long long lvl_t0 = 0;
     long long cyc_levelsync = 0, cyc_owner = 0, cyc_busy = 0, cyc_drain = 0;
     // ---- the first level: global minimum of the pending keys, one barrier.  Level e then
@@ -1308,29 +1352,29 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     // (three slots, so a slot is reset only after every CTA has left the level that used
     // it before) ----
     {
-        uint32_t m = OIFT_KEY_INF;
+        K m = KINF;
         for (int j = threadIdx.x; team_cta + j * team_ctas < A.ntiles; j += blockDim.x) {
-            const uint32_t v = __ldcg(&A.tpend[team_cta + j * team_ctas]);
+            const K v = __ldcg(&tpend[team_cta + j * team_ctas]);
             m = v < m ? v : m;
         }
         for (int o = 16; o > 0; o >>= 1) {
-            const uint32_t v = __shfl_xor_sync(FULL, m, o);
+            const K v = __shfl_xor_sync(FULL, m, o);
             m = v < m ? v : m;
         }
         if (lane == 0) blk_min[warp] = m;
         __syncthreads();
         if (threadIdx.x == 0) {
-            uint32_t bm = blk_min[0];
-            for (int w = 1; w < OIFT_WARPS; w++) bm = blk_min[w] < bm ? blk_min[w] : bm;
-            if (bm != OIFT_KEY_INF) atomicMin(&g->first, bm);
+            K bm = (K)blk_min[0];
+            for (int w = 1; w < OIFT_WARPS; w++) bm = (K)blk_min[w] < bm ? (K)blk_min[w] : bm;
+            if (bm != KINF) atomicMin(first_of<K>(g), bm);
             if (leader_cta) {
                 g->outstanding[0] = team_ctas;  // one token per CTA for its scan
-                g->runmin[0] = OIFT_KEY_INF;
+                runmin_of<K>(g)[0] = KINF;
             }
         }
         team_barrier(g, A.spin_limit, team_ctas);
         if (threadIdx.x == 0) {
-            cs.level = vload(&g->first);
+            cs.level = vload(first_of<K>(g));
             cs.err = vload(&g->error);
         }
         __syncthreads();
@@ -1347,8 +1391,8 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         }
         // the level and the error flag were read once for the whole CTA: every warp leaves
         // the loop in the same iteration, so the CTA's barriers stay matched
-        const uint32_t kk = cs.level;
-        if (kk == OIFT_KEY_INF || cs.err) break;
+        const K kk = (K)cs.level;
+        if (kk == KINF || cs.err) break;
         // levels strictly increase; a repeat or a runaway level count is a fault
         if ((e > 0 && kk <= prev_level) || e >= A.max_levels) {
             if (threadIdx.x == 0) atomicCAS(&g->error, 0, OIFT_DEV_TIMEOUT);
@@ -1356,7 +1400,9 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         }
         prev_level = kk;
         if (leader_cta && threadIdx.x == 0) g->levels = e + 1;
-        const int c = key_level_cost(kk), l = key_label(kk);
+        const int c = key_level_cost_t<K>(kk), l = key_label_t<K>(kk);
+        // the largest base weight of the run bounds the per-level thresholds
+        const int maxb = sizeof(K) == 8 ? A.wcap : OIFT_MAX_BASE;
         const double per = (double)polarity_of(A, l);
         double fgt, flt;
         int bgt, blt;
@@ -1364,13 +1410,13 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             const float alpha = (float)(per / 100.0);
             fgt = 1.0 + (double)alpha;
             flt = 1.0 - (double)alpha;
-            bgt = max_base_for_cost_round(c, fgt);
-            blt = max_base_for_cost_round(c, flt);
+            bgt = max_base_for_cost_round(c, fgt, maxb);
+            blt = max_base_for_cost_round(c, flt, maxb);
         } else {
             fgt = 1.0 + per / 100.0;
             flt = 1.0 - per / 100.0;
-            bgt = max_base_for_cost(c, fgt);
-            blt = max_base_for_cost(c, flt);
+            bgt = max_base_for_cost(c, fgt, maxb);
+            blt = max_base_for_cost(c, flt, maxb);
         }
         // ---- S: the tiles of this CTA whose pending key equals the level become wanted; the
         // smallest pending key of its other tiles joins the level's running minimum ----
@@ -1379,12 +1425,12 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         cyc_levelsync += t_s0 - t_r0;
         {
             int h = 0;
-            uint32_t m = OIFT_KEY_INF;
+            K m = KINF;
             for (int j = threadIdx.x; team_cta + j * team_ctas < A.ntiles; j += blockDim.x) {
                 const int t = team_cta + j * team_ctas;
-                const uint32_t v = __ldcg(&A.tpend[t]);
+                const K v = __ldcg(&tpend[t]);
                 if (v == kk) {
-                    A.tpend[t] = OIFT_KEY_INF;
+                    tpend[t] = KINF;
                     atomicOr(&cs.want[j >> 6], 1ull << (j & 63));
                     h++;
                 } else if (v < m) {
@@ -1393,7 +1439,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             }
             for (int o = 16; o > 0; o >>= 1) {
                 h += __shfl_xor_sync(FULL, h, o);
-                const uint32_t v = __shfl_xor_sync(FULL, m, o);
+                const K v = __shfl_xor_sync(FULL, m, o);
                 m = v < m ? v : m;
             }
             if (lane == 0) {
@@ -1406,11 +1452,11 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         if (threadIdx.x == 0) {
             if (leader_cta) {  // the slot of the next level, free since every CTA left e - 2
                 g->outstanding[(e + 1) % 3] = team_ctas;
-                g->runmin[(e + 1) % 3] = OIFT_KEY_INF;
+                runmin_of<K>(g)[(e + 1) % 3] = KINF;
             }
-            uint32_t bm = blk_min[0];
-            for (int w = 1; w < OIFT_WARPS; w++) bm = blk_min[w] < bm ? blk_min[w] : bm;
-            if (bm != OIFT_KEY_INF) atomicMin(&g->runmin[par], bm);
+            K bm = (K)blk_min[0];
+            for (int w = 1; w < OIFT_WARPS; w++) bm = (K)blk_min[w] < bm ? (K)blk_min[w] : bm;
+            if (bm != KINF) atomicMin(&runmin_of<K>(g)[par], bm);
             // the resets and the running minimum precede any count of this CTA given back
             __threadfence();
             // the CTA's token of the level becomes one count per wanted tile, before any of
@@ -1490,10 +1536,10 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 const long long tb = clock64();
                 const int t = team_cta + j * team_ctas;
                 if constexpr (FULLN)
-                    process_tile_full<TY, TZ, TI, BLEND>(A, t, par, kk, c, l, fgt, flt, bgt, blt,
-                                                         skey, reinterpret_cast<int32_t *>(sw),
-                                                         reinterpret_cast<uint16_t *>(wl), nfm,
-                                                         rmask, cyc_tile);
+                    process_tile_full<TY, TZ, TI, BLEND, K, FACES>(
+                        A, t, par, kk, c, l, fgt, flt, bgt, blt, reinterpret_cast<K *>(skey),
+                        reinterpret_cast<int32_t *>(sw), reinterpret_cast<uint16_t *>(wl), nfm,
+                        rmask, cyc_tile);
                 else
                     process_tile<TY, TZ>(A, t, par, kk, c, l, fgt, flt, bgt, blt, skey, sw, shx,
                                          shy, shz, wl, nfm, rmask, cyc_tile);
@@ -1565,7 +1611,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                         // every key the level's tile steps left pending reached the running
                         // minimum before their counts were given back: it is the next level
                         fence_acq_rel_gpu();
-                        cs.level = vload(&g->runmin[par]);
+                        cs.level = vload(&runmin_of<K>(g)[par]);
                         cs.err = vload(&g->error);
                         __threadfence_block();
                         *(volatile int *)&cs.level_done = e + 1;
@@ -1601,7 +1647,8 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     }
 }
 
-template <int TY, int TZ, bool FULLN = false, typename TI = int16_t, bool BLEND = false>
+template <int TY, int TZ, bool FULLN = false, typename TI = int16_t, bool BLEND = false,
+          typename K = uint32_t, bool FACES = BLEND>
 __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(OiftArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ OiftCtaSmem cs;
@@ -1611,7 +1658,7 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1) oift_persistent_kernel(Oif
     if (threadIdx.x == 0) s_bad = A.seed_flag ? *(volatile const int *)A.seed_flag : 0;
     __syncthreads();
     if (s_bad) return;
-    oift_solve<TY, TZ, FULLN, TI, BLEND>(A, blockIdx.x, gridDim.x, cs, smem_raw);
+    oift_solve<TY, TZ, FULLN, TI, BLEND, K, FACES>(A, blockIdx.x, gridDim.x, cs, smem_raw);
 }
 
 // Batched OIFT: CTA b belongs to team b / team_ctas.  A team draws jobs from a shared
@@ -1746,14 +1793,15 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
     }
 }
 
-__global__ void oift_seed_kernel(uint32_t *key, uint32_t *tpend, const int32_t *seeds,
+template <typename K>
+__global__ void oift_seed_kernel(K *key, K *tpend, const int32_t *seeds,
                                  const int32_t *labels, int nseeds, int X, int Y, int Z,
                                  int ntx, int nty, int TY, int TZ, int *bad) {
     // every lane of the warp reaches the tile aggregation below (no early return)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t N = (size_t)X * Y * Z;
     int t = -1;
-    uint32_t k = OIFT_KEY_INF;
+    K k = key_inf_t<K>();
     if (i < nseeds) {
         const int p = seeds[i];
         const int lb = labels[i] < 0 ? 0 : labels[i];
@@ -1762,26 +1810,30 @@ __global__ void oift_seed_kernel(uint32_t *key, uint32_t *tpend, const int32_t *
         } else if (lb > OIFT_MAX_LABEL) {
             atomicExch(bad, 2);
         } else {
-            k = seed_key(lb);
+            k = seed_key_t<K>(lb);
             atomicMin(&key[p], k);
             const int x = p % X, y = (p / X) % Y, z = (int)(p / ((size_t)X * Y));
             t = (x >> 5) + (y / TY) * ntx + (z / TZ) * ntx * nty;
         }
     }
     // seed lists in address order put many seeds of a warp in one tile: one pending-key
-    // update per tile and warp
+    // update per tile and warp (64-bit keys, which have no warp reduction: one per seed)
+    if constexpr (sizeof(K) == 8) {
+        if (t >= 0) atomicMin(&tpend[t], k);
+        return;
+    }
     const unsigned peers = __match_any_sync(0xffffffffu, t);
-    const uint32_t km = __reduce_min_sync(peers, k);
+    const K km = __reduce_min_sync(peers, (uint32_t)k);
     if (t >= 0 && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicMin(&tpend[t], km);
 }
 
-__global__ void oift_finalize_kernel(const uint32_t *key, size_t n, int32_t *cost,
-                                     int32_t *label) {
+template <typename K>
+__global__ void oift_finalize_kernel(const K *key, size_t n, int32_t *cost, int32_t *label) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        uint32_t k = key[i];
-        if (cost) cost[i] = (k == OIFT_KEY_INF) ? 0x7fffffff : key_cost(k);
-        if (label) label[i] = (k == OIFT_KEY_INF) ? -1 : key_label(k);
+        const K k = key[i];
+        if (cost) cost[i] = (k == key_inf_t<K>()) ? 0x7fffffff : key_cost_t<K>(k);
+        if (label) label[i] = (k == key_inf_t<K>()) ? -1 : key_label_t<K>(k);
     }
 }
 
@@ -1853,22 +1905,35 @@ int oift_enqueue(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int
                  cudaEvent_t ev_end, const OiftFullN *fn, bool round_orient,
                  const uint16_t *Wt) {
     size_t N = (size_t)X * Y * Z;
-    cudaMemsetAsync(S.key, 0xFF, N * sizeof(uint32_t), st);
-    cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * sizeof(uint32_t), st);
+    // a wide-range run keeps 64-bit keys and pending keys at the scratch addresses
+    const bool wide = fn && fn->wide;
+    const size_t ksz = wide ? sizeof(unsigned long long) : sizeof(uint32_t);
+    unsigned long long *key64 = wide ? reinterpret_cast<unsigned long long *>(S.key) : nullptr;
+    unsigned long long *tpend64 = wide ? reinterpret_cast<unsigned long long *>(S.tpend) : nullptr;
+    cudaMemsetAsync(S.key, 0xFF, N * ksz, st);
+    cudaMemsetAsync(S.tpend, 0xFF, (size_t)P.ntiles * ksz, st);
     cudaMemsetAsync(S.mbox, 0, oift_mbox_bytes(P, sms), st);
     cudaMemsetAsync(S.g, 0, sizeof(OiftGlobals), st);
     cudaMemsetAsync(&S.g->first, 0xFF, sizeof(S.g->first), st);
+    cudaMemsetAsync(&S.g->first64, 0xFF, sizeof(S.g->first64), st);
     cudaMemsetAsync(d_flag, 0, sizeof(int), st);
-    if (nseeds > 0)
-        oift_seed_kernel<<<(nseeds + 255) / 256, 256, 0, st>>>(S.key, S.tpend, d_seeds,
-                                                               d_seed_labels, nseeds, X, Y,
-                                                               Z, P.ntx, P.nty, P.TY, P.TZ,
-                                                               d_flag);
+    if (nseeds > 0) {
+        if (wide)
+            oift_seed_kernel<unsigned long long><<<(nseeds + 255) / 256, 256, 0, st>>>(
+                key64, tpend64, d_seeds, d_seed_labels, nseeds, X, Y, Z, P.ntx, P.nty, P.TY, P.TZ,
+                d_flag);
+        else
+            oift_seed_kernel<uint32_t><<<(nseeds + 255) / 256, 256, 0, st>>>(
+                S.key, S.tpend, d_seeds, d_seed_labels, nseeds, X, Y, Z, P.ntx, P.nty, P.TY, P.TZ,
+                d_flag);
+    }
 
     OiftArgs A;
     A.key = S.key;
     A.W = W;
     A.tpend = S.tpend;
+    A.key64 = key64;
+    A.tpend64 = tpend64;
     A.mbox = S.mbox;
     A.lprof = S.lprof;
     A.lprof_cap = S.lprof_cap;
@@ -1909,7 +1974,24 @@ int oift_enqueue(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return cudaLaunchCooperativeKernel(kfn, dim3(sms), dim3(OIFT_WARPS * 32), args, smem, st);
     };
-    if (fn && fn->blend) {
+    using u64 = unsigned long long;
+    if (wide) {
+        if (P.TZ == 1) {
+            if (fn->faces)
+                err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<16, 1, true, int16_t, false, u64, true>)
+                                  : launch((const void *)oift_persistent_kernel<16, 1, true, int32_t, false, u64, true>);
+            else
+                err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<16, 1, true, int16_t, false, u64, false>)
+                                  : launch((const void *)oift_persistent_kernel<16, 1, true, int32_t, false, u64, false>);
+        } else {
+            if (fn->faces)
+                err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<4, 4, true, int16_t, false, u64, true>)
+                                  : launch((const void *)oift_persistent_kernel<4, 4, true, int32_t, false, u64, true>);
+            else
+                err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<4, 4, true, int16_t, false, u64, false>)
+                                  : launch((const void *)oift_persistent_kernel<4, 4, true, int32_t, false, u64, false>);
+        }
+    } else if (fn && fn->blend) {
         if (P.TZ == 1)
             err = fn->img_i16 ? launch((const void *)oift_persistent_kernel<16, 1, true, int16_t, true>)
                               : launch((const void *)oift_persistent_kernel<16, 1, true, int32_t, true>);
@@ -1933,7 +2015,10 @@ int oift_enqueue(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int
     if (cost || label) {
         int blocks = (int)((N + 255) / 256);
         if (blocks > sms * 16) blocks = sms * 16;
-        oift_finalize_kernel<<<blocks, 256, 0, st>>>(S.key, N, cost, label);
+        if (wide)
+            oift_finalize_kernel<unsigned long long><<<blocks, 256, 0, st>>>(key64, N, cost, label);
+        else
+            oift_finalize_kernel<uint32_t><<<blocks, 256, 0, st>>>(S.key, N, cost, label);
     }
     return cudaGetLastError() == cudaSuccess ? OIFT_OK : OIFT_E_CUDA;
 }

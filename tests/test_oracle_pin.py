@@ -403,3 +403,41 @@ def test_bottleneck_arcs_carry_the_cost_and_gradient_is_exact(oracle_lib, adj, s
         fd = (AD.cost_loss(img.reshape(c.shape), lab, arcs, truth, *(th + e), adj=adj, g=g)[0] -
               AD.cost_loss(img.reshape(c.shape), lab, arcs, truth, *(th - e), adj=adj, g=g)[0]) / (2 * h)
         assert abs(grad[k] - fd) <= 1e-6 * abs(grad[k]) + 1e-9
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("seed,shape,pol,adj,nl,scale", [
+    (21, (10, 14, 18), -0.3, 6, 1, 97), (22, (8, 12, 16), 0.4, 26, 2, 131),
+    (23, (1, 40, 44), 0.5, 4, 1, 53), (24, (1, 30, 36), -0.2, 8, 2, 211)])
+def test_wide_range_oracle_matches_live_reference(oracle_lib, seed, shape, pol, adj, nl, scale):
+    """The restatement for exact weights wider than the 14-bit edge codes: at polarity 0 its
+    cost map plus one is the reference IFT_fmax cost map, and at any polarity the reference
+    OIFT_Multi labels and its labels have the same oriented cut energy."""
+    c = synth.small_case(seed=seed, shape=shape, pol=pol, adjacency=adj, nlabels=nl,
+                         noise=150, contrast=300)
+    img = (c.image.astype(np.int64) * scale).astype(np.int32)
+    assert int(img.max()) - int(img.min()) > 16383
+    ns = np.ones(img.size, bool)
+    ns[c.seeds] = False
+    cost0, _ = O.oift_fmax_wide(img, adj, c.seeds, c.seed_labels, pol=0.0)
+    ref_cost, _ = O.ref_ift_fmax(img, adj, c.seeds, c.seed_labels)
+    assert int(cost0.max()) > 16383
+    assert np.array_equal(ref_cost[ns] - 1, cost0[ns])
+    cost, lab = O.oift_fmax_wide(img, adj, c.seeds, c.seed_labels, pol=pol)
+    lab_ref = O.ref_oift_multi(img, adj, c.seeds, c.seed_labels, pol=pol)
+    assert O.energy_wide(img, adj, lab_ref, pol=pol) == O.energy_wide(img, adj, lab, pol=pol)
+
+
+def test_wide_range_oracle_equals_code_oracle_on_narrow_ranges(oracle_lib):
+    """Within the 14-bit range the wide restatement and R2 on edge codes agree exactly."""
+    for seed, shape, pol, adj, nl in [(31, (9, 12, 20), -0.3, 6, 2), (32, (7, 9, 12), 0.5, 26, 3),
+                                      (33, (1, 30, 40), 0.2, 8, 2)]:
+        c = synth.small_case(seed=seed, shape=shape, pol=pol, adjacency=adj, nlabels=nl,
+                             noise=150, contrast=300)
+        img = c.image.astype(np.int32)
+        Z, Y, X = c.shape
+        W, _ = O.build_weights(img, adj, "grad")
+        cost, lab, _ = O.oift_fmax(W, (X, Y, Z), adj, c.seeds, c.seed_labels, pol=pol)
+        cw, lw = O.oift_fmax_wide(img, adj, c.seeds, c.seed_labels, pol=pol)
+        assert np.array_equal(cost, cw)
+        assert np.array_equal(lab, lw)
