@@ -127,3 +127,24 @@ def test_range_beyond_wide_keys_is_rejected(roift):
     with pytest.raises(roift.OiftError) as e:
         ctx.run_host(p, img, lab, seeds)
     assert e.value.status == roift.E_RANGE
+
+
+def test_wide_range_through_the_reference_entry(roift, oracle_lib):
+    """oift_fmax_gpu_run (the reference's entry, gpu/oift_fmax_gpu.cu:139-149) on an int
+    image whose neighbouring intensities differ by far more than 16383: the labels equal the
+    wide-range R2's, and where the reference library is present, the reference OIFT_Multi
+    labels have the same cut energy."""
+    shape, adj = (12, 30, 40), 6
+    c, img = _wide_case(shape, -0.4, adj, 2, 157)
+    Z, Y, X = c.shape
+    per_class = np.array([40.0, -40.0, -40.0], np.float32)
+    lab = c.label_map()
+    levels = roift.oift_fmax_gpu_run(img, lab, X, Y, Z, per_class, c.seeds)
+    _, lab_r = O.oift_fmax_wide(img.reshape(shape), adj, c.seeds, c.seed_labels,
+                                per_class=per_class)
+    assert levels > 0
+    assert np.array_equal(lab, lab_r)
+    if O.ref_available():
+        lab_ref = O.ref_oift_multi(img, adj, c.seeds, c.seed_labels, per_class=per_class)
+        assert O.energy_wide(img.reshape(shape), adj, lab, per_class=per_class) == \
+            O.energy_wide(img.reshape(shape), adj, lab_ref, per_class=per_class)
