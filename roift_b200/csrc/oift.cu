@@ -33,6 +33,26 @@
 namespace oiftb {
 
 
+// n / d for 0 <= n < 2^31 by a multiply-high, for divisors known only at run time: with
+// s = floor(log2 d) and m = ceil(2^(32+s) / d) (m = 0 for a power of two, a shift alone),
+// q = umulhi(n, m) >> s is exact on that range, since m exceeds 2^(32+s) / d by less than 1
+// and 2^(32+s) / d >= 2^31.
+struct FastDiv {
+    uint32_t m, s;
+};
+__host__ __device__ inline FastDiv make_fastdiv(uint32_t d) {
+    uint32_t s = 0;
+    while ((d >> (s + 1)) != 0u) s++;
+    FastDiv f;
+    f.s = s;
+    f.m = (d == (1u << s)) ? 0u
+                           : (uint32_t)((((unsigned long long)1 << (32 + s)) + d - 1) / d);
+    return f;
+}
+__device__ __forceinline__ uint32_t fast_div(uint32_t n, FastDiv f) {
+    return (f.m ? __umulhi(n, f.m) : n) >> f.s;
+}
+
 struct OiftArgs {
     uint32_t *key;
     const uint16_t *W;
@@ -49,6 +69,7 @@ struct OiftArgs {
     int X, Y, Z;
     size_t N;
     int ntx, nty, ntz, ntiles;
+    FastDiv fd_ntx, fd_ntxy, fd_nctas;  // division by ntx, ntx * nty and nctas
     const float *pol_table;  // device, per label (x100)
     int npol;
     float pol_default;
@@ -122,6 +143,12 @@ __device__ __forceinline__ unsigned long long vload(const volatile unsigned long
 #ifndef OIFT_PROBE
 #define OIFT_PROBE 0
 #endif
+// 1 (the default): the tile steps and the level loop sum their SM cycles per phase into the
+// run's statistics; 0: those sums stay zero
+#ifndef OIFT_CYCLES
+#define OIFT_CYCLES 1
+#endif
+#define OIFT_CLOCK() (OIFT_CYCLES ? clock64() : 0ll)
 #if OIFT_PROBE
 // latency probes (globaltimer ns): [0,1] publish -> claim, [2,3] claim -> first publish,
 // [4,5] claim -> end of step
@@ -266,7 +293,7 @@ __device__ __forceinline__ void publish_reactivations(const OiftArgs &A, int par
     fence_acq_rel_gpu();
     __syncwarp();
     if (tq >= 0) {
-        const int w = tq % A.nctas, j = tq / A.nctas;
+        const int j = (int)fast_div((uint32_t)tq, A.fd_nctas), w = tq - j * A.nctas;
         const unsigned long long b = 1ull << (j & 63);
         old |= atomicOr(&A.mbox[((size_t)par * A.nctas + w) * A.mbox_words + (j >> 6)], b) & b;
         bit |= b;
@@ -284,12 +311,13 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
                              double fgt, double flt, int bgt, int blt, uint32_t *skey,
                              uint16_t *sw, uint16_t *shx, uint16_t *shy, uint16_t *shz,
                              uint32_t *wl, uint32_t *nfm, uint32_t *rmask, long long *cyc) {
-    long long tc0 = clock64();
+    long long tc0 = OIFT_CLOCK();
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int X = A.X, Y = A.Y, Z = A.Z;
     const size_t XY = (size_t)X * Y, N = A.N;
-    const int tx = t % A.ntx, ty = (t / A.ntx) % A.nty, tz = t / (A.ntx * A.nty);
+    const int tyz = (int)fast_div((uint32_t)t, A.fd_ntx), tz = (int)fast_div((uint32_t)t, A.fd_ntxy);
+    const int tx = t - tyz * A.ntx, ty = tyz - tz * A.nty;
     const int x0 = tx * 32, y0 = ty * TY, z0 = tz * TZ;
     const int x = x0 + lane;
     const bool has_z = (Z > 1);
@@ -495,7 +523,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
     }
     int nf0 = __popc(rowF);
     for (int o = 16; o > 0; o >>= 1) nf0 += __shfl_xor_sync(FULL, nf0, o);
-    const long long tcount = clock64();
+    const long long tcount = OIFT_CLOCK();
     cyc[0] += tcount - tc0;
     if (nf0 == 0) {  // stale activation: only the pending key is refreshed
         pending();
@@ -611,11 +639,11 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             }
             return base + total;
         };
-        const long long ts0 = clock64();
+        const long long ts0 = OIFT_CLOCK();
         nfm[lane] = 0u;
         cnt = append_rows(rowF, 0);
         __syncwarp();
-        const long long ts1 = clock64();
+        const long long ts1 = OIFT_CLOCK();
         cyc[12] += ts1 - ts0;
         for (;;) {
             if (done >= cnt) break;
@@ -672,10 +700,10 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             __syncwarp();
         }
         __syncwarp();
-        const long long ts2 = clock64();
+        const long long ts2 = OIFT_CLOCK();
         push_out(done < OIFT_WORKLIST ? done : OIFT_WORKLIST);
         __syncwarp();
-        const long long ts3 = clock64();
+        const long long ts3 = OIFT_CLOCK();
         cyc[13] += ts2 - ts1;
         cyc[14] += ts3 - ts2;
         cyc[17] += rounds;
@@ -684,9 +712,9 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             cyc[19] += (*(volatile uint32_t *)rmask != 0u);
             flush_reactivations();
             give_back_duplicates(A, par, pub_old);
-            const long long ts4 = clock64();
+            const long long ts4 = OIFT_CLOCK();
             pending();
-            const long long ts5 = clock64();
+            const long long ts5 = OIFT_CLOCK();
             cyc[15] += ts4 - ts3;
             cyc[16] += ts5 - ts4;
             cyc[1] += ts5 - tcount;
@@ -695,7 +723,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         }
     }
     // ---- bit mode ----
-    const long long tb0 = clock64();
+    const long long tb0 = OIFT_CLOCK();
     // lane r: row r's flooded voxels not yet expanded (P) and its open voxels (Om: key above
     // the level, neither final nor flooded at this level).  Straight from the level rows
     // when no sparse round ran; rebuilt from the keys otherwise.
@@ -842,7 +870,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         Fm |= g;
         fr = g;
     }
-    const long long tb1 = clock64();
+    const long long tb1 = OIFT_CLOCK();
     // ---- expansion of the closure.  The voxels on the tile's faces go first: they are
     // expanded in global memory, their arcs across the faces are pushed and the tile's
     // same-level crossings are published, so that the flood continues next door while this
@@ -891,13 +919,13 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             push_out(nb);
             __syncwarp();
         }
-        const long long tf1 = clock64();
+        const long long tf1 = OIFT_CLOCK();
         flush_reactivations();
-        const long long tf2 = clock64();
+        const long long tf2 = OIFT_CLOCK();
         cyc[16] += tf1 - tb1;
         cyc[17] += tf2 - tf1;
     }
-    const long long tf3 = clock64();
+    const long long tf3 = OIFT_CLOCK();
     uint32_t rem = Fm;
     while (__any_sync(FULL, rem != 0u)) {
         const int nb = compact(rem);
@@ -935,12 +963,12 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         }
         __syncwarp();
     }
-    const long long tb2 = clock64();
+    const long long tb2 = OIFT_CLOCK();
     cyc[18] += tb2 - tf3;
     // ---- pending key of this tile; published activations that merged give their counts back
     pending();
     give_back_duplicates(A, par, pub_old);
-    const long long tb3 = clock64();
+    const long long tb3 = OIFT_CLOCK();
 #if OIFT_PROBE
     if (lane == 0) {
         const unsigned long long dt = gtimer() - probe_t0;
@@ -989,12 +1017,13 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     constexpr int HZ = TZ > 1 ? TZ + 2 : 1;
     constexpr int ZO = TZ > 1 ? 1 : 0;    // halo offset along z
     static_assert(NR <= 16, "full-neighbourhood tiles hold at most 16 rows");
-    long long tc0 = clock64();
+    long long tc0 = OIFT_CLOCK();
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int X = A.X, Y = A.Y, Z = A.Z;
     const size_t XY = (size_t)X * Y;
-    const int tx = t % A.ntx, ty = (t / A.ntx) % A.nty, tz = t / (A.ntx * A.nty);
+    const int tyz = (int)fast_div((uint32_t)t, A.fd_ntx), tz = (int)fast_div((uint32_t)t, A.fd_ntxy);
+    const int tx = t - tyz * A.ntx, ty = tyz - tz * A.nty;
     const int x0 = tx * 32, y0 = ty * TY, z0 = tz * TZ;
     const int x = x0 + lane;
     const K kexp = kk - (K)1;
@@ -1124,7 +1153,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     }
     int nf0 = __popc(rowF);
     for (int o = 16; o > 0; o >>= 1) nf0 += __shfl_xor_sync(FULL, nf0, o);
-    const long long tcount = clock64();
+    const long long tcount = OIFT_CLOCK();
     cyc[0] += tcount - tc0;
     if (nf0 == 0) {
         pending();
@@ -1268,7 +1297,7 @@ __device__ __forceinline__ void process_tile_full(const OiftArgs &A, int t, int 
     }
     __syncwarp();
     pending();
-    cyc[1] += clock64() - tcount;
+    cyc[1] += OIFT_CLOCK() - tcount;
     cyc[4] += 1;
     cyc[17] += rounds;
     cyc[18] += cnt;
@@ -1381,7 +1410,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
     }
     for (int e = 0;; e++) {
         const int par = e % 3;
-        const long long t_r0 = clock64();
+        const long long t_r0 = OIFT_CLOCK();
         if (leader_cta && threadIdx.x == 0 && A.lprof && e > 0 && e - 1 < A.lprof_cap) {
             const long long now = clock64();
             A.lprof[2 * (e - 1)] = (unsigned int)min(now - lvl_t0, 0xffffffffll);
@@ -1421,7 +1450,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         // ---- S: the tiles of this CTA whose pending key equals the level become wanted; the
         // smallest pending key of its other tiles joins the level's running minimum ----
         unsigned long long steps = 0;
-        const long long t_s0 = clock64();
+        const long long t_s0 = OIFT_CLOCK();
         cyc_levelsync += t_s0 - t_r0;
         {
             int h = 0;
@@ -1466,7 +1495,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
             if (h != 1) atomicAdd(&g->outstanding[par], h - 1);
         }
         __syncthreads();
-        const long long t_p0 = clock64();
+        const long long t_p0 = OIFT_CLOCK();
         cyc_owner += t_p0 - t_s0;
         // ---- P: the CTA's warps claim its wanted tiles, one warp per tile, and fetch the
         // CTA's mailbox into the wanted set, until the level's outstanding count is zero ----
@@ -1533,7 +1562,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                 }
                 // the activations merged into this claim precede the staging of the tile
                 __threadfence_block();
-                const long long tb = clock64();
+                const long long tb = OIFT_CLOCK();
                 const int t = team_cta + j * team_ctas;
                 if constexpr (FULLN)
                     process_tile_full<TY, TZ, TI, BLEND, K, FACES>(
@@ -1550,7 +1579,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
                     atomicAnd(&cs.run[j >> 6], ~(1ull << (j & 63)));
                     atomicSub(&g->outstanding[par], 1);
                 }
-                cyc_busy += clock64() - tb;
+                cyc_busy += OIFT_CLOCK() - tb;
                 spins = 0;
                 idle = 0;
                 nap = 64;
@@ -1633,7 +1662,7 @@ __device__ void oift_solve(const OiftArgs &A, int team_cta, int team_ctas, OiftC
         if (lane == 0 && steps) atomicAdd(&g->tile_steps, steps);
         if (lane == 0 && steps && A.lprof && e < A.lprof_cap)
             atomicAdd(&A.lprof[2 * e + 1], (unsigned int)steps);
-        cyc_drain += clock64() - t_p0;
+        cyc_drain += OIFT_CLOCK() - t_p0;
         // every warp has left the level; a warp whose own wait ran out has set the error
         // flag, which the watching warp reads before it ends the level
         __syncthreads();
@@ -1727,6 +1756,9 @@ __global__ void __launch_bounds__(OIFT_WARPS * 32, 1)
             sA.Z = Z;
             sA.N = N;
             sA.ntx = ntx;
+            sA.fd_ntx = make_fastdiv((uint32_t)ntx);
+            sA.fd_ntxy = make_fastdiv((uint32_t)(ntx * nty));
+            sA.fd_nctas = make_fastdiv((uint32_t)team_ctas);
             sA.nty = nty;
             sA.ntz = J->ntz;
             sA.ntiles = ntiles;
@@ -1950,6 +1982,9 @@ int oift_enqueue(const OiftPlan &P, const OiftScratch &S, const uint16_t *W, int
     A.nty = P.nty;
     A.ntz = P.ntz;
     A.ntiles = P.ntiles;
+    A.fd_ntx = make_fastdiv((uint32_t)P.ntx);
+    A.fd_ntxy = make_fastdiv((uint32_t)(P.ntx * P.nty));
+    A.fd_nctas = make_fastdiv((uint32_t)sms);
     A.pol_table = d_pol_table;
     A.npol = npol;
     A.pol_default = pol_default;
