@@ -68,3 +68,11 @@ def test_replicas_reduce_over_two_gloo_ranks(tmp_path):
     assert res[0]["checksum"] != res[1]["checksum"]      # independent volumes
     assert res[0]["gvox"] == pytest.approx(world * n / 0.025 / 1e9)
     assert res[1]["ref"] is None
+
+
+def test_bench_reads_the_committed_dram_traffic_table():
+    """The roofline's `traffic` comes from the committed ncu summary: the headline OIFT
+    launch's DRAM bytes are there, and they exceed its 12 B/voxel algorithmic bytes."""
+    import bench
+    t = bench.read_traffic("oift_persistent_kernel", "256^3")
+    assert t is not None and t > 12 * 256 ** 3
