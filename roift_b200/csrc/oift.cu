@@ -349,6 +349,12 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
     // A successful out-of-tile push either continues this level next door (the
     // face-neighbour tile is marked for re-activation; all marks of the tile step are
     // published together by flush_reactivations) or lowers the neighbour's pending key.
+    // A push that only lowers a neighbour tile's pending key adds that key to the level's
+    // running minimum at the end of the step (with the tile's own pending key, one update per
+    // warp), not before the step's re-activations are published: every warp updates that one
+    // word, and the publication's release fence would wait for the update
+    // (256^3 ellipsoid: 30.33 -> 30.10 ms).
+    uint32_t runmin_def = OIFT_KEY_INF;
     auto settle = [&](uint32_t nk, uint32_t old, int qx, int qy, int qz) {
         if (nk < old) {
             if (nk == kk) {
@@ -357,7 +363,7 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
                 atomicOr(rmask, 1u << face);
             } else {
                 atomicMin(&A.tpend[tile_of<TY, TZ>(A, qx, qy, qz)], nk);
-                atomicMin(&A.g->runmin[par], nk);
+                runmin_def = nk < runmin_def ? nk : runmin_def;
             }
         }
     };
@@ -397,14 +403,16 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
             if (v.z > kk && v.z < m) m = v.z;
             if (v.w > kk && v.w < m) m = v.w;
         }
+        // the keys the step's pushes left pending next door join the level's minimum here
+        uint32_t r = runmin_def < m ? runmin_def : m;
         for (int o = 16; o > 0; o >>= 1) {
             uint32_t v = __shfl_xor_sync(FULL, m, o);
             m = v < m ? v : m;
+            v = __shfl_xor_sync(FULL, r, o);
+            r = v < r ? v : r;
         }
-        if (lane == 0 && m != OIFT_KEY_INF) {
-            atomicMin(&A.tpend[t], m);
-            atomicMin(&A.g->runmin[par], m);
-        }
+        if (lane == 0 && m != OIFT_KEY_INF) atomicMin(&A.tpend[t], m);
+        if (lane == 0 && r != OIFT_KEY_INF) atomicMin(&A.g->runmin[par], r);
     };
     // ---- stage keys, edge codes and the -x/-y/-z halo codes in shared memory ----
     // shx holds the -x halo as 32-bit pairs (codes of x0-2, x0-1): entry 2r+1 is row r's.
@@ -871,11 +879,15 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         fr = g;
     }
     const long long tb1 = OIFT_CLOCK();
-    // ---- expansion of the closure.  The voxels on the tile's faces go first: they are
-    // expanded in global memory, their arcs across the faces are pushed and the tile's
-    // same-level crossings are published, so that the flood continues next door while this
-    // tile gives its in-tile heads that the closure did not reach the arc's key (the arc is
-    // closed there).  Voxels join the worklist OIFT_WORKLIST at a time ----
+    // ---- expansion of the closure.  The voxels on the tile's faces go first: their arcs
+    // across the faces are pushed and the tile's same-level crossings are published, so that
+    // the flood continues next door while this tile marks its closure expanded in global
+    // memory and gives its in-tile heads that the closure did not reach the arc's key (the
+    // arc is closed there).  The face voxels are marked expanded only then, with the rest of
+    // the closure: the publication's release fence does not wait for those stores, and a
+    // neighbour's push that meets such a voxel before its mark re-activates this tile once
+    // more, which finds nothing left (256^3 ellipsoid: 31.04 -> 30.30 ms).  Voxels join the
+    // worklist OIFT_WORKLIST at a time ----
     nfm[lane] = Fm;
     // compact(m): the voxels of row `lane` in m join the worklist (up to OIFT_WORKLIST in all)
     // and leave m; returns how many joined
@@ -908,14 +920,6 @@ __device__ __forceinline__ void process_tile(const OiftArgs &A, int t, int par, 
         uint32_t frem = Fm & (((ROWS_FACE >> lane) & 1u) ? FULL : 0x80000001u);
         while (__any_sync(FULL, frem != 0u)) {
             const int nb = compact(frem);
-            for (int base = 0; base < nb; base += 32) {
-                const int idx = base + lane;
-                if (idx < nb) {
-                    const uint32_t li = wl[idx];
-                    const int r = (int)(li >> 5), xl = (int)(li & 31);
-                    A.key[(size_t)(x0 + xl) + (size_t)(y0 + (r % TY)) * X + (size_t)(z0 + (r / TY)) * XY] = kexp;
-                }
-            }
             push_out(nb);
             __syncwarp();
         }
