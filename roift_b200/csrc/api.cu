@@ -933,11 +933,17 @@ int oift_b200_run_host(oift_b200_ctx *c, const oift_b200_params *p, const int32_
         std::vector<int> rcs(nthreads, OIFT_OK);
         std::vector<std::thread> pool;
         const int chunk = (nseeds + nthreads - 1) / nthreads;
-        for (int k = 1; k < nthreads; k++)
-            pool.emplace_back([&, k]() {
-                rcs[k] = gather(std::min(nseeds, k * chunk), std::min(nseeds, (k + 1) * chunk));
-            });
-        rcs[0] = gather(0, std::min(nseeds, chunk));
+        auto run_chunk = [&](int k) {
+            rcs[k] = gather(std::min(nseeds, k * chunk), std::min(nseeds, (k + 1) * chunk));
+        };
+        int spawned = 1;  // chunk 0 runs on the calling thread
+        try {
+            for (int k = 1; k < nthreads; k++, spawned++) pool.emplace_back(run_chunk, k);
+        } catch (...) {
+            // no exception leaves the C ABI: chunks that got no thread run here
+        }
+        for (int k = spawned; k < nthreads; k++) run_chunk(k);
+        run_chunk(0);
         for (auto &th : pool) th.join();
         for (int k = 0; k < nthreads; k++) TRY(rcs[k]);
     }
