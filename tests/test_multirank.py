@@ -76,3 +76,22 @@ def test_bench_reads_the_committed_dram_traffic_table():
     import bench
     t = bench.read_traffic("oift_persistent_kernel", "256^3")
     assert t is not None and t > 12 * 256 ** 3
+
+
+def test_batch_cpu_baseline_runs_the_reference_on_host_processes():
+    """The batch workload's cpu_baseline: each job of a small mix through the reference
+    OIFT_Multi + ORelax_1_Multi in its own spawned process; the throughput is the jobs'
+    count and voxels over the wall time."""
+    import oracle as O
+    if not O.ref_available():
+        pytest.skip("reference library not built here")
+    import bench
+    from roift_b200 import synth
+    jobs = []
+    for seed in range(2):
+        c = synth.small_case(seed=seed, shape=(12, 16, 20), pol=-0.3, adjacency=6, nlabels=1)
+        jobs.append((c.image.reshape(-1), c.shape, c.seeds, c.seed_labels, c.pol, 5))
+    sets_s, gvox_s, vox = bench.cpu_reference_batch(jobs, 2)
+    assert vox == 2 * 12 * 16 * 20
+    assert sets_s > 0 and gvox_s > 0
+    assert abs(gvox_s / sets_s * 1e9 - vox / 2) < 1e-6 * vox
